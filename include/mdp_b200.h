@@ -1,0 +1,122 @@
+/*
+ * mdp_b200 -- B200-native SNAP force path and velocity-Verlet MD (C ABI).
+ *
+ * All entry points return 0 on success and -1 on error; mdp_last_error()
+ * returns the text of the last error of the calling thread.  No entry point
+ * exits or aborts the process.
+ *
+ * This header is the project's own engine interface.  The drop-in
+ * replacements for MDP's existing interfaces are declared in
+ *   include/mdp_b200_cpusnap.h   (MDP's Julia ccall library, cpuSnap.h)
+ *   include/mdp_b200_gpucore.h   (MDP's backend dispatch, mdpgpucore.h)
+ */
+#ifndef MDP_B200_H
+#define MDP_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* SNAP hyper-parameters and coefficients: the snaparam[12] vector of MDP
+ * (src/Julia/Preprocessing/Preprocessing.jl:266, read at
+ * src/C++/Descriptors/snappotential.cpp:151-162) for a single element. */
+typedef struct {
+    int twojmax;          /* 2J: 4, 6 or 8 */
+    double rcutfac;
+    double rfac0;
+    double rmin0;
+    double radelem;       /* element radius; rcut = 2 * radelem * rcutfac */
+    double wjelem;        /* element weight */
+    int switchflag;
+    int bzeroflag;
+    int bnormflag;
+    int wselfallflag;
+    int quadraticflag;    /* must be 0 */
+    int chemflag;         /* must be 0 */
+    int ncoeffall;        /* 1 + number of bispectrum components */
+    const double *coeff;  /* ncoeffall values; coeff[0] = beta_0 */
+} mdp_snap_params;
+
+enum { MDP_PREC_FP64 = 0, MDP_PREC_FP32 = 1 };
+
+const char *mdp_last_error(void);
+
+/* number of bispectrum components for 2J (MDP idxbcount, cpuSnap.cpp:23) */
+int mdp_snap_ncoeff(int twojmax);
+
+/* ---------------------------------------------------------------------------
+ * One SNAP force evaluation on DEVICE arrays (replaces the body of
+ * ComputePairSnap3, src/C++/Descriptors/snappotential.cpp:634-760).
+ *   x        anum x 3 positions, AoS (locals first, then ghosts)
+ *   alist    anum owner index of every atom (identity for locals)
+ *   neighlist inum x neighmax rows, neighnum[inum]
+ *   eatom    inum, fatom inum x 3 AoS, vatom 6 x inum SoA (may be NULL)
+ * Outputs are overwritten (the reference accumulates into zeroed arrays).
+ * ------------------------------------------------------------------------- */
+int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const double *x, const int *alist,
+                            const int *neighlist, const int *neighnum, int inum, int anum, int neighmax,
+                            double *eatom, double *fatom, double *vatom, void *cuda_stream);
+
+/* Same on HOST arrays, including the ghost/neighbour build: natoms positions
+ * in an orthogonal or triclinic periodic box with vectors a, b, c (box[0..8]).
+ * Optional outputs (NULL to skip): neighlist (natoms x neighmax), neighnum,
+ * anum_out, alist_out (capacity alist_cap), xall_out (3 x alist_cap). */
+int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, const double *x,
+                          const double *box, double skin, int neighmax, double *eatom, double *fatom,
+                          double *vatom, int *neighlist, int *neighnum, int *anum_out, int *alist_out,
+                          double *xall_out, int alist_cap);
+
+/* ---------------------------------------------------------------------------
+ * MD engine: NVE velocity Verlet with SNAP forces, neighbour list rebuilt on
+ * the reference's criterion (src/C++/Integration/Integration.cpp:260-303).
+ * ------------------------------------------------------------------------- */
+typedef struct mdp_md mdp_md;
+
+typedef struct {
+    int natoms;
+    double box[9];        /* a, b, c */
+    double mass;          /* amu */
+    double dt;            /* ps */
+    double skin;          /* A */
+    int neighmax;
+    int neighevery;       /* rebuild check every n steps (reference default 1) */
+    int neighdelay;       /* no check before this many steps (reference default 0) */
+    int neighcheck;       /* 1: rebuild when max displacement > skin/2 */
+    int precision;        /* MDP_PREC_FP64 or MDP_PREC_FP32 */
+    int device;
+} mdp_md_config;
+
+int mdp_md_create(mdp_md **h, const mdp_snap_params *p, const mdp_md_config *cfg);
+void mdp_md_destroy(mdp_md *h);
+/* host positions/velocities (natoms x 3, A and A/ps) */
+int mdp_md_set_state(mdp_md *h, const double *x, const double *v);
+/* device positions/velocities already resident (natoms x 3 AoS) */
+int mdp_md_set_state_device(mdp_md *h, const double *x_dev, const double *v_dev);
+/* neighbour list + first force + thermo (IntegrationSetup, Integration.cpp:158) */
+int mdp_md_setup(mdp_md *h);
+/* nsteps velocity-Verlet steps; thermo rows (step, T, PE/atom, TE/atom, P)
+ * every thermo_every steps into thermo (may be NULL); returns rows written
+ * via *nrows.  elapsed_ms (may be NULL): CUDA-event time of the steps on the
+ * engine's stream. */
+int mdp_md_run(mdp_md *h, int nsteps, int thermo_every, double *thermo, int thermo_cap, int *nrows,
+               float *elapsed_ms);
+int mdp_md_get_state(mdp_md *h, double *x, double *v, double *f, double *eatom);
+int mdp_md_thermo(mdp_md *h, double *out5);
+/* counters: [0] steps, [1] neighbour rebuilds, [2] current pairs, [3] ghosts,
+ * [4] neighbour entries */
+int mdp_md_counters(mdp_md *h, long long *out5);
+/* per-stage CUDA-event timing over the next runs: 1 on, 0 off; read back as
+ * ms totals [pairs, ui, yi, fi, tally, force] and the number of force calls */
+int mdp_md_stage_timing(mdp_md *h, int enable);
+int mdp_md_stage_times(mdp_md *h, double *ms6, long long *calls);
+/* the CUDA stream the engine launches on (for callers that time with events) */
+void *mdp_md_stream(mdp_md *h);
+
+/* measured FP64 / FP32 FMA throughput of this GPU (TFLOP/s), from a
+ * register-resident FMA loop timed with CUDA events */
+int mdp_probe_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,103 @@
+// Host-side structures of the B200 SNAP engine (internal; the public C ABI is
+// include/mdp_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <vector>
+
+#include "../../include/mdp_b200.h"
+#include "snap_kernels.cuh"
+
+namespace mdp {
+
+struct BoxParams {
+    double s2r[9];        // inverse of [a b c] (column-major)
+    double lo[3], hi[3];  // enlarged bounding box in fractional coordinates
+    double pim[27][3];    // periodic image shifts, reference order
+    int nc[3];            // cell grid (fractional)
+    double cinv[3];       // nc / (hi - lo)
+    long ncell;
+};
+int box_setup(BoxParams &bp, const double *a, const double *b, const double *c, double offset, double rc_cells);
+
+// kernels defined in neighbor.cu
+__global__ void k_ghost_count(const double4 *, int, const __grid_constant__ BoxParams, int *, unsigned *);
+__global__ void k_ghost_emit(double4 *, int *, int, const __grid_constant__ BoxParams, const int *, const unsigned *);
+__global__ void k_cell_index(const double4 *, int, const __grid_constant__ BoxParams, int *, int *);
+__global__ void k_cell_fill(int, const int *, const int *, int *, int *);
+__global__ void k_neigh_build(const double4 *, int, const __grid_constant__ BoxParams, const int *, const int *,
+                              const int *, double, int, int *, int *, int *);
+__global__ void k_rev_count(const int *, const int *, const int *, int, int, int *);
+__global__ void k_rev_fill(const int *, const int *, const int *, int, int, const int *, int *, long long *);
+__global__ void k_rev_sort(int, const int *, long long *);
+__global__ void k_pair_count(const double4 *, const int *, const int *, int, int, double, double4 *, int *);
+__global__ void k_pair_emit(const double4 *, const int *, int, int, const int *, double4 *, int2 *);
+__global__ void k_tally(const double4 *, const double4 *, const int *, int, int, const int *, const long long *,
+                        double4 *, double *);
+__global__ void k_nve_initial(double4 *, double4 *, const double4 *, double4 *, int, double, double);
+__global__ void k_nve_final(double4 *, const double4 *, int, double);
+__global__ void k_maxdisp(const double4 *, const double4 *, int, unsigned long long *);
+__global__ void k_pbc_orth(double4 *, int, double, double, double, double, double, double);
+__global__ void k_ghost_shift(double4 *, const double4 *, const int *, int, int);
+__global__ void k_thermo(const double *, const double *, const double4 *, int, double *);
+
+// SNAP model: validated parameters plus the derived kernel parameter blocks
+struct SnapModel {
+    mdp_snap_params p;
+    std::vector<double> coeff;
+    SnapGeom geom;
+    YParams<double> yd;
+    YParams<float> yf;
+    int nu, nyh, ncoeff;
+};
+int model_init(SnapModel &m, const mdp_snap_params *p);
+
+// device buffers of one force evaluation (capacities grow on demand)
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n);
+    void release();
+    template <typename X> X *as() const { return reinterpret_cast<X *>(p); }
+};
+
+struct ForcePath {
+    DevBuf pcount, poff, prij, pinfo, rslot, dE, Ut, Y, scan_tmp;
+    int natoms_cap = 0, nm_cap = 0;
+    // per-stage timing (CUDA events on the launching stream), enabled on demand
+    bool timing = false;
+    cudaEvent_t ev[8] = {};
+    double stage_ms[6] = {0, 0, 0, 0, 0, 0};   // pairs, ui, yi, fi, tally, total
+    long stage_calls = 0;
+    void release();
+};
+
+// per-stage launchers, one translation unit per (stage, precision)
+template <typename T, int TJ> int launch_ui(const SnapModel &m, ForcePath &fp, int inum, cudaStream_t s);
+template <typename T, int TJ>
+int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum, double *eatom, cudaStream_t s);
+template <typename T, int TJ> int launch_fi(const SnapModel &m, ForcePath &fp, int inum, int nm, cudaStream_t s);
+
+// One plain-SNAP force evaluation on device data: x (anum, double4, ghosts
+// appended), neighbour list (inum x nm), reverse list.  Writes eatom[inum],
+// f[inum] (double4) and, when vatom != nullptr, the SoA per-atom virial 6 x inum.
+int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double4 *x, int inum,
+                  const int *nlist, const int *nnum, int nm, long pair_cap, const int *roff,
+                  const long long *rlist, double *eatom, double4 *f, double *vatom, cudaStream_t s);
+
+// Neighbour structure (ghosts + list + reverse list) owned by a caller
+struct Neighbors {
+    DevBuf gcount, goff, gmask, alist, cidx, ccount, cstart, cursor, catoms, nlist, nnum, rcount, roff, rlist,
+        status, scan_tmp;
+    int inum = 0, gnum = 0, anum = 0, nm = 0;
+    long nsum = 0;   // total neighbour entries
+    long anum_cap = 0;
+    void release();
+};
+// builds ghosts into x[inum..] (x must hold anum_cap entries), the list and its
+// reverse.  Returns 0, or -1 on error (capacity, CUDA); overflow of neighmax is
+// an error (the reference truncates silently).
+int neighbor_build(Neighbors &nb, const BoxParams &bp, double4 *x, int inum, double rc, int nm, long anum_cap,
+                   cudaStream_t s);
+
+}  // namespace mdp

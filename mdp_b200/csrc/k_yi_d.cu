@@ -1,0 +1,33 @@
+// Y + energy stage launchers (k_snap_yi), double.
+#include "engine.h"
+
+#include <algorithm>
+
+namespace mdp {
+
+template <typename T, int TJ>
+int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum, double *eatom, cudaStream_t s)
+{
+    typedef typename cplx<T>::type T2;
+    if (tu_ensure_tables()) return -1;
+    constexpr int NU = idxu_count(TJ);
+    const size_t sm = (size_t)NU * 32 * sizeof(T2) + YI_WARPS * 32 * sizeof(double);
+    static int per_sm = 0;
+    if (!per_sm) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<T, TJ>, YI_WARPS * 32, sm));
+        if (per_sm < 1) { set_error("k_snap_yi does not fit on an SM (%zu B shared)", sm); return -1; }
+    }
+    const int ntiles = (inum + 31) / 32;
+    const int blocks = std::min(ntiles, num_sms() * per_sm);
+    if (fp.timing) cudaEventRecord(fp.ev[2], s);
+    k_snap_yi<T, TJ><<<blocks, YI_WARPS * 32, sm, s>>>(fp.Ut.as<T2>(), inum, yp, fp.Y.as<T2>(), eatom);
+    return 0;
+}
+
+#define MDP_INST(T, TJ) \
+    template int launch_yi<T, TJ>(const SnapModel &, const YParams<T> &, ForcePath &, int, double *, cudaStream_t);
+MDP_INST(double, 4) MDP_INST(double, 6) MDP_INST(double, 8)
+#undef MDP_INST
+
+}  // namespace mdp

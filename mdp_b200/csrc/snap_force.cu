@@ -1,0 +1,302 @@
+// SNAP model set-up, the force-path driver and the neighbour-structure
+// builder.  Kernel templates live in snap_kernels.cuh / neighbor.cu.
+#include "common.cuh"
+#include "engine.h"
+
+#include <algorithm>
+#include <math.h>
+#include <string.h>
+
+namespace mdp {
+
+int DevBuf::ensure(size_t n)
+{
+    if (n <= bytes) return 0;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = n + n / 8 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        set_error("cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
+        p = nullptr;
+        return -1;
+    }
+    cudaMemset(p, 0, want);
+    bytes = want;
+    return 0;
+}
+void DevBuf::release()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+void ForcePath::release()
+{
+    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &rslot, &dE, &Ut, &Y, &scan_tmp};
+    for (auto x : b) x->release();
+    for (auto &e : ev)
+        if (e) { cudaEventDestroy(e); e = nullptr; }
+}
+
+void Neighbors::release()
+{
+    DevBuf *b[] = {&gcount, &goff, &gmask, &alist, &cidx, &ccount, &cstart, &cursor, &catoms,
+                   &nlist, &nnum, &rcount, &roff, &rlist, &status, &scan_tmp};
+    for (auto x : b) x->release();
+}
+
+// ---------------------------------------------------------------------------
+// model
+// ---------------------------------------------------------------------------
+static int triple_ok(int j1, int j2, int j, int tj)
+{
+    return j2 <= j1 && j1 <= tj && j <= tj && j1 - j2 <= j && j <= j1 + j2 && ((j1 + j2 + j) % 2 == 0);
+}
+
+int model_init(SnapModel &m, const mdp_snap_params *p)
+{
+    if (!p) { set_error("null SNAP parameters"); return -1; }
+    const int tj = p->twojmax;
+    if (tj != 4 && tj != 6 && tj != 8) {
+        set_error("twojmax=%d not supported (4, 6 or 8)", tj);
+        return -1;
+    }
+    if (p->chemflag != 0 || p->quadraticflag != 0) {
+        set_error("chemflag/quadraticflag SNAP is not supported (single-element linear SNAP only)");
+        return -1;
+    }
+    if (p->switchflag != 0 && p->switchflag != 1) { set_error("switchflag must be 0 or 1"); return -1; }
+    // idxb enumeration (cpuSnap.cpp:44-68)
+    int jjb[JD][JD][JD];
+    int nb = 0;
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= std::min(tj, j1 + j2); j += 2)
+                if (j >= j1) jjb[j1][j2][j] = nb++;
+    if (p->ncoeffall != nb + 1) {
+        set_error("ncoeffall=%d but 2J=%d needs %d coefficients", p->ncoeffall, tj, nb + 1);
+        return -1;
+    }
+    if (!p->coeff) { set_error("null coefficient array"); return -1; }
+    m.p = *p;
+    m.coeff.assign(p->coeff, p->coeff + p->ncoeffall);
+    m.p.coeff = m.coeff.data();
+    m.ncoeff = nb;
+    m.nu = idxu_count(tj);
+    m.nyh = yh_count(tj);
+    const double rcut = 2.0 * p->radelem * p->rcutfac;
+    m.geom.rcut = rcut;
+    m.geom.rcutsq = rcut * rcut;
+    m.geom.rfac0 = p->rfac0;
+    m.geom.rmin0 = p->rmin0;
+    m.geom.wj = p->wjelem;
+    m.geom.switchflag = p->switchflag;
+
+    // beta' per coupling triple (cpuSnap4.cpp:763-787)
+    memset(&m.yd, 0, sizeof(m.yd));
+    memset(&m.yf, 0, sizeof(m.yf));
+    const double *c = m.coeff.data();
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = 0; j <= tj; j++) {
+                if (!triple_ok(j1, j2, j, tj)) continue;
+                double b;
+                if (j >= j1) {
+                    b = c[1 + jjb[j1][j2][j]];
+                    if (j1 == j) b *= (j2 == j) ? 3.0 : 2.0;
+                } else if (j >= j2) {
+                    b = c[1 + jjb[j][j2][j1]];
+                    if (j2 == j) b *= 2.0;
+                } else {
+                    b = c[1 + jjb[j2][j][j1]];
+                }
+                if (!p->bnormflag && j1 > j) b *= (j1 + 1) / (j + 1.0);
+                if (p->bnormflag) b /= (j + 1);
+                m.yd.betaY[tri_index(j1, j2, j)] = b;
+                m.yf.betaY[tri_index(j1, j2, j)] = (float)b;
+            }
+    double e0 = c[0];
+    if (p->bzeroflag) {
+        for (int j1 = 0; j1 <= tj; j1++)
+            for (int j2 = 0; j2 <= j1; j2++)
+                for (int j = j1 - j2; j <= std::min(tj, j1 + j2); j += 2)
+                    if (j >= j1) e0 -= c[1 + jjb[j1][j2][j]] * (p->bnormflag ? 1.0 : (double)(j + 1));
+    }
+    m.yd.e0 = e0;
+    m.yf.e0 = e0;
+
+    // Y-kernel units (j, mb) with their term counts, longest-first onto warps
+    struct Unit { int j, mb; long cost; };
+    std::vector<Unit> units;
+    for (int j = 0; j <= tj; j++)
+        for (int mb = 0; 2 * mb <= j; mb++) {
+            long cost = 0;
+            for (int j1 = 0; j1 <= tj; j1++)
+                for (int j2 = 0; j2 <= j1; j2++) {
+                    if (!triple_ok(j1, j2, j, tj)) continue;
+                    int mb1min = std::max(0, (2 * mb - j - j2 + j1) / 2);
+                    int nbb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
+                    for (int ma = 0; ma <= j; ma++) {
+                        int ma1min = std::max(0, (2 * ma - j - j2 + j1) / 2);
+                        int na = std::min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
+                        cost += (long)na * nbb;
+                    }
+                }
+            units.push_back({j, mb, cost + 8});
+        }
+    std::sort(units.begin(), units.end(), [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
+    long load[YI_WARPS] = {0};
+    for (auto &u : units) {
+        int w = 0;
+        for (int k = 1; k < YI_WARPS; k++)
+            if (load[k] < load[w]) w = k;
+        if (m.yd.nunits[w] >= YI_MAXU) { set_error("Y schedule overflow"); return -1; }
+        int n = m.yd.nunits[w]++;
+        m.yd.unit_j[w][n] = (unsigned char)u.j;
+        m.yd.unit_mb[w][n] = (unsigned char)u.mb;
+        load[w] += u.cost;
+    }
+    memcpy(m.yf.nunits, m.yd.nunits, sizeof(m.yd.nunits));
+    memcpy(m.yf.unit_j, m.yd.unit_j, sizeof(m.yd.unit_j));
+    memcpy(m.yf.unit_mb, m.yd.unit_mb, sizeof(m.yd.unit_mb));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// stage sequence per (T, TJ)
+// ---------------------------------------------------------------------------
+template <typename T, int TJ>
+static int launch_snap(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum, int nm,
+                       double *eatom, cudaStream_t s)
+{
+    if (launch_ui<T, TJ>(m, fp, inum, s)) return -1;
+    if (launch_yi<T, TJ>(m, yp, fp, inum, eatom, s)) return -1;
+    return launch_fi<T, TJ>(m, fp, inum, nm, s);
+}
+
+template <typename T>
+static int launch_snap_tj(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum, int nm, double *eatom,
+                          cudaStream_t s)
+{
+    switch (m.p.twojmax) {
+    case 4: return launch_snap<T, 4>(m, yp, fp, inum, nm, eatom, s);
+    case 6: return launch_snap<T, 6>(m, yp, fp, inum, nm, eatom, s);
+    case 8: return launch_snap<T, 8>(m, yp, fp, inum, nm, eatom, s);
+    }
+    set_error("twojmax %d not instantiated", m.p.twojmax);
+    return -1;
+}
+
+int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double4 *x, int inum, const int *nlist,
+                  const int *nnum, int nm, long pair_cap, const int *roff, const long long *rlist, double *eatom,
+                  double4 *f, double *vatom, cudaStream_t s)
+{
+    if (inum <= 0) { set_error("no atoms"); return -1; }
+    const size_t tsz = (precision == MDP_PREC_FP32) ? sizeof(float2) : sizeof(double2);
+    const long ntiles = (inum + 31) / 32;
+    if (pair_cap < 1) pair_cap = 1;
+    if (fp.pcount.ensure(sizeof(int) * (size_t)inum) || fp.poff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
+        fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
+        fp.rslot.ensure(sizeof(double4) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)inum * nm) ||
+        fp.Ut.ensure(tsz * (size_t)ntiles * m.nu * 32) || fp.Y.ensure(tsz * (size_t)inum * m.nyh) ||
+        fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(inum)))
+        return -1;
+    if (fp.timing && !fp.ev[0])
+        for (auto &e : fp.ev) cudaEventCreate(&e);
+    const int tb = 256;
+    const int gb = (inum + tb - 1) / tb;
+    if (fp.timing) cudaEventRecord(fp.ev[0], s);
+    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.rslot.as<double4>(), fp.pcount.as<int>());
+    if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
+    k_pair_emit<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), nnum, inum, nm, fp.poff.as<int>(), fp.prij.as<double4>(),
+                                  fp.pinfo.as<int2>());
+    int rc = (precision == MDP_PREC_FP32) ? launch_snap_tj<float>(m, m.yf, fp, inum, nm, eatom, s)
+                                           : launch_snap_tj<double>(m, m.yd, fp, inum, nm, eatom, s);
+    if (rc) return rc;
+    if (fp.timing) cudaEventRecord(fp.ev[4], s);
+    k_tally<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), fp.dE.as<double4>(), nnum, inum, nm, roff, rlist, f, vatom);
+    if (fp.timing) {
+        cudaEventRecord(fp.ev[5], s);
+        cudaEventSynchronize(fp.ev[5]);
+        float t[5];
+        for (int k = 0; k < 5; k++) cudaEventElapsedTime(&t[k], fp.ev[k], fp.ev[k + 1]);
+        for (int k = 0; k < 5; k++) fp.stage_ms[k] += t[k];
+        float tot;
+        cudaEventElapsedTime(&tot, fp.ev[0], fp.ev[5]);
+        fp.stage_ms[5] += tot;
+        fp.stage_calls++;
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour structure
+// ---------------------------------------------------------------------------
+int neighbor_build(Neighbors &nb, const BoxParams &bp, double4 *x, int inum, double rc, int nm, long anum_cap,
+                   cudaStream_t s)
+{
+    const int tb = 256;
+    if (nb.gcount.ensure(sizeof(int) * (size_t)inum) || nb.goff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
+        nb.gmask.ensure(sizeof(unsigned) * (size_t)inum) || nb.alist.ensure(sizeof(int) * (size_t)anum_cap) ||
+        nb.cidx.ensure(sizeof(int) * (size_t)anum_cap) || nb.ccount.ensure(sizeof(int) * (size_t)bp.ncell) ||
+        nb.cstart.ensure(sizeof(int) * ((size_t)bp.ncell + 1)) || nb.cursor.ensure(sizeof(int) * std::max((size_t)bp.ncell, (size_t)inum)) ||
+        nb.catoms.ensure(sizeof(int) * (size_t)anum_cap) || nb.nlist.ensure(sizeof(int) * (size_t)inum * nm) ||
+        nb.nnum.ensure(sizeof(int) * (size_t)inum) || nb.rcount.ensure(sizeof(int) * (size_t)inum) ||
+        nb.roff.ensure(sizeof(int) * ((size_t)inum + 1)) || nb.rlist.ensure(sizeof(long long) * (size_t)inum * nm) ||
+        nb.status.ensure(sizeof(int) * 4) ||
+        nb.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(std::max((long)inum, bp.ncell))))
+        return -1;
+    int *tmp = nb.scan_tmp.as<int>();
+    k_ghost_count<<<(inum + tb - 1) / tb, tb, 0, s>>>(x, inum, bp, nb.gcount.as<int>(), nb.gmask.as<unsigned>());
+    if (exclusive_scan(nb.gcount.as<int>(), nb.goff.as<int>(), inum, tmp, s)) return -1;
+    int gnum = 0;
+    MDP_CUDA_TRY(cudaMemcpyAsync(&gnum, nb.goff.as<int>() + inum, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(s));
+    if ((long)inum + gnum > anum_cap) {
+        set_error("ghost capacity exceeded: %d local + %d ghosts > %ld", inum, gnum, anum_cap);
+        return -1;
+    }
+    const int anum = inum + gnum;
+    k_ghost_emit<<<(inum + tb - 1) / tb, tb, 0, s>>>(x, nb.alist.as<int>(), inum, bp, nb.goff.as<int>(),
+                                                     nb.gmask.as<unsigned>());
+    MDP_CUDA_TRY(cudaMemsetAsync(nb.ccount.p, 0, sizeof(int) * bp.ncell, s));
+    k_cell_index<<<(anum + tb - 1) / tb, tb, 0, s>>>(x, anum, bp, nb.cidx.as<int>(), nb.ccount.as<int>());
+    if (exclusive_scan(nb.ccount.as<int>(), nb.cstart.as<int>(), bp.ncell, tmp, s)) return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(nb.cursor.p, 0, sizeof(int) * bp.ncell, s));
+    k_cell_fill<<<(anum + tb - 1) / tb, tb, 0, s>>>(anum, nb.cidx.as<int>(), nb.cstart.as<int>(), nb.cursor.as<int>(),
+                                                    nb.catoms.as<int>());
+    MDP_CUDA_TRY(cudaMemsetAsync(nb.status.p, 0, sizeof(int), s));
+    k_neigh_build<<<(inum + 127) / 128, 128, 0, s>>>(x, inum, bp, nb.cidx.as<int>(), nb.cstart.as<int>(),
+                                                     nb.catoms.as<int>(), rc * rc, nm, nb.nlist.as<int>(),
+                                                     nb.nnum.as<int>(), nb.status.as<int>());
+    MDP_CUDA_TRY(cudaMemsetAsync(nb.rcount.p, 0, sizeof(int) * inum, s));
+    k_rev_count<<<(inum + tb - 1) / tb, tb, 0, s>>>(nb.nlist.as<int>(), nb.nnum.as<int>(), nb.alist.as<int>(), inum,
+                                                    nm, nb.rcount.as<int>());
+    if (exclusive_scan(nb.rcount.as<int>(), nb.roff.as<int>(), inum, tmp, s)) return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(nb.cursor.p, 0, sizeof(int) * inum, s));
+    k_rev_fill<<<(inum + tb - 1) / tb, tb, 0, s>>>(nb.nlist.as<int>(), nb.nnum.as<int>(), nb.alist.as<int>(), inum, nm,
+                                                   nb.roff.as<int>(), nb.cursor.as<int>(), nb.rlist.as<long long>());
+    k_rev_sort<<<(inum + tb - 1) / tb, tb, 0, s>>>(inum, nb.roff.as<int>(), nb.rlist.as<long long>());
+    int hs[2] = {0, 0};
+    MDP_CUDA_TRY(cudaMemcpyAsync(&hs[0], nb.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MDP_CUDA_TRY(cudaMemcpyAsync(&hs[1], nb.roff.as<int>() + inum, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(s));
+    MDP_CUDA_TRY(cudaGetLastError());
+    if (hs[0] & 1) {
+        set_error("neighbour list overflow: an atom has more than neighmax=%d neighbours within %.4f A", nm, rc);
+        return -1;
+    }
+    nb.inum = inum;
+    nb.gnum = gnum;
+    nb.anum = anum;
+    nb.nm = nm;
+    nb.nsum = hs[1];
+    nb.anum_cap = anum_cap;
+    return 0;
+}
+
+}  // namespace mdp

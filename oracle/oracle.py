@@ -56,7 +56,7 @@ def tables(twojmax):
     idxu_block = np.zeros(twojmax + 1, dtype=np.int32)
     lib().orc_tables_copy(twojmax, cg, rootpq, idxz, idxb, idxu_block)
     return dict(cg=cg, rootpq=rootpq, idxz=idxz.reshape(-1, 10), idxb=idxb.reshape(-1, 3),
-                idxu_block=idxu_block, **s)
+                idxu_block=idxu_block, n_cg=s["idxcg"], n_u=s["idxu"], n_b=s["idxb"], n_z=s["idxz"])
 
 
 def neighbor_list(x_local, box, rcut, skin, neighmax=64):

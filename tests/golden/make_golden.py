@@ -1,0 +1,120 @@
+"""Generate the committed golden fixtures from the reference's own CPU code.
+
+Run in a container that has the reference tree (the reference is compiled by
+`make -C oracle ref`, into oracle/_ref/):
+
+    python tests/golden/make_golden.py
+
+Each fixture holds a seeded synthetic Ta configuration and what MDP's CPU
+implementation computes for it:
+  * the ghost atoms (positions and owners) and the full neighbour list, built
+    by cpuNeighborList3D.cpp in both its O(N^2) and cell forms;
+  * per-atom energy, forces and virial from the cpuSnap4.cpp chain
+    (ComputePairSnap3 order);
+  * for the MD fixtures, a short NVE velocity-Verlet trajectory in the order of
+    CIntegration::VelocityVerlet (Integration.cpp:17-139), with thermo rows.
+The inputs are regenerated by the tests from the stored seeds and checked
+against the stored copies, so the fixtures also pin the input generator.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from mdp_b200 import configs  # noqa: E402
+from oracle import refpy  # noqa: E402
+
+# (name, cells, 2J, temp, jitter, seed, coeff seed, flag overrides, md steps, dt)
+CASES = [
+    ("bcc128_2j6", (4, 4, 4), 6, 300.0, 0.05, 11, 101, {}, 40, 0.0005),
+    ("bcc250_2j8", (5, 5, 5), 8, 600.0, 0.05, 12, 102, {}, 20, 0.001),
+    ("bcc128_2j4", (4, 4, 4), 4, 1000.0, 0.10, 13, 103, {}, 20, 0.001),
+    ("bcc54_2j8_flags", (3, 3, 3), 8, 300.0, 0.08, 14, 104,
+     {"bnormflag": 1, "bzeroflag": 1, "switchflag": 0}, 0, 0.001),
+    ("bcc250_2j8_hot", (5, 5, 5), 8, 3000.0, 0.20, 15, 105, {}, 0, 0.001),
+]
+SKIN = 1.0
+NEIGHMAX = 80
+
+
+def thermo_row(step, e, v, vatom, box, mass):
+    n = e.size
+    tdof = (n - 1) * 3.0
+    temp = configs.MVV2E / (tdof * configs.BOLTZ) * mass * np.sum(v * v)
+    pe = e.sum() / n
+    ke = 0.5 * tdof * configs.BOLTZ * temp / n
+    vol = box[0] * box[1] * box[2]
+    pres = (tdof * configs.BOLTZ * temp + vatom[0].sum() + vatom[1].sum() + vatom[2].sum()) / 3.0 / vol * configs.NKTV2P
+    return [step, temp, pe, pe + ke, pres]
+
+
+def ref_md(x0, v0, box, p, nsteps, dt, mass):
+    """NVE in the reference's step order using the reference's own kernels."""
+    dtf = 0.5 * dt * configs.FTM2V
+    ilist = np.arange(x0.shape[0], dtype=np.int32)
+    typ = np.ones(x0.shape[0] + 1, dtype=np.int32)
+    massarr = np.array([0.0, mass])
+    x = x0.copy(); v = v0.copy()
+    xa, al, nl, nn = refpy.neighbor_list(x, box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+    xhold = x.copy()
+    e, f, va = refpy.snap_force(xa, al, nl, nn, p)
+    rows = [thermo_row(0, e, v, va, box, mass)]
+    rebuilds = 1
+    n = x.shape[0]
+    lib = refpy.lib()
+    for step in range(1, nsteps + 1):
+        xstart = x.copy()
+        xf = np.ascontiguousarray(x).ravel(); vf = np.ascontiguousarray(v).ravel()
+        lib.ref_nve_initial(xf, vf, np.ascontiguousarray(f).ravel(), massarr, dtf, dt, typ, ilist, n)
+        x = xf.reshape(n, 3); v = vf.reshape(n, 3)
+        if np.max(np.sum((x - xhold) ** 2, axis=1)) > 0.25 * SKIN * SKIN:
+            x = np.where(x < 0.0, x + box, x)
+            x = np.where(x >= box, np.maximum(x - box, 0.0), x)
+            xa, al, nl, nn = refpy.neighbor_list(x, box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+            xhold = x.copy()
+            rebuilds += 1
+        else:
+            xa = xa.copy()
+            xa[:n] = x
+            xa[n:] += (x - xstart)[al[n:]]
+        e, f, va = refpy.snap_force(xa, al, nl, nn, p)
+        vf = np.ascontiguousarray(v).ravel()
+        lib.ref_nve_final(np.ascontiguousarray(x).ravel(), vf, np.ascontiguousarray(f).ravel(), massarr, dtf, typ,
+                          ilist, n)
+        v = vf.reshape(n, 3)
+        rows.append(thermo_row(step, e, v, va, box, mass))
+    return np.array(rows), x, v, f, e, rebuilds
+
+
+def main():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    for (name, cells, tj, temp, jit, seed, cseed, flags, nsteps, dt) in CASES:
+        p = configs.snap_params(tj, seed=cseed, **flags)
+        cfg = configs.ta_config(cells, temp=temp, jitter=jit, seed=seed)
+        xa0, al0, nl0, nn0 = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+        xa1, al1, nl1, nn1 = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=1)
+        e, f, va = refpy.snap_force(xa0, al0, nl0, nn0, p)
+        out = dict(cells=np.array(cells), twojmax=tj, temp=temp, jitter=jit, seed=seed, coeff_seed=cseed,
+                   flags=np.array([p.bnormflag, p.bzeroflag, p.switchflag]), skin=SKIN, neighmax=NEIGHMAX,
+                   x=cfg.x, v=cfg.v, box=cfg.box, coeff=p.coeff,
+                   xall=xa0, alist=al0, neighlist=nl0, neighnum=nn0,
+                   neighlist_cell=nl1, neighnum_cell=nn1,
+                   eatom=e, fatom=f, vatom=va)
+        if nsteps:
+            th, x, v, ff, ee, nreb = ref_md(cfg.x, cfg.v, cfg.box, p, nsteps, dt, configs.TA_MASS)
+            out.update(md_dt=dt, md_steps=nsteps, md_thermo=th, md_x=x, md_v=v, md_f=ff, md_e=ee,
+                       md_rebuilds=nreb)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, **out)
+        print(name, cfg.natoms, "atoms", xa0.shape[0] - cfg.natoms, "ghosts", os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()
