@@ -1,0 +1,338 @@
+"""SNAP atom-steps/s on the 2,000,000-atom BCC Ta, 2J=8 workload (one B200).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one velocity-Verlet MD step of the whole system (neighbour check,
+SNAP energy/force/virial, both half-kicks), as in cpuMDP's time loop.
+Workload: 100x100x100 BCC Ta cells (2,000,000 atoms, a = 3.316 A), jitter
+N(0, 0.05 A), Maxwell-Boltzmann velocities at 300 K, SNAP 2J=8 with seeded
+coefficients, dt = 1 fs, skin 1 A; synthetic, seeded.  Every array the step
+touches (U tiles 9 GB, Y 5 GB, pair lists) is far larger than the 126 MB L2,
+so no L2 flush is needed between timed steps.
+
+value      plain FP64 path, inputs resident on the device, CUDA-event time
+           of K steps on the engine stream.
+e2e        the same through the host API: every step uploads positions and
+           velocities from pinned host memory and downloads forces and
+           per-atom energies.
+fp32       the reduced-precision form on the same workload, with its force
+           RMSE against the FP64 path.
+roofline   the Y kernel (dominant): algorithmic FLOPs / its CUDA-event time,
+           against this GPU's FP64 FMA rate measured by the library's probe.
+cpu_baseline  MDP's own CPU SNAP (oracle/_ref build of src/C++/Core/cpuSnap4.cpp
+           chain) on a bounded sample (16,000 atoms, same lattice and model),
+           on the host's cores.
+
+With --gpus N (torchrun), every rank runs an independent replica of the
+workload (the MD system is not decomposed across GPUs); value sums the ranks'
+atom-steps over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "SNAP atom-steps/s, 2M-atom Ta 2J=8, 1 B200: FP64 vs FP32/surrogate @force err"
+CELLS = (100, 100, 100)
+TWOJ = 8
+DT = 0.001
+SKIN = 1.0
+NEIGHMAX = 64
+SAMPLE_CELLS = (20, 20, 20)        # CPU-baseline sample: 16,000 atoms
+
+# algorithmic FLOPs (2J=8), per atom or pair, counted on the reference's
+# minimal algorithm: Z/Y 41,889 complex terms x 11, energy 1,413 x 4,
+# U 154 half-plane elements x 22 per pair, dU/dr 154 x 156 per pair
+FLOP_Y_PER_ATOM = 41889 * 11 + 1413 * 4
+FLOP_U_PER_PAIR = 154 * 22
+FLOP_F_PER_PAIR = 154 * 156
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [t.strip() for t in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1])); smax = float(c[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, c[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+class CpuSample:
+    """The 16,000-atom sample of the workload, prepared once for MDP's own CPU
+    SNAP (reference build of the cpuSnap4.cpp chain)."""
+
+    def __init__(self):
+        from mdp_b200 import configs
+        from oracle import refpy
+        if not refpy.available():
+            subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "oracle"), "ref"])
+        self.refpy = refpy
+        self.p = configs.snap_params(TWOJ, seed=2024)
+        self.cfg = configs.ta_config(SAMPLE_CELLS, temp=300.0, jitter=0.05, seed=2024)
+        self.threads = os.cpu_count() or 1
+        self.nb = refpy.neighbor_list(self.cfg.x, self.cfg.box, self.p.rcut, SKIN, NEIGHMAX, neighcell=1)
+
+    def step(self) -> float:
+        xa, al, nl, nn = self.nb
+        t0 = time.perf_counter()
+        self.refpy.snap_force(xa, al, nl, nn, self.p, nblocks=4 * self.threads, nthreads=self.threads)
+        return time.perf_counter() - t0
+
+    def describe(self, seconds: float, steps: int) -> str:
+        return (f"{self.cfg.natoms} atoms (20^3 BCC Ta of the same lattice/model, 2J=8), {steps} SNAP force "
+                f"evaluation(s) of MDP's cpuSnap4 chain (reference build, -O3 -ffast-math), {self.threads} host "
+                f"threads over atom blocks, {seconds:.2f} s")
+
+
+def cpu_baseline() -> dict:
+    s = CpuSample()
+    s.step()
+    dt = s.step()
+    return {"value": s.cfg.natoms / dt, "unit": "atom-steps/s", "cores": s.threads, "kind": "reference",
+            "sample": s.describe(dt, 1)}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    s = CpuSample()
+    for _ in range(args.warmup):
+        s.step()
+    el = sum(s.step() for _ in range(args.steps))
+    natoms = s.cfg.natoms
+    value = natoms * args.steps / el
+    line = {"metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "BCC Ta 2J=8 SNAP force path; MDP's CPU code timed on a 16,000-atom sample of "
+                                   "the 2,000,000-atom workload (a step = one force evaluation of the sample)",
+                       "atoms": 2000000, "sample_atoms": natoms},
+            "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": s.threads, "kind": "reference",
+                             "sample": s.describe(el, args.steps)},
+            "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def build_md(precision, device):
+    from mdp_b200 import configs
+    from mdp_b200.snap import SnapMD
+    p = configs.snap_params(TWOJ, seed=2024)
+    cfg = configs.ta_config(CELLS, temp=300.0, jitter=0.05, seed=2024 + device)
+    md = SnapMD(p, cfg.box, cfg.natoms, DT, skin=SKIN, neighmax=NEIGHMAX, precision=precision, device=device)
+    md.set_state(cfg.x, cfg.v)
+    md.setup()
+    return md, cfg
+
+
+def run_ours(args):
+    import torch
+    ws, rank, local = dist_env()
+    dev = local if torch.cuda.device_count() > local else 0
+    torch.cuda.set_device(dev)
+    if ws > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", dev))
+    from mdp_b200.snap import launch_count, probe_fma_peak
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+
+    md, cfg = build_md("fp64", dev)
+    n = cfg.natoms
+    md.run(args.warmup)
+    clocks = Clocks(dev)
+    barrier()
+    clocks.start()
+    l0 = launch_count()
+    _, ms = md.run(args.steps)
+    l1 = launch_count()
+    barrier()
+    clk = clocks.stop()
+    launches = l1 - l0
+    if ws > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = ws * n * args.steps / (ms * 1e-3)
+
+    # stage timing (CUDA events per stage on the engine stream) for the roofline
+    md.stage_timing(True)
+    md.run(2)
+    st = md.stage_times()
+    md.stage_timing(False)
+    cnt = md.counters()
+    pairs = cnt["pairs"]
+    yi_ms = st["yi"] / max(st["calls"], 1)
+    fi_ms = st["fi"] / max(st["calls"], 1)
+    ui_ms = st["ui"] / max(st["calls"], 1)
+    fp64_peak, fp32_peak = probe_fma_peak(dev)
+    y_tf = FLOP_Y_PER_ATOM * n / (yi_ms * 1e-3) / 1e12
+
+    # end-to-end through the host API, pinned buffers, one upload + download per step
+    x, v, f, e = md.state()
+    hx = torch.from_numpy(x).pin_memory(); hv = torch.from_numpy(v).pin_memory()
+    hf = torch.empty((n, 3), dtype=torch.float64).pin_memory(); he = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_steps = max(2, args.steps // 2)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        md.upload(hx.data_ptr(), hv.data_ptr())
+        md.run(1)
+        md.download(hf.data_ptr(), he.data_ptr())
+        md.sync()
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    e2e_value = ws * n * e2e_steps / e2e_s
+    f64_now = hf.numpy().copy()
+    x_now, v_now, _, _ = md.state()
+    md.close()
+
+    # FP32 form on the same state: force error vs FP64, then its own timing
+    from mdp_b200 import configs
+    from mdp_b200.snap import SnapMD, snap_compute
+    p = configs.snap_params(TWOJ, seed=2024)
+    ref64 = snap_compute(p, x_now, cfg.box, SKIN, NEIGHMAX, precision="fp64")
+    ref32 = snap_compute(p, x_now, cfg.box, SKIN, NEIGHMAX, precision="fp32")
+    df = ref32["fatom"] - ref64["fatom"]
+    fp32_rmse = float(np.sqrt(np.mean(df ** 2)))
+    fp32_max = float(np.abs(df).max())
+    md32 = SnapMD(p, cfg.box, n, DT, skin=SKIN, neighmax=NEIGHMAX, precision="fp32", device=dev)
+    md32.set_state(x_now, v_now)
+    md32.setup()
+    md32.run(args.warmup)
+    barrier()
+    _, ms32 = md32.run(args.steps)
+    barrier()
+    md32.close()
+    if ws > 1:
+        t = torch.tensor([ms32], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms32 = float(t.item())
+    value32 = ws * n * args.steps / (ms32 * 1e-3)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline()
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "error": str(ex)[:200]}
+
+    traffic = None
+    prof = os.path.join(HERE, "profiles", "k_snap_yi_fp64_traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as fh:
+            tr = json.load(fh)
+        traffic = tr["bytes_per_atom"] * n
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "NVE MD, BCC Ta 100x100x100 cells = 2,000,000 atoms, 300 K, jitter 0.05 A, "
+                                   "SNAP 2J=8 (55 components), seeded beta, dt 1 fs, skin 1 A",
+                       "atoms": n, "twojmax": TWOJ, "pairs_per_atom": pairs / n,
+                       "l2": "inputs larger than L2 (U 9 GB, Y 5 GB per step)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+            "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": int(hx.nbytes + hv.nbytes),
+                    "d2h_bytes_per_step": int(hf.nbytes + he.nbytes)},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "fp64", "kernel": "k_snap_yi<double,8>", "achieved": y_tf, "peak": fp64_peak,
+                         "unit": "TFLOP/s", "frac": y_tf / fp64_peak,
+                         "peak_source": "measured FP64 FMA rate of this GPU (library probe); "
+                                        "MEASURED_PEAKS.json has no FP64 figure",
+                         "traffic": traffic, "ms_per_launch": yi_ms},
+            "stages_ms": {"pairs": st["pairs"] / max(st["calls"], 1), "ui": ui_ms, "yi": yi_ms, "fi": fi_ms,
+                          "tally": st["tally"] / max(st["calls"], 1), "force": st["force"] / max(st["calls"], 1)},
+            "fi_tflops": FLOP_F_PER_PAIR * pairs / (fi_ms * 1e-3) / 1e12,
+            "ui_tflops": FLOP_U_PER_PAIR * pairs / (ui_ms * 1e-3) / 1e12,
+            "fp32": {"value": value32, "unit": "atom-steps/s", "speedup_vs_fp64": value32 / value,
+                     "force_rmse_vs_fp64": fp32_rmse, "force_maxerr_vs_fp64": fp32_max, "unit_err": "eV/A",
+                     "fp32_fma_peak_tflops": fp32_peak},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

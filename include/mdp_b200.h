@@ -101,6 +101,15 @@ int mdp_md_setup(mdp_md *h);
 int mdp_md_run(mdp_md *h, int nsteps, int thermo_every, double *thermo, int thermo_cap, int *nrows,
                float *elapsed_ms);
 int mdp_md_get_state(mdp_md *h, double *x, double *v, double *f, double *eatom);
+/* Asynchronous state upload / result download on the engine's stream, for
+ * callers that keep the state on the host between steps (pinned host memory
+ * makes the copies truly asynchronous).  The uploaded positions must be ones
+ * this engine produced (the neighbour list is kept).  mdp_md_sync waits. */
+int mdp_md_upload(mdp_md *h, const double *x, const double *v);
+int mdp_md_download(mdp_md *h, double *f, double *eatom);
+int mdp_md_sync(mdp_md *h);
+/* number of kernels this library has launched so far (all handles) */
+long long mdp_launch_count(void);
 int mdp_md_thermo(mdp_md *h, double *out5);
 /* counters: [0] steps, [1] neighbour rebuilds, [2] current pairs, [3] ghosts,
  * [4] neighbour entries */

@@ -68,6 +68,10 @@ def lib():
     L.mdp_md_stage_times.argtypes = [C.c_void_p, _dp, C.POINTER(C.c_longlong)]
     L.mdp_md_stream.argtypes = [C.c_void_p]
     L.mdp_md_stream.restype = C.c_void_p
+    L.mdp_md_upload.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mdp_md_download.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mdp_md_sync.argtypes = [C.c_void_p]
+    L.mdp_launch_count.restype = C.c_longlong
     L.mdp_probe_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     _lib = L
     return L

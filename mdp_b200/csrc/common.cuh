@@ -129,6 +129,10 @@ template <> __device__ __forceinline__ float cgc<float>(int k) { return c_cg_f[k
         }                                                                          \
     } while (0)
 
+// count of kernels this library has launched (all streams, all devices)
+void count_launches(long n);
+long long launch_count();
+
 // exclusive scan of n ints (n <= 16M) into out[0..n]; out[n] = total.
 // tmp must hold scan_tmp_ints(n) ints.
 size_t scan_tmp_ints(long n);

@@ -97,7 +97,7 @@ struct mdp_md {
     cudaStream_t s = nullptr;
     int device = 0;
     long anum_cap = 0;
-    DevBuf x, v, f, xstart, xhold, e, vatom, scal;
+    DevBuf x, v, f, xstart, xhold, e, vatom, scal, stage;
     Neighbors nb;
     ForcePath fp;
     long long step = 0, rebuilds = 0;
@@ -156,7 +156,7 @@ void mdp_md_destroy(mdp_md *m)
     if (!m) return;
     cudaSetDevice(m->device);
     if (m->s) cudaStreamSynchronize(m->s);
-    DevBuf *b[] = {&m->x, &m->v, &m->f, &m->xstart, &m->xhold, &m->e, &m->vatom, &m->scal};
+    DevBuf *b[] = {&m->x, &m->v, &m->f, &m->xstart, &m->xhold, &m->e, &m->vatom, &m->scal, &m->stage};
     for (auto x : b) x->release();
     m->nb.release();
     m->fp.release();
@@ -200,6 +200,7 @@ static int md_rebuild(mdp_md *m)
     const int n = m->cfg.natoms;
     const double *b = m->cfg.box;
     k_pbc_orth<<<(n + 255) / 256, 256, 0, m->s>>>(m->x.as<double4>(), n, 0.0, 0.0, 0.0, b[0], b[4], b[8]);
+    count_launches(1);
     const double rc = m->model.geom.rcut + m->cfg.skin;
     if (neighbor_build(m->nb, m->bp, m->x.as<double4>(), n, rc, m->cfg.neighmax, m->anum_cap, m->s)) return -1;
     MDP_CUDA_TRY(cudaMemcpyAsync(m->xhold.p, m->x.p, sizeof(double4) * n, cudaMemcpyDeviceToDevice, m->s));
@@ -270,6 +271,7 @@ int mdp_md_run(mdp_md *m, int nsteps, int thermo_every, double *thermo, int ther
         m->step++;
         k_nve_initial<<<(n + 255) / 256, 256, 0, m->s>>>(m->x.as<double4>(), m->v.as<double4>(), m->f.as<double4>(),
                                                          m->xstart.as<double4>(), n, dtfm, dtv);
+        count_launches(1);
         const long long ago = m->step;
         int build = 0;
         if (ago >= m->cfg.neighdelay && ago % m->cfg.neighevery == 0) {
@@ -277,6 +279,7 @@ int mdp_md_run(mdp_md *m, int nsteps, int thermo_every, double *thermo, int ther
             else {
                 MDP_CUDA_TRY(cudaMemsetAsync(dmax, 0, sizeof(unsigned long long), m->s));
                 k_maxdisp<<<(n + 255) / 256, 256, 0, m->s>>>(m->x.as<double4>(), m->xhold.as<double4>(), n, dmax);
+                count_launches(1);
                 unsigned long long hm = 0;
                 MDP_CUDA_TRY(cudaMemcpyAsync(&hm, dmax, sizeof(hm), cudaMemcpyDeviceToHost, m->s));
                 MDP_CUDA_TRY(cudaStreamSynchronize(m->s));
@@ -290,9 +293,11 @@ int mdp_md_run(mdp_md *m, int nsteps, int thermo_every, double *thermo, int ther
         } else if (m->nb.gnum > 0) {
             k_ghost_shift<<<(m->nb.gnum + 255) / 256, 256, 0, m->s>>>(m->x.as<double4>(), m->xstart.as<double4>(),
                                                                       m->nb.alist.as<int>(), n, m->nb.gnum);
+            count_launches(1);
         }
         if (md_force(m)) return -1;
         k_nve_final<<<(n + 255) / 256, 256, 0, m->s>>>(m->v.as<double4>(), m->f.as<double4>(), n, dtfm);
+        count_launches(1);
         if (thermo_every > 0 && m->step % thermo_every == 0) {
             double row[5];
             if (md_thermo(m, row)) return -1;
@@ -311,6 +316,47 @@ int mdp_md_run(mdp_md *m, int nsteps, int thermo_every, double *thermo, int ther
     MDP_CUDA_TRY(cudaGetLastError());
     return 0;
 }
+
+int mdp_md_upload(mdp_md *m, const double *x, const double *v)
+{
+    if (!m || !x || !v) { set_error("null argument"); return -1; }
+    if (!m->ready) { set_error("mdp_md_setup must run before mdp_md_upload"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(m->device));
+    const long n = m->cfg.natoms;
+    if (m->stage.ensure(sizeof(double) * 6 * n)) return -1;
+    double *t = m->stage.as<double>();
+    MDP_CUDA_TRY(cudaMemcpyAsync(t, x, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, m->s));
+    MDP_CUDA_TRY(cudaMemcpyAsync(t + 3 * n, v, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, m->s));
+    k_aos_to_d4<<<(n + 255) / 256, 256, 0, m->s>>>(t, m->x.as<double4>(), n);
+    k_aos_to_d4<<<(n + 255) / 256, 256, 0, m->s>>>(t + 3 * n, m->v.as<double4>(), n);
+    count_launches(2);
+    return 0;
+}
+
+int mdp_md_download(mdp_md *m, double *f, double *eatom)
+{
+    if (!m) { set_error("null handle"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(m->device));
+    const long n = m->cfg.natoms;
+    if (m->stage.ensure(sizeof(double) * 6 * n)) return -1;
+    double *t = m->stage.as<double>();
+    if (f) {
+        k_d4_to_aos<<<(n + 255) / 256, 256, 0, m->s>>>(m->f.as<double4>(), t, n);
+        count_launches(1);
+        MDP_CUDA_TRY(cudaMemcpyAsync(f, t, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, m->s));
+    }
+    if (eatom) MDP_CUDA_TRY(cudaMemcpyAsync(eatom, m->e.p, sizeof(double) * n, cudaMemcpyDeviceToHost, m->s));
+    return 0;
+}
+
+int mdp_md_sync(mdp_md *m)
+{
+    if (!m) { set_error("null handle"); return -1; }
+    MDP_CUDA_TRY(cudaStreamSynchronize(m->s));
+    return 0;
+}
+
+long long mdp_launch_count(void) { return launch_count(); }
 
 int mdp_md_get_state(mdp_md *m, double *x, double *v, double *f, double *eatom)
 {

@@ -10,8 +10,7 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
 {
     typedef typename cplx<T>::type T2;
     if (tu_ensure_tables()) return -1;
-    constexpr int NU = idxu_count(TJ);
-    const size_t sm = (size_t)NU * 32 * sizeof(T2) + YI_WARPS * 32 * sizeof(double);
+    const size_t sm = yi_smem_bytes<T, TJ>();
     static int per_sm = 0;
     if (!per_sm) {
         MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

@@ -128,40 +128,46 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
     m.yd.e0 = e0;
     m.yf.e0 = e0;
 
-    // Y-kernel units (j, mb) with their term counts, longest-first onto warps
-    struct Unit { int j, mb; long cost; };
-    std::vector<Unit> units;
-    for (int j = 0; j <= tj; j++)
+    // Y-kernel schedule: units (j, mb) in a fixed order shared by all warps; the
+    // couplings of each unit are spread over the warps longest-first
+    int nu = 0;
+    for (int j = tj; j >= 0; j--)
         for (int mb = 0; 2 * mb <= j; mb++) {
-            long cost = 0;
+            if (nu >= YI_MAXUNITS) { set_error("Y schedule overflow"); return -1; }
+            struct Cp { int c; long cost; };
+            std::vector<Cp> cps;
+            int c = 0;
             for (int j1 = 0; j1 <= tj; j1++)
                 for (int j2 = 0; j2 <= j1; j2++) {
-                    if (!triple_ok(j1, j2, j, tj)) continue;
+                    if (!coupling_ok(j1, j2, j)) continue;
                     int mb1min = std::max(0, (2 * mb - j - j2 + j1) / 2);
                     int nbb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
+                    long cost = 0;
                     for (int ma = 0; ma <= j; ma++) {
                         int ma1min = std::max(0, (2 * ma - j - j2 + j1) / 2);
                         int na = std::min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
                         cost += (long)na * nbb;
                     }
+                    cps.push_back({c, cost + 2L * (j1 + j2 + 2) * nbb});
+                    c++;
                 }
-            units.push_back({j, mb, cost + 8});
+            if (c > 32) { set_error("more than 32 couplings for j=%d", j); return -1; }
+            std::sort(cps.begin(), cps.end(), [](const Cp &x, const Cp &y) { return x.cost > y.cost; });
+            long load[YI_WARPS] = {0};
+            unsigned mask[YI_WARPS] = {0};
+            for (auto &cp : cps) {
+                int w = 0;
+                for (int k = 1; k < YI_WARPS; k++)
+                    if (load[k] < load[w]) w = k;
+                mask[w] |= 1u << cp.c;
+                load[w] += cp.cost;
+            }
+            m.yd.unit_j[nu] = m.yf.unit_j[nu] = (unsigned char)j;
+            m.yd.unit_mb[nu] = m.yf.unit_mb[nu] = (unsigned char)mb;
+            for (int w = 0; w < YI_WARPS; w++) m.yd.unit_mask[nu][w] = m.yf.unit_mask[nu][w] = mask[w];
+            nu++;
         }
-    std::sort(units.begin(), units.end(), [](const Unit &a, const Unit &b) { return a.cost > b.cost; });
-    long load[YI_WARPS] = {0};
-    for (auto &u : units) {
-        int w = 0;
-        for (int k = 1; k < YI_WARPS; k++)
-            if (load[k] < load[w]) w = k;
-        if (m.yd.nunits[w] >= YI_MAXU) { set_error("Y schedule overflow"); return -1; }
-        int n = m.yd.nunits[w]++;
-        m.yd.unit_j[w][n] = (unsigned char)u.j;
-        m.yd.unit_mb[w][n] = (unsigned char)u.mb;
-        load[w] += u.cost;
-    }
-    memcpy(m.yf.nunits, m.yd.nunits, sizeof(m.yd.nunits));
-    memcpy(m.yf.unit_j, m.yd.unit_j, sizeof(m.yd.unit_j));
-    memcpy(m.yf.unit_mb, m.yd.unit_mb, sizeof(m.yd.unit_mb));
+    m.yd.nunits = m.yf.nunits = nu;
     return 0;
 }
 
@@ -218,6 +224,7 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (rc) return rc;
     if (fp.timing) cudaEventRecord(fp.ev[4], s);
     k_tally<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), fp.dE.as<double4>(), nnum, inum, nm, roff, rlist, f, vatom);
+    count_launches(6);   // pair_count, pair_emit, ui, yi, fi, tally (+ the scan counts itself)
     if (fp.timing) {
         cudaEventRecord(fp.ev[5], s);
         cudaEventSynchronize(fp.ev[5]);
@@ -281,6 +288,7 @@ int neighbor_build(Neighbors &nb, const BoxParams &bp, double4 *x, int inum, dou
     k_rev_fill<<<(inum + tb - 1) / tb, tb, 0, s>>>(nb.nlist.as<int>(), nb.nnum.as<int>(), nb.alist.as<int>(), inum, nm,
                                                    nb.roff.as<int>(), nb.cursor.as<int>(), nb.rlist.as<long long>());
     k_rev_sort<<<(inum + tb - 1) / tb, tb, 0, s>>>(inum, nb.roff.as<int>(), nb.rlist.as<long long>());
+    count_launches(8);
     int hs[2] = {0, 0};
     MDP_CUDA_TRY(cudaMemcpyAsync(&hs[0], nb.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     MDP_CUDA_TRY(cudaMemcpyAsync(&hs[1], nb.roff.as<int>() + inum, sizeof(int), cudaMemcpyDeviceToHost, s));

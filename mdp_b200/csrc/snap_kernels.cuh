@@ -24,18 +24,28 @@ struct SnapGeom {
     int switchflag;
 };
 
-// per-unit schedule of the Y kernel: a unit is one output row (j, mb)
+// Y-kernel schedule.  A unit is one output row (j, mb) of Y for the tile's 32
+// atoms; every warp of the CTA works on the same unit at the same time, each on
+// its own subset of the (j1, j2) couplings (bit c of unit_mask[u][w] selects the
+// c-th coupling of j in enumeration order), so the code the warps execute at
+// any moment is a few kilobytes and stays in the instruction cache.
 constexpr int YI_WARPS = 8;
-constexpr int YI_MAXU = 8;
+constexpr int YI_MAXUNITS = 32;
 
 template <typename T>
 struct YParams {
     T betaY[NTRI];          // beta' of each coupling triple (bnorm 1/(j+1) folded in)
     double e0;              // beta0 - sum_k beta_k bzero_k
-    int nunits[YI_WARPS];
-    unsigned char unit_j[YI_WARPS][YI_MAXU];
-    unsigned char unit_mb[YI_WARPS][YI_MAXU];
+    int nunits;
+    unsigned char unit_j[YI_MAXUNITS];
+    unsigned char unit_mb[YI_MAXUNITS];
+    unsigned int unit_mask[YI_MAXUNITS][YI_WARPS];
 };
+
+__host__ __device__ constexpr bool coupling_ok(int j1, int j2, int j)
+{
+    return j2 <= j1 && j1 - j2 <= j && j <= j1 + j2 && ((j1 + j2 + j) % 2 == 0);
+}
 
 // ---------------------------------------------------------------------------
 // pair geometry (cpuSnap4.cpp:15-53, 803-874), evaluated in double
@@ -262,58 +272,58 @@ __device__ __forceinline__ void zrow_acc(const int mb, const typename cplx<T>::t
     }
 }
 
-template <typename T, int TJ, int J, int J1, int J2>
-__device__ __forceinline__ void y_couplings(const int mb, const typename cplx<T>::type *__restrict__ Us,
-                                            const int lane, const YParams<T> &P, T (&yr)[JD], T (&yi)[JD])
+template <typename T, int TJ, int J, int J1, int J2, int C>
+__device__ __forceinline__ void y_couplings(const int mb, const unsigned mask,
+                                            const typename cplx<T>::type *__restrict__ Us, const int lane,
+                                            const YParams<T> &P, T (&yr)[JD], T (&yi)[JD])
 {
     if constexpr (J1 <= TJ) {
         if constexpr (J2 <= J1) {
-            if constexpr (J1 - J2 <= J && J <= J1 + J2 && ((J1 + J2 + J) % 2 == 0))
-                zrow_acc<T, J1, J2, J>(mb, Us, lane, P.betaY[tri_index(J1, J2, J)], yr, yi);
-            y_couplings<T, TJ, J, J1, J2 + 1>(mb, Us, lane, P, yr, yi);
+            if constexpr (coupling_ok(J1, J2, J)) {
+                if (mask & (1u << C)) zrow_acc<T, J1, J2, J>(mb, Us, lane, P.betaY[tri_index(J1, J2, J)], yr, yi);
+                y_couplings<T, TJ, J, J1, J2 + 1, C + 1>(mb, mask, Us, lane, P, yr, yi);
+            } else {
+                y_couplings<T, TJ, J, J1, J2 + 1, C>(mb, mask, Us, lane, P, yr, yi);
+            }
         } else {
-            y_couplings<T, TJ, J, J1 + 1, 0>(mb, Us, lane, P, yr, yi);
+            y_couplings<T, TJ, J, J1 + 1, 0, C>(mb, mask, Us, lane, P, yr, yi);
         }
     }
 }
 
-// one output row Y_J(., mb) for the tile's 32 atoms; returns this lane's
-// contribution sum_ma w Re(U* Y) to the energy identity
+// this warp's share of output row Y_J(., mb), written to red[ma][lane]
 template <typename T, int TJ, int J>
-__device__ __forceinline__ double y_unit(const int mb, const typename cplx<T>::type *__restrict__ Us,
-                                         const int lane, const YParams<T> &P,
-                                         typename cplx<T>::type *__restrict__ yout)
+__device__ __forceinline__ void y_unit(const int mb, const unsigned mask, const typename cplx<T>::type *__restrict__ Us,
+                                       const int lane, const YParams<T> &P, typename cplx<T>::type *__restrict__ red)
 {
     typedef typename cplx<T>::type T2;
     T yr[JD], yi[JD];
 #pragma unroll
     for (int ma = 0; ma < JD; ma++) { yr[ma] = T(0); yi[ma] = T(0); }
-    y_couplings<T, TJ, J, 0, 0>(mb, Us, lane, P, yr, yi);
-    double e = 0.0;
-    const T2 *urow = Us + (idxu_block(J) + (J + 1) * mb) * 32 + lane;
+    y_couplings<T, TJ, J, 0, 0, 0>(mb, mask, Us, lane, P, yr, yi);
 #pragma unroll
-    for (int ma = 0; ma <= J; ma++) {
-        const T2 u = urow[ma * 32];
-        const double w = (2 * mb < J) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
-        e += w * ((double)u.x * (double)yr[ma] + (double)u.y * (double)yi[ma]);
-        if (yout) yout[yh_block(J) + (J + 1) * mb + ma] = T2{yr[ma], yi[ma]};
-    }
-    return e;
+    for (int ma = 0; ma <= J; ma++) red[ma * 32 + lane] = T2{yr[ma], yi[ma]};
 }
 
 template <typename T, int TJ>
-__device__ __forceinline__ double y_dispatch(const int j, const int mb, const typename cplx<T>::type *__restrict__ Us,
-                                             const int lane, const YParams<T> &P,
-                                             typename cplx<T>::type *__restrict__ yout)
+__device__ __forceinline__ void y_dispatch(const int j, const int mb, const unsigned mask,
+                                           const typename cplx<T>::type *__restrict__ Us, const int lane,
+                                           const YParams<T> &P, typename cplx<T>::type *__restrict__ red)
 {
     switch (j) {
 #define MDP_YCASE(JJ) \
-    case JJ: if constexpr (JJ <= TJ) return y_unit<T, TJ, JJ>(mb, Us, lane, P, yout); break;
+    case JJ: if constexpr (JJ <= TJ) y_unit<T, TJ, JJ>(mb, mask, Us, lane, P, red); break;
         MDP_YCASE(0) MDP_YCASE(1) MDP_YCASE(2) MDP_YCASE(3) MDP_YCASE(4)
         MDP_YCASE(5) MDP_YCASE(6) MDP_YCASE(7) MDP_YCASE(8)
 #undef MDP_YCASE
     }
-    return 0.0;
+}
+
+template <typename T, int TJ>
+constexpr size_t yi_smem_bytes()
+{
+    return (size_t)idxu_count(TJ) * 32 * sizeof(typename cplx<T>::type) +
+           (size_t)YI_WARPS * JD * 32 * sizeof(typename cplx<T>::type) + YI_WARPS * 32 * sizeof(double);
 }
 
 template <typename T, int TJ>
@@ -326,7 +336,8 @@ k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __gri
     constexpr int NYH = yh_count(TJ);
     extern __shared__ __align__(16) unsigned char smraw[];
     T2 *Us = reinterpret_cast<T2 *>(smraw);
-    double *ered = reinterpret_cast<double *>(Us + NU * 32);
+    T2 *red = Us + NU * 32;                                   // [warp][ma][lane]
+    double *ered = reinterpret_cast<double *>(red + YI_WARPS * JD * 32);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int ntiles = (natoms + 31) >> 5;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -334,11 +345,27 @@ k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __gri
         for (int k = threadIdx.x; k < NU * 32; k += YI_WARPS * 32) Us[k] = src[k];
         __syncthreads();
         const int atom = tile * 32 + lane;
-        T2 *yout = (atom < natoms) ? Y + (size_t)atom * NYH : nullptr;
+        T2 *yout = Y + (size_t)atom * NYH;
         double e = 0.0;
-        const int nu = P.nunits[w];
-        for (int u = 0; u < nu; u++)
-            e += y_dispatch<T, TJ>(P.unit_j[w][u], P.unit_mb[w][u], Us, lane, P, yout);
+        for (int u = 0; u < P.nunits; u++) {
+            const int j = P.unit_j[u], mb = P.unit_mb[u];
+            y_dispatch<T, TJ>(j, mb, P.unit_mask[u][w], Us, lane, P, red + w * JD * 32);
+            __syncthreads();
+            // reduce the warps' partial rows; warp w finalises entries ma = w, w+8
+            for (int ma = w; ma <= j; ma += YI_WARPS) {
+                T yr = T(0), yi = T(0);
+#pragma unroll
+                for (int k = 0; k < YI_WARPS; k++) {
+                    const T2 v = red[(k * JD + ma) * 32 + lane];
+                    yr += v.x; yi += v.y;
+                }
+                const T2 uu = Us[(idxu_block(j) + (j + 1) * mb + ma) * 32 + lane];
+                const double wgt = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
+                e += wgt * ((double)uu.x * (double)yr + (double)uu.y * (double)yi);
+                if (atom < natoms) yout[yh_block(j) + (j + 1) * mb + ma] = T2{yr, yi};
+            }
+            __syncthreads();
+        }
         ered[w * 32 + lane] = e;
         __syncthreads();
         if (w == 0 && atom < natoms) {

@@ -7,10 +7,14 @@
 #include <stdarg.h>
 #include <string.h>
 #include <mutex>
+#include <atomic>
 
 namespace mdp {
 
 static thread_local char g_err[1024] = "";
+static std::atomic<long long> g_launches{0};
+void count_launches(long n) { g_launches += n; }
+long long launch_count() { return g_launches.load(); }
 
 void set_error(const char *fmt, ...)
 {
@@ -149,6 +153,7 @@ int exclusive_scan(const int *in, int *out, long n, int *tmp, cudaStream_t s)
     k_scan_local<<<(unsigned)nb, SCAN_T, 0, s>>>(in, out, n, tmp);
     k_scan_top<<<1, SCAN_T, 0, s>>>(tmp, (int)nb, out + n);
     k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, tmp);
+    count_launches(3);
     MDP_CUDA_TRY(cudaGetLastError());
     return 0;
 }

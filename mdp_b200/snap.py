@@ -119,6 +119,17 @@ class SnapMD:
                                                e.ctypes.data), "mdp_md_get_state")
         return x, v, f, e
 
+    def upload(self, x_ptr: int, v_ptr: int):
+        """Async H2D of positions/velocities (AoS, host pointers) on the engine stream."""
+        _lib.check(_lib.lib().mdp_md_upload(self._h, C.c_void_p(x_ptr), C.c_void_p(v_ptr)), "mdp_md_upload")
+
+    def download(self, f_ptr: int, e_ptr: int):
+        """Async D2H of forces (AoS) and per-atom energies on the engine stream."""
+        _lib.check(_lib.lib().mdp_md_download(self._h, C.c_void_p(f_ptr), C.c_void_p(e_ptr)), "mdp_md_download")
+
+    def sync(self):
+        _lib.check(_lib.lib().mdp_md_sync(self._h), "mdp_md_sync")
+
     def thermo(self) -> np.ndarray:
         out = np.zeros(5)
         _lib.check(_lib.lib().mdp_md_thermo(self._h, out), "mdp_md_thermo")
@@ -143,6 +154,10 @@ class SnapMD:
     @property
     def stream(self) -> int:
         return int(_lib.lib().mdp_md_stream(self._h) or 0)
+
+
+def launch_count() -> int:
+    return int(_lib.lib().mdp_launch_count())
 
 
 def probe_fma_peak(device: int = 0) -> tuple[float, float]:
