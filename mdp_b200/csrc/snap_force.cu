@@ -128,46 +128,59 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
     m.yd.e0 = e0;
     m.yf.e0 = e0;
 
-    // Y-kernel schedule: units (j, mb) in a fixed order shared by all warps; the
-    // couplings of each unit are spread over the warps longest-first
-    int nu = 0;
-    for (int j = tj; j >= 0; j--)
-        for (int mb = 0; 2 * mb <= j; mb++) {
-            if (nu >= YI_MAXUNITS) { set_error("Y schedule overflow"); return -1; }
-            struct Cp { int c; long cost; };
-            std::vector<Cp> cps;
-            int c = 0;
-            for (int j1 = 0; j1 <= tj; j1++)
-                for (int j2 = 0; j2 <= j1; j2++) {
-                    if (!coupling_ok(j1, j2, j)) continue;
-                    int mb1min = std::max(0, (2 * mb - j - j2 + j1) / 2);
-                    int nbb = std::min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
-                    long cost = 0;
-                    for (int ma = 0; ma <= j; ma++) {
-                        int ma1min = std::max(0, (2 * ma - j - j2 + j1) / 2);
-                        int na = std::min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
-                        cost += (long)na * nbb;
+    // Y-kernel warp assignment per output layer j: rows mb get warps in
+    // proportion to their cost (sum over couplings of items x terms per item);
+    // a row with k warps is split by row-pair index ib modulo k
+    auto assign = [&](int nw, unsigned char (*lmb)[YI_MAXW], unsigned char (*lo)[YI_MAXW],
+                      unsigned char (*lst)[YI_MAXW]) {
+        for (int j = 0; j < JD; j++)
+            for (int w = 0; w < YI_MAXW; w++) { lmb[j][w] = 255; lo[j][w] = 0; lst[j][w] = 1; }
+        for (int j = 0; j <= tj; j++) {
+            const int R = j / 2 + 1;
+            std::vector<double> cost(R, 0.0);
+            for (int mb = 0; mb < R; mb++)
+                for (int j1 = 0; j1 <= tj; j1++)
+                    for (int j2 = 0; j2 <= j1; j2++) {
+                        if (!coupling_ok(j1, j2, j)) continue;
+                        int terms = 0;
+                        for (int ma = 0; ma <= j; ma++) {
+                            int ma1min = std::max(0, (2 * ma - j - j2 + j1) / 2);
+                            terms += std::min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
+                        }
+                        cost[mb] += (double)nb_of(j1, j2, j, mb) * (terms + j1 + j2 + 2);
                     }
-                    cps.push_back({c, cost + 2L * (j1 + j2 + 2) * nbb});
-                    c++;
-                }
-            if (c > 32) { set_error("more than 32 couplings for j=%d", j); return -1; }
-            std::sort(cps.begin(), cps.end(), [](const Cp &x, const Cp &y) { return x.cost > y.cost; });
-            long load[YI_WARPS] = {0};
-            unsigned mask[YI_WARPS] = {0};
-            for (auto &cp : cps) {
-                int w = 0;
-                for (int k = 1; k < YI_WARPS; k++)
-                    if (load[k] < load[w]) w = k;
-                mask[w] |= 1u << cp.c;
-                load[w] += cp.cost;
+            std::vector<int> nw_row(R, 1);
+            int used = std::min(R, nw);
+            if (R > nw) return -1;
+            while (used < nw) {
+                int best = 0;
+                for (int r = 1; r < R; r++)
+                    if (cost[r] / nw_row[r] > cost[best] / nw_row[best]) best = r;
+                // splitting a row beyond its largest item count buys nothing
+                int maxnb = 0;
+                for (int j1 = 0; j1 <= tj; j1++)
+                    for (int j2 = 0; j2 <= j1; j2++)
+                        if (coupling_ok(j1, j2, j)) maxnb = std::max(maxnb, nb_of(j1, j2, j, best));
+                if (nw_row[best] >= maxnb) break;
+                nw_row[best]++;
+                used++;
             }
-            m.yd.unit_j[nu] = m.yf.unit_j[nu] = (unsigned char)j;
-            m.yd.unit_mb[nu] = m.yf.unit_mb[nu] = (unsigned char)mb;
-            for (int w = 0; w < YI_WARPS; w++) m.yd.unit_mask[nu][w] = m.yf.unit_mask[nu][w] = mask[w];
-            nu++;
+            int w = 0;
+            for (int r = 0; r < R; r++)
+                for (int k = 0; k < nw_row[r]; k++, w++) {
+                    lmb[j][w] = (unsigned char)r;
+                    lo[j][w] = (unsigned char)k;
+                    lst[j][w] = (unsigned char)nw_row[r];
+                }
         }
-    m.yd.nunits = m.yf.nunits = nu;
+        return 0;
+    };
+    if (assign(YiWarps<double>::n, m.yd.lay_mb, m.yd.lay_o, m.yd.lay_st) ||
+        assign(YiWarps<float>::n, m.yf.lay_mb, m.yf.lay_o, m.yf.lay_st)) {
+        set_error("Y-kernel warp assignment failed");
+        return -1;
+    }
+
     return 0;
 }
 
@@ -207,7 +220,7 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (fp.pcount.ensure(sizeof(int) * (size_t)inum) || fp.poff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
         fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
         fp.rslot.ensure(sizeof(double4) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)inum * nm) ||
-        fp.Ut.ensure(tsz * (size_t)ntiles * m.nu * 32) || fp.Y.ensure(tsz * (size_t)inum * m.nyh) ||
+        fp.Ut.ensure(tsz * (size_t)ntiles * m.nu * 32) || fp.Y.ensure(tsz * (size_t)ntiles * 32 * m.nyh) ||
         fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(inum)))
         return -1;
     if (fp.timing && !fp.ev[0])

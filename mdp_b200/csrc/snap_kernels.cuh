@@ -24,23 +24,22 @@ struct SnapGeom {
     int switchflag;
 };
 
-// Y-kernel schedule.  A unit is one output row (j, mb) of Y for the tile's 32
-// atoms; every warp of the CTA works on the same unit at the same time, each on
-// its own subset of the (j1, j2) couplings (bit c of unit_mask[u][w] selects the
-// c-th coupling of j in enumeration order), so the code the warps execute at
-// any moment is a few kilobytes and stays in the instruction cache.
-constexpr int YI_WARPS = 8;
-constexpr int YI_MAXUNITS = 32;
-
+// Y-kernel parameters.  Work is organised coupling by coupling: for each
+// (j1, j2, j) triple, the items (mb, ib) -- one Clebsch-Gordan row product each,
+// all the same code and cost -- are spread round-robin over the CTA's warps, so
+// every warp executes the same few kilobytes of code at the same time.  Lanes
+// are the 32 atoms of a tile.
+constexpr int YI_MAXW = 16;
 template <typename T>
 struct YParams {
     T betaY[NTRI];          // beta' of each coupling triple (bnorm 1/(j+1) folded in)
     double e0;              // beta0 - sum_k beta_k bzero_k
-    int nunits;
-    unsigned char unit_j[YI_MAXUNITS];
-    unsigned char unit_mb[YI_MAXUNITS];
-    unsigned int unit_mask[YI_MAXUNITS][YI_WARPS];
+    // per output layer j and warp w: the row mb the warp accumulates (255: idle)
+    // and the residue / stride of the row-pair index ib it takes in every coupling
+    unsigned char lay_mb[JD][YI_MAXW], lay_o[JD][YI_MAXW], lay_st[JD][YI_MAXW];
 };
+template <typename T> struct YiWarps { static constexpr int n = 8; };
+template <> struct YiWarps<float> { static constexpr int n = 16; };
 
 __host__ __device__ constexpr bool coupling_ok(int j1, int j2, int j)
 {
@@ -234,10 +233,24 @@ k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int na
 // k_snap_yi
 // ---------------------------------------------------------------------------
 
-// accumulate s*Z_{J1 J2 J}(ma, mb) for ma = 0..J into yr/yi (s = beta')
+// C++ truncating division as the reference's index formulas use it
+__host__ __device__ constexpr int nb_of(int j1, int j2, int j, int mb)
+{
+    return cmin(j1, (2 * mb - j + j2 + j1) / 2) - cmax(0, (2 * mb - j - j2 + j1) / 2) + 1;
+}
+__host__ __device__ constexpr int items_of(int j1, int j2, int j)
+{
+    int n = 0;
+    for (int mb = 0; 2 * mb <= j; mb++) n += nb_of(j1, j2, j, mb);
+    return n;
+}
+
+// Row mb of beta' Z_{J1 J2 J}, restricted to the row pairs ib = o, o+st, ...,
+// accumulated into yr/yi (registers).
 template <typename T, int J1, int J2, int J>
-__device__ __forceinline__ void zrow_acc(const int mb, const typename cplx<T>::type *__restrict__ Us,
-                                         const int lane, const T beta, T (&yr)[JD], T (&yi)[JD])
+__device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
+                                       const typename cplx<T>::type *__restrict__ Us, const int lane, const T beta,
+                                       T (&yr)[JD], T (&yi)[JD])
 {
     typedef typename cplx<T>::type T2;
     constexpr int N1 = J1 + 1, N2 = J2 + 1;
@@ -245,7 +258,7 @@ __device__ __forceinline__ void zrow_acc(const int mb, const typename cplx<T>::t
     const int mb1min = max(0, (2 * mb - J - J2 + J1) / 2);
     const int mb2max = (2 * mb - J - (2 * mb1min - J1) + J2) / 2;
     const int nb = min(J1, (2 * mb - J + J2 + J1) / 2) - mb1min + 1;
-    for (int ib = 0; ib < nb; ib++) {
+    for (int ib = o; ib < nb; ib += st) {
         const int mb1 = mb1min + ib, mb2 = mb2max - ib;
         const T s = beta * cgc<T>(CGB + mb1 * N2 + mb2);
         const T2 *r1 = Us + (idxu_block(J1) + N1 * mb1) * 32 + lane;
@@ -272,50 +285,71 @@ __device__ __forceinline__ void zrow_acc(const int mb, const typename cplx<T>::t
     }
 }
 
-template <typename T, int TJ, int J, int J1, int J2, int C>
-__device__ __forceinline__ void y_couplings(const int mb, const unsigned mask,
-                                            const typename cplx<T>::type *__restrict__ Us, const int lane,
-                                            const YParams<T> &P, T (&yr)[JD], T (&yi)[JD])
+// all couplings of output layer J, in enumeration order (every warp walks the
+// same sequence, so the code in flight is one coupling's)
+template <typename T, int TJ, int J, int J1, int J2>
+__device__ __forceinline__ void z_layer(const int mb, const int o, const int st,
+                                        const typename cplx<T>::type *__restrict__ Us, const int lane,
+                                        const YParams<T> &P, T (&yr)[JD], T (&yi)[JD])
 {
     if constexpr (J1 <= TJ) {
         if constexpr (J2 <= J1) {
-            if constexpr (coupling_ok(J1, J2, J)) {
-                if (mask & (1u << C)) zrow_acc<T, J1, J2, J>(mb, Us, lane, P.betaY[tri_index(J1, J2, J)], yr, yi);
-                y_couplings<T, TJ, J, J1, J2 + 1, C + 1>(mb, mask, Us, lane, P, yr, yi);
-            } else {
-                y_couplings<T, TJ, J, J1, J2 + 1, C>(mb, mask, Us, lane, P, yr, yi);
-            }
+            if constexpr (coupling_ok(J1, J2, J))
+                z_rows<T, J1, J2, J>(mb, o, st, Us, lane, P.betaY[tri_index(J1, J2, J)], yr, yi);
+            z_layer<T, TJ, J, J1, J2 + 1>(mb, o, st, Us, lane, P, yr, yi);
         } else {
-            y_couplings<T, TJ, J, J1 + 1, 0, C>(mb, mask, Us, lane, P, yr, yi);
+            z_layer<T, TJ, J, J1 + 1, 0>(mb, o, st, Us, lane, P, yr, yi);
         }
     }
 }
 
-// this warp's share of output row Y_J(., mb), written to red[ma][lane]
-template <typename T, int TJ, int J>
-__device__ __forceinline__ void y_unit(const int mb, const unsigned mask, const typename cplx<T>::type *__restrict__ Us,
-                                       const int lane, const YParams<T> &P, typename cplx<T>::type *__restrict__ red)
+// layer J: each warp builds its partial row, the partials are summed per row,
+// written out (tiled) and folded into the energy identity
+template <typename T, int TJ, int NW, int J>
+__device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict__ Us,
+                                        typename cplx<T>::type *__restrict__ red,
+                                        typename cplx<T>::type *__restrict__ dst, const int lane, const int w,
+                                        const YParams<T> &P, double &e)
 {
     typedef typename cplx<T>::type T2;
-    T yr[JD], yi[JD];
+    const int mb = P.lay_mb[J][w];
+    if (mb != 255) {
+        T yr[JD], yi[JD];
 #pragma unroll
-    for (int ma = 0; ma < JD; ma++) { yr[ma] = T(0); yi[ma] = T(0); }
-    y_couplings<T, TJ, J, 0, 0, 0>(mb, mask, Us, lane, P, yr, yi);
+        for (int ma = 0; ma < JD; ma++) { yr[ma] = T(0); yi[ma] = T(0); }
+        z_layer<T, TJ, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w], Us, lane, P, yr, yi);
 #pragma unroll
-    for (int ma = 0; ma <= J; ma++) red[ma * 32 + lane] = T2{yr[ma], yi[ma]};
+        for (int ma = 0; ma <= J; ma++) red[(w * JD + ma) * 32 + lane] = T2{yr[ma], yi[ma]};
+    }
+    __syncthreads();
+    constexpr int NE = (J / 2 + 1) * (J + 1);
+    for (int k = w; k < NE; k += NW) {
+        const int rmb = k / (J + 1), ma = k - rmb * (J + 1);
+        if (2 * rmb == J && ma > rmb) continue;   // right of a middle row's centre: unused
+        T yr = T(0), yi = T(0);
+#pragma unroll
+        for (int v = 0; v < NW; v++)
+            if (P.lay_mb[J][v] == rmb) {
+                const T2 t = red[(v * JD + ma) * 32 + lane];
+                yr += t.x; yi += t.y;
+            }
+        const T2 u = Us[(idxu_block(J) + k) * 32 + lane];
+        const double wgt = (2 * rmb < J) ? 1.0 : (ma < rmb ? 1.0 : 0.5);
+        e += wgt * ((double)u.x * (double)yr + (double)u.y * (double)yi);
+        dst[(yh_block(J) + k) * 32 + lane] = T2{yr, yi};
+    }
+    __syncthreads();
 }
 
-template <typename T, int TJ>
-__device__ __forceinline__ void y_dispatch(const int j, const int mb, const unsigned mask,
-                                           const typename cplx<T>::type *__restrict__ Us, const int lane,
-                                           const YParams<T> &P, typename cplx<T>::type *__restrict__ red)
+template <typename T, int TJ, int NW, int J>
+__device__ __forceinline__ void y_all(const typename cplx<T>::type *__restrict__ Us,
+                                      typename cplx<T>::type *__restrict__ red,
+                                      typename cplx<T>::type *__restrict__ dst, const int lane, const int w,
+                                      const YParams<T> &P, double &e)
 {
-    switch (j) {
-#define MDP_YCASE(JJ) \
-    case JJ: if constexpr (JJ <= TJ) y_unit<T, TJ, JJ>(mb, mask, Us, lane, P, red); break;
-        MDP_YCASE(0) MDP_YCASE(1) MDP_YCASE(2) MDP_YCASE(3) MDP_YCASE(4)
-        MDP_YCASE(5) MDP_YCASE(6) MDP_YCASE(7) MDP_YCASE(8)
-#undef MDP_YCASE
+    if constexpr (J >= 0) {
+        y_layer<T, TJ, NW, J>(Us, red, dst, lane, w, P, e);
+        y_all<T, TJ, NW, J - 1>(Us, red, dst, lane, w, P, e);
     }
 }
 
@@ -323,55 +357,38 @@ template <typename T, int TJ>
 constexpr size_t yi_smem_bytes()
 {
     return (size_t)idxu_count(TJ) * 32 * sizeof(typename cplx<T>::type) +
-           (size_t)YI_WARPS * JD * 32 * sizeof(typename cplx<T>::type) + YI_WARPS * 32 * sizeof(double);
+           (size_t)YiWarps<T>::n * JD * 32 * sizeof(typename cplx<T>::type) + YiWarps<T>::n * 32 * sizeof(double);
 }
 
+// Output Y in 32-atom tiles: Y[tile][k][lane], k = half-plane index.
 template <typename T, int TJ>
-__global__ void __launch_bounds__(YI_WARPS * 32, 1)
+__global__ void __launch_bounds__(YiWarps<T>::n * 32, 1)
 k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __grid_constant__ YParams<T> P,
           typename cplx<T>::type *__restrict__ Y, double *__restrict__ eatom)
 {
     typedef typename cplx<T>::type T2;
+    constexpr int NW = YiWarps<T>::n;
     constexpr int NU = idxu_count(TJ);
     constexpr int NYH = yh_count(TJ);
     extern __shared__ __align__(16) unsigned char smraw[];
     T2 *Us = reinterpret_cast<T2 *>(smraw);
-    T2 *red = Us + NU * 32;                                   // [warp][ma][lane]
-    double *ered = reinterpret_cast<double *>(red + YI_WARPS * JD * 32);
+    T2 *red = Us + NU * 32;                                // [warp][ma][lane]
+    double *ered = reinterpret_cast<double *>(red + NW * JD * 32);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int ntiles = (natoms + 31) >> 5;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const T2 *src = Ut + (size_t)tile * NU * 32;
-        for (int k = threadIdx.x; k < NU * 32; k += YI_WARPS * 32) Us[k] = src[k];
+        for (int k = threadIdx.x; k < NU * 32; k += NW * 32) Us[k] = src[k];
         __syncthreads();
-        const int atom = tile * 32 + lane;
-        T2 *yout = Y + (size_t)atom * NYH;
         double e = 0.0;
-        for (int u = 0; u < P.nunits; u++) {
-            const int j = P.unit_j[u], mb = P.unit_mb[u];
-            y_dispatch<T, TJ>(j, mb, P.unit_mask[u][w], Us, lane, P, red + w * JD * 32);
-            __syncthreads();
-            // reduce the warps' partial rows; warp w finalises entries ma = w, w+8
-            for (int ma = w; ma <= j; ma += YI_WARPS) {
-                T yr = T(0), yi = T(0);
-#pragma unroll
-                for (int k = 0; k < YI_WARPS; k++) {
-                    const T2 v = red[(k * JD + ma) * 32 + lane];
-                    yr += v.x; yi += v.y;
-                }
-                const T2 uu = Us[(idxu_block(j) + (j + 1) * mb + ma) * 32 + lane];
-                const double wgt = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
-                e += wgt * ((double)uu.x * (double)yr + (double)uu.y * (double)yi);
-                if (atom < natoms) yout[yh_block(j) + (j + 1) * mb + ma] = T2{yr, yi};
-            }
-            __syncthreads();
-        }
+        y_all<T, TJ, NW, TJ>(Us, red, Y + (size_t)tile * NYH * 32, lane, w, P, e);
         ered[w * 32 + lane] = e;
         __syncthreads();
+        const int atom = tile * 32 + lane;
         if (w == 0 && atom < natoms) {
             double s = 0.0;
 #pragma unroll
-            for (int k = 0; k < YI_WARPS; k++) s += ered[k * 32 + lane];
+            for (int k = 0; k < NW; k++) s += ered[k * 32 + lane];
             eatom[atom] = P.e0 + (2.0 / 3.0) * s;
         }
         __syncthreads();
@@ -498,14 +515,14 @@ __device__ __forceinline__ void fi_layer(FiRow<T, TJ, ND> &st, const FiGeo<T, ND
         }
     }
     // contract this row with Y (half plane; centre of a middle row at 1/2)
-    const T2 *yrow = Yi + yh_block(J) + (J + 1) * MB;
+    const T2 *yrow = Yi + (yh_block(J) + (J + 1) * MB) * 32;
     constexpr int MAMAX = (2 * MB == J) ? MB : J;
     T s0 = T(0), sk[ND];
 #pragma unroll
     for (int k = 0; k < ND; k++) sk[k] = T(0);
 #pragma unroll
     for (int ma = 0; ma <= MAMAX; ma++) {
-        T2 y = yrow[ma];
+        T2 y = yrow[ma * 32];
         if (2 * MB == J && ma == MB) { y.x *= T(0.5); y.y *= T(0.5); }
         if constexpr (K0 == 0) s0 += st.pr[ma] * y.x + st.pi[ma] * y.y;
 #pragma unroll
@@ -582,11 +599,11 @@ __device__ __forceinline__ void fi_pair(const int p, const double4 *__restrict__
     T dar[3], dai[3], dbr[3], dbi[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) { dar[k] = (T)g.dar[k]; dai[k] = (T)g.dai[k]; dbr[k] = (T)g.dbr[k]; dbi[k] = (T)g.dbi[k]; }
-    const T2 *Yi = Y + (size_t)inf.x * NYH;
+    const T2 *Yi = Y + (size_t)(inf.x >> 5) * NYH * 32 + (inf.x & 31);   // tiled: element k at Yi[k*32]
 
     // A0 = sum w Re(Y* U), Ak = sum w Re(Y* dU/dx_k); dE/dx_k = 2(dsfac u_k A0 + sfac Ak)
     Acc A0, A[3];
-    A0.init((T)(0.5 * (double)Yi[0].x));
+    A0.init((T)(0.5 * (double)Yi[0].x));   // j = 0 element
 #pragma unroll
     for (int k = 0; k < 3; k++) A[k].init(T(0));
     constexpr int N1 = FiSplit<T, TJ>::first;
