@@ -333,7 +333,7 @@ __global__ void k_pair_emit(const double4 *__restrict__ rslot, const int *__rest
         const double4 r = rslot[(size_t)i * nm + l];
         if (r.w != 0.0) {
             prij[p] = r;
-            pinfo[p] = make_int2(i, l);
+            pinfo[p] = make_int2(i, (int)((size_t)i * nm + l));
             p++;
         }
     }

@@ -24,11 +24,13 @@ struct SnapGeom {
     int switchflag;
 };
 
-// Y-kernel parameters.  Work is organised coupling by coupling: for each
-// (j1, j2, j) triple, the items (mb, ib) -- one Clebsch-Gordan row product each,
-// all the same code and cost -- are spread round-robin over the CTA's warps, so
-// every warp executes the same few kilobytes of code at the same time.  Lanes
-// are the 32 atoms of a tile.
+// Y-kernel parameters.  Lanes are the 32 atoms of a tile.  Output layers j are
+// processed one after another by the whole CTA; within a layer every warp walks
+// the same sequence of (j1, j2) couplings, so the code in flight is one
+// coupling's few kilobytes and stays in the instruction cache.  Each warp owns
+// one output row mb of the layer and a residue class of the row-pair index ib,
+// accumulates its share of that row in registers across all couplings, and the
+// warps' partial rows are summed once per layer through shared memory.
 constexpr int YI_MAXW = 16;
 template <typename T>
 struct YParams {
@@ -160,10 +162,13 @@ __device__ __forceinline__ void u_rows(const T ar, const T ai, const T br, const
 // ---------------------------------------------------------------------------
 constexpr int UI_WARPS = 4;
 
-template <typename T, int TJ>
+// REF = true: no wself/mirror; the computed rows are added into the reference's
+// layout Ur/Ui[k * natoms + atom] (cpuSnapComputeUi semantics, cpuSnap4.cpp:11-187)
+template <typename T, int TJ, bool REF = false>
 __global__ void __launch_bounds__(UI_WARPS * 32)
 k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int natoms, SnapGeom gp,
-          typename cplx<T>::type *__restrict__ Ut)
+          typename cplx<T>::type *__restrict__ Ut, double *__restrict__ Uref_r = nullptr,
+          double *__restrict__ Uref_i = nullptr)
 {
     typedef typename cplx<T>::type T2;
     constexpr int NU = idxu_count(TJ);
@@ -207,6 +212,19 @@ k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int na
         for (int o = 16; o > 0; o >>= 1) ssum += __shfl_xor_sync(0xffffffffu, ssum, o);
         if (lane == 0) acc[0].x += ssum;
         __syncwarp();
+        if constexpr (REF) {
+            for (int k = lane; k < NU; k += 32) {
+                int j = 0;
+                while (idxu_block(j + 1) <= k) j++;
+                const int mb = (k - idxu_block(j)) / (j + 1);
+                if (2 * mb <= j) {
+                    Uref_r[(size_t)k * natoms + i] += (double)acc[k].x;
+                    Uref_i[(size_t)k * natoms + i] += (double)acc[k].y;
+                }
+            }
+            __syncwarp();
+            continue;
+        }
         // wself = 1 on the diagonal of the computed half (cpuAddWself2Ui)
         for (int j = lane; j <= TJ; j += 32)
             for (int m = 0; 2 * m <= j; m++) acc[idxu_block(j) + (j + 1) * m + m].x += T(1);
@@ -325,7 +343,6 @@ __device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict
     constexpr int NE = (J / 2 + 1) * (J + 1);
     for (int k = w; k < NE; k += NW) {
         const int rmb = k / (J + 1), ma = k - rmb * (J + 1);
-        if (2 * rmb == J && ma > rmb) continue;   // right of a middle row's centre: unused
         T yr = T(0), yi = T(0);
 #pragma unroll
         for (int v = 0; v < NW; v++)
@@ -334,7 +351,7 @@ __device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict
                 yr += t.x; yi += t.y;
             }
         const T2 u = Us[(idxu_block(J) + k) * 32 + lane];
-        const double wgt = (2 * rmb < J) ? 1.0 : (ma < rmb ? 1.0 : 0.5);
+        const double wgt = (2 * rmb < J) ? 1.0 : (ma < rmb ? 1.0 : (ma == rmb ? 0.5 : 0.0));
         e += wgt * ((double)u.x * (double)yr + (double)u.y * (double)yi);
         dst[(yh_block(J) + k) * 32 + lane] = T2{yr, yi};
     }
@@ -396,7 +413,77 @@ k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __gri
 }
 
 // ---------------------------------------------------------------------------
-// k_snap_fi: one thread per pair.  dEslot[i*nm + slot] = dE/d(r_j - r_i).
+// k_snap_bi: per-atom bispectrum B_k = 2 sum_half w Re(U_j* Z_{j1 j2 j}) (- bzero)
+// for the triples j >= j1 (cpuSnap4.cpp:427-592, cpuSnapComputeBi).  Tiles of 32
+// atoms, warps take triples round-robin.  Output bout[k * bstride + atom].
+// ---------------------------------------------------------------------------
+constexpr int BI_WARPS = 8;
+
+template <typename T, int TJ, int J1, int J2, int J, int C>
+__device__ __forceinline__ void b_triples(const typename cplx<T>::type *__restrict__ Us, const int lane, const int w,
+                                          const int atom, const int natoms, const int bnorm, const int bzero,
+                                          double *__restrict__ bout, const long bstride)
+{
+    typedef typename cplx<T>::type T2;
+    if constexpr (J1 <= TJ) {
+        if constexpr (J2 <= J1) {
+            if constexpr (J <= cmin(TJ, J1 + J2)) {
+                if constexpr (J >= J1) {
+                    if (C % BI_WARPS == w) {
+                        double sum = 0.0;
+                        for (int mb = 0; 2 * mb <= J; mb++) {
+                            T zr[JD], zi[JD];
+#pragma unroll
+                            for (int ma = 0; ma < JD; ma++) { zr[ma] = T(0); zi[ma] = T(0); }
+                            z_rows<T, J1, J2, J>(mb, 0, 1, Us, lane, T(1), zr, zi);
+                            const T2 *urow = Us + (idxu_block(J) + (J + 1) * mb) * 32 + lane;
+#pragma unroll
+                            for (int ma = 0; ma <= J; ma++) {
+                                const double wgt = (2 * mb < J) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
+                                const T2 u = urow[ma * 32];
+                                sum += wgt * ((double)u.x * (double)zr[ma] + (double)u.y * (double)zi[ma]);
+                            }
+                        }
+                        double b = 2.0 * sum;
+                        if (bnorm) b /= (J + 1);
+                        if (bzero) b -= bnorm ? 1.0 : (double)(J + 1);
+                        if (atom < natoms) bout[(long)C * bstride + atom] = b;
+                    }
+                    b_triples<T, TJ, J1, J2, J + 2, C + 1>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+                } else {
+                    b_triples<T, TJ, J1, J2, J + 2, C>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+                }
+            } else {
+                b_triples<T, TJ, J1, J2 + 1, J1 - J2 - 1, C>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+            }
+        } else {
+            b_triples<T, TJ, J1 + 1, 0, J1 + 1, C>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+        }
+    }
+}
+
+template <typename T, int TJ>
+__global__ void __launch_bounds__(BI_WARPS * 32, 1)
+k_snap_bi(const typename cplx<T>::type *__restrict__ Ut, int natoms, int bnorm, int bzero,
+          double *__restrict__ bout, long bstride)
+{
+    typedef typename cplx<T>::type T2;
+    constexpr int NU = idxu_count(TJ);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T2 *Us = reinterpret_cast<T2 *>(smraw);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ntiles = (natoms + 31) >> 5;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const T2 *src = Ut + (size_t)tile * NU * 32;
+        for (int k = threadIdx.x; k < NU * 32; k += BI_WARPS * 32) Us[k] = src[k];
+        __syncthreads();
+        b_triples<T, TJ, 0, 0, 0, 0>(Us, lane, w, tile * 32 + lane, natoms, bnorm, bzero, bout, bstride);
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_snap_fi: one thread per pair.  dEslot[pinfo.y] = dE/d(r_j - r_i).
 // ---------------------------------------------------------------------------
 template <typename T>
 struct FAcc {   // plain accumulator
@@ -616,7 +703,7 @@ __device__ __forceinline__ void fi_pair(const int p, const double4 *__restrict__
     out.y = 2.0 * (g.dsfac * g.u[1] * a0 + g.sfac * A[1].val());
     out.z = 2.0 * (g.dsfac * g.u[2] * a0 + g.sfac * A[2].val());
     out.w = 0.0;
-    dEslot[(size_t)inf.x * nm + inf.y] = out;
+    dEslot[inf.y] = out;   // inf.y: global output slot
 }
 
 // grid-stride over the pairs; the pair count is read on the device (the

@@ -1,0 +1,91 @@
+"""Drives a cpuSnap.h-style library through the call sequence of MDP's
+snappotential (src/Julia/Potential/snapcpp.jl:323-426): pair list, pairs, Ui,
+wself, Ei, Yi, Fi, plus Bi.  Used to run the reference library and ours on
+identical inputs."""
+import ctypes as C
+
+import numpy as np
+
+D = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+I = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def bind(path):
+    L = C.CDLL(path)
+    L.cpuInitSna.argtypes = [D, D, D, I, I, I, I, I, I, I, C.c_int]
+    L.cpuNeighPairList.argtypes = [I, I, D, D, I, I, I, I, I, C.c_int, C.c_int, C.c_int]
+    L.cpuNeighPairs.argtypes = [D, D, I, I, I, I, I, I, I, I, I, I, C.c_int, C.c_int]
+    L.cpuSnapComputeUi.argtypes = [D, D, D, D, D, D, C.c_double, C.c_double, C.c_double, I, I, I, I] + [C.c_int] * 6
+    L.cpuAddWself2Ui.argtypes = [D, D, C.c_double, I, I, I] + [C.c_int] * 6
+    L.cpuSnapComputeEi.argtypes = [D, D, D, D, D, D, I, I, I, I, I, I] + [C.c_int] * 10
+    L.cpuSnapComputeBi.argtypes = [D, D, D, D, D, I, I, I, I] + [C.c_int] * 9
+    L.cpuSnapComputeYi.argtypes = [D, D, D, D, D, D, I, I, I, I, I, I] + [C.c_int] * 9
+    L.cpuSnapComputeFi.argtypes = [D, D, D, D, D, D, D, D, C.c_double, C.c_double, C.c_double, I, I, I, I, I, I] + \
+        [C.c_int] * 7
+    for f in ("idxbcount", "idxcgcount", "idxucount", "idxzcount"):
+        getattr(L, f).argtypes = [C.c_int]
+    return L
+
+
+def tables(L, tj):
+    nb, ncg, nu, nz = L.idxbcount(tj), L.idxcgcount(tj), L.idxucount(tj), L.idxzcount(tj)
+    jd = tj + 1
+    fac = np.ones(168)
+    for k in range(1, 168):
+        fac[k] = fac[k - 1] * k
+    t = dict(rootpq=np.zeros((jd + 1) ** 2), cg=np.zeros(ncg), fac=fac,
+             idx_max=np.zeros(5, dtype=np.int32), idxz=np.zeros(10 * nz, dtype=np.int32),
+             idxz_block=np.zeros(jd ** 3, dtype=np.int32), idxb=np.zeros(3 * nb, dtype=np.int32),
+             idxb_block=np.zeros(jd ** 3, dtype=np.int32), idxu_block=np.zeros(jd, dtype=np.int32),
+             idxcg_block=np.zeros(jd ** 3, dtype=np.int32), nb=nb, nu=nu, nz=nz, ncg=ncg)
+    L.cpuInitSna(t["rootpq"], t["cg"], t["fac"], t["idx_max"], t["idxz"], t["idxz_block"], t["idxb"],
+                 t["idxb_block"], t["idxu_block"], t["idxcg_block"], tj)
+    return t
+
+
+def snap_sequence(L, g, p):
+    """Returns every stage's output for the configuration in golden fixture g."""
+    tj = p.twojmax
+    t = tables(L, tj)
+    x = np.ascontiguousarray(g["xall"]).ravel()
+    n = g["x"].shape[0]
+    nl, nn = g["neighlist"], g["neighnum"]
+    csr = np.zeros(n + 1, dtype=np.int32); csr[1:] = np.cumsum(nn)
+    flat = np.concatenate([nl[i, : nn[i]] for i in range(n)]).astype(np.int32)
+    ilist = np.arange(n, dtype=np.int32)
+    anum = g["xall"].shape[0]
+    atype = np.ones(anum, dtype=np.int32)
+    alist = np.ascontiguousarray(g["alist"], dtype=np.int32)
+    rc = p.rcut
+    rcutsq = np.array([0.0, 0.0, 0.0, rc * rc])
+    pairnum = np.zeros(n, dtype=np.int32)
+    pairlist = np.zeros(flat.size + 1, dtype=np.int32)
+    L.cpuNeighPairList(pairnum, pairlist, x, rcutsq, ilist, flat, csr, atype, alist, n, 3, 1)
+    pns = np.zeros(n + 1, dtype=np.int32); pns[1:] = np.cumsum(pairnum)
+    ij = int(pns[-1])
+    rij = np.zeros(3 * ij); aii = np.zeros(ij, dtype=np.int32); ai = np.zeros(ij, dtype=np.int32)
+    aj = np.zeros(ij, dtype=np.int32); ti = np.zeros(ij, dtype=np.int32); tjv = np.zeros(ij, dtype=np.int32)
+    L.cpuNeighPairs(rij, x, aii, ai, aj, ti, tjv, pairlist, pns, ilist, atype, alist, n, 3)
+    radelem = np.array([0.0, p.radelem]); wjelem = np.array([0.0, p.wjelem]); mp = np.zeros(2, dtype=np.int32)
+    nu = t["nu"]
+    ur = np.zeros(n * nu); ui = np.zeros(n * nu)
+    L.cpuSnapComputeUi(ur, ui, t["rootpq"], rij, wjelem, radelem, p.rmin0, p.rfac0, p.rcutfac, mp, ai, ti, tjv,
+                       tj, nu, n, ij, p.switchflag, 0)
+    u_pairs = (ur.copy(), ui.copy())
+    L.cpuAddWself2Ui(ur, ui, 1.0, t["idxu_block"], atype, mp, p.wselfallflag, 0, nu, 1, tj, n)
+    bzero = np.array([1.0 if p.bnormflag else j + 1.0 for j in range(tj + 1)])
+    coeff = np.ascontiguousarray(p.coeff)
+    e = np.zeros(n)
+    L.cpuSnapComputeEi(e, ur, ui, t["cg"], bzero, coeff, ilist, mp, atype, t["idxb"], t["idxcg_block"],
+                       t["idxu_block"], tj, t["nb"], nu, 1, coeff.size, p.bnormflag, p.bzeroflag, p.wselfallflag, 0, n)
+    b = np.zeros(n * t["nb"])
+    L.cpuSnapComputeBi(b, ur, ui, t["cg"], bzero, t["idxb"], t["idxcg_block"], t["idxu_block"], t["idxz_block"],
+                       tj, t["nb"], nu, t["nz"], 1, p.bnormflag, p.bzeroflag, p.wselfallflag, n)
+    yr = np.zeros(n * nu); yi = np.zeros(n * nu)
+    L.cpuSnapComputeYi(yr, yi, ur, ui, t["cg"], coeff, mp, atype, t["idxz"], t["idxb_block"], t["idxu_block"],
+                       t["idxcg_block"], tj, t["nb"], nu, t["nz"], 1, coeff.size, p.bnormflag, 0, n)
+    f = np.zeros(3 * n); v = np.zeros(6 * n)
+    L.cpuSnapComputeFi(f, v, yr, yi, t["rootpq"], rij, wjelem, radelem, p.rmin0, p.rfac0, p.rcutfac, mp, ai, ai, aj,
+                       ti, tjv, tj, nu, n, n, ij, p.switchflag, 0)
+    return dict(tables=t, pairnum=pairnum, pairlist=pairlist[:ij], rij=rij, aii=aii, ai=ai, aj=aj, u_pairs=u_pairs,
+                u=(ur, ui), eatom=e, blist=b, y=(yr, yi), fatom=f, vatom=v)
