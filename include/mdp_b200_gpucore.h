@@ -62,6 +62,21 @@ void mdp_gpu_neigh_pairs_f64(double *xij, const double *x, int *aii, int *ai, in
                              const int *pairnum, const int *pairlist, const int *pairnumsum, const int *ilist,
                              const int *atomtype, const int *alist, int inum, int jnum, int dim);
 
+/* No counterpart in the reference.  The per-atom bispectrum of
+ * mdp_gpu_snap_compute_bi_f64 for callers that must not allocate device memory
+ * (a host application whose memory pool owns the device, or a loop that cannot
+ * take the implicit synchronisation of cudaMalloc/cudaFree): its 32-atom-tile
+ * scratch is a fixed array inside the library, so the call allocates nothing.
+ * U in MDP's layout [idxu][inum] (device), blist[jjb * inum + ii] (device),
+ * launched on `stream`.  Limits: inum <= 2048 (larger is rejected with an
+ * error), 2J = 4, 6, 8; the array costs 9,338,880 bytes on every GPU that
+ * loads the library.  All calls share the array: calls whose GPU work overlaps
+ * race, so serialise them on one stream.  The first call on a device sets up
+ * the array's address (and the library's constant tables) and should come
+ * before any stream capture.  Returns 0, or -1 with mdp_last_error(). */
+int mdp_gpu_snap_compute_bi_noalloc_f64(double *blist, const double *Utotr, const double *Utoti, int twojmax,
+                                        int bnorm_flag, int bzero_flag, int inum, void *stream);
+
 #ifdef __cplusplus
 }
 
