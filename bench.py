@@ -50,12 +50,35 @@ SKIN = 1.0
 NEIGHMAX = 64
 SAMPLE_CELLS = (20, 20, 20)        # CPU-baseline sample: 16,000 atoms
 
-# algorithmic FLOPs (2J=8), per atom or pair, counted on the reference's
-# minimal algorithm: Z/Y 41,889 complex terms x 11, energy 1,413 x 4,
-# U 154 half-plane elements x 22 per pair, dU/dr 154 x 156 per pair
+
+
+def fr_flops_per_pair(tj):
+    """FLOPs of the reverse-mode dE/dr of one pair (an FMA counts 2).
+
+    Forward row step of layer J: 2 end entries x 8 + (J-1) inner x 18.
+    Adjoint step of layer J: gradient 10 per coupling term (2J of them),
+    parent adjoint 18 per entry (J), weighted Y 2 per entry of layer J-1.
+    Rows recomputed: the seed sweep (layers 2mb, 2mb+1 of columns
+    mb < tj/2) and each column's layers below tj.
+    """
+    def fwd(j):
+        return 16 + 18 * (j - 1)
+    fl = 0
+    for mb in range(tj // 2):                       # seed sweep
+        fl += sum(fwd(j) for j in ((1,) if mb == 0 else (2 * mb, 2 * mb + 1)))
+    for mb in range(tj // 2 + 1):
+        j0 = 1 if mb == 0 else 2 * mb
+        fl += sum(fwd(j) for j in range(j0, tj))     # column recompute
+        fl += sum(10 * 2 * j + 18 * j + 2 * j for j in range(j0, tj + 1))   # adjoint
+    return fl
+
+
+# algorithmic FLOPs (2J=8), per atom or pair: Z/Y 41,889 complex terms x 11
+# and energy 1,413 x 4 (the reference's minimal contraction count), U 154
+# half-plane elements x 22 per pair, dE/dr as implemented (reverse mode)
 FLOP_Y_PER_ATOM = 41889 * 11 + 1413 * 4
 FLOP_U_PER_PAIR = 154 * 22
-FLOP_F_PER_PAIR = 154 * 156
+FLOP_F_PER_PAIR = fr_flops_per_pair(8)
 
 
 def dist_env():

@@ -1,4 +1,4 @@
-// dE/dr stage launchers (k_snap_fi), float.
+// dE/dr stage launchers (k_snap_fr, reverse-mode dE/dr), float.
 #include "engine.h"
 
 #include <algorithm>
@@ -6,22 +6,22 @@
 namespace mdp {
 
 template <typename T, int TJ>
-int launch_fi(const SnapModel &m, ForcePath &fp, int inum, int nm, cudaStream_t s)
+int launch_fi(const SnapModel &m, ForcePath &fp, int inum, int /*nm*/, cudaStream_t s)
 {
     typedef typename cplx<T>::type T2;
     if (tu_ensure_tables()) return -1;
-    const size_t sm = fi_smem_bytes<T, TJ>();
+    if (fp.timing) cudaEventRecord(fp.ev[3], s);
+    const size_t sm = fr_smem_bytes<T, TJ>();
     static int per_sm = 0;
     if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_fi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_fi<T, TJ>, FI_THREADS, sm));
-        if (per_sm < 1) { set_error("k_snap_fi does not fit on an SM"); return -1; }
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_fr<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_fr<T, TJ>, FR_THREADS, sm));
+        if (per_sm < 1) { set_error("k_snap_fr does not fit on an SM"); return -1; }
     }
     const int blocks = num_sms() * per_sm;
-    if (fp.timing) cudaEventRecord(fp.ev[3], s);
-    k_snap_fi<T, TJ><<<blocks, FI_THREADS, sm, s>>>(fp.prij.as<double4>(), fp.pinfo.as<int2>(),
+    k_snap_fr<T, TJ><<<blocks, FR_THREADS, sm, s>>>(fp.prij.as<double4>(), fp.pinfo.as<int2>(),
                                                     fp.poff.as<int>() + inum, m.geom, fp.Y.as<T2>(),
-                                                    fp.dE.as<double4>(), nm);
+                                                    fp.dE.as<double4>());
     return 0;
 }
 

@@ -11,8 +11,9 @@
 //               memory, every (j1,j2,j) row of Z specialised at compile time
 //               so CG coefficients are constant-bank operands and the U rows
 //               it needs are held in registers
-//   k_snap_fi   dE/dr_ij = 2 sum_half w Re(Y* dU/dr)         (:798-1175)
-//               one thread per pair, forward-mode dU recursion
+//   k_snap_fr   dE/dr_ij = 2 sum_half w Re(Y* dU/dr)         (:798-1175)
+//               one thread per pair, reverse-mode (adjoint) differentiation
+//               of the U recursion seeded with Y
 #pragma once
 
 #include "common.cuh"
@@ -483,7 +484,7 @@ k_snap_bi(const typename cplx<T>::type *__restrict__ Ut, int natoms, int bnorm, 
 }
 
 // ---------------------------------------------------------------------------
-// k_snap_fi: one thread per pair.  dEslot[pinfo.y] = dE/d(r_j - r_i).
+// accumulators of the dE/dr kernel's gradient sums
 // ---------------------------------------------------------------------------
 template <typename T>
 struct FAcc {   // plain accumulator
@@ -506,218 +507,304 @@ struct FAccComp {   // compensated (Neumaier) float accumulator
 template <typename T> struct FAccSel { typedef FAcc<T> type; };
 template <> struct FAccSel<float> { typedef FAccComp type; };
 
-constexpr int FI_THREADS = 128;
-template <typename T, int TJ> constexpr size_t fi_smem_bytes() { return sizeof(T) * 8 * (TJ + 1) * FI_THREADS; }
-
-// One forward-mode pass over the U recursion of a pair, carrying the value and
-// ND derivative directions k = K0..K0+ND-1.  The (mb, j) loop nest is written
-// as compile-time recursion so every array index is a constant and the row
-// state stays in registers.  Seed rows of the next mb level are parked in this
-// thread's shared-memory slots qs[c * (TJ+1) * FI_THREADS + ma * FI_THREADS],
-// c = 0,1 (value re/im), 2..1+ND (derivative re), 2+ND..1+2ND (derivative im).
-// A0 (sum w Re(Y* U)) is accumulated by the pass with K0 == 0.
-template <typename T, int TJ, int ND>
-struct FiRow {
-    T pr[TJ + 1], pi[TJ + 1], dr[ND][TJ + 1], di[ND][TJ + 1];
-};
-
-template <typename T, int ND>
-struct FiGeo {
-    T ar, ai, br, bi;
-    T dar[ND], dai[ND], dbr[ND], dbi[ND];
-};
-
-template <typename T, int TJ, int ND, int K0, int MB, int J, typename Acc>
-__device__ __forceinline__ void fi_layer(FiRow<T, TJ, ND> &st, const FiGeo<T, ND> &g,
-                                         const typename cplx<T>::type *__restrict__ Yi, Acc &A0, Acc (&A)[3],
-                                         T *__restrict__ qs)
+// ---------------------------------------------------------------------------
+// k_snap_fr: dE/dr of every pair by reverse-mode (adjoint) differentiation of
+// the U recursion.  One thread per pair; dEslot[pinfo.y] = dE/d(r_j - r_i).
+//
+// With F(a, b) = sum_half w Re(Y* u(a, b)) (the same half-plane sum as the
+// forward-mode kernel), dE/dx_k = 2 (dsfac u_k F + sfac dF/dx_k) and
+// dF/dx_k = grad_(ar,ai,br,bi) F . d(a,b)/dx_k.  Each U row (layer J, column
+// mb) is n[ma] = A_ma conj(a) p[ma] - B_ma conj(b) p[ma-1] of its parent row p
+// (layer J-1), A_ma = rootpq(J-ma, J-mb), B_ma = rootpq(ma, J-mb).  Its
+// adjoint, for an adjoint row l of layer J, is
+//     l'[k] = A_k a l[k] - B_(k+1) b l[k+1]           (parent row's adjoint)
+//     dF/d(ar + i ai) += A_ma conj(l[ma]) p[ma]        (as (re, im) pairs)
+//     dF/d(br + i bi) -= B_ma conj(l[ma]) p[ma-1]
+// and F itself is the real part of the adjoint of the root u_0 = 1.  This is
+// about 5,100 operations per pair at 2J=8 against about 14,000 for carrying
+// the three derivative directions forward through the recursion, which is how
+// cpuSnap4.cpp:798-1175 computes dU/dr.
+//
+// Columns mb depend on each other only through the seed rows (the parent of
+// row (2mb, mb) is the mirror of row (2mb-1, mb-1)), so the pass is:
+//   A. value-only sweep that builds the seed rows S_1..S_(TJ/2) (shared memory)
+//   B. for mb = TJ/2 .. 0: recompute column mb's rows from its seed, keeping
+//      them in registers, then walk back from layer TJ accumulating the
+//      gradient; the adjoint reaching the seed is mirrored into a link that
+//      column mb-1 adds at layer 2mb-1 (stored over the seed's slot).
+// The middle-row mirror of the forward values is exact on |a|^2 + |b|^2 = 1,
+// and d(a,b)/dr stays on that sphere, so the adjoint treats the recursion's
+// own right half as the row.
+// ---------------------------------------------------------------------------
+constexpr int FR_THREADS = 128;
+// per-thread shared memory: seeds/links (2 * sum_mb 2mb values) + 16 geometry values
+template <int TJ> constexpr int fr_seed_vals() { return 2 * (TJ / 2) * (TJ / 2 + 1); }
+template <typename T, int TJ> constexpr size_t fr_smem_bytes()
 {
-    typedef typename cplx<T>::type T2;
-    constexpr int QS = (TJ + 1) * FI_THREADS;
-    const T ar = g.ar, ai = g.ai, br = g.br, bi = g.bi;
-    {   // ma = J
+    return (sizeof(T) * fr_seed_vals<TJ>() + sizeof(double) * 16) * FR_THREADS;
+}
+__host__ __device__ constexpr int fr_seed_off(int mb) { return mb * (mb - 1); }   // complex offset of S_mb
+__host__ __device__ constexpr int fr_row_off(int j) { return j * (j + 1) / 2; }   // stored row j
+
+template <typename T, int TJ>
+struct FrState {
+    T ar, ai, br, bi;
+    T ur[fr_row_off(TJ)], ui[fr_row_off(TJ)];   // parent rows 0..TJ-1 of the current column
+    T lr[TJ + 1], li[TJ + 1];                   // adjoint row
+};
+
+// row J-1 -> row J of column MB, in place (entries 0..J), as u_rows does
+template <typename T, int TJ, int J, int MB>
+__device__ __forceinline__ void fr_fwd(const T ar, const T ai, const T br, const T bi, T (&pr)[TJ + 1],
+                                       T (&pi)[TJ + 1])
+{
+    {
         const T rp = rootpq<T>(J, J - MB);
-        const T wr = st.pr[J - 1], wi = st.pi[J - 1];
-#pragma unroll
-        for (int k = 0; k < ND; k++) {
-            const T xr = st.dr[k][J - 1], xi = st.di[k][J - 1];
-            st.dr[k][J] = -rp * (g.dbr[k] * wr + g.dbi[k] * wi + br * xr + bi * xi);
-            st.di[k][J] = -rp * (g.dbr[k] * wi - g.dbi[k] * wr + br * xi - bi * xr);
-        }
-        st.pr[J] = -rp * (br * wr + bi * wi);
-        st.pi[J] = -rp * (br * wi - bi * wr);
+        const T nr = -rp * (br * pr[J - 1] + bi * pi[J - 1]);
+        const T ni = -rp * (br * pi[J - 1] - bi * pr[J - 1]);
+        pr[J] = nr; pi[J] = ni;
     }
 #pragma unroll
-    for (int ma = J - 1; ma >= 0; ma--) {
-        const T rpa = rootpq<T>(J - ma, J - MB);
-        const T ur = st.pr[ma], ui = st.pi[ma];
-        T nr = rpa * (ar * ur + ai * ui);
-        T ni = rpa * (ar * ui - ai * ur);
-        T ndr[ND], ndi[ND];
-#pragma unroll
-        for (int k = 0; k < ND; k++) {
-            ndr[k] = rpa * (g.dar[k] * ur + g.dai[k] * ui + ar * st.dr[k][ma] + ai * st.di[k][ma]);
-            ndi[k] = rpa * (g.dar[k] * ui - g.dai[k] * ur + ar * st.di[k][ma] - ai * st.dr[k][ma]);
-        }
-        if (ma > 0) {
-            const T rpb = rootpq<T>(ma, J - MB);
-            const T vr = st.pr[ma - 1], vi = st.pi[ma - 1];
-            nr -= rpb * (br * vr + bi * vi);
-            ni -= rpb * (br * vi - bi * vr);
-#pragma unroll
-            for (int k = 0; k < ND; k++) {
-                ndr[k] -= rpb * (g.dbr[k] * vr + g.dbi[k] * vi + br * st.dr[k][ma - 1] + bi * st.di[k][ma - 1]);
-                ndi[k] -= rpb * (g.dbr[k] * vi - g.dbi[k] * vr + br * st.di[k][ma - 1] - bi * st.dr[k][ma - 1]);
-            }
-        }
-        st.pr[ma] = nr; st.pi[ma] = ni;
-#pragma unroll
-        for (int k = 0; k < ND; k++) { st.dr[k][ma] = ndr[k]; st.di[k][ma] = ndi[k]; }
+    for (int ma = J - 1; ma >= 1; ma--) {
+        const T rpa = rootpq<T>(J - ma, J - MB), rpb = rootpq<T>(ma, J - MB);
+        const T nr = rpa * (ar * pr[ma] + ai * pi[ma]) - rpb * (br * pr[ma - 1] + bi * pi[ma - 1]);
+        const T ni = rpa * (ar * pi[ma] - ai * pr[ma]) - rpb * (br * pi[ma - 1] - bi * pr[ma - 1]);
+        pr[ma] = nr; pi[ma] = ni;
+    }
+    {
+        const T rpa = rootpq<T>(J, J - MB);
+        const T nr = rpa * (ar * pr[0] + ai * pi[0]);
+        const T ni = rpa * (ar * pi[0] - ai * pr[0]);
+        pr[0] = nr; pi[0] = ni;
     }
     if constexpr (MB > 0 && J == 2 * MB) {
-        // middle row mirror; the reference leaves the derivative centre as
-        // computed (its two mirror passes cancel, cpuSnap4.cpp:1061-1104)
 #pragma unroll
         for (int ma = 0; ma <= MB; ma++) {
             const T s = (ma & 1) ? T(-1) : T(1);
-            st.pr[MB + ma] = s * st.pr[MB - ma];
-            st.pi[MB + ma] = -s * st.pi[MB - ma];
-            if (ma > 0) {
-#pragma unroll
-                for (int k = 0; k < ND; k++) { st.dr[k][MB + ma] = s * st.dr[k][MB - ma]; st.di[k][MB + ma] = -s * st.di[k][MB - ma]; }
-            }
+            pr[MB + ma] = s * pr[MB - ma];
+            pi[MB + ma] = -s * pi[MB - ma];
         }
     }
-    if constexpr (J == 2 * MB + 1 && 2 * (MB + 1) <= TJ) {
+}
+
+// seed S_(MB+1)[J - ma] = (-1)^(MB+ma) conj(row (J = 2MB+1, MB)[ma])
+template <typename T, int TJ, int MB>
+__device__ __forceinline__ void fr_put_seed(const T (&pr)[TJ + 1], const T (&pi)[TJ + 1], T *__restrict__ qs)
+{
+    constexpr int J = 2 * MB + 1, O = fr_seed_off(MB + 1);
+#pragma unroll
+    for (int ma = 0; ma <= J; ma++) {
+        const T s = ((MB + ma) & 1) ? T(-1) : T(1);
+        qs[(2 * (O + J - ma) + 0) * FR_THREADS] = s * pr[ma];
+        qs[(2 * (O + J - ma) + 1) * FR_THREADS] = -s * pi[ma];
+    }
+}
+
+// phase A: seeds of columns 1..TJ/2
+template <typename T, int TJ, int MB>
+__device__ __forceinline__ void fr_seeds(const T ar, const T ai, const T br, const T bi, T (&pr)[TJ + 1],
+                                         T (&pi)[TJ + 1], T *__restrict__ qs)
+{
+    if constexpr (2 * (MB + 1) <= TJ) {
+        if constexpr (MB == 0) {
+            pr[0] = T(1); pi[0] = T(0);
+            fr_fwd<T, TJ, 1, 0>(ar, ai, br, bi, pr, pi);
+        } else {
+            // pr/pi hold S_MB (entries 0..2MB-1)
+            fr_fwd<T, TJ, 2 * MB, MB>(ar, ai, br, bi, pr, pi);
+            fr_fwd<T, TJ, 2 * MB + 1, MB>(ar, ai, br, bi, pr, pi);
+        }
+        fr_put_seed<T, TJ, MB>(pr, pi, qs);
+        // the next column starts from the seed just written
+        constexpr int J = 2 * MB + 1;
+        T nr[TJ + 1], ni[TJ + 1];
 #pragma unroll
         for (int ma = 0; ma <= J; ma++) {
             const T s = ((MB + ma) & 1) ? T(-1) : T(1);
-            qs[0 * QS + (J - ma) * FI_THREADS] = s * st.pr[ma];
-            qs[1 * QS + (J - ma) * FI_THREADS] = -s * st.pi[ma];
-#pragma unroll
-            for (int k = 0; k < ND; k++) {
-                qs[(2 + k) * QS + (J - ma) * FI_THREADS] = s * st.dr[k][ma];
-                qs[(2 + ND + k) * QS + (J - ma) * FI_THREADS] = -s * st.di[k][ma];
-            }
+            nr[J - ma] = s * pr[ma]; ni[J - ma] = -s * pi[ma];
         }
+#pragma unroll
+        for (int ma = 0; ma <= J; ma++) { pr[ma] = nr[ma]; pi[ma] = ni[ma]; }
+        fr_seeds<T, TJ, MB + 1>(ar, ai, br, bi, pr, pi, qs);
     }
-    // contract this row with Y (half plane; centre of a middle row at 1/2)
+}
+
+// phase B forward: rows J..TJ-1 of column MB from the row J-1 in (pr, pi), stored
+template <typename T, int TJ, int J, int MB>
+__device__ __forceinline__ void fr_col_fwd(FrState<T, TJ> &st, T (&pr)[TJ + 1], T (&pi)[TJ + 1])
+{
+    if constexpr (J < TJ) {
+        fr_fwd<T, TJ, J, MB>(st.ar, st.ai, st.br, st.bi, pr, pi);
+#pragma unroll
+        for (int ma = 0; ma <= J; ma++) { st.ur[fr_row_off(J) + ma] = pr[ma]; st.ui[fr_row_off(J) + ma] = pi[ma]; }
+        fr_col_fwd<T, TJ, J + 1, MB>(st, pr, pi);
+    }
+}
+
+// weighted Y row (J, MB) added into the adjoint row (entries 0..J)
+template <typename T, int TJ, int J, int MB>
+__device__ __forceinline__ void fr_add_y(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi)
+{
+    typedef typename cplx<T>::type T2;
     const T2 *yrow = Yi + (yh_block(J) + (J + 1) * MB) * 32;
     constexpr int MAMAX = (2 * MB == J) ? MB : J;
-    T s0 = T(0), sk[ND];
-#pragma unroll
-    for (int k = 0; k < ND; k++) sk[k] = T(0);
 #pragma unroll
     for (int ma = 0; ma <= MAMAX; ma++) {
         T2 y = yrow[ma * 32];
         if (2 * MB == J && ma == MB) { y.x *= T(0.5); y.y *= T(0.5); }
-        if constexpr (K0 == 0) s0 += st.pr[ma] * y.x + st.pi[ma] * y.y;
-#pragma unroll
-        for (int k = 0; k < ND; k++) sk[k] += st.dr[k][ma] * y.x + st.di[k][ma] * y.y;
-    }
-    if constexpr (K0 == 0) A0.add(s0);
-#pragma unroll
-    for (int k = 0; k < ND; k++) A[K0 + k].add(sk[k]);
-    if constexpr (J < TJ) {
-        asm volatile("" ::: "memory");
-        fi_layer<T, TJ, ND, K0, MB, J + 1>(st, g, Yi, A0, A, qs);
+        st.lr[ma] += y.x; st.li[ma] += y.y;
     }
 }
 
-template <typename T, int TJ, int ND, int K0, int MB, typename Acc>
-__device__ __forceinline__ void fi_rows(FiRow<T, TJ, ND> &st, const FiGeo<T, ND> &g,
-                                        const typename cplx<T>::type *__restrict__ Yi, Acc &A0, Acc (&A)[3],
-                                        T *__restrict__ qs)
+// phase B backward: adjoint row of layer J (column MB) in st.l*; parent row J-1
+template <typename T, int TJ, int J, int MB, typename Acc>
+__device__ __forceinline__ void fr_col_bwd(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi,
+                                           Acc (&G)[4], T *__restrict__ qs)
 {
-    if constexpr (2 * MB <= TJ) {
-        constexpr int QS = (TJ + 1) * FI_THREADS;
-        if constexpr (MB == 0) {
-            st.pr[0] = T(1); st.pi[0] = T(0);
+    constexpr int PO = fr_row_off(J - 1);
+    const T ar = st.ar, ai = st.ai, br = st.br, bi = st.bi;
+    // gradient of this layer
+    T gar = T(0), gai = T(0), gbr = T(0), gbi = T(0);
 #pragma unroll
-            for (int k = 0; k < ND; k++) { st.dr[k][0] = T(0); st.di[k][0] = T(0); }
-        } else {
+    for (int ma = 0; ma <= J; ma++) {
+        const T lr = st.lr[ma], li = st.li[ma];
+        if (ma < J) {
+            const T A = rootpq<T>(J - ma, J - MB);
+            const T pr = st.ur[PO + ma], pi = st.ui[PO + ma];
+            gar += A * (lr * pr + li * pi);
+            gai += A * (lr * pi - li * pr);
+        }
+        if (ma >= 1) {
+            const T B = rootpq<T>(ma, J - MB);
+            const T pr = st.ur[PO + ma - 1], pi = st.ui[PO + ma - 1];
+            gbr -= B * (lr * pr + li * pi);
+            gbi -= B * (lr * pi - li * pr);
+        }
+    }
+    G[0].add(gar); G[1].add(gai); G[2].add(gbr); G[3].add(gbi);
+    // adjoint of the parent row, in place (ascending k reads l[k+1] before it changes)
 #pragma unroll
-            for (int ma = 0; ma < 2 * MB; ma++) {
-                st.pr[ma] = qs[0 * QS + ma * FI_THREADS]; st.pi[ma] = qs[1 * QS + ma * FI_THREADS];
+    for (int k = 0; k < J; k++) {
+        const T A = rootpq<T>(J - k, J - MB), B = rootpq<T>(k + 1, J - MB);
+        const T lr = st.lr[k], li = st.li[k], mr = st.lr[k + 1], mi = st.li[k + 1];
+        st.lr[k] = A * (ar * lr - ai * li) - B * (br * mr - bi * mi);
+        st.li[k] = A * (ar * li + ai * lr) - B * (br * mi + bi * mr);
+    }
+    if constexpr (J - 1 >= 2 * MB) {
+        // parent is row (J-1, MB) of this column
+        fr_add_y<T, TJ, J - 1, MB>(st, Yi);
+        if constexpr (J - 1 == 2 * MB + 1 && 2 * (MB + 1) <= TJ) {
+            constexpr int O = fr_seed_off(MB + 1);
 #pragma unroll
-                for (int k = 0; k < ND; k++) {
-                    st.dr[k][ma] = qs[(2 + k) * QS + ma * FI_THREADS];
-                    st.di[k][ma] = qs[(2 + ND + k) * QS + ma * FI_THREADS];
-                }
+            for (int ma = 0; ma < J; ma++) {
+                st.lr[ma] += qs[(2 * (O + ma) + 0) * FR_THREADS];
+                st.li[ma] += qs[(2 * (O + ma) + 1) * FR_THREADS];
             }
         }
-        fi_layer<T, TJ, ND, K0, MB, (MB == 0 ? 1 : 2 * MB)>(st, g, Yi, A0, A, qs);
-        asm volatile("" ::: "memory");
-        fi_rows<T, TJ, ND, K0, MB + 1>(st, g, Yi, A0, A, qs);
+        // the column's first computed row is layer max(1, 2MB)
+        if constexpr (J - 1 >= (MB == 0 ? 1 : 2 * MB)) fr_col_bwd<T, TJ, J - 1, MB>(st, Yi, G, qs);
+    } else {
+        // parent is the seed S_MB = mirror of row (J' = 2MB-1, MB-1): store the
+        // adjoint of that row, L[ma] = (-1)^(MB-1+ma) conj(l'[J' - ma])
+        constexpr int JP = 2 * MB - 1, O = fr_seed_off(MB);
+#pragma unroll
+        for (int ma = 0; ma <= JP; ma++) {
+            const T s = ((MB - 1 + ma) & 1) ? T(-1) : T(1);
+            qs[(2 * (O + ma) + 0) * FR_THREADS] = s * st.lr[JP - ma];
+            qs[(2 * (O + ma) + 1) * FR_THREADS] = -s * st.li[JP - ma];
+        }
     }
 }
 
-template <typename T, int TJ, int ND, int K0, typename Acc>
-__device__ __forceinline__ void fi_pass(const T ar, const T ai, const T br, const T bi, const T (&dar)[3],
-                                        const T (&dai)[3], const T (&dbr)[3], const T (&dbi)[3],
-                                        const typename cplx<T>::type *__restrict__ Yi, Acc &A0, Acc (&A)[3],
-                                        T *__restrict__ qs)
+template <typename T, int TJ, int MB, typename Acc>
+__device__ __forceinline__ void fr_columns(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi,
+                                           Acc (&G)[4], T *__restrict__ qs)
 {
-    FiGeo<T, ND> g;
-    g.ar = ar; g.ai = ai; g.br = br; g.bi = bi;
+    if constexpr (MB >= 0) {
+        T pr[TJ + 1], pi[TJ + 1];
+        if constexpr (MB == 0) {
+            pr[0] = T(1); pi[0] = T(0);
+            st.ur[0] = T(1); st.ui[0] = T(0);
+        } else {
+            constexpr int O = fr_seed_off(MB), JP = 2 * MB - 1;
 #pragma unroll
-    for (int k = 0; k < ND; k++) { g.dar[k] = dar[K0 + k]; g.dai[k] = dai[K0 + k]; g.dbr[k] = dbr[K0 + k]; g.dbi[k] = dbi[K0 + k]; }
-    FiRow<T, TJ, ND> st;
-    fi_rows<T, TJ, ND, K0, 0>(st, g, Yi, A0, A, qs);
+            for (int ma = 0; ma <= JP; ma++) {
+                pr[ma] = qs[(2 * (O + ma) + 0) * FR_THREADS];
+                pi[ma] = qs[(2 * (O + ma) + 1) * FR_THREADS];
+                st.ur[fr_row_off(JP) + ma] = pr[ma]; st.ui[fr_row_off(JP) + ma] = pi[ma];
+            }
+        }
+        fr_col_fwd<T, TJ, (MB == 0 ? 1 : 2 * MB), MB>(st, pr, pi);
+        // adjoint row of layer TJ = its weighted Y row
+#pragma unroll
+        for (int ma = 0; ma <= TJ; ma++) { st.lr[ma] = T(0); st.li[ma] = T(0); }
+        fr_add_y<T, TJ, TJ, MB>(st, Yi);
+        fr_col_bwd<T, TJ, TJ, MB>(st, Yi, G, qs);
+        asm volatile("" ::: "memory");
+        fr_columns<T, TJ, MB - 1>(st, Yi, G, qs);
+    }
 }
 
-// number of derivative directions carried by the first pass; the rest follow
-// one at a time.  Chosen so the recursion state stays in registers.
-template <typename T, int TJ> struct FiSplit { static constexpr int first = 3; };
-
 template <typename T, int TJ>
-__device__ __forceinline__ void fi_pair(const int p, const double4 *__restrict__ prij, const int2 *__restrict__ pinfo,
+__device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__ prij, const int2 *__restrict__ pinfo,
                                         const SnapGeom &gp, const typename cplx<T>::type *__restrict__ Y,
-                                        double4 *__restrict__ dEslot, const int nm, T *__restrict__ qs)
+                                        double4 *__restrict__ dEslot, T *__restrict__ qs, double *__restrict__ qg)
 {
     typedef typename cplx<T>::type T2;
     typedef typename FAccSel<T>::type Acc;
     constexpr int NYH = yh_count(TJ);
     const double4 r = prij[p];
     const int2 inf = pinfo[p];
-    PairGeo g;
-    pair_geometry<true>(g, r.x, r.y, r.z, gp);
-    const T ar = (T)g.ar, ai = (T)g.ai, br = (T)g.br, bi = (T)g.bi;
-    T dar[3], dai[3], dbr[3], dbi[3];
+    FrState<T, TJ> st;
+    {
+        PairGeo g;
+        pair_geometry<true>(g, r.x, r.y, r.z, gp);
+        st.ar = (T)g.ar; st.ai = (T)g.ai; st.br = (T)g.br; st.bi = (T)g.bi;
+        // d(a,b)/dx_k and the radial terms wait in shared memory until the end
 #pragma unroll
-    for (int k = 0; k < 3; k++) { dar[k] = (T)g.dar[k]; dai[k] = (T)g.dai[k]; dbr[k] = (T)g.dbr[k]; dbi[k] = (T)g.dbi[k]; }
+        for (int k = 0; k < 3; k++) {
+            qg[(4 * k + 0) * FR_THREADS] = g.dar[k];
+            qg[(4 * k + 1) * FR_THREADS] = g.dai[k];
+            qg[(4 * k + 2) * FR_THREADS] = g.dbr[k];
+            qg[(4 * k + 3) * FR_THREADS] = g.dbi[k];
+            qg[(12 + k) * FR_THREADS] = 2.0 * g.dsfac * g.u[k];
+        }
+        qg[15 * FR_THREADS] = 2.0 * g.sfac;
+    }
     const T2 *Yi = Y + (size_t)(inf.x >> 5) * NYH * 32 + (inf.x & 31);   // tiled: element k at Yi[k*32]
-
-    // A0 = sum w Re(Y* U), Ak = sum w Re(Y* dU/dx_k); dE/dx_k = 2(dsfac u_k A0 + sfac Ak)
-    Acc A0, A[3];
-    A0.init((T)(0.5 * (double)Yi[0].x));   // j = 0 element
+    {
+        T pr[TJ + 1], pi[TJ + 1];
+        fr_seeds<T, TJ, 0>(st.ar, st.ai, st.br, st.bi, pr, pi, qs);
+    }
+    Acc G[4];
 #pragma unroll
-    for (int k = 0; k < 3; k++) A[k].init(T(0));
-    constexpr int N1 = FiSplit<T, TJ>::first;
-    fi_pass<T, TJ, N1, 0>(ar, ai, br, bi, dar, dai, dbr, dbi, Yi, A0, A, qs);
-    if constexpr (N1 < 3) fi_pass<T, TJ, 1, N1>(ar, ai, br, bi, dar, dai, dbr, dbi, Yi, A0, A, qs);
-    if constexpr (N1 < 2) fi_pass<T, TJ, 1, 2>(ar, ai, br, bi, dar, dai, dbr, dbi, Yi, A0, A, qs);
-    const double a0 = A0.val();
-    double4 out;
-    out.x = 2.0 * (g.dsfac * g.u[0] * a0 + g.sfac * A[0].val());
-    out.y = 2.0 * (g.dsfac * g.u[1] * a0 + g.sfac * A[1].val());
-    out.z = 2.0 * (g.dsfac * g.u[2] * a0 + g.sfac * A[2].val());
-    out.w = 0.0;
-    dEslot[inf.y] = out;   // inf.y: global output slot
+    for (int k = 0; k < 4; k++) G[k].init(T(0));
+    fr_columns<T, TJ, TJ / 2>(st, Yi, G, qs);
+    // after column 0, st.l[0] is the adjoint of the root u_0 = 1 (its own
+    // half-weighted Y term included), whose real part is F
+    const double F = (double)st.lr[0];
+    const double g0 = G[0].val(), g1 = G[1].val(), g2 = G[2].val(), g3 = G[3].val();
+    double o[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double dF = g0 * qg[(4 * k + 0) * FR_THREADS] + g1 * qg[(4 * k + 1) * FR_THREADS] +
+                          g2 * qg[(4 * k + 2) * FR_THREADS] + g3 * qg[(4 * k + 3) * FR_THREADS];
+        o[k] = qg[(12 + k) * FR_THREADS] * F + qg[15 * FR_THREADS] * dF;
+    }
+    dEslot[inf.y] = make_double4(o[0], o[1], o[2], 0.0);
 }
 
-// grid-stride over the pairs; the pair count is read on the device (the
-// last entry of the pair offsets), so no host synchronisation is needed
 template <typename T, int TJ>
-__global__ void __launch_bounds__(FI_THREADS)
-k_snap_fi(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
-          SnapGeom gp, const typename cplx<T>::type *__restrict__ Y, double4 *__restrict__ dEslot, int nm)
+__global__ void __launch_bounds__(FR_THREADS)
+k_snap_fr(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
+          SnapGeom gp, const typename cplx<T>::type *__restrict__ Y, double4 *__restrict__ dEslot)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
-    T *qs = reinterpret_cast<T *>(smraw) + threadIdx.x;
+    double *qg = reinterpret_cast<double *>(smraw) + threadIdx.x;
+    T *qs = reinterpret_cast<T *>(reinterpret_cast<double *>(smraw) + 16 * FR_THREADS) + threadIdx.x;
     const int npairs = *pnum;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x)
-        fi_pair<T, TJ>(p, prij, pinfo, gp, Y, dEslot, nm, qs);
+        fr_pair<T, TJ>(p, prij, pinfo, gp, Y, dEslot, qs, qg);
 }
 
 }  // namespace mdp
