@@ -55,6 +55,7 @@ constexpr int NTRI = (TJMAX + 1) * (TJMAX + 2) / 2 * JD;
 // host-side table construction (tables.cu)
 void host_cg_table(double *cg /*NCG*/);
 void host_rootpq_table(double *rp /*JD*JD*/);
+void host_unorm_table(double *un /*JD*JD*JD*/);
 void set_error(const char *fmt, ...);
 const char *get_error();
 
@@ -63,6 +64,10 @@ const char *get_error();
 // fills it through tu_ensure_tables() before its first launch on a device.
 static __constant__ double c_rootpq_d[JD * JD];
 static __constant__ float c_rootpq_f[JD * JD];
+// unorm[(J*JD + mb)*JD + ma] = sqrt(ma! (J-ma)! / ((J-mb)! mb!)): the factor
+// between a U entry of row mb, layer J and its coefficient-free form (below)
+static __constant__ double c_unorm_d[JD * JD * JD];
+static __constant__ float c_unorm_f[JD * JD * JD];
 static __constant__ double c_cg_d[NCG];
 static __constant__ float c_cg_f[NCG];
 
@@ -77,16 +82,20 @@ static inline int tu_ensure_tables()
     }
     std::lock_guard<std::mutex> lk(mu);
     if (done[dev]) return 0;
-    static double cg[NCG], rp[JD * JD];
-    static float cgf[NCG], rpf[JD * JD];
+    static double cg[NCG], rp[JD * JD], un[JD * JD * JD];
+    static float cgf[NCG], rpf[JD * JD], unf[JD * JD * JD];
     host_cg_table(cg);
     host_rootpq_table(rp);
+    host_unorm_table(un);
     for (int i = 0; i < NCG; i++) cgf[i] = (float)cg[i];
     for (int i = 0; i < JD * JD; i++) rpf[i] = (float)rp[i];
+    for (int i = 0; i < JD * JD * JD; i++) unf[i] = (float)un[i];
     if (cudaMemcpyToSymbol(c_cg_d, cg, sizeof(cg)) != cudaSuccess ||
         cudaMemcpyToSymbol(c_cg_f, cgf, sizeof(cgf)) != cudaSuccess ||
         cudaMemcpyToSymbol(c_rootpq_d, rp, sizeof(rp)) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_rootpq_f, rpf, sizeof(rpf)) != cudaSuccess) {
+        cudaMemcpyToSymbol(c_rootpq_f, rpf, sizeof(rpf)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_unorm_d, un, sizeof(un)) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_unorm_f, unf, sizeof(unf)) != cudaSuccess) {
         set_error("uploading SNAP constant tables failed");
         return -1;
     }
@@ -113,6 +122,10 @@ template <> struct cplx<float> { typedef float2 type; };
 template <typename T> __device__ __forceinline__ T rootpq(int p, int q);
 template <> __device__ __forceinline__ double rootpq<double>(int p, int q) { return c_rootpq_d[p * JD + q]; }
 template <> __device__ __forceinline__ float rootpq<float>(int p, int q) { return c_rootpq_f[p * JD + q]; }
+
+template <typename T> __device__ __forceinline__ T unorm(int j, int mb, int ma);
+template <> __device__ __forceinline__ double unorm<double>(int j, int mb, int ma) { return c_unorm_d[(j * JD + mb) * JD + ma]; }
+template <> __device__ __forceinline__ float unorm<float>(int j, int mb, int ma) { return c_unorm_f[(j * JD + mb) * JD + ma]; }
 
 template <typename T> __device__ __forceinline__ T cgc(int k);
 template <> __device__ __forceinline__ double cgc<double>(int k) { return c_cg_d[k]; }

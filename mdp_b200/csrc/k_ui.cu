@@ -1,4 +1,4 @@
-// U stage launchers (k_snap_ui), all precisions.
+// U stage launchers (k_snap_uc), all precisions.
 #include "engine.h"
 
 #include <algorithm>
@@ -10,17 +10,18 @@ int launch_ui(const SnapModel &m, ForcePath &fp, int inum, cudaStream_t s)
 {
     typedef typename cplx<T>::type T2;
     if (tu_ensure_tables()) return -1;
-    constexpr int NU = idxu_count(TJ);
-    const size_t sm = (size_t)UI_WARPS * (NU + 32 * (TJ + 1)) * sizeof(T2);
-    static bool attr = false;
-    if (!attr) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_ui<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        attr = true;
+    const size_t sm = uc_smem_bytes<T, TJ>();
+    static int per_sm = 0;
+    if (!per_sm) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_uc<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_uc<T, TJ>, uc_warps<TJ>() * 32, sm));
+        if (per_sm < 1) { set_error("k_snap_uc does not fit on an SM"); return -1; }
     }
-    const int blocks = std::min((inum + UI_WARPS - 1) / UI_WARPS, num_sms() * 16);
+    const int ntiles = (inum + 31) / 32;
+    const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[1], s);
-    k_snap_ui<T, TJ><<<blocks, UI_WARPS * 32, sm, s>>>(fp.poff.as<int>(), fp.prij.as<double4>(), inum, m.geom,
-                                                       fp.Ut.as<T2>());
+    k_snap_uc<T, TJ><<<blocks, uc_warps<TJ>() * 32, sm, s>>>(fp.poff.as<int>(), fp.prij.as<double4>(),
+                                                             fp.pab.as<double4>(), inum, fp.Ut.as<T2>());
     return 0;
 }
 

@@ -322,8 +322,11 @@ __global__ void k_pair_count(const double4 *__restrict__ x, const int *__restric
     pcount[i] = cnt;
 }
 
+// compact pair list of the atoms' slots in order; each pair also gets its
+// Cayley-Klein parameters (a, b) in pab and its sfac in prij.w
 __global__ void k_pair_emit(const double4 *__restrict__ rslot, const int *__restrict__ nnum, int inum, int nm,
-                            const int *__restrict__ poff, double4 *__restrict__ prij, int2 *__restrict__ pinfo)
+                            const int *__restrict__ poff, SnapGeom gp, double4 *__restrict__ prij,
+                            int2 *__restrict__ pinfo, double4 *__restrict__ pab)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= inum) return;
@@ -332,7 +335,10 @@ __global__ void k_pair_emit(const double4 *__restrict__ rslot, const int *__rest
     for (int l = 0; l < n; l++) {
         const double4 r = rslot[(size_t)i * nm + l];
         if (r.w != 0.0) {
-            prij[p] = r;
+            PairGeo g;
+            pair_geometry<false>(g, r.x, r.y, r.z, gp);
+            prij[p] = make_double4(r.x, r.y, r.z, g.sfac);
+            pab[p] = make_double4(g.ar, g.ai, g.br, g.bi);
             pinfo[p] = make_int2(i, (int)((size_t)i * nm + l));
             p++;
         }

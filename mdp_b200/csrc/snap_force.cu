@@ -35,7 +35,7 @@ void DevBuf::release()
 
 void ForcePath::release()
 {
-    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &rslot, &dE, &Ut, &Y, &scan_tmp};
+    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &rslot, &dE, &Ut, &Y, &scan_tmp};
     for (auto x : b) x->release();
     for (auto &e : ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
@@ -219,6 +219,7 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (pair_cap < 1) pair_cap = 1;
     if (fp.pcount.ensure(sizeof(int) * (size_t)inum) || fp.poff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
         fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
+        fp.pab.ensure(sizeof(double4) * (size_t)pair_cap) ||
         fp.rslot.ensure(sizeof(double4) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)inum * nm) ||
         fp.Ut.ensure(tsz * (size_t)ntiles * m.nu * 32) || fp.Y.ensure(tsz * (size_t)ntiles * 32 * m.nyh) ||
         fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(inum)))
@@ -230,8 +231,8 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (fp.timing) cudaEventRecord(fp.ev[0], s);
     k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.rslot.as<double4>(), fp.pcount.as<int>());
     if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
-    k_pair_emit<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), nnum, inum, nm, fp.poff.as<int>(), fp.prij.as<double4>(),
-                                  fp.pinfo.as<int2>());
+    k_pair_emit<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), nnum, inum, nm, fp.poff.as<int>(), m.geom,
+                                  fp.prij.as<double4>(), fp.pinfo.as<int2>(), fp.pab.as<double4>());
     int rc = (precision == MDP_PREC_FP32) ? launch_snap_tj<float>(m, m.yf, fp, inum, nm, eatom, s)
                                            : launch_snap_tj<double>(m, m.yd, fp, inum, nm, eatom, s);
     if (rc) return rc;

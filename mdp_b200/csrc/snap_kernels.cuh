@@ -248,6 +248,214 @@ k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int na
     }
 }
 
+// Coefficient-free row step of column MB: v_J[ma] = conj(a) v_(J-1)[ma] -
+// conj(b) v_(J-1)[ma-1], in place (entries 0..J).  The U entry is
+// unorm(J, MB, ma) * v[ma]; the middle-row mirror is the same in both forms
+// (unorm is symmetric about ma = MB there), and with the mb factor of unorm a
+// column's seed is its predecessor's row 2MB-1 mirrored without any scale.
+template <typename T, int TJ, int J, int MB>
+__device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const T bi, T (&pr)[TJ + 1],
+                                       T (&pi)[TJ + 1])
+{
+    {
+        const T vr = pr[J - 1], vi = pi[J - 1];
+        pr[J] = -br * vr - bi * vi;
+        pi[J] = -br * vi + bi * vr;
+    }
+#pragma unroll
+    for (int ma = J - 1; ma >= 1; ma--) {
+        const T ur = pr[ma], ui = pi[ma], vr = pr[ma - 1], vi = pi[ma - 1];
+        pr[ma] = ar * ur + ai * ui - br * vr - bi * vi;
+        pi[ma] = ar * ui - ai * ur - br * vi + bi * vr;
+    }
+    {
+        const T ur = pr[0], ui = pi[0];
+        pr[0] = ar * ur + ai * ui;
+        pi[0] = ar * ui - ai * ur;
+    }
+    if constexpr (MB > 0 && J == 2 * MB) {
+#pragma unroll
+        for (int ma = 0; ma <= MB; ma++) {
+            const T sg = (ma & 1) ? T(-1) : T(1);
+            pr[MB + ma] = sg * pr[MB - ma];
+            pi[MB + ma] = -sg * pi[MB - ma];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// k_snap_uc: U of a 32-atom tile, one warp per column of the half plane.
+//
+// Lane = atom.  Each lane walks its own atom's pairs, UC_PB per iteration, and
+// per pair recomputes the recursion path that reaches its warp's column: the
+// seed chain (rows 1, 2c..2c+1 of the columns c below, each mirrored into the
+// next column's seed) and then the column's own rows, which it adds into a
+// half-plane tile in shared memory ([yh index][lane]).  Every column's path
+// has one row per layer 1..TJ, so the warps' work is equal; the top two
+// columns share the last warp (the top one continues from the row the other
+// ends its chain with).  Warps own disjoint tile entries: no atomics.  The
+// tile is then written out as the full plane with wself on the diagonal and
+// rows mb > j/2 by inversion symmetry (cpuSnap4.cpp:11-244, cpuAddWself2Ui).
+// (a, b, sfac) of each pair come from the pair stage.
+// ---------------------------------------------------------------------------
+constexpr int UC_PB = 1;
+template <int TJ> __host__ __device__ constexpr int uc_warps() { return TJ / 2; }
+template <typename T, int TJ> constexpr size_t uc_smem_bytes()
+{
+    return (size_t)yh_count(TJ) * 32 * sizeof(typename cplx<T>::type);
+}
+
+// per-pair state; the root of the recursion is v_0 = sfac, so every row comes
+// out weighted by sfac (the recursion is linear in its root)
+template <typename T, int TJ>
+struct UcPairs {
+    T ar[UC_PB], ai[UC_PB], br[UC_PB], bi[UC_PB];
+    T pr[UC_PB][TJ + 1], pi[UC_PB][TJ + 1];
+};
+
+// seed chain up to column MB: column C's last chain row (2C+1) mirrored into
+// column C+1's seed, for C = 0..MB-1
+template <typename T, int TJ, int MB, int C>
+__device__ __forceinline__ void uc_chain(UcPairs<T, TJ> &s)
+{
+    if constexpr (C < MB) {
+        constexpr int J = 2 * C + 1;
+#pragma unroll
+        for (int q = 0; q < UC_PB; q++) {
+            if constexpr (C > 0) cf_fwd<T, TJ, 2 * C, C>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
+            cf_fwd<T, TJ, J, C>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
+            T nr[J + 1], ni[J + 1];
+#pragma unroll
+            for (int ma = 0; ma <= J; ma++) {
+                const T sg = ((C + ma) & 1) ? T(-1) : T(1);
+                nr[J - ma] = sg * s.pr[q][ma]; ni[J - ma] = -sg * s.pi[q][ma];
+            }
+#pragma unroll
+            for (int ma = 0; ma <= J; ma++) { s.pr[q][ma] = nr[ma]; s.pi[q][ma] = ni[ma]; }
+        }
+        uc_chain<T, TJ, MB, C + 1>(s);
+    }
+}
+
+// rows J..JEND of column MB (row J's parent in s.pr/pi), each added into the tile
+template <typename T, int TJ, int MB, int J, int JEND>
+__device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
+{
+    typedef typename cplx<T>::type T2;
+    if constexpr (J <= JEND) {
+        if constexpr (J > 0) {
+#pragma unroll
+            for (int q = 0; q < UC_PB; q++)
+                cf_fwd<T, TJ, J, MB>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
+        }
+        T2 *row = acc + (yh_block(J) + (J + 1) * MB) * 32;
+#pragma unroll
+        for (int ma = 0; ma <= J; ma++) {
+            const T nu = unorm<T>(J, MB, ma);
+            T2 v = row[ma * 32];
+#pragma unroll
+            for (int q = 0; q < UC_PB; q++) { v.x += nu * s.pr[q][ma]; v.y += nu * s.pi[q][ma]; }
+            row[ma * 32] = v;
+        }
+        uc_column<T, TJ, MB, J + 1, JEND>(s, acc);
+    }
+}
+
+// the work of warp MB: column MB (and, for the last warp, column MB+1)
+template <typename T, int TJ, int MB>
+__device__ __forceinline__ void uc_path(UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
+{
+    uc_chain<T, TJ, MB, 0>(s);
+    if constexpr (MB + 1 < uc_warps<TJ>()) {
+        uc_column<T, TJ, MB, (MB == 0 ? 0 : 2 * MB), TJ>(s, acc);
+    } else {
+        // last warp: column MB up to its row 2MB+1, mirror to the seed of
+        // column MB+1 = TJ/2, then column MB's remaining rows continue from a
+        // copy while column TJ/2 takes its single row TJ
+        constexpr int MT = MB + 1;
+        uc_column<T, TJ, MB, (MB == 0 ? 0 : 2 * MB), 2 * MB + 1>(s, acc);
+        T kr[UC_PB][TJ + 1], ki[UC_PB][TJ + 1];
+#pragma unroll
+        for (int q = 0; q < UC_PB; q++)
+#pragma unroll
+            for (int ma = 0; ma <= 2 * MB + 1; ma++) { kr[q][ma] = s.pr[q][ma]; ki[q][ma] = s.pi[q][ma]; }
+        uc_column<T, TJ, MB, 2 * MB + 2, TJ>(s, acc);
+#pragma unroll
+        for (int q = 0; q < UC_PB; q++) {
+            constexpr int J = 2 * MB + 1;
+#pragma unroll
+            for (int ma = 0; ma <= J; ma++) {
+                const T sg = ((MB + ma) & 1) ? T(-1) : T(1);
+                s.pr[q][J - ma] = sg * kr[q][ma]; s.pi[q][J - ma] = -sg * ki[q][ma];
+            }
+        }
+        uc_column<T, TJ, MT, 2 * MT, TJ>(s, acc);
+    }
+}
+
+template <typename T, int TJ, int MB>
+__device__ __forceinline__ void uc_dispatch(const int w, UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
+{
+    if constexpr (MB < uc_warps<TJ>()) {
+        if (w == MB) uc_path<T, TJ, MB>(s, acc);
+        else uc_dispatch<T, TJ, MB + 1>(w, s, acc);
+    }
+}
+
+template <typename T, int TJ>
+__global__ void __launch_bounds__(uc_warps<TJ>() * 32)
+k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const double4 *__restrict__ pab,
+          int natoms, typename cplx<T>::type *__restrict__ Ut)
+{
+    typedef typename cplx<T>::type T2;
+    constexpr int NW = uc_warps<TJ>();
+    constexpr int NU = idxu_count(TJ), NYH = yh_count(TJ);
+    extern __shared__ __align__(16) unsigned char smraw[];
+    T2 *acc = reinterpret_cast<T2 *>(smraw);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ntiles = (natoms + 31) >> 5;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        for (int k = threadIdx.x; k < NYH * 32; k += NW * 32) acc[k] = T2{T(0), T(0)};
+        __syncthreads();
+        const int i = tile * 32 + lane;
+        int p = 0, pend = 0;
+        if (i < natoms) { p = poff[i]; pend = poff[i + 1]; }
+        for (; p < pend; p += UC_PB) {
+            UcPairs<T, TJ> s;
+#pragma unroll
+            for (int q = 0; q < UC_PB; q++) {
+                const bool ok = p + q < pend;
+                const double4 g = ok ? pab[p + q] : make_double4(1.0, 0.0, 0.0, 0.0);
+                s.ar[q] = (T)g.x; s.ai[q] = (T)g.y; s.br[q] = (T)g.z; s.bi[q] = (T)g.w;
+                s.pr[q][0] = ok ? (T)prij[p + q].w : T(0);   // v_0 = sfac
+                s.pi[q][0] = T(0);
+            }
+            uc_dispatch<T, TJ, 0>(w, s, acc + lane);
+        }
+        __syncthreads();
+        // full plane out: wself on the diagonal, rows mb > j/2 mirrored
+        T2 *dst = Ut + (size_t)tile * NU * 32;
+        for (int e = threadIdx.x; e < NU * 32; e += NW * 32) {
+            const int k = e >> 5, l = e & 31;
+            int j = 0;
+            while (idxu_block(j + 1) <= k) j++;
+            const int rem = k - idxu_block(j), mb = rem / (j + 1), ma = rem - mb * (j + 1);
+            T2 v;
+            if (2 * mb <= j) {
+                v = acc[(yh_block(j) + rem) * 32 + l];
+                if (ma == mb) v.x += T(1);
+            } else {
+                const int sb = j - mb, sa = j - ma;
+                const T2 u = acc[(yh_block(j) + (j + 1) * sb + sa) * 32 + l];
+                const T sg = ((sa + sb) & 1) ? T(-1) : T(1);
+                v = T2{sg * (u.x + (sa == sb ? T(1) : T(0))), -sg * u.y};
+            }
+            dst[e] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // k_snap_yi
 // ---------------------------------------------------------------------------

@@ -67,6 +67,22 @@ void host_rootpq_table(double *rp)
             rp[p * JD + q] = (p >= 1 && q >= 1) ? sqrt((double)p / q) : 0.0;
 }
 
+// Row mb of U at layer J is u[ma] = unorm(J, mb, ma) * v[ma], where v obeys the
+// coefficient-free recursion v_J[ma] = conj(a) v_(J-1)[ma] - conj(b) v_(J-1)[ma-1]
+// (the sqrt(ma!(J-ma)!/(mb!(J-mb)!)) normalisation of the Wigner D-matrix,
+// which turns cpuSnap4.cpp's rootpq factors into ratios of these numbers).
+void host_unorm_table(double *un)
+{
+    double fac[2 * JD];
+    fac[0] = 1.0;
+    for (int i = 1; i < 2 * JD; i++) fac[i] = fac[i - 1] * i;
+    for (int j = 0; j < JD; j++)
+        for (int mb = 0; mb < JD; mb++)
+            for (int ma = 0; ma < JD; ma++)
+                un[(j * JD + mb) * JD + ma] =
+                    (mb <= j && ma <= j) ? sqrt(fac[ma] * fac[j - ma] / (fac[j - mb] * fac[mb])) : 0.0;
+}
+
 // ---------------------------------------------------------------------------
 // exclusive scan: 4096 elements per block (1024 threads x 4), two levels
 // ---------------------------------------------------------------------------
