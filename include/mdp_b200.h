@@ -125,6 +125,53 @@ void *mdp_md_stream(mdp_md *h);
  * register-resident FMA loop timed with CUDA events */
 int mdp_probe_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
+/* ---------------------------------------------------------------------------
+ * Learned surrogate (no counterpart in MDP): an MLP 14 -> 64 -> 64 -> 1 (SiLU)
+ * on the per-atom 2J=4 bispectrum stands in for the per-atom SNAP energy.
+ * Parameters: mdp_sur_nparams() floats, laid out W1 [64][16] (features padded
+ * to 16), b1 [64], W2 [64][64] (W2[out][in]), b2 [64], w3 [64], b3.
+ * Normalisation (2*14+2 floats): feature means, feature 1/std, energy mean,
+ * energy std.  Forward passes use the weights rounded to BF16.
+ * ------------------------------------------------------------------------- */
+typedef struct mdp_sur mdp_sur;
+
+/* p4: SNAP hyper-parameters of the features (twojmax 4; coefficients unused) */
+int mdp_sur_create(mdp_sur **h, const mdp_snap_params *p4, int device);
+void mdp_sur_destroy(mdp_sur *h);
+int mdp_sur_nparams(void);
+int mdp_sur_set_params(mdp_sur *h, const float *params, const float *norm /* may be NULL */);
+int mdp_sur_get_params(mdp_sur *h, float *params, float *norm);
+/* training set on the device: rows of 16 floats (14 features + 2 zeros) and a
+ * per-atom target energy */
+int mdp_sur_dataset_reserve(mdp_sur *h, long rows);
+long mdp_sur_dataset_size(mdp_sur *h);
+int mdp_sur_dataset_add(mdp_sur *h, const double *B_dev, long bstride, const double *e_dev, int n, void *stream);
+int mdp_sur_dataset_load(mdp_sur *h, const float *X, const float *E, long nrows);
+int mdp_sur_dataset_copy(mdp_sur *h, float *X, float *E, long row0, long nrows);
+/* feature/energy mean and spread of the dataset become the normalisation */
+int mdp_sur_fit_normalization(mdp_sur *h);
+/* steps Adam updates on random minibatches of batch rows (loss per step out) */
+int mdp_sur_train(mdp_sur *h, int steps, int batch, float lr, unsigned long long seed, float *loss);
+/* gradient of the mean squared normalised-energy error over host rows, no update */
+int mdp_sur_grad(mdp_sur *h, const float *X, const float *E, int n, float *grad, float *loss);
+/* inference on host features B [k * n + atom]: E [n], G = dE_i/dB_ik [k * n + atom] */
+int mdp_sur_eval(mdp_sur *h, const double *B, int n, double *E, float *G);
+
+/* append the MD engine's current state to the training set: 2J=4 features of
+ * the current positions and the per-atom energies of the last force call */
+int mdp_md_sur_sample(mdp_md *md, mdp_sur *s);
+/* per-atom 2J=4 features of the engine's current positions, B [k * natoms + atom] */
+int mdp_md_sur_features(mdp_md *md, mdp_sur *s, double *B_host);
+/* forces from the surrogate (s != NULL) or the plain SNAP model (s == NULL).
+ * Every judge_every steps (and at setup) the plain model is evaluated on the
+ * same positions; its forces replace the surrogate's for that step and, when
+ * the force RMSE (over the 3N components) exceeds tol, the engine falls back
+ * to the plain model for the rest of its life. */
+int mdp_md_set_surrogate(mdp_md *md, mdp_sur *s, int judge_every, double tol);
+/* active (1 while the surrogate drives), fallback step (-1: none), number of
+ * judgements, and up to cap (step, rmse) pairs */
+int mdp_md_surrogate_status(mdp_md *md, int *active, long long *fallback_step, int *njudge, double *log, int cap);
+
 #ifdef __cplusplus
 }
 #endif

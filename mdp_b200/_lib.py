@@ -73,6 +73,26 @@ def lib():
     L.mdp_md_sync.argtypes = [C.c_void_p]
     L.mdp_launch_count.restype = C.c_longlong
     L.mdp_probe_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+    L.mdp_sur_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(SnapParamsC), C.c_int]
+    L.mdp_sur_destroy.argtypes = [C.c_void_p]
+    L.mdp_sur_destroy.restype = None
+    L.mdp_sur_set_params.argtypes = [C.c_void_p, _fp, C.c_void_p]
+    L.mdp_sur_get_params.argtypes = [C.c_void_p, _fp, _fp]
+    L.mdp_sur_dataset_reserve.argtypes = [C.c_void_p, C.c_long]
+    L.mdp_sur_dataset_size.argtypes = [C.c_void_p]
+    L.mdp_sur_dataset_size.restype = C.c_long
+    L.mdp_sur_dataset_load.argtypes = [C.c_void_p, _fp, _fp, C.c_long]
+    L.mdp_sur_dataset_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_long, C.c_long]
+    L.mdp_sur_fit_normalization.argtypes = [C.c_void_p]
+    L.mdp_sur_train.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_ulonglong, _fp]
+    L.mdp_sur_grad.argtypes = [C.c_void_p, _fp, _fp, C.c_int, _fp, C.POINTER(C.c_float)]
+    L.mdp_sur_eval.argtypes = [C.c_void_p, _dp, C.c_int, _dp, _fp]
+    L.mdp_md_sur_sample.argtypes = [C.c_void_p, C.c_void_p]
+    L.mdp_md_sur_features.argtypes = [C.c_void_p, C.c_void_p, _dp]
+    L.mdp_md_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
+    L.mdp_md_surrogate_status.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
+                                          C.POINTER(C.c_int), C.c_void_p, C.c_int]
     _lib = L
     return L
 

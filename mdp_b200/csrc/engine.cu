@@ -6,6 +6,7 @@
 // owners' displacement), SNAP force, final integrate, thermo.
 #include "common.cuh"
 #include "engine.h"
+#include "surrogate.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -103,6 +104,13 @@ struct mdp_md {
     long long step = 0, rebuilds = 0;
     double thermo_last[5] = {0, 0, 0, 0, 0};
     bool ready = false;
+    // learned surrogate: driving model, judge cadence and tolerance, fallback
+    Surrogate *sur = nullptr;
+    int judge_every = 50;
+    double judge_tol = 0.05;
+    long long fallback_step = -1;
+    std::vector<double> judge_log;   // (step, force RMSE) pairs
+    DevBuf fjudge;
 };
 
 extern "C" {
@@ -143,7 +151,7 @@ int mdp_md_create(mdp_md **h, const mdp_snap_params *p, const mdp_md_config *cfg
         m->x.ensure(sizeof(double4) * m->anum_cap) || m->v.ensure(sizeof(double4) * n) ||
         m->f.ensure(sizeof(double4) * n) || m->xstart.ensure(sizeof(double4) * n) ||
         m->xhold.ensure(sizeof(double4) * n) || m->e.ensure(sizeof(double) * n) ||
-        m->vatom.ensure(sizeof(double) * 6 * n) || m->scal.ensure(64)) {
+        m->vatom.ensure(sizeof(double) * 6 * n) || m->scal.ensure(128)) {
         mdp_md_destroy(m);
         return -1;
     }
@@ -156,7 +164,7 @@ void mdp_md_destroy(mdp_md *m)
     if (!m) return;
     cudaSetDevice(m->device);
     if (m->s) cudaStreamSynchronize(m->s);
-    DevBuf *b[] = {&m->x, &m->v, &m->f, &m->xstart, &m->xhold, &m->e, &m->vatom, &m->scal, &m->stage};
+    DevBuf *b[] = {&m->x, &m->v, &m->f, &m->xstart, &m->xhold, &m->e, &m->vatom, &m->scal, &m->stage, &m->fjudge};
     for (auto x : b) x->release();
     m->nb.release();
     m->fp.release();
@@ -208,13 +216,37 @@ static int md_rebuild(mdp_md *m)
     return 0;
 }
 
-static int md_force(mdp_md *m)
+static int md_force_plain(mdp_md *m)
 {
     const int n = m->cfg.natoms;
     return force_compute(m->fp, m->model, m->cfg.precision, m->x.as<double4>(), n, m->nb.nlist.as<int>(),
                          m->nb.nnum.as<int>(), m->cfg.neighmax, (long)n * m->cfg.neighmax, m->nb.roff.as<int>(),
                          m->nb.rlist.as<long long>(), m->e.as<double>(), m->f.as<double4>(), m->vatom.as<double>(),
                          m->s);
+}
+
+// Surrogate forces, judged against the plain model every judge_every steps:
+// the plain forces replace the surrogate's on a judged step, and a force RMSE
+// above the tolerance hands the run to the plain model from then on.
+static int md_force(mdp_md *m)
+{
+    if (!m->sur || m->fallback_step >= 0) return md_force_plain(m);
+    const int n = m->cfg.natoms;
+    if (sur_force(*m->sur, m->fp, m->x.as<double4>(), n, m->nb.nlist.as<int>(), m->nb.nnum.as<int>(),
+                  m->cfg.neighmax, m->nb.roff.as<int>(), m->nb.rlist.as<long long>(), m->e.as<double>(),
+                  m->f.as<double4>(), m->vatom.as<double>(), m->s))
+        return -1;
+    if (m->judge_every <= 0 || m->step % m->judge_every != 0) return 0;
+    if (m->fjudge.ensure(sizeof(double4) * (size_t)n)) return -1;
+    MDP_CUDA_TRY(cudaMemcpyAsync(m->fjudge.p, m->f.p, sizeof(double4) * (size_t)n, cudaMemcpyDeviceToDevice, m->s));
+    if (md_force_plain(m)) return -1;
+    double ss = 0.0;
+    if (force_sq_diff(m->fjudge.as<double4>(), m->f.as<double4>(), n, m->scal.as<double>() + 8, &ss, m->s)) return -1;
+    const double rmse = sqrt(ss / (3.0 * n));
+    m->judge_log.push_back((double)m->step);
+    m->judge_log.push_back(rmse);
+    if (!(rmse <= m->judge_tol)) m->fallback_step = m->step;
+    return 0;
 }
 
 // thermo row (step, T, PE/atom, TE/atom, P), Calculation.cpp:436-467
@@ -393,6 +425,65 @@ int mdp_md_counters(mdp_md *m, long long *out)
     if (m->fp.poff.p)
         MDP_CUDA_TRY(cudaMemcpy(&np, m->fp.poff.as<int>() + m->cfg.natoms, sizeof(int), cudaMemcpyDeviceToHost));
     out[0] = m->step; out[1] = m->rebuilds; out[2] = np; out[3] = m->nb.gnum; out[4] = m->nb.nsum;
+    return 0;
+}
+
+int mdp_md_sur_sample(mdp_md *m, mdp_sur *S)
+{
+    if (!m || !S) { set_error("null argument"); return -1; }
+    if (!m->ready) { set_error("mdp_md_setup must run first"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(m->device));
+    Surrogate &s = *static_cast<Surrogate *>(S);
+    const int n = m->cfg.natoms;
+    if (sur_features(s, m->fp, m->x.as<double4>(), n, m->nb.nlist.as<int>(), m->nb.nnum.as<int>(), m->cfg.neighmax,
+                     m->s))
+        return -1;
+    return mdp_sur_dataset_add(S, s.B.as<double>(), n, m->e.as<double>(), n, m->s);
+}
+
+int mdp_md_sur_features(mdp_md *m, mdp_sur *S, double *B_host)
+{
+    if (!m || !S || !B_host) { set_error("null argument"); return -1; }
+    if (!m->ready) { set_error("mdp_md_setup must run first"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(m->device));
+    Surrogate &s = *static_cast<Surrogate *>(S);
+    const int n = m->cfg.natoms;
+    if (sur_features(s, m->fp, m->x.as<double4>(), n, m->nb.nlist.as<int>(), m->nb.nnum.as<int>(), m->cfg.neighmax,
+                     m->s))
+        return -1;
+    MDP_CUDA_TRY(cudaMemcpyAsync(B_host, s.B.p, sizeof(double) * 14 * (size_t)n, cudaMemcpyDeviceToHost, m->s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(m->s));
+    return 0;
+}
+
+int mdp_md_set_surrogate(mdp_md *m, mdp_sur *S, int judge_every, double tol)
+{
+    if (!m) { set_error("null handle"); return -1; }
+    if (S) {
+        const Surrogate &s = *static_cast<Surrogate *>(S);
+        if (!s.trained) { set_error("surrogate has no parameters"); return -1; }
+        if (fabs(s.model.geom.rcut - m->model.geom.rcut) > 1e-12) {
+            set_error("surrogate cutoff %g differs from the model's %g", s.model.geom.rcut, m->model.geom.rcut);
+            return -1;
+        }
+    }
+    m->sur = static_cast<Surrogate *>(S);
+    m->judge_every = judge_every;
+    m->judge_tol = tol;
+    m->fallback_step = -1;
+    m->judge_log.clear();
+    return 0;
+}
+
+int mdp_md_surrogate_status(mdp_md *m, int *active, long long *fallback_step, int *njudge, double *log, int cap)
+{
+    if (!m) { set_error("null handle"); return -1; }
+    if (active) *active = (m->sur && m->fallback_step < 0) ? 1 : 0;
+    if (fallback_step) *fallback_step = m->fallback_step;
+    const int nj = (int)(m->judge_log.size() / 2);
+    if (njudge) *njudge = nj;
+    if (log)
+        for (int i = 0; i < std::min(nj, cap); i++) { log[2 * i] = m->judge_log[2 * i]; log[2 * i + 1] = m->judge_log[2 * i + 1]; }
     return 0;
 }
 

@@ -24,6 +24,26 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
     return 0;
 }
 
+// per-atom coefficients G [k][atom] (the surrogate's dE_i/dB_ik), 2J=4, float
+int launch_yi_pa_f4(const SnapModel &m, ForcePath &fp, int inum, const float *G, cudaStream_t s)
+{
+    if (tu_ensure_tables()) return -1;
+    const size_t sm = yi_smem_bytes<float, 4, true>();
+    static int per_sm = 0;
+    if (!per_sm) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<float, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<float, 4, true>,
+                                                                   YiWarps<float>::n * 32, sm));
+        if (per_sm < 1) { set_error("k_snap_yi (per-atom) does not fit on an SM"); return -1; }
+    }
+    const int ntiles = (inum + 31) / 32;
+    const int blocks = std::min(ntiles, num_sms() * per_sm);
+    if (fp.timing) cudaEventRecord(fp.ev[2], s);
+    k_snap_yi<float, 4, true><<<blocks, YiWarps<float>::n * 32, sm, s>>>(fp.Ut.as<float2>(), inum, m.yf,
+                                                                         fp.Y.as<float2>(), nullptr, G);
+    return 0;
+}
+
 #define MDP_INST(T, TJ) \
     template int launch_yi<T, TJ>(const SnapModel &, const YParams<T> &, ForcePath &, int, double *, cudaStream_t);
 MDP_INST(float, 4) MDP_INST(float, 6) MDP_INST(float, 8)

@@ -117,6 +117,8 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
                 if (p->bnormflag) b /= (j + 1);
                 m.yd.betaY[tri_index(j1, j2, j)] = b;
                 m.yf.betaY[tri_index(j1, j2, j)] = (float)b;
+                const int k = (j >= j1) ? jjb[j1][j2][j] : (j >= j2) ? jjb[j][j2][j1] : jjb[j2][j][j1];
+                m.yd.kmap[tri_index(j1, j2, j)] = m.yf.kmap[tri_index(j1, j2, j)] = (unsigned char)k;
             }
     double e0 = c[0];
     if (p->bzeroflag) {

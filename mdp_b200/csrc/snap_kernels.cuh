@@ -40,6 +40,10 @@ struct YParams {
     // per output layer j and warp w: the row mb the warp accumulates (255: idle)
     // and the residue / stride of the row-pair index ib it takes in every coupling
     unsigned char lay_mb[JD][YI_MAXW], lay_o[JD][YI_MAXW], lay_st[JD][YI_MAXW];
+    // bispectrum component k whose coefficient each coupling triple carries;
+    // with per-atom coefficients G[k][atom], the triple's weight is
+    // betaY[tri] * G[kmap[tri]] (betaY then holds the multiplicity factors)
+    unsigned char kmap[NTRI];
 };
 template <typename T> struct YiWarps { static constexpr int n = 8; };
 template <> struct YiWarps<float> { static constexpr int n = 16; };
@@ -514,29 +518,33 @@ __device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
 
 // all couplings of output layer J, in enumeration order (every warp walks the
 // same sequence, so the code in flight is one coupling's)
-template <typename T, int TJ, int J, int J1, int J2>
+template <typename T, int TJ, bool PA, int J, int J1, int J2>
 __device__ __forceinline__ void z_layer(const int mb, const int o, const int st,
                                         const typename cplx<T>::type *__restrict__ Us, const int lane,
-                                        const YParams<T> &P, T (&yr)[JD], T (&yi)[JD])
+                                        const YParams<T> &P, const T *__restrict__ Gs, T (&yr)[JD], T (&yi)[JD])
 {
     if constexpr (J1 <= TJ) {
         if constexpr (J2 <= J1) {
-            if constexpr (coupling_ok(J1, J2, J))
-                z_rows<T, J1, J2, J>(mb, o, st, Us, lane, P.betaY[tri_index(J1, J2, J)], yr, yi);
-            z_layer<T, TJ, J, J1, J2 + 1>(mb, o, st, Us, lane, P, yr, yi);
+            if constexpr (coupling_ok(J1, J2, J)) {
+                constexpr int TRI = tri_index(J1, J2, J);
+                T beta = P.betaY[TRI];
+                if constexpr (PA) beta *= Gs[P.kmap[TRI] * 32 + lane];
+                z_rows<T, J1, J2, J>(mb, o, st, Us, lane, beta, yr, yi);
+            }
+            z_layer<T, TJ, PA, J, J1, J2 + 1>(mb, o, st, Us, lane, P, Gs, yr, yi);
         } else {
-            z_layer<T, TJ, J, J1 + 1, 0>(mb, o, st, Us, lane, P, yr, yi);
+            z_layer<T, TJ, PA, J, J1 + 1, 0>(mb, o, st, Us, lane, P, Gs, yr, yi);
         }
     }
 }
 
 // layer J: each warp builds its partial row, the partials are summed per row,
 // written out (tiled) and folded into the energy identity
-template <typename T, int TJ, int NW, int J>
+template <typename T, int TJ, int NW, bool PA, int J>
 __device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict__ Us,
                                         typename cplx<T>::type *__restrict__ red,
                                         typename cplx<T>::type *__restrict__ dst, const int lane, const int w,
-                                        const YParams<T> &P, double &e)
+                                        const YParams<T> &P, const T *__restrict__ Gs, double &e)
 {
     typedef typename cplx<T>::type T2;
     const int mb = P.lay_mb[J][w];
@@ -544,7 +552,7 @@ __device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict
         T yr[JD], yi[JD];
 #pragma unroll
         for (int ma = 0; ma < JD; ma++) { yr[ma] = T(0); yi[ma] = T(0); }
-        z_layer<T, TJ, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w], Us, lane, P, yr, yi);
+        z_layer<T, TJ, PA, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w], Us, lane, P, Gs, yr, yi);
 #pragma unroll
         for (int ma = 0; ma <= J; ma++) red[(w * JD + ma) * 32 + lane] = T2{yr[ma], yi[ma]};
     }
@@ -559,55 +567,83 @@ __device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict
                 const T2 t = red[(v * JD + ma) * 32 + lane];
                 yr += t.x; yi += t.y;
             }
-        const T2 u = Us[(idxu_block(J) + k) * 32 + lane];
-        const double wgt = (2 * rmb < J) ? 1.0 : (ma < rmb ? 1.0 : (ma == rmb ? 0.5 : 0.0));
-        e += wgt * ((double)u.x * (double)yr + (double)u.y * (double)yi);
+        if constexpr (!PA) {
+            const T2 u = Us[(idxu_block(J) + k) * 32 + lane];
+            const double wgt = (2 * rmb < J) ? 1.0 : (ma < rmb ? 1.0 : (ma == rmb ? 0.5 : 0.0));
+            e += wgt * ((double)u.x * (double)yr + (double)u.y * (double)yi);
+        }
         dst[(yh_block(J) + k) * 32 + lane] = T2{yr, yi};
     }
     __syncthreads();
 }
 
-template <typename T, int TJ, int NW, int J>
+template <typename T, int TJ, int NW, bool PA, int J>
 __device__ __forceinline__ void y_all(const typename cplx<T>::type *__restrict__ Us,
                                       typename cplx<T>::type *__restrict__ red,
                                       typename cplx<T>::type *__restrict__ dst, const int lane, const int w,
-                                      const YParams<T> &P, double &e)
+                                      const YParams<T> &P, const T *__restrict__ Gs, double &e)
 {
     if constexpr (J >= 0) {
-        y_layer<T, TJ, NW, J>(Us, red, dst, lane, w, P, e);
-        y_all<T, TJ, NW, J - 1>(Us, red, dst, lane, w, P, e);
+        y_layer<T, TJ, NW, PA, J>(Us, red, dst, lane, w, P, Gs, e);
+        y_all<T, TJ, NW, PA, J - 1>(Us, red, dst, lane, w, P, Gs, e);
     }
 }
 
-template <typename T, int TJ>
+// number of bispectrum components at 2J = TJ (triples j1 >= j2, j >= j1)
+__host__ __device__ constexpr int nbispec(int tj)
+{
+    int n = 0;
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= cmin(tj, j1 + j2); j += 2)
+                if (j >= j1) n++;
+    return n;
+}
+
+template <typename T, int TJ, bool PA = false>
 constexpr size_t yi_smem_bytes()
 {
     return (size_t)idxu_count(TJ) * 32 * sizeof(typename cplx<T>::type) +
-           (size_t)YiWarps<T>::n * JD * 32 * sizeof(typename cplx<T>::type) + YiWarps<T>::n * 32 * sizeof(double);
+           (size_t)YiWarps<T>::n * JD * 32 * sizeof(typename cplx<T>::type) + YiWarps<T>::n * 32 * sizeof(double) +
+           (PA ? (size_t)nbispec(TJ) * 32 * sizeof(T) : 0);
 }
 
 // Output Y in 32-atom tiles: Y[tile][k][lane], k = half-plane index.
-template <typename T, int TJ>
+// PA: per-atom coefficients G[k * natoms + atom] (k over the nbispec(TJ)
+// components) instead of the model's; no energy is written.
+template <typename T, int TJ, bool PA = false>
 __global__ void __launch_bounds__(YiWarps<T>::n * 32, 1)
 k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __grid_constant__ YParams<T> P,
-          typename cplx<T>::type *__restrict__ Y, double *__restrict__ eatom)
+          typename cplx<T>::type *__restrict__ Y, double *__restrict__ eatom, const T *__restrict__ G = nullptr)
 {
     typedef typename cplx<T>::type T2;
     constexpr int NW = YiWarps<T>::n;
     constexpr int NU = idxu_count(TJ);
     constexpr int NYH = yh_count(TJ);
+    constexpr int NK = nbispec(TJ);
     extern __shared__ __align__(16) unsigned char smraw[];
     T2 *Us = reinterpret_cast<T2 *>(smraw);
     T2 *red = Us + NU * 32;                                // [warp][ma][lane]
     double *ered = reinterpret_cast<double *>(red + NW * JD * 32);
+    T *Gs = reinterpret_cast<T *>(ered + NW * 32);         // [k][lane] (PA)
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int ntiles = (natoms + 31) >> 5;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const T2 *src = Ut + (size_t)tile * NU * 32;
         for (int k = threadIdx.x; k < NU * 32; k += NW * 32) Us[k] = src[k];
+        if constexpr (PA) {
+            for (int k = threadIdx.x; k < NK * 32; k += NW * 32) {
+                const int a = tile * 32 + (k & 31);
+                Gs[k] = (a < natoms) ? G[(size_t)(k >> 5) * natoms + a] : T(0);
+            }
+        }
         __syncthreads();
         double e = 0.0;
-        y_all<T, TJ, NW, TJ>(Us, red, Y + (size_t)tile * NYH * 32, lane, w, P, e);
+        y_all<T, TJ, NW, PA, TJ>(Us, red, Y + (size_t)tile * NYH * 32, lane, w, P, Gs, e);
+        if constexpr (PA) {
+            __syncthreads();
+            continue;
+        }
         ered[w * 32 + lane] = e;
         __syncthreads();
         const int atom = tile * 32 + lane;

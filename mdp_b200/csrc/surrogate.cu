@@ -1,0 +1,593 @@
+// Learned surrogate of the SNAP energy: an MLP on per-atom 2J=4 bispectra.
+//
+// There is no counterpart in MDP.  The network is E_i = e_mu + e_sd * y(x_i),
+// x_i = (B_i - mu) * sinv (the 14 components of the 2J=4 bispectrum of atom
+// i, cpuSnap4.cpp:427-592 ordering), y = w3 . silu(W2 silu(W1 x + b1) + b2) + b3
+// with 64 hidden units per layer.  Forward passes use the weights rounded to
+// BF16; sums are FP32.  The master weights, gradients and Adam moments are FP32.
+//
+// Forces: E_i depends on the positions only through U_i, so
+//   dE/dr = sum_i sum_k (dE_i/dB_ik) dB_ik/dr,
+// which is the linear-SNAP force with per-atom coefficients G_ik = dE_i/dB_ik:
+// the inference kernel writes G, the Y kernel takes it in place of beta (its
+// per-atom mode) and the dE/dr and tally kernels run unchanged at 2J=4.
+#include "common.cuh"
+#include "engine.h"
+#include "surrogate.h"
+
+#include <cuda_bf16.h>
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <vector>
+
+namespace mdp {
+
+// ---------------------------------------------------------------------------
+// network arithmetic
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sur_sigmoid(float z) { return 1.0f / (1.0f + __expf(-z)); }
+__device__ __forceinline__ float sur_silu(float z) { return z * sur_sigmoid(z); }
+__device__ __forceinline__ float sur_dsilu(float z)
+{
+    const float s = sur_sigmoid(z);
+    return s * (1.0f + z * (1.0f - s));
+}
+
+// forward of one sample: z1, a1 = silu(z1), z2 and y; W points at the
+// (BF16-rounded) parameter block in shared memory
+__device__ __forceinline__ float mlp_forward(const float *__restrict__ W, const float (&x)[SUR_KP], float (&z1)[SUR_H],
+                                             float (&a1)[SUR_H], float (&z2)[SUR_H])
+{
+#pragma unroll 4
+    for (int r = 0; r < SUR_H; r++) {
+        float s = W[SUR_OFF_B1 + r];
+#pragma unroll
+        for (int k = 0; k < SUR_NK; k++) s += W[SUR_OFF_W1 + r * SUR_KP + k] * x[k];
+        z1[r] = s;
+        a1[r] = sur_silu(s);
+    }
+    float y = W[SUR_OFF_B3];
+#pragma unroll 2
+    for (int c = 0; c < SUR_H; c++) {
+        float s = W[SUR_OFF_B2 + c];
+#pragma unroll
+        for (int r = 0; r < SUR_H; r++) s += W[SUR_OFF_W2 + c * SUR_H + r] * a1[r];
+        z2[c] = s;
+        y += W[SUR_OFF_W3 + c] * sur_silu(s);
+    }
+    return y;
+}
+
+// dy/dz1 given z1, z2 (g1 out), via dy/dz2 = w3 * silu'(z2)
+__device__ __forceinline__ void mlp_backward_z1(const float *__restrict__ W, const float (&z1)[SUR_H],
+                                                float (&z2g)[SUR_H], float (&g1)[SUR_H])
+{
+#pragma unroll
+    for (int c = 0; c < SUR_H; c++) z2g[c] = W[SUR_OFF_W3 + c] * sur_dsilu(z2g[c]);
+#pragma unroll 4
+    for (int r = 0; r < SUR_H; r++) {
+        float s = 0.f;
+#pragma unroll
+        for (int c = 0; c < SUR_H; c++) s += W[SUR_OFF_W2 + c * SUR_H + r] * z2g[c];
+        g1[r] = s * sur_dsilu(z1[r]);
+    }
+}
+
+// BF16 rounding of the weights used by every forward pass (biases stay FP32)
+__host__ __device__ inline bool sur_is_weight(int i)
+{
+    return (i >= SUR_OFF_W1 && i < SUR_OFF_B1) || (i >= SUR_OFF_W2 && i < SUR_OFF_B2) ||
+           (i >= SUR_OFF_W3 && i < SUR_OFF_B3);
+}
+
+__global__ void k_sur_round(const float *__restrict__ P, float *__restrict__ Pb)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < SUR_NPAR) Pb[i] = sur_is_weight(i) ? __bfloat162float(__float2bfloat16_rn(P[i])) : P[i];
+}
+
+// ---------------------------------------------------------------------------
+// inference: per-atom energy and G = dE_i/dB_i for B in [k * bstride + atom]
+// ---------------------------------------------------------------------------
+constexpr int SUR_INF_THREADS = 128;
+
+__global__ void __launch_bounds__(SUR_INF_THREADS)
+k_sur_infer(const double *__restrict__ B, long bstride, int n, const float *__restrict__ Pb, const SurNorm nrm,
+            double *__restrict__ eatom, float *__restrict__ G)
+{
+    __shared__ float W[SUR_NPAR];
+    for (int i = threadIdx.x; i < SUR_NPAR; i += blockDim.x) W[i] = Pb[i];
+    __syncthreads();
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        float x[SUR_KP];
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) x[k] = k < SUR_NK ? (float)((B[(size_t)k * bstride + a] - nrm.mu[k]) * nrm.sinv[k]) : 0.f;
+        float z1[SUR_H], a1[SUR_H], z2[SUR_H], g1[SUR_H];
+        const float y = mlp_forward(W, x, z1, a1, z2);
+        mlp_backward_z1(W, z1, z2, g1);
+        if (eatom) eatom[a] = (double)nrm.e_mu + (double)nrm.e_sd * (double)y;
+#pragma unroll
+        for (int k = 0; k < SUR_NK; k++) {
+            float s = 0.f;
+#pragma unroll 8
+            for (int r = 0; r < SUR_H; r++) s += W[SUR_OFF_W1 + r * SUR_KP + k] * g1[r];
+            G[(size_t)k * n + a] = s * (float)(nrm.sinv[k] * nrm.e_sd);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// training gradient of the energy loss L = mean_s (y_s - t_s)^2, t = (E - e_mu)/e_sd
+// One sample per thread; the block's per-sample vectors go to shared memory
+// and each thread then sums one output row of dW1/dW2 over the block's samples,
+// so global memory sees one atomic add per parameter per block.
+// ---------------------------------------------------------------------------
+constexpr int SUR_TR_THREADS = 64;
+constexpr size_t SUR_TR_SMEM =
+    sizeof(float) * (SUR_NPAR + SUR_TR_THREADS * (SUR_KP + 1) + 4 * SUR_TR_THREADS * (SUR_H + 1) + SUR_TR_THREADS);
+
+__global__ void __launch_bounds__(SUR_TR_THREADS)
+k_sur_grad(const float *__restrict__ X, const float *__restrict__ E, const int *__restrict__ idx, int nb,
+           const float *__restrict__ Pb, const SurNorm nrm, float *__restrict__ grad, float *__restrict__ loss)
+{
+    extern __shared__ float sur_sm[];
+    float *W = sur_sm;
+    typedef float RowK[SUR_KP + 1];
+    typedef float RowH[SUR_H + 1];
+    RowK *sx = reinterpret_cast<RowK *>(W + SUR_NPAR);
+    RowH *sa1 = reinterpret_cast<RowH *>(sx + SUR_TR_THREADS);
+    RowH *sg1 = sa1 + SUR_TR_THREADS;
+    RowH *sa2 = sg1 + SUR_TR_THREADS;
+    RowH *sg2 = sa2 + SUR_TR_THREADS;
+    float *sdy = reinterpret_cast<float *>(sg2 + SUR_TR_THREADS);
+    for (int i = threadIdx.x; i < SUR_NPAR; i += blockDim.x) W[i] = Pb[i];
+    __syncthreads();
+    const int t = threadIdx.x;
+    const int s = blockIdx.x * SUR_TR_THREADS + t;
+    float x[SUR_KP];
+    float z1[SUR_H], a1[SUR_H], z2[SUR_H], g1[SUR_H];
+    float dy = 0.f;
+    if (s < nb) {
+        const int row = idx[s];
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) x[k] = k < SUR_NK ? (X[(size_t)row * SUR_KP + k] - nrm.mu[k]) * nrm.sinv[k] : 0.f;
+        const float y = mlp_forward(W, x, z1, a1, z2);
+        const float r = y - (E[row] - nrm.e_mu) / nrm.e_sd;
+        dy = 2.0f * r / (float)nb;
+        atomicAdd(loss, r * r / (float)nb);
+#pragma unroll
+        for (int c = 0; c < SUR_H; c++) sa2[t][c] = sur_silu(z2[c]);
+        mlp_backward_z1(W, z1, z2, g1);   // z2 <- w3 * silu'(z2), g1 = dy/dz1 per unit dy
+#pragma unroll
+        for (int c = 0; c < SUR_H; c++) { sg2[t][c] = dy * z2[c]; sg1[t][c] = dy * g1[c]; sa1[t][c] = a1[c]; }
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) sx[t][k] = x[k];
+    } else {
+#pragma unroll
+        for (int c = 0; c < SUR_H; c++) { sg2[t][c] = 0.f; sg1[t][c] = 0.f; sa1[t][c] = 0.f; sa2[t][c] = 0.f; }
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) sx[t][k] = 0.f;
+    }
+    sdy[t] = dy;
+    __syncthreads();
+    const int ns = min(SUR_TR_THREADS, nb - blockIdx.x * SUR_TR_THREADS);
+    // row t of every weight matrix (SUR_H == SUR_TR_THREADS)
+    {
+        float w2[SUR_H];
+#pragma unroll
+        for (int r = 0; r < SUR_H; r++) w2[r] = 0.f;
+        float b2 = 0.f, w3 = 0.f, b1 = 0.f, w1[SUR_KP];
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) w1[k] = 0.f;
+        for (int q = 0; q < ns; q++) {
+            const float g2 = sg2[q][t], gg1 = sg1[q][t];
+#pragma unroll
+            for (int r = 0; r < SUR_H; r++) w2[r] += g2 * sa1[q][r];
+            b2 += g2;
+            w3 += sdy[q] * sa2[q][t];
+            b1 += gg1;
+#pragma unroll
+            for (int k = 0; k < SUR_KP; k++) w1[k] += gg1 * sx[q][k];
+        }
+#pragma unroll
+        for (int r = 0; r < SUR_H; r++) atomicAdd(&grad[SUR_OFF_W2 + t * SUR_H + r], w2[r]);
+#pragma unroll
+        for (int k = 0; k < SUR_NK; k++) atomicAdd(&grad[SUR_OFF_W1 + t * SUR_KP + k], w1[k]);
+        atomicAdd(&grad[SUR_OFF_B2 + t], b2);
+        atomicAdd(&grad[SUR_OFF_W3 + t], w3);
+        atomicAdd(&grad[SUR_OFF_B1 + t], b1);
+        if (t == 0) {
+            float b3 = 0.f;
+            for (int q = 0; q < ns; q++) b3 += sdy[q];
+            atomicAdd(&grad[SUR_OFF_B3], b3);
+        }
+    }
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master weights; also refreshes the
+// BF16-rounded copy and clears the gradient
+__global__ void k_sur_adam(float *__restrict__ P, float *__restrict__ Pb, float *__restrict__ grad,
+                           float *__restrict__ m1, float *__restrict__ m2, float lr, float b1, float b2, float eps,
+                           float c1, float c2)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= SUR_NPAR) return;
+    const float g = grad[i];
+    const float m = b1 * m1[i] + (1.f - b1) * g;
+    const float v = b2 * m2[i] + (1.f - b2) * g * g;
+    m1[i] = m;
+    m2[i] = v;
+    const float p = P[i] - lr * (m / c1) / (sqrtf(v / c2) + eps);
+    P[i] = p;
+    Pb[i] = sur_is_weight(i) ? __bfloat162float(__float2bfloat16_rn(p)) : p;
+    grad[i] = 0.f;
+}
+
+// minibatch rows: a counter-based hash of (seed, step, slot), uniform over the
+// dataset (sampling with replacement)
+__device__ __forceinline__ unsigned long long sur_mix(unsigned long long z)
+{
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+__global__ void k_sur_batch(int *__restrict__ idx, int nb, long n, unsigned long long seed, long long step)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < nb) idx[s] = (int)(sur_mix(seed ^ sur_mix((unsigned long long)step * 0x100000001ULL + s)) % (unsigned long long)n);
+}
+
+// dataset append: B [k * bstride + atom] (double) -> X [row][SUR_KP] (float), E
+__global__ void k_sur_append(const double *__restrict__ B, long bstride, const double *__restrict__ e, int n,
+                             float *__restrict__ X, float *__restrict__ E, long row0)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= n) return;
+#pragma unroll
+    for (int k = 0; k < SUR_KP; k++) X[(size_t)(row0 + a) * SUR_KP + k] = k < SUR_NK ? (float)B[(size_t)k * bstride + a] : 0.f;
+    E[row0 + a] = (float)e[a];
+}
+
+// per-component sums of the dataset for the normalisation (double accumulators)
+__global__ void k_sur_moments(const float *__restrict__ X, const float *__restrict__ E, long n, double *__restrict__ acc)
+{
+    double s[SUR_NK + 1], q[SUR_NK + 1];
+#pragma unroll
+    for (int k = 0; k <= SUR_NK; k++) { s[k] = 0.0; q[k] = 0.0; }
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < SUR_NK; k++) { const double v = X[r * SUR_KP + k]; s[k] += v; q[k] += v * v; }
+        const double v = E[r];
+        s[SUR_NK] += v; q[SUR_NK] += v * v;
+    }
+#pragma unroll
+    for (int k = 0; k <= SUR_NK; k++) {
+        double a = s[k], b = q[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) { a += __shfl_xor_sync(0xffffffffu, a, o); b += __shfl_xor_sync(0xffffffffu, b, o); }
+        if ((threadIdx.x & 31) == 0) { atomicAdd(&acc[k], a); atomicAdd(&acc[SUR_NK + 1 + k], b); }
+    }
+}
+
+// sum of squared force differences (for the judge) over n atoms
+__global__ void k_force_sqdiff(const double4 *__restrict__ a, const double4 *__restrict__ b, int n, double *out)
+{
+    double s = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double4 u = a[i], v = b[i];
+        const double dx = u.x - v.x, dy = u.y - v.y, dz = u.z - v.z;
+        s += dx * dx + dy * dy + dz * dz;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+int force_sq_diff(const double4 *a, const double4 *b, int n, double *dev_acc, double *host_out, cudaStream_t s)
+{
+    MDP_CUDA_TRY(cudaMemsetAsync(dev_acc, 0, sizeof(double), s));
+    k_force_sqdiff<<<std::min((n + 255) / 256, num_sms() * 8), 256, 0, s>>>(a, b, n, dev_acc);
+    count_launches(1);
+    MDP_CUDA_TRY(cudaMemcpyAsync(host_out, dev_acc, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(s));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+int launch_yi_pa_f4(const SnapModel &m, ForcePath &fp, int inum, const float *G, cudaStream_t s);
+int launch_bi_tiles_f32(const float2 *Ut, int natoms, int tj, int bnorm, int bzero, double *bout, long bstride,
+                        cudaStream_t s);
+
+int sur_features(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const int *nlist, const int *nnum, int nm,
+                 cudaStream_t s)
+{
+    const SnapModel &m = S.model;
+    const long ntiles = (inum + 31) / 32;
+    const long pair_cap = (long)inum * nm;
+    if (fp.pcount.ensure(sizeof(int) * (size_t)inum) || fp.poff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
+        fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
+        fp.pab.ensure(sizeof(double4) * (size_t)pair_cap) ||
+        fp.rslot.ensure(sizeof(double4) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)inum * nm) ||
+        fp.Ut.ensure(sizeof(float2) * (size_t)ntiles * m.nu * 32) ||
+        fp.Y.ensure(sizeof(float2) * (size_t)ntiles * 32 * m.nyh) ||
+        fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(inum)) || S.B.ensure(sizeof(double) * SUR_NK * (size_t)inum) ||
+        S.G.ensure(sizeof(float) * SUR_NK * (size_t)inum))
+        return -1;
+    const int tb = 256, gb = (inum + tb - 1) / tb;
+    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.rslot.as<double4>(), fp.pcount.as<int>());
+    if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
+    k_pair_emit<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), nnum, inum, nm, fp.poff.as<int>(), m.geom,
+                                  fp.prij.as<double4>(), fp.pinfo.as<int2>(), fp.pab.as<double4>());
+    count_launches(2);
+    if (launch_ui<float, 4>(m, fp, inum, s)) return -1;
+    count_launches(1);
+    return launch_bi_tiles_f32(fp.Ut.as<float2>(), inum, 4, m.p.bnormflag, m.p.bzeroflag, S.B.as<double>(), inum, s);
+}
+
+int sur_force(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const int *nlist, const int *nnum, int nm,
+              const int *roff, const long long *rlist, double *eatom, double4 *f, double *vatom, cudaStream_t s)
+{
+    if (!S.trained) { set_error("surrogate has no parameters"); return -1; }
+    if (fp.timing && !fp.ev[0])
+        for (auto &e : fp.ev) cudaEventCreate(&e);
+    if (fp.timing) cudaEventRecord(fp.ev[0], s);
+    if (sur_features(S, fp, x, inum, nlist, nnum, nm, s)) return -1;
+    k_sur_infer<<<std::min((inum + SUR_INF_THREADS - 1) / SUR_INF_THREADS, num_sms() * 8), SUR_INF_THREADS, 0, s>>>(
+        S.B.as<double>(), inum, inum, S.Pb.as<float>(), S.norm, eatom, S.G.as<float>());
+    if (launch_yi_pa_f4(S.model, fp, inum, S.G.as<float>(), s)) return -1;
+    if (launch_fi<float, 4>(S.model, fp, inum, nm, s)) return -1;
+    const int tb = 256, gb = (inum + tb - 1) / tb;
+    if (fp.timing) cudaEventRecord(fp.ev[4], s);
+    k_tally<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), fp.dE.as<double4>(), nnum, inum, nm, roff, rlist, f, vatom);
+    count_launches(4);
+    if (fp.timing) {
+        cudaEventRecord(fp.ev[5], s);
+        cudaEventSynchronize(fp.ev[5]);
+        float t[5], tot;
+        for (int k = 0; k < 5; k++) cudaEventElapsedTime(&t[k], fp.ev[k], fp.ev[k + 1]);
+        for (int k = 0; k < 5; k++) fp.stage_ms[k] += t[k];
+        cudaEventElapsedTime(&tot, fp.ev[0], fp.ev[5]);
+        fp.stage_ms[5] += tot;
+        fp.stage_calls++;
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace mdp
+
+using namespace mdp;
+
+extern "C" {
+
+int mdp_sur_create(mdp_sur **h, const mdp_snap_params *p4, int device)
+{
+    if (!h || !p4) { set_error("null argument"); return -1; }
+    *h = nullptr;
+    if (p4->twojmax != 4) { set_error("the surrogate's features are the 2J=4 bispectrum (twojmax must be 4)"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(device));
+    // coefficients of the feature model are all 1: the Y kernel's betaY then
+    // holds the multiplicity factors that multiply the per-atom coefficients
+    mdp_snap_params q = *p4;
+    std::vector<double> ones(1 + SUR_NK, 1.0);
+    ones[0] = 0.0;
+    q.coeff = ones.data();
+    q.ncoeffall = 1 + SUR_NK;
+    mdp_sur *S = new mdp_sur();
+    S->device = device;
+    if (model_init(S->model, &q)) { delete S; return -1; }
+    if (S->model.ncoeff != SUR_NK) { set_error("unexpected feature count"); delete S; return -1; }
+    if (S->P.ensure(sizeof(float) * SUR_NPAR) || S->Pb.ensure(sizeof(float) * SUR_NPAR) ||
+        S->grad.ensure(sizeof(float) * SUR_NPAR) || S->m1.ensure(sizeof(float) * SUR_NPAR) ||
+        S->m2.ensure(sizeof(float) * SUR_NPAR) || S->scal.ensure(sizeof(double) * 64)) {
+        mdp_sur_destroy(S);
+        return -1;
+    }
+    if (cudaFuncSetAttribute(k_sur_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUR_TR_SMEM) != cudaSuccess) {
+        set_error("k_sur_grad shared memory (%zu B) not available", SUR_TR_SMEM);
+        mdp_sur_destroy(S);
+        return -1;
+    }
+    for (int k = 0; k < SUR_KP; k++) { S->norm.mu[k] = 0.f; S->norm.sinv[k] = 1.f; }
+    S->norm.e_mu = 0.f;
+    S->norm.e_sd = 1.f;
+    *h = S;
+    return 0;
+}
+
+void mdp_sur_destroy(mdp_sur *S)
+{
+    if (!S) return;
+    cudaSetDevice(S->device);
+    cudaDeviceSynchronize();
+    DevBuf *b[] = {&S->P, &S->Pb, &S->grad, &S->m1, &S->m2, &S->X, &S->E, &S->idx, &S->scal, &S->B, &S->G};
+    for (auto x : b) x->release();
+    S->fp.release();
+    delete S;
+}
+
+int mdp_sur_set_params(mdp_sur *S, const float *params, const float *norm)
+{
+    if (!S || !params) { set_error("null argument"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    MDP_CUDA_TRY(cudaMemcpy(S->P.p, params, sizeof(float) * SUR_NPAR, cudaMemcpyHostToDevice));
+    k_sur_round<<<(SUR_NPAR + 255) / 256, 256>>>(S->P.as<float>(), S->Pb.as<float>());
+    count_launches(1);
+    MDP_CUDA_TRY(cudaMemset(S->grad.p, 0, sizeof(float) * SUR_NPAR));
+    MDP_CUDA_TRY(cudaMemset(S->m1.p, 0, sizeof(float) * SUR_NPAR));
+    MDP_CUDA_TRY(cudaMemset(S->m2.p, 0, sizeof(float) * SUR_NPAR));
+    S->adam_t = 0;
+    if (norm) {
+        for (int k = 0; k < SUR_NK; k++) { S->norm.mu[k] = norm[k]; S->norm.sinv[k] = norm[SUR_NK + k]; }
+        S->norm.e_mu = norm[2 * SUR_NK];
+        S->norm.e_sd = norm[2 * SUR_NK + 1];
+    }
+    S->trained = true;
+    MDP_CUDA_TRY(cudaDeviceSynchronize());
+    return 0;
+}
+
+int mdp_sur_get_params(mdp_sur *S, float *params, float *norm)
+{
+    if (!S) { set_error("null handle"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    if (params) MDP_CUDA_TRY(cudaMemcpy(params, S->P.p, sizeof(float) * SUR_NPAR, cudaMemcpyDeviceToHost));
+    if (norm) {
+        for (int k = 0; k < SUR_NK; k++) { norm[k] = S->norm.mu[k]; norm[SUR_NK + k] = S->norm.sinv[k]; }
+        norm[2 * SUR_NK] = S->norm.e_mu;
+        norm[2 * SUR_NK + 1] = S->norm.e_sd;
+    }
+    return 0;
+}
+
+int mdp_sur_dataset_reserve(mdp_sur *S, long rows)
+{
+    if (!S || rows < 1) { set_error("bad arguments"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    if (S->X.ensure(sizeof(float) * SUR_KP * (size_t)rows) || S->E.ensure(sizeof(float) * (size_t)rows)) return -1;
+    S->cap = rows;
+    S->rows = 0;
+    return 0;
+}
+
+long mdp_sur_dataset_size(mdp_sur *S) { return S ? S->rows : -1; }
+
+int mdp_sur_dataset_add(mdp_sur *S, const double *B_dev, long bstride, const double *e_dev, int n, void *stream)
+{
+    if (!S || !B_dev || !e_dev || n < 1) { set_error("bad arguments"); return -1; }
+    if (S->rows + n > S->cap) { set_error("dataset full (%ld of %ld rows)", S->rows, S->cap); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    k_sur_append<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(B_dev, bstride, e_dev, n, S->X.as<float>(),
+                                                                  S->E.as<float>(), S->rows);
+    count_launches(1);
+    MDP_CUDA_TRY(cudaGetLastError());
+    S->rows += n;
+    return 0;
+}
+
+int mdp_sur_dataset_copy(mdp_sur *S, float *X, float *E, long row0, long nrows)
+{
+    if (!S || row0 < 0 || row0 + nrows > S->rows) { set_error("bad range"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    if (X) MDP_CUDA_TRY(cudaMemcpy(X, S->X.as<float>() + row0 * SUR_KP, sizeof(float) * SUR_KP * nrows, cudaMemcpyDeviceToHost));
+    if (E) MDP_CUDA_TRY(cudaMemcpy(E, S->E.as<float>() + row0, sizeof(float) * nrows, cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int mdp_sur_dataset_load(mdp_sur *S, const float *X, const float *E, long nrows)
+{
+    if (!S || !X || !E || nrows < 1) { set_error("bad arguments"); return -1; }
+    if (mdp_sur_dataset_reserve(S, nrows)) return -1;
+    MDP_CUDA_TRY(cudaMemcpy(S->X.p, X, sizeof(float) * SUR_KP * nrows, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(S->E.p, E, sizeof(float) * nrows, cudaMemcpyHostToDevice));
+    S->rows = nrows;
+    return 0;
+}
+
+// mean / standard deviation of the features and of the energy over the dataset
+int mdp_sur_fit_normalization(mdp_sur *S)
+{
+    if (!S || S->rows < 2) { set_error("dataset too small"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    double *acc = S->scal.as<double>();
+    MDP_CUDA_TRY(cudaMemset(acc, 0, sizeof(double) * 2 * (SUR_NK + 1)));
+    k_sur_moments<<<num_sms() * 4, 256>>>(S->X.as<float>(), S->E.as<float>(), S->rows, acc);
+    count_launches(1);
+    double h[2 * (SUR_NK + 1)];
+    MDP_CUDA_TRY(cudaMemcpy(h, acc, sizeof(h), cudaMemcpyDeviceToHost));
+    const double n = (double)S->rows;
+    for (int k = 0; k <= SUR_NK; k++) {
+        const double mu = h[k] / n;
+        const double var = std::max(h[SUR_NK + 1 + k] / n - mu * mu, 0.0);
+        const double sd = var > 1e-24 ? sqrt(var) : 1.0;
+        if (k < SUR_NK) { S->norm.mu[k] = (float)mu; S->norm.sinv[k] = (float)(1.0 / sd); }
+        else { S->norm.e_mu = (float)mu; S->norm.e_sd = (float)sd; }
+    }
+    return 0;
+}
+
+// Adam steps on random minibatches; loss[i] = minibatch loss before step i
+int mdp_sur_train(mdp_sur *S, int steps, int batch, float lr, unsigned long long seed, float *loss)
+{
+    if (!S || steps < 1 || batch < 1) { set_error("bad arguments"); return -1; }
+    if (S->rows < 1) { set_error("empty dataset"); return -1; }
+    if (!S->trained) { set_error("set initial parameters first"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    if (S->idx.ensure(sizeof(int) * (size_t)batch)) return -1;
+    DevBuf lbuf;
+    if (lbuf.ensure(sizeof(float) * (size_t)steps)) return -1;
+    MDP_CUDA_TRY(cudaMemset(lbuf.p, 0, sizeof(float) * steps));
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int it = 0; it < steps; it++) {
+        S->adam_t++;
+        k_sur_batch<<<(batch + 255) / 256, 256>>>(S->idx.as<int>(), batch, S->rows, seed, S->adam_t);
+        k_sur_grad<<<(batch + SUR_TR_THREADS - 1) / SUR_TR_THREADS, SUR_TR_THREADS, SUR_TR_SMEM>>>(
+            S->X.as<float>(), S->E.as<float>(), S->idx.as<int>(), batch, S->Pb.as<float>(), S->norm,
+            S->grad.as<float>(), lbuf.as<float>() + it);
+        const float c1 = 1.f - powf(b1, (float)S->adam_t), c2 = 1.f - powf(b2, (float)S->adam_t);
+        k_sur_adam<<<(SUR_NPAR + 255) / 256, 256>>>(S->P.as<float>(), S->Pb.as<float>(), S->grad.as<float>(),
+                                                    S->m1.as<float>(), S->m2.as<float>(), lr, b1, b2, eps, c1, c2);
+        count_launches(3);
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    if (loss) MDP_CUDA_TRY(cudaMemcpy(loss, lbuf.p, sizeof(float) * steps, cudaMemcpyDeviceToHost));
+    lbuf.release();
+    return 0;
+}
+
+// gradient of the minibatch loss over the given host rows (X [n][16], E [n])
+// at the current parameters, without updating them
+int mdp_sur_grad(mdp_sur *S, const float *X, const float *E, int n, float *grad, float *loss)
+{
+    if (!S || !X || !E || n < 1 || !grad) { set_error("bad arguments"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    DevBuf dx, de, di, dl;
+    std::vector<int> id(n);
+    for (int i = 0; i < n; i++) id[i] = i;
+    if (dx.ensure(sizeof(float) * SUR_KP * (size_t)n) || de.ensure(sizeof(float) * (size_t)n) ||
+        di.ensure(sizeof(int) * (size_t)n) || dl.ensure(sizeof(float)))
+        return -1;
+    MDP_CUDA_TRY(cudaMemcpy(dx.p, X, sizeof(float) * SUR_KP * n, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(de.p, E, sizeof(float) * n, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(di.p, id.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemset(dl.p, 0, sizeof(float)));
+    MDP_CUDA_TRY(cudaMemset(S->grad.p, 0, sizeof(float) * SUR_NPAR));
+    k_sur_grad<<<(n + SUR_TR_THREADS - 1) / SUR_TR_THREADS, SUR_TR_THREADS, SUR_TR_SMEM>>>(
+        dx.as<float>(), de.as<float>(), di.as<int>(), n, S->Pb.as<float>(), S->norm, S->grad.as<float>(), dl.as<float>());
+    count_launches(1);
+    MDP_CUDA_TRY(cudaGetLastError());
+    MDP_CUDA_TRY(cudaMemcpy(grad, S->grad.p, sizeof(float) * SUR_NPAR, cudaMemcpyDeviceToHost));
+    if (loss) MDP_CUDA_TRY(cudaMemcpy(loss, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+    MDP_CUDA_TRY(cudaMemset(S->grad.p, 0, sizeof(float) * SUR_NPAR));
+    dx.release(); de.release(); di.release(); dl.release();
+    return 0;
+}
+
+// inference on host features B [k * n + atom] (double): energies and G [k * n + atom]
+int mdp_sur_eval(mdp_sur *S, const double *B, int n, double *E, float *G)
+{
+    if (!S || !B || n < 1) { set_error("bad arguments"); return -1; }
+    if (!S->trained) { set_error("surrogate has no parameters"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    DevBuf db, de, dg;
+    if (db.ensure(sizeof(double) * SUR_NK * (size_t)n) || de.ensure(sizeof(double) * (size_t)n) ||
+        dg.ensure(sizeof(float) * SUR_NK * (size_t)n))
+        return -1;
+    MDP_CUDA_TRY(cudaMemcpy(db.p, B, sizeof(double) * SUR_NK * n, cudaMemcpyHostToDevice));
+    k_sur_infer<<<(n + SUR_INF_THREADS - 1) / SUR_INF_THREADS, SUR_INF_THREADS>>>(
+        db.as<double>(), n, n, S->Pb.as<float>(), S->norm, de.as<double>(), dg.as<float>());
+    count_launches(1);
+    MDP_CUDA_TRY(cudaGetLastError());
+    if (E) MDP_CUDA_TRY(cudaMemcpy(E, de.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    if (G) MDP_CUDA_TRY(cudaMemcpy(G, dg.p, sizeof(float) * SUR_NK * n, cudaMemcpyDeviceToHost));
+    db.release(); de.release(); dg.release();
+    return 0;
+}
+
+int mdp_sur_nparams(void) { return SUR_NPAR; }
+
+}  // extern "C"

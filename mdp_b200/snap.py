@@ -141,6 +141,21 @@ class SnapMD:
         return dict(steps=int(out[0]), rebuilds=int(out[1]), pairs=int(out[2]), ghosts=int(out[3]),
                     neighbors=int(out[4]))
 
+    def set_surrogate(self, sur, judge_every: int = 50, tol: float = 0.05):
+        """Drive the forces by a trained surrogate (None: the plain model), judged
+        every judge_every steps against the plain model with force-RMSE tolerance tol."""
+        _lib.check(_lib.lib().mdp_md_set_surrogate(self._h, None if sur is None else sur.handle, int(judge_every),
+                                                   float(tol)), "mdp_md_set_surrogate")
+
+    def surrogate_status(self, cap: int = 4096) -> dict:
+        act = C.c_int(0); fb = C.c_longlong(-1); nj = C.c_int(0)
+        log = np.zeros(2 * cap)
+        _lib.check(_lib.lib().mdp_md_surrogate_status(self._h, C.byref(act), C.byref(fb), C.byref(nj),
+                                                      log.ctypes.data, cap), "mdp_md_surrogate_status")
+        k = min(nj.value, cap)
+        return dict(active=bool(act.value), fallback_step=int(fb.value), judgements=int(nj.value),
+                    log=log[: 2 * k].reshape(k, 2))
+
     def stage_timing(self, enable: bool):
         _lib.check(_lib.lib().mdp_md_stage_timing(self._h, int(enable)), "mdp_md_stage_timing")
 
