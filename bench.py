@@ -205,6 +205,56 @@ def build_md(precision, device):
     return md, cfg
 
 
+def surrogate_leg(args, dev, barrier, ws):
+    """Form (4): MLP on 2J=4 bispectra trained on plain 2J=8 MD snapshots, then NVE
+    on the 2M-atom box at 1,000 K with the plain model judging every 50 steps."""
+    from mdp_b200 import configs, surrogate as su
+    from mdp_b200.snap import SnapMD
+    p8 = configs.snap_params(TWOJ, seed=2024)
+    ts = su.TrainingSet(snapshots=args.sur_snapshots, cells=(10, 10, 10), every=5)
+    sur, info = su.train_default(p8, ts, steps=args.sur_train_steps, batch=8192, lr=2e-3, seed=1, device=dev,
+                                 log=lambda m: print(m, file=sys.stderr))
+    errs = su.force_errors(p8, sur, info["lin_coeff"], cells=(10, 10, 10), temp=1000.0, seed=4242, device=dev)
+    cfg = configs.ta_config(CELLS, temp=1000.0, jitter=0.05 * np.sqrt(1000.0 / 300.0), seed=2025 + dev)
+    n = cfg.natoms
+    out = {"unit": "atom-steps/s", "workload": "NVE, BCC Ta 2,000,000 atoms at 1,000 K, dt 1 fs",
+           "features": "2J=4 bispectrum (14)", "network": "14-64-64-1 SiLU, BF16 weights, FP32 sums",
+           "training": {"snapshots": ts.snapshots, "atoms_per_snapshot": 2000, "rows": info["rows"],
+                        "temps_K": list(ts.temps), "adam_steps": args.sur_train_steps, "batch": 8192,
+                        "loss_first": info["loss_first"], "loss_last": info["loss_last"],
+                        "generate_s": info["gen_s"], "train_s": info["train_s"]},
+           "heldout_2000_atoms_1000K": errs}
+    for mode, judge in (("unjudged", 0), ("judged", 50)):
+        md = SnapMD(p8, cfg.box, n, DT, skin=SKIN, neighmax=96, precision="fp64", device=dev)
+        md.set_surrogate(sur, judge_every=judge, tol=0.05)
+        md.set_state(cfg.x, cfg.v)
+        md.setup()
+        md.run(args.warmup)
+        barrier()
+        _, ms = md.run(args.steps)
+        barrier()
+        st = md.surrogate_status()
+        md.close()
+        if ws > 1:
+            import torch
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        v = ws * n * args.steps / (ms * 1e-3)
+        if mode == "judged":
+            out["value"] = v
+            out["judge_every"] = 50
+            out["tolerance_eV_per_A"] = 0.05
+            out["judgements"] = st["judgements"]
+            out["judge_log"] = st["log"].tolist()
+            out["force_rmse_vs_fp64"] = float(st["log"][0, 1]) if st["judgements"] else None
+            out["fallback_step"] = st["fallback_step"]
+        else:
+            out["unjudged_value"] = v
+    sur.close()
+    return out
+
+
 def run_ours(args):
     import torch
     ws, rank, local = dist_env()
@@ -294,6 +344,10 @@ def run_ours(args):
         ms32 = float(t.item())
     value32 = ws * n * args.steps / (ms32 * 1e-3)
 
+    sur_line = None
+    if not args.no_surrogate:
+        sur_line = surrogate_leg(args, dev, barrier, ws)
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         try:
@@ -333,6 +387,7 @@ def run_ours(args):
             "fp32": {"value": value32, "unit": "atom-steps/s", "speedup_vs_fp64": value32 / value,
                      "force_rmse_vs_fp64": fp32_rmse, "force_maxerr_vs_fp64": fp32_max, "unit_err": "eV/A",
                      "fp32_fma_peak_tflops": fp32_peak},
+            "surrogate": sur_line,
             "clocks": clk,
             "cpu_baseline": cpu,
         }
@@ -348,6 +403,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate leg")
+    ap.add_argument("--sur-snapshots", type=int, default=20000, help="2,000-atom MD snapshots to train on")
+    ap.add_argument("--sur-train-steps", type=int, default=20000)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

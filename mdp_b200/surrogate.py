@@ -169,26 +169,138 @@ class TrainingSet:
     snapshots: int = 20000          # total, split evenly over the temperatures
     cells: tuple = (10, 10, 10)     # 2,000 BCC atoms
     every: int = 10                 # MD steps between snapshots
+    segment: int = 100              # snapshots per trajectory before a fresh start
     equilibrate: int = 50
     dt: float = 0.001
     seed: int = 7
+    neighmax: int = 128             # hot snapshots crowd more atoms into rcut + skin
 
 
 def generate(sur: Surrogate, p8: SnapParams, ts: TrainingSet, precision: str = "fp64", device: int = 0) -> int:
-    """Runs plain 2J=8 SNAP MD at each temperature and appends snapshots to sur's set."""
+    """Runs plain 2J=8 SNAP MD at each temperature and appends snapshots to sur's set.
+
+    Each temperature's snapshots come from short trajectories (ts.segment
+    snapshots each) restarted from a freshly jittered lattice with new
+    velocities: the seeded-coefficient potential has no repulsive core, so one
+    long hot trajectory drifts into collapsed configurations no deployment
+    visits."""
     from .snap import SnapMD
     per = max(1, ts.snapshots // len(ts.temps))
     natoms = 2 * int(np.prod(ts.cells))
     sur.reserve(per * len(ts.temps) * natoms)
     for it, T in enumerate(ts.temps):
-        # displacement scale grows with temperature so hot snapshots start disordered
-        cfg = ta_config(ts.cells, temp=T, jitter=0.05 * np.sqrt(T / 300.0), seed=ts.seed + it)
-        md = SnapMD(p8, cfg.box, cfg.natoms, ts.dt, mass=TA_MASS, precision=precision, device=device)
-        md.set_state(cfg.x, cfg.v)
-        md.setup()
-        md.run(ts.equilibrate)
-        for _ in range(per):
-            md.run(ts.every)
-            sur.sample(md)
+        done, seg = 0, 0
+        md = None
+        while done < per:
+            # displacement scale grows with temperature so hot snapshots start disordered
+            cfg = ta_config(ts.cells, temp=T, jitter=0.05 * np.sqrt(T / 300.0), seed=ts.seed + 1000 * it + seg)
+            if md is None:
+                md = SnapMD(p8, cfg.box, cfg.natoms, ts.dt, mass=TA_MASS, precision=precision, device=device,
+                            neighmax=ts.neighmax)
+            md.set_state(cfg.x, cfg.v)
+            md.setup()
+            md.run(ts.equilibrate)
+            for _ in range(min(ts.segment, per - done)):
+                md.run(ts.every)
+                sur.sample(md)
+                done += 1
+            seg += 1
         md.close()
     return sur.size()
+
+
+def linear_fit(X: np.ndarray, E: np.ndarray) -> np.ndarray:
+    """Least-squares linear SNAP on the same features: E_i ~ c0 + c . B_i (the
+    model the surrogate is compared against); returns the 15 coefficients."""
+    A = np.hstack([np.ones((X.shape[0], 1)), X[:, :NK].astype(np.float64)])
+    c, *_ = np.linalg.lstsq(A, E.astype(np.float64), rcond=None)
+    return c
+
+
+def force_errors(p8: SnapParams, sur: Surrogate | None, lin_coeff: np.ndarray | None, cells=(10, 10, 10),
+                 temp: float = 1000.0, seed: int = 99, precision: str = "fp64", device: int = 0) -> dict:
+    """Force and per-atom energy RMSE against plain 2J=8 SNAP on one configuration,
+    for the surrogate and for the linear 2J=4 fit."""
+    from .snap import SnapMD
+    cfg = ta_config(cells, temp=temp, jitter=0.05 * np.sqrt(temp / 300.0), seed=seed)
+    out = {}
+    md = SnapMD(p8, cfg.box, cfg.natoms, 0.001, precision=precision, device=device, neighmax=128)
+    md.set_state(cfg.x, cfg.v)
+    md.setup()
+    _, _, f8, e8 = md.state()
+    out["force_rms_2j8"] = float(np.sqrt(np.mean(f8 ** 2)))
+    if sur is not None:
+        md.set_surrogate(sur, judge_every=0)
+        md.set_state(cfg.x, cfg.v)
+        md.setup()
+        _, _, fs, es = md.state()
+        out["surrogate_force_rmse"] = float(np.sqrt(np.mean((fs - f8) ** 2)))
+        out["surrogate_energy_rmse"] = float(np.sqrt(np.mean((es - e8) ** 2)))
+    md.close()
+    if lin_coeff is not None:
+        p4 = dataclasses.replace(sur.params4 if sur is not None else snap_params(4, seed=0), coeff=np.asarray(lin_coeff))
+        m4 = SnapMD(p4, cfg.box, cfg.natoms, 0.001, precision="fp64", device=device, neighmax=128)
+        m4.set_state(cfg.x, cfg.v)
+        m4.setup()
+        _, _, fl, el = m4.state()
+        out["linear_force_rmse"] = float(np.sqrt(np.mean((fl - f8) ** 2)))
+        out["linear_energy_rmse"] = float(np.sqrt(np.mean((el - e8) ** 2)))
+        m4.close()
+    return out
+
+
+def train_default(p8: SnapParams, ts: TrainingSet, steps: int = 20000, batch: int = 8192, lr: float = 2e-3,
+                  seed: int = 1, device: int = 0, log=print) -> tuple[Surrogate, dict]:
+    """Generate the training set, fit the normalisation and train with Adam
+    (learning rate decayed 10x over the last half of the steps)."""
+    import time
+    sur = Surrogate(snap_params(4, seed=0), device=device)
+    t0 = time.time()
+    n = generate(sur, p8, ts, device=device)
+    t1 = time.time()
+    log(f"training set: {n} atoms from {ts.snapshots} snapshots in {t1 - t0:.1f} s")
+    sur.set_params(init_params(seed))
+    sur.fit_normalization()
+    P, norm = sur.params()
+    sur.set_params(P, norm)
+    losses = []
+    chunk = max(1, steps // 10)
+    for i in range(0, steps, chunk):
+        frac = i / steps
+        lri = lr if frac < 0.5 else lr * 10 ** (-(frac - 0.5) * 2)
+        losses.append(sur.train(min(chunk, steps - i), batch=batch, lr=lri, seed=seed + i))
+    loss = np.concatenate(losses)
+    t2 = time.time()
+    log(f"trained {steps} steps (batch {batch}) in {t2 - t1:.1f} s; loss {loss[:20].mean():.4f} -> {loss[-200:].mean():.4f}")
+    X, E = sur.dataset()
+    info = dict(rows=n, gen_s=t1 - t0, train_s=t2 - t1, loss_first=float(loss[:20].mean()),
+                loss_last=float(loss[-200:].mean()), lin_coeff=linear_fit(X, E))
+    return sur, info
+
+
+def main(argv=None):
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="train the 2J=4 MLP surrogate of 2J=8 SNAP on MD snapshots")
+    ap.add_argument("--snapshots", type=int, default=20000)
+    ap.add_argument("--cells", type=int, default=10, help="BCC cells per side of the snapshot box")
+    ap.add_argument("--every", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--coeff-seed", type=int, default=1, help="seed of the 2J=8 SNAP coefficients")
+    ap.add_argument("--out", default="surrogate_weights.npz")
+    a = ap.parse_args(argv)
+    p8 = snap_params(8, seed=a.coeff_seed)
+    ts = TrainingSet(snapshots=a.snapshots, cells=(a.cells,) * 3, every=a.every)
+    sur, info = train_default(p8, ts, steps=a.steps, batch=a.batch, lr=a.lr)
+    sur.save(a.out)
+    res = {}
+    for T in (300.0, 1000.0, 3000.0):
+        res[str(T)] = force_errors(p8, sur, info["lin_coeff"], cells=(a.cells,) * 3, temp=T)
+    info["lin_coeff"] = info["lin_coeff"].tolist()
+    print(json.dumps(dict(info=info, errors=res), indent=1))
+
+
+if __name__ == "__main__":
+    main()
