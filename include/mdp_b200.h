@@ -172,6 +172,36 @@ int mdp_md_set_surrogate(mdp_md *md, mdp_sur *s, int judge_every, double tol);
  * judgements, and up to cap (step, rmse) pairs */
 int mdp_md_surrogate_status(mdp_md *md, int *active, long long *fallback_step, int *njudge, double *log, int cap);
 
+/* ---------------------------------------------------------------------------
+ * Batched descriptors and linear-fit normal equations (ComputeSnap,
+ * snappotential.cpp:762-910, per configuration; assembly as Regression.cpp:
+ * 386-404).  A batch holds configurations of any atom counts, each in an
+ * orthogonal periodic box whose lengths exceed the cutoff.
+ * ------------------------------------------------------------------------- */
+typedef struct mdp_fit mdp_fit;
+
+/* p: SNAP hyper-parameters (twojmax 4, 6 or 8; coefficients unused) */
+int mdp_fit_create(mdp_fit **h, const mdp_snap_params *p, int device);
+void mdp_fit_destroy(mdp_fit *h);
+int mdp_fit_ncoeff(mdp_fit *h);
+/* natoms[c], box[3c..3c+2], x (3 per atom, all configurations concatenated);
+ * targets e[c], f (3 per atom) and weights we[c], wf[c] may be NULL */
+int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *box, const double *x,
+                      const double *e, const double *f, const double *we, const double *wf);
+long long mdp_fit_npairs(mdp_fit *h);
+/* bi [nconf][ncoeff]; bd [atom][3][ncoeff] with the reference's sign
+ * (cpuSnapTallyBispectrumDeriv: -d(sum_i B_i)/dx); bv [nconf][ncoeff][6];
+ * blist [ncoeff][atom].  Any output may be NULL. */
+int mdp_fit_descriptors(mdp_fit *h, double *bi, double *bd, double *bv, double *blist);
+/* A [64][64], b [64] of the normal equations over the whole batch: rows
+ * we*(N, bi) -> we*E per configuration and wf*(0, d(sum B)/dx_ic) -> -wf*f_ic
+ * per force component; mode 0 FP64, mode 1 BF16 hi/lo split with FP32 sums on
+ * tensor cores.  One CUDA graph per mode, captured once and replayed. */
+int mdp_fit_run(mdp_fit *h, int mode, double *A, double *b, float *elapsed_ms);
+/* time candidate launch shapes on the current batch and keep the fastest;
+ * out3 (may be NULL): du threads, dB/dR threads, Gram rows per CTA */
+int mdp_fit_tune(mdp_fit *h, int *out3);
+
 #ifdef __cplusplus
 }
 #endif

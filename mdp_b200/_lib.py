@@ -91,6 +91,18 @@ def lib():
     L.mdp_md_sur_sample.argtypes = [C.c_void_p, C.c_void_p]
     L.mdp_md_sur_features.argtypes = [C.c_void_p, C.c_void_p, _dp]
     L.mdp_md_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
+    _ip32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    L.mdp_fit_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(SnapParamsC), C.c_int]
+    L.mdp_fit_destroy.argtypes = [C.c_void_p]
+    L.mdp_fit_destroy.restype = None
+    L.mdp_fit_ncoeff.argtypes = [C.c_void_p]
+    L.mdp_fit_set_batch.argtypes = [C.c_void_p, C.c_int, _ip32, _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
+    L.mdp_fit_npairs.argtypes = [C.c_void_p]
+    L.mdp_fit_npairs.restype = C.c_longlong
+    L.mdp_fit_descriptors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mdp_fit_run.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(C.c_float)]
+    L.mdp_fit_tune.argtypes = [C.c_void_p, _ip32]
     L.mdp_md_surrogate_status.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong),
                                           C.POINTER(C.c_int), C.c_void_p, C.c_int]
     _lib = L

@@ -1,0 +1,1041 @@
+// Batched SNAP descriptors, dB/dR and the linear-fit normal equations.
+//
+// For a batch of periodic configurations (orthogonal boxes, every width at
+// least rcut + skin so that one shell of images holds every pair, as MDP's
+// cpuPeriodicImages3D assumes) this computes what MDP's ComputeSnap
+// (snappotential.cpp:762-910, cpuSnap2.cpp) computes per configuration:
+//   bi[k]          = sum_i B_ik
+//   G[i][c][k]     = d(sum_a B_ak)/dx_ic  (= -bd of cpuSnapTallyBispectrumDeriv)
+//   bv[k][6]       virial (cpuSnapTallyBispectrumVirial)
+// and assembles the normal equations of the linear fit as Regression.cpp:386-404
+// does with dd = G: rows r = [we * (N, bi)] (target we * E) and
+// [wf * (0, G[i][c])] (target -wf * f_ic), A = R^T R, b = R^T t.
+//
+// Pipeline (all on one stream, captured into one CUDA graph by mdp_fit_run):
+//   pairs (brute force over each configuration's atoms and 27 images)
+//   U      (k_snap_uc, the MD engine's kernel)
+//   Z, B   (k_fit_zb: every coupling's Z rows per atom, B for j >= j1)
+//   dU/dr  (k_fit_du: forward-mode, coefficient-free recursion, per pair and direction)
+//   dB/dr  (k_fit_dbdr: the three Z . dU terms of cpuComputeDbidrj:826-1013)
+//   rows   (k_fit_rows: atomic-free gather over own and reverse pairs)
+//   A, b   (k_fit_gram: FP64, or BF16 hi/lo split with FP32 tensor-core sums)
+#include "common.cuh"
+#include "engine.h"
+
+#include <cuda_bf16.h>
+#include <math.h>
+#include <string.h>
+#include <algorithm>
+#include <vector>
+
+namespace mdp {
+
+constexpr int FIT_KP = 64;       // row width: 1 + ncoeff (<= 56 at 2J=8) padded to 64
+constexpr int FIT_NCP = 256;     // couplings (j1 >= j2, j) at most (125 at 2J=8)
+constexpr int FIT_NT = 64;       // bispectrum triples at most (55 at 2J=8)
+
+struct FitCoupling {
+    int j1, j2, j, zoff;          // Z rows of this coupling start at zoff (per atom)
+};
+struct FitTriple {
+    int j1, j2, j;
+    int layer[3], coup[3];        // the three dB/dR terms: dU layer and Z coupling
+    double fac[3];
+};
+struct FitTables {
+    int ncoup, ntri, nz, tj, bnorm, bzero;
+    FitCoupling cp[FIT_NCP];
+    FitTriple tr[FIT_NT];
+};
+
+// ---------------------------------------------------------------------------
+// pairs: every atom against every atom of its configuration and the 27 images
+// ---------------------------------------------------------------------------
+template <bool EMIT>
+__global__ void k_fit_pairs(const double4 *__restrict__ x, const int *__restrict__ cfg, const int *__restrict__ ca0,
+                            const int *__restrict__ cn, const double4 *__restrict__ cbox, int natoms, SnapGeom gp,
+                            int *__restrict__ pcount, const int *__restrict__ poff, double4 *__restrict__ prij,
+                            double4 *__restrict__ pab, int2 *__restrict__ pinfo)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natoms) return;
+    const int c = cfg[i], a0 = ca0[c], n = cn[c];
+    const double4 L = cbox[c], xi = x[i];
+    int cnt = 0, p = EMIT ? poff[i] : 0;
+    for (int jj = 0; jj < n; jj++) {
+        const double4 xj = x[a0 + jj];
+        for (int im = 0; im < 27; im++) {
+            const double sx = (im % 3 - 1) * L.x, sy = ((im / 3) % 3 - 1) * L.y, sz = (im / 9 - 1) * L.z;
+            const double d0 = xj.x + sx - xi.x, d1 = xj.y + sy - xi.y, d2 = xj.z + sz - xi.z;
+            const double rsq = d0 * d0 + d1 * d1 + d2 * d2;
+            if (rsq < gp.rcutsq && rsq > 1e-20) {
+                if (EMIT) {
+                    PairGeo g;
+                    pair_geometry<false>(g, d0, d1, d2, gp);
+                    prij[p] = make_double4(d0, d1, d2, g.sfac);
+                    pab[p] = make_double4(g.ar, g.ai, g.br, g.bi);
+                    pinfo[p] = make_int2(i, a0 + jj);
+                    p++;
+                } else {
+                    cnt++;
+                }
+            }
+        }
+    }
+    if (!EMIT) pcount[i] = cnt;
+}
+
+// ---------------------------------------------------------------------------
+// Z rows of every coupling and B for j >= j1, per 32-atom tile (lane = atom)
+// Z layout [tile][zoff + (j+1) mb + ma][lane]; B layout [k][atom]
+// ---------------------------------------------------------------------------
+constexpr int FIT_ZB_WARPS = 8;
+
+__global__ void __launch_bounds__(FIT_ZB_WARPS * 32)
+k_fit_zb(const double2 *__restrict__ Ut, int natoms, const FitTables *__restrict__ T, double2 *__restrict__ Z,
+         double *__restrict__ B)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double2 *Us = reinterpret_cast<double2 *>(smraw);
+    const int tj = T->tj, nu = idxu_count(tj), nz = T->nz;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int ntiles = (natoms + 31) >> 5;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const double2 *src = Ut + (size_t)tile * nu * 32;
+        for (int k = threadIdx.x; k < nu * 32; k += blockDim.x) Us[k] = src[k];
+        __syncthreads();
+        double2 *Zt = Z + (size_t)tile * nz * 32 + lane;
+        // work items: (coupling, row mb)
+        int item = 0;
+        for (int c = 0; c < T->ncoup; c++) {
+            const FitCoupling cp = T->cp[c];
+            const int j1 = cp.j1, j2 = cp.j2, j = cp.j;
+            const int cgb = cg_block(j1, j2, j);
+            const double scale = T->bnorm ? 1.0 / (j + 1) : 1.0;
+            for (int mb = 0; 2 * mb <= j; mb++, item++) {
+                if (item % FIT_ZB_WARPS != w) continue;
+                const int mb1min = max(0, (2 * mb - j - j2 + j1) / 2);
+                const int mb2max = (2 * mb - j - (2 * mb1min - j1) + j2) / 2;
+                const int nb = min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
+                for (int ma = 0; ma <= j; ma++) {
+                    const int ma1min = max(0, (2 * ma - j - j2 + j1) / 2);
+                    const int ma2max = (2 * ma - j - (2 * ma1min - j1) + j2) / 2;
+                    const int na = min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
+                    double zr = 0.0, zi = 0.0;
+                    for (int ib = 0; ib < nb; ib++) {
+                        const int mb1 = mb1min + ib, mb2 = mb2max - ib;
+                        const double cb = cgc<double>(cgb + mb1 * (j2 + 1) + mb2);
+                        const double2 *r1 = Us + (idxu_block(j1) + (j1 + 1) * mb1) * 32 + lane;
+                        const double2 *r2 = Us + (idxu_block(j2) + (j2 + 1) * mb2) * 32 + lane;
+                        double sr = 0.0, si = 0.0;
+                        for (int ia = 0; ia < na; ia++) {
+                            const int ma1 = ma1min + ia, ma2 = ma2max - ia;
+                            const double ca = cgc<double>(cgb + ma1 * (j2 + 1) + ma2);
+                            const double2 u1 = r1[ma1 * 32], u2 = r2[ma2 * 32];
+                            sr += ca * (u1.x * u2.x - u1.y * u2.y);
+                            si += ca * (u1.x * u2.y + u1.y * u2.x);
+                        }
+                        zr += cb * sr;
+                        zi += cb * si;
+                    }
+                    Zt[(size_t)(cp.zoff + (j + 1) * mb + ma) * 32] = make_double2(zr * scale, zi * scale);
+                }
+            }
+        }
+        __syncthreads();
+        // B_k = 2 sum_half w Re(U_j* Z) (- bzero), cpuComputeBi2 (cpuSnap2.cpp:516-541)
+        const int atom = tile * 32 + lane;
+        for (int k = w; k < T->ntri; k += FIT_ZB_WARPS) {
+            const FitTriple tr = T->tr[k];
+            const int j = tr.j;
+            const FitCoupling cp = T->cp[tr.coup[0]];
+            double s = 0.0;
+            for (int mb = 0; 2 * mb <= j; mb++)
+                for (int ma = 0; ma <= j; ma++) {
+                    const double wgt = (2 * mb < j) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
+                    if (wgt == 0.0) continue;
+                    const double2 u = Us[(idxu_block(j) + (j + 1) * mb + ma) * 32 + lane];
+                    const double2 z = Zt[(size_t)(cp.zoff + (j + 1) * mb + ma) * 32];
+                    s += wgt * (u.x * z.x + u.y * z.y);
+                }
+            double b = 2.0 * s;
+            if (T->bzero) b -= T->bnorm ? 1.0 : (double)(j + 1);
+            if (atom < natoms) B[(size_t)k * natoms + atom] = b;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dU/dr of one pair along one axis, forward mode through the coefficient-free
+// recursion (v_J[ma] = conj(a) v[ma] - conj(b) v[ma-1], u = unorm v):
+//   dul[yh][t] = unorm * (dsfac u_dir v + sfac dv)   (ComputeSij's dulist)
+// t = pair * 3 + dir; the half plane in yh order (rows of a middle layer full)
+// ---------------------------------------------------------------------------
+template <int TJ, int J, int MB>
+__device__ __forceinline__ void fdu_row(const double ar, const double ai, const double br, const double bi,
+                                        const double dar, const double dai, const double dbr, const double dbi,
+                                        double (&pr)[TJ + 1], double (&pi)[TJ + 1], double (&qr)[TJ + 1],
+                                        double (&qi)[TJ + 1])
+{
+    {
+        const double vr = pr[J - 1], vi = pi[J - 1], wr = qr[J - 1], wi = qi[J - 1];
+        pr[J] = -(br * vr + bi * vi);
+        pi[J] = -(br * vi - bi * vr);
+        qr[J] = -(dbr * vr + dbi * vi + br * wr + bi * wi);
+        qi[J] = -(dbr * vi - dbi * vr + br * wi - bi * wr);
+    }
+#pragma unroll
+    for (int ma = J - 1; ma >= 0; ma--) {
+        const double ur = pr[ma], ui = pi[ma], xr = qr[ma], xi = qi[ma];
+        double nr = ar * ur + ai * ui, ni = ar * ui - ai * ur;
+        double mr = dar * ur + dai * ui + ar * xr + ai * xi, mi = dar * ui - dai * ur + ar * xi - ai * xr;
+        if (ma > 0) {
+            const double vr = pr[ma - 1], vi = pi[ma - 1], wr = qr[ma - 1], wi = qi[ma - 1];
+            nr -= br * vr + bi * vi;
+            ni -= br * vi - bi * vr;
+            mr -= dbr * vr + dbi * vi + br * wr + bi * wi;
+            mi -= dbr * vi - dbi * vr + br * wi - bi * wr;
+        }
+        pr[ma] = nr; pi[ma] = ni; qr[ma] = mr; qi[ma] = mi;
+    }
+    if constexpr (MB > 0 && J == 2 * MB) {
+#pragma unroll
+        for (int ma = 0; ma <= MB; ma++) {
+            const double s = (ma & 1) ? -1.0 : 1.0;
+            pr[MB + ma] = s * pr[MB - ma]; pi[MB + ma] = -s * pi[MB - ma];
+            qr[MB + ma] = s * qr[MB - ma]; qi[MB + ma] = -s * qi[MB - ma];
+        }
+    }
+}
+
+template <int TJ>
+struct FduState {
+    double ar, ai, br, bi, dar, dai, dbr, dbi, sf, dsu;
+    double pr[TJ + 1], pi[TJ + 1], qr[TJ + 1], qi[TJ + 1];   // current row and its derivative
+    double sr[TJ + 1], si[TJ + 1], tr[TJ + 1], ti[TJ + 1];   // next column's seed
+};
+
+template <int TJ, int J, int MB>
+__device__ __forceinline__ void fdu_column(FduState<TJ> &s, double2 *__restrict__ out, const long stride)
+{
+    if constexpr (J <= TJ) {
+        if constexpr (J > 0) fdu_row<TJ, J, MB>(s.ar, s.ai, s.br, s.bi, s.dar, s.dai, s.dbr, s.dbi, s.pr, s.pi, s.qr, s.qi);
+#pragma unroll
+        for (int ma = 0; ma <= J; ma++) {
+            const double nu = unorm<double>(J, MB, ma);
+            out[(long)(yh_block(J) + (J + 1) * MB + ma) * stride] =
+                make_double2(nu * (s.dsu * s.pr[ma] + s.sf * s.qr[ma]), nu * (s.dsu * s.pi[ma] + s.sf * s.qi[ma]));
+        }
+        if constexpr (J == 2 * MB + 1 && 2 * (MB + 1) <= TJ) {
+#pragma unroll
+            for (int ma = 0; ma <= J; ma++) {
+                const double sg = ((MB + ma) & 1) ? -1.0 : 1.0;
+                s.sr[J - ma] = sg * s.pr[ma]; s.si[J - ma] = -sg * s.pi[ma];
+                s.tr[J - ma] = sg * s.qr[ma]; s.ti[J - ma] = -sg * s.qi[ma];
+            }
+        }
+        fdu_column<TJ, J + 1, MB>(s, out, stride);
+    }
+}
+
+template <int TJ, int MB>
+__device__ __forceinline__ void fdu_columns(FduState<TJ> &s, double2 *__restrict__ out, const long stride)
+{
+    if constexpr (2 * MB <= TJ) {
+        if constexpr (MB == 0) {
+            s.pr[0] = 1.0; s.pi[0] = 0.0; s.qr[0] = 0.0; s.qi[0] = 0.0;
+        } else {
+#pragma unroll
+            for (int ma = 0; ma < 2 * MB; ma++) { s.pr[ma] = s.sr[ma]; s.pi[ma] = s.si[ma]; s.qr[ma] = s.tr[ma]; s.qi[ma] = s.ti[ma]; }
+        }
+        fdu_column<TJ, (MB == 0 ? 0 : 2 * MB), MB>(s, out, stride);
+        fdu_columns<TJ, MB + 1>(s, out, stride);
+    }
+}
+
+template <int TJ>
+__global__ void __launch_bounds__(128)
+k_fit_du(const double4 *__restrict__ prij, long npairs, SnapGeom gp, double2 *__restrict__ dul, long stride)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * npairs) return;
+    const long p = t / 3;
+    const int dir = (int)(t - 3 * p);
+    const double4 r = prij[p];
+    PairGeo g;
+    pair_geometry<true>(g, r.x, r.y, r.z, gp);
+    FduState<TJ> s;
+    s.ar = g.ar; s.ai = g.ai; s.br = g.br; s.bi = g.bi;
+    s.dar = g.dar[dir]; s.dai = g.dai[dir]; s.dbr = g.dbr[dir]; s.dbi = g.dbi[dir];
+    s.sf = g.sfac;
+    s.dsu = g.dsfac * g.u[dir];
+    fdu_columns<TJ, 0>(s, dul + t, stride);
+}
+
+// ---------------------------------------------------------------------------
+// dB_ik/dr_p along one axis: 2 sum over the three terms of cpuComputeDbidrj
+// (Z of the centre atom's couplings against the pair's dU rows), half plane
+// with the middle row's centre at 1/2.  dbdr[k * stride + t]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128)
+k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int2 *__restrict__ pinfo, long npairs,
+                           const FitTables *__restrict__ T, const double2 *__restrict__ Z, double *__restrict__ dbdr)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * npairs) return;
+    const int atom = pinfo[t / 3].x;
+    const int nz = T->nz;
+    const double2 *Zi = Z + (size_t)(atom >> 5) * nz * 32 + (atom & 31);
+    const double2 *d = dul + t;
+    for (int k = 0; k < T->ntri; k++) {
+        double acc = 0.0;
+        for (int q = 0; q < 3; q++) {
+            const int L = T->tr[k].layer[q];
+            const int zo = T->cp[T->tr[k].coup[q]].zoff, yo = yh_block(L);
+            double s = 0.0;
+            for (int mb = 0; 2 * mb <= L; mb++) {
+                const int mamax = (2 * mb < L) ? L : mb;
+                for (int ma = 0; ma <= mamax; ma++) {
+                    const double wgt = (2 * mb < L || ma < mb) ? 1.0 : 0.5;
+                    const int e = (L + 1) * mb + ma;
+                    const double2 du = d[(long)(yo + e) * stride];
+                    const double2 z = Zi[(size_t)(zo + e) * 32];
+                    s += wgt * (du.x * z.x + du.y * z.y);
+                }
+            }
+            acc += 2.0 * T->tr[k].fac[q] * s;
+        }
+        dbdr[(long)k * stride + t] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// reverse pairs (pairs whose neighbour is atom a), sorted for a fixed sum order
+// ---------------------------------------------------------------------------
+__global__ void k_fit_rev_count(const int2 *__restrict__ pinfo, long npairs, int *__restrict__ rcount)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < npairs) atomicAdd(&rcount[pinfo[p].y], 1);
+}
+__global__ void k_fit_rev_fill(const int2 *__restrict__ pinfo, long npairs, const int *__restrict__ roff,
+                               int *__restrict__ cursor, int *__restrict__ rlist)
+{
+    const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int a = pinfo[p].y;
+    rlist[roff[a] + atomicAdd(&cursor[a], 1)] = (int)p;
+}
+__global__ void k_fit_rev_sort(int natoms, const int *__restrict__ roff, int *__restrict__ rlist)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= natoms) return;
+    const int s = roff[a], e = roff[a + 1];
+    for (int i = s + 1; i < e; i++) {
+        const int v = rlist[i];
+        int j = i - 1;
+        while (j >= s && rlist[j] > v) { rlist[j + 1] = rlist[j]; j--; }
+        rlist[j + 1] = v;
+    }
+}
+
+// rows of atom a: G[a][c][k] = sum_(p: j = a) dbdr - sum_(p: i = a) dbdr,
+// written as fit rows [wf * (0, G)] with target -wf * f; row = 3 a + c
+__global__ void k_fit_rows(int natoms, int ntri, const int *__restrict__ poff, const int *__restrict__ roff,
+                           const int *__restrict__ rlist, const double *__restrict__ dbdr, long stride,
+                           const int *__restrict__ cfg, const double *__restrict__ wf, const double *__restrict__ f,
+                           double *__restrict__ G, double *__restrict__ R, double *__restrict__ tgt, long row0)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (atom, k)
+    if (t >= (long)natoms * FIT_KP) return;
+    const int a = (int)(t / FIT_KP), k = (int)(t % FIT_KP);
+    const double w = wf ? wf[cfg[a]] : 1.0;
+    double g[3] = {0.0, 0.0, 0.0};
+    if (k >= 1 && k <= ntri) {
+        const int kk = k - 1;
+        for (int q = roff[a]; q < roff[a + 1]; q++) {
+            const long p = rlist[q];
+#pragma unroll
+            for (int c = 0; c < 3; c++) g[c] += dbdr[(long)kk * stride + 3 * p + c];
+        }
+        for (int p = poff[a]; p < poff[a + 1]; p++) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) g[c] -= dbdr[(long)kk * stride + 3 * (long)p + c];
+        }
+        if (G)
+            for (int c = 0; c < 3; c++) G[((size_t)a * 3 + c) * ntri + kk] = g[c];
+    }
+    if (R) {
+        for (int c = 0; c < 3; c++) R[(size_t)(row0 + 3 * a + c) * FIT_KP + k] = w * g[c];
+        if (k == 0 && tgt)
+            for (int c = 0; c < 3; c++) tgt[row0 + 3 * a + c] = f ? -w * f[3 * (size_t)a + c] : 0.0;
+    }
+}
+
+// per configuration: bi, the virial, and the energy row [we * (N, bi)] / we * E
+__global__ void k_fit_cfg(int nconf, int ntri, const int *__restrict__ ca0, const int *__restrict__ cn,
+                          const int *__restrict__ poff, const double *__restrict__ B, int natoms,
+                          const double *__restrict__ dbdr, long stride, const double4 *__restrict__ prij,
+                          const double *__restrict__ we, const double *__restrict__ e, double *__restrict__ bi,
+                          double *__restrict__ bv, double *__restrict__ R, double *__restrict__ tgt, long erow0)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (config, k)
+    if (t >= (long)nconf * FIT_KP) return;
+    const int c = (int)(t / FIT_KP), k = (int)(t % FIT_KP);
+    const int a0 = ca0[c], n = cn[c];
+    double v = 0.0;
+    if (k == 0) v = (double)n;
+    if (k >= 1 && k <= ntri) {
+        const int kk = k - 1;
+        for (int a = a0; a < a0 + n; a++) v += B[(size_t)kk * natoms + a];
+        if (bi) bi[(size_t)c * ntri + kk] = v;
+        if (bv) {
+            double s[6] = {0, 0, 0, 0, 0, 0};
+            for (long p = poff[a0]; p < poff[a0 + n]; p++) {
+                const double4 r = prij[p];
+                const double bx = dbdr[(long)kk * stride + 3 * p], by = dbdr[(long)kk * stride + 3 * p + 1],
+                             bz = dbdr[(long)kk * stride + 3 * p + 2];
+                s[0] -= r.x * bx; s[1] -= r.y * by; s[2] -= r.z * bz;
+                s[3] -= r.x * by; s[4] -= r.x * bz; s[5] -= r.y * bz;
+            }
+            for (int q = 0; q < 6; q++) bv[((size_t)c * ntri + kk) * 6 + q] = s[q];
+        }
+    }
+    if (R) {
+        const double w = we ? we[c] : 1.0;
+        R[(size_t)(erow0 + c) * FIT_KP + k] = (k <= ntri) ? w * v : 0.0;
+        if (k == 0 && tgt) tgt[erow0 + c] = e ? w * e[c] : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// A = R^T R, b = R^T t over rows [0, nrows)
+// FP64: each CTA sums a slab of rows into a 64 x 64 (+ 64) partial; the
+// partials are added in a fixed order by k_fit_reduce.
+// BF16: R = hi + lo (two BF16 terms); hi^T hi + hi^T lo + lo^T hi with FP32
+// accumulation by warp-level tensor-core MMA (m16n8k16), partials per CTA.
+// ---------------------------------------------------------------------------
+constexpr int FIT_GRAM_THREADS = 256;
+
+__global__ void __launch_bounds__(FIT_GRAM_THREADS)
+k_fit_gram64(const double *__restrict__ R, const double *__restrict__ tgt, long nrows, int rows_per_cta,
+             double *__restrict__ part)
+{
+    __shared__ double sr[16][FIT_KP + 1];
+    __shared__ double st[16];
+    const long r0 = (long)blockIdx.x * rows_per_cta, r1 = min(nrows, r0 + rows_per_cta);
+    const int tid = threadIdx.x;
+    double acc[16], accb = 0.0;
+#pragma unroll
+    for (int q = 0; q < 16; q++) acc[q] = 0.0;
+    const int row = tid >> 2, col0 = (tid & 3) * 16;   // thread owns A[row][col0 .. col0+15]
+    for (long rb = r0; rb < r1; rb += 16) {
+        __syncthreads();
+        for (int e = tid; e < 16 * FIT_KP; e += FIT_GRAM_THREADS) {
+            const int rr = e / FIT_KP, cc = e % FIT_KP;
+            sr[rr][cc] = (rb + rr < r1) ? R[(size_t)(rb + rr) * FIT_KP + cc] : 0.0;
+        }
+        if (tid < 16) st[tid] = (rb + tid < r1) ? tgt[rb + tid] : 0.0;
+        __syncthreads();
+#pragma unroll 4
+        for (int rr = 0; rr < 16; rr++) {
+            const double a = sr[rr][row];
+#pragma unroll
+            for (int q = 0; q < 16; q++) acc[q] += a * sr[rr][col0 + q];
+            if ((tid & 3) == 0) accb += a * st[rr];
+        }
+    }
+    double *o = part + (size_t)blockIdx.x * (FIT_KP * FIT_KP + FIT_KP);
+#pragma unroll
+    for (int q = 0; q < 16; q++) o[row * FIT_KP + col0 + q] = acc[q];
+    if ((tid & 3) == 0) o[FIT_KP * FIT_KP + row] = accb;
+}
+
+// hi / lo BF16 split of the rows, [row][64] each
+__global__ void k_fit_split(const double *__restrict__ R, long n, __nv_bfloat16 *__restrict__ hi,
+                            __nv_bfloat16 *__restrict__ lo)
+{
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = R[i];
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    hi[i] = h;
+    lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const unsigned (&a)[4], const unsigned (&b)[2])
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// one CTA of 4 warps: warp w owns output rows 16w .. 16w+15 of the 64 x 64
+// product and all 8 column tiles; k runs over the CTA's slab of data rows in
+// steps of 16.  The slab tile (16 rows x 64, hi and lo) is staged in shared
+// memory, from which the A (R^T, row-major m x k) and B (R, column-major k x n)
+// fragments are read.
+__global__ void __launch_bounds__(128)
+k_fit_gram_bf16(const __nv_bfloat16 *__restrict__ hi, const __nv_bfloat16 *__restrict__ lo, long nrows,
+                int rows_per_cta, float *__restrict__ part)
+{
+    __shared__ __nv_bfloat16 sh[2][16][FIT_KP + 8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, tq = lane & 3;
+    const long r0 = (long)blockIdx.x * rows_per_cta, r1 = min(nrows, r0 + rows_per_cta);
+    float acc[8][4];
+#pragma unroll
+    for (int n = 0; n < 8; n++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) acc[n][q] = 0.f;
+    for (long rb = r0; rb < r1; rb += 16) {
+        __syncthreads();
+        for (int e = threadIdx.x; e < 16 * FIT_KP; e += blockDim.x) {
+            const int rr = e / FIT_KP, cc = e % FIT_KP;
+            const bool ok = rb + rr < r1;
+            sh[0][rr][cc] = ok ? hi[(size_t)(rb + rr) * FIT_KP + cc] : __float2bfloat16(0.f);
+            sh[1][rr][cc] = ok ? lo[(size_t)(rb + rr) * FIT_KP + cc] : __float2bfloat16(0.f);
+        }
+        __syncthreads();
+        // A fragment (16 x 16, row-major): element (m, k) = R[k][16w + m]
+        auto afrag = [&](int s, unsigned (&a)[4]) {
+            const int m0 = 16 * w + g, m1 = m0 + 8, k0 = 2 * tq, k1 = k0 + 8;
+            __nv_bfloat162 v;
+            v.x = sh[s][k0][m0]; v.y = sh[s][k0 + 1][m0]; a[0] = *reinterpret_cast<unsigned *>(&v);
+            v.x = sh[s][k0][m1]; v.y = sh[s][k0 + 1][m1]; a[1] = *reinterpret_cast<unsigned *>(&v);
+            v.x = sh[s][k1][m0]; v.y = sh[s][k1 + 1][m0]; a[2] = *reinterpret_cast<unsigned *>(&v);
+            v.x = sh[s][k1][m1]; v.y = sh[s][k1 + 1][m1]; a[3] = *reinterpret_cast<unsigned *>(&v);
+        };
+        // B fragment (16 x 8, column-major): element (k, n) = R[k][8 nt + n]
+        auto bfrag = [&](int s, int nt, unsigned (&b)[2]) {
+            const int n = 8 * nt + g, k0 = 2 * tq, k1 = k0 + 8;
+            __nv_bfloat162 v;
+            v.x = sh[s][k0][n]; v.y = sh[s][k0 + 1][n]; b[0] = *reinterpret_cast<unsigned *>(&v);
+            v.x = sh[s][k1][n]; v.y = sh[s][k1 + 1][n]; b[1] = *reinterpret_cast<unsigned *>(&v);
+        };
+        unsigned ah[4], al[4];
+        afrag(0, ah);
+        afrag(1, al);
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            unsigned bh[2], bl[2];
+            bfrag(0, nt, bh);
+            bfrag(1, nt, bl);
+            mma_bf16_16816(acc[nt], ah, bh);
+            mma_bf16_16816(acc[nt], ah, bl);
+            mma_bf16_16816(acc[nt], al, bh);
+        }
+    }
+    float *o = part + (size_t)blockIdx.x * FIT_KP * FIT_KP;
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        const int m0 = 16 * w + g, n0 = 8 * nt + 2 * tq;
+        o[m0 * FIT_KP + n0] = acc[nt][0];
+        o[m0 * FIT_KP + n0 + 1] = acc[nt][1];
+        o[(m0 + 8) * FIT_KP + n0] = acc[nt][2];
+        o[(m0 + 8) * FIT_KP + n0 + 1] = acc[nt][3];
+    }
+}
+
+// b in the BF16 form: FP32 products of the split rows with the FP64 target
+// rounded to FP32, one partial per CTA (R^T t is a 64-vector; no MMA needed)
+__global__ void k_fit_rhs_bf16(const __nv_bfloat16 *__restrict__ hi, const __nv_bfloat16 *__restrict__ lo,
+                               const double *__restrict__ tgt, long nrows, int rows_per_cta, float *__restrict__ part)
+{
+    const int c = threadIdx.x;   // 64 threads
+    const long r0 = (long)blockIdx.x * rows_per_cta, r1 = min(nrows, r0 + rows_per_cta);
+    float s = 0.f;
+    for (long r = r0; r < r1; r++) {
+        const float t = (float)tgt[r];
+        s += (__bfloat162float(hi[r * FIT_KP + c]) + __bfloat162float(lo[r * FIT_KP + c])) * t;
+    }
+    part[(size_t)blockIdx.x * FIT_KP + c] = s;
+}
+
+template <typename P>
+__global__ void k_fit_reduce(const P *__restrict__ part, int nparts, int width, long pstride, double *__restrict__ out)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= width) return;
+    double s = 0.0;
+    for (int q = 0; q < nparts; q++) s += (double)part[(size_t)q * pstride + e];
+    out[e] += s;
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+static void fit_tables(FitTables &T, int tj, int bnorm, int bzero)
+{
+    memset(&T, 0, sizeof(T));
+    T.tj = tj; T.bnorm = bnorm; T.bzero = bzero;
+    int idx[JD][JD][JD];
+    for (int a = 0; a < JD; a++) for (int b = 0; b < JD; b++) for (int c = 0; c < JD; c++) idx[a][b][c] = -1;
+    int nz = 0;
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= std::min(tj, j1 + j2); j += 2) {
+                FitCoupling &c = T.cp[T.ncoup];
+                c.j1 = j1; c.j2 = j2; c.j = j; c.zoff = nz;
+                idx[j1][j2][j] = T.ncoup++;
+                nz += (j / 2 + 1) * (j + 1);
+            }
+    T.nz = nz;
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= std::min(tj, j1 + j2); j += 2) {
+                if (j < j1) continue;
+                FitTriple &t = T.tr[T.ntri++];
+                t.j1 = j1; t.j2 = j2; t.j = j;
+                // cpuComputeDbidrj:826-1013: z(j1,j2,j) with dU_j; z(j,j2,j1) with dU_j1
+                // times (j+1)/(j1+1); z(j,j1,j2) with dU_j2 times (j+1)/(j2+1)
+                t.layer[0] = j; t.coup[0] = idx[j1][j2][j]; t.fac[0] = 1.0;
+                t.layer[1] = j1; t.coup[1] = idx[j][j2][j1]; t.fac[1] = bnorm ? 1.0 : (j + 1) / (j1 + 1.0);
+                t.layer[2] = j2; t.coup[2] = idx[j][j1][j2]; t.fac[2] = bnorm ? 1.0 : (j + 1) / (j2 + 1.0);
+            }
+}
+
+}  // namespace mdp
+
+using namespace mdp;
+
+struct mdp_fit {
+    SnapModel model;
+    FitTables tab;
+    int device = 0;
+    cudaStream_t s = nullptr;
+    // batch
+    int nconf = 0, natoms = 0;
+    std::vector<int> h_cn, h_ca0;
+    DevBuf x, cfg, ca0, cn, cbox, we, wf, e, f;
+    // work (sized for the whole batch)
+    DevBuf tabs, pcount, poff, roff, rcount, cursor, rlist, B, Z, dul, dbdr, G, R, tgt, hi, lo, part, out, scan_tmp;
+    ForcePath fp;
+    long npairs = 0, nrows = 0;
+    bool pairs_ready = false;
+    // launch shapes (autotuned): threads of the per-pair kernels, rows per Gram CTA
+    int du_threads = 128, db_threads = 128, gram_rows = 4096;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_mode = -1;
+};
+
+namespace mdp {
+
+static int fit_pairs(mdp_fit *h)
+{
+    const int n = h->natoms;
+    const int tb = 128, gb = (n + tb - 1) / tb;
+    if (h->pcount.ensure(sizeof(int) * n) || h->poff.ensure(sizeof(int) * (n + 1)) ||
+        h->scan_tmp.ensure(sizeof(int) * scan_tmp_ints(n + 1)))
+        return -1;
+    k_fit_pairs<false><<<gb, tb, 0, h->s>>>(h->x.as<double4>(), h->cfg.as<int>(), h->ca0.as<int>(), h->cn.as<int>(),
+                                            h->cbox.as<double4>(), n, h->model.geom, h->pcount.as<int>(), nullptr,
+                                            nullptr, nullptr, nullptr);
+    if (exclusive_scan(h->pcount.as<int>(), h->poff.as<int>(), n, h->scan_tmp.as<int>(), h->s)) return -1;
+    int np = 0;
+    MDP_CUDA_TRY(cudaMemcpyAsync(&np, h->poff.as<int>() + n, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(h->s));
+    h->npairs = np;
+    ForcePath &fp = h->fp;
+    const long pc = std::max(1L, h->npairs);
+    if (fp.poff.ensure(sizeof(int) * (n + 1)) || fp.prij.ensure(sizeof(double4) * pc) ||
+        fp.pab.ensure(sizeof(double4) * pc) || fp.pinfo.ensure(sizeof(int2) * pc))
+        return -1;
+    MDP_CUDA_TRY(cudaMemcpyAsync(fp.poff.p, h->poff.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToDevice, h->s));
+    k_fit_pairs<true><<<gb, tb, 0, h->s>>>(h->x.as<double4>(), h->cfg.as<int>(), h->ca0.as<int>(), h->cn.as<int>(),
+                                           h->cbox.as<double4>(), n, h->model.geom, nullptr, h->poff.as<int>(),
+                                           fp.prij.as<double4>(), fp.pab.as<double4>(), fp.pinfo.as<int2>());
+    // reverse pairs
+    if (h->rcount.ensure(sizeof(int) * n) || h->roff.ensure(sizeof(int) * (n + 1)) ||
+        h->cursor.ensure(sizeof(int) * n) || h->rlist.ensure(sizeof(int) * pc))
+        return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(h->rcount.p, 0, sizeof(int) * n, h->s));
+    MDP_CUDA_TRY(cudaMemsetAsync(h->cursor.p, 0, sizeof(int) * n, h->s));
+    const int pb = (int)((h->npairs + 255) / 256);
+    if (h->npairs) k_fit_rev_count<<<pb, 256, 0, h->s>>>(fp.pinfo.as<int2>(), h->npairs, h->rcount.as<int>());
+    if (exclusive_scan(h->rcount.as<int>(), h->roff.as<int>(), n, h->scan_tmp.as<int>(), h->s)) return -1;
+    if (h->npairs) k_fit_rev_fill<<<pb, 256, 0, h->s>>>(fp.pinfo.as<int2>(), h->npairs, h->roff.as<int>(),
+                                                        h->cursor.as<int>(), h->rlist.as<int>());
+    k_fit_rev_sort<<<gb, tb, 0, h->s>>>(n, h->roff.as<int>(), h->rlist.as<int>());
+    count_launches(5);
+    MDP_CUDA_TRY(cudaGetLastError());
+    h->pairs_ready = true;
+    return 0;
+}
+
+template <int TJ>
+static int fit_launch_du(mdp_fit *h)
+{
+    if (tu_ensure_tables()) return -1;
+    const long nt = 3 * h->npairs;
+    if (nt == 0) return 0;
+    k_fit_du<TJ><<<(unsigned)((nt + h->du_threads - 1) / h->du_threads), h->du_threads, 0, h->s>>>(
+        h->fp.prij.as<double4>(), h->npairs, h->model.geom, h->dul.as<double2>(), nt);
+    count_launches(1);
+    return 0;
+}
+
+// descriptors of the whole batch: U, Z, B, dU, dB/dR, rows; no host synchronisation
+static int fit_descriptor_stages(mdp_fit *h, bool rows)
+{
+    const int n = h->natoms, tj = h->model.p.twojmax;
+    const int ntiles = (n + 31) / 32;
+    const long nt = 3 * h->npairs;
+    if (tu_ensure_tables()) return -1;
+    const int urc = tj == 8 ? launch_ui<double, 8>(h->model, h->fp, n, h->s)
+                  : tj == 6 ? launch_ui<double, 6>(h->model, h->fp, n, h->s)
+                            : launch_ui<double, 4>(h->model, h->fp, n, h->s);
+    if (urc) return -1;
+    count_launches(1);
+    const size_t zsm = (size_t)idxu_count(tj) * 32 * sizeof(double2);
+    static bool attr = false;
+    if (!attr) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_fit_zb, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)((size_t)idxu_count(TJMAX) * 32 * sizeof(double2))));
+        attr = true;
+    }
+    k_fit_zb<<<std::min(ntiles, num_sms() * 1), FIT_ZB_WARPS * 32, zsm, h->s>>>(
+        h->fp.Ut.as<double2>(), n, h->tabs.as<FitTables>(), h->Z.as<double2>(), h->B.as<double>());
+    count_launches(1);
+    if (tj == 8) { if (fit_launch_du<8>(h)) return -1; }
+    else if (tj == 6) { if (fit_launch_du<6>(h)) return -1; }
+    else { if (fit_launch_du<4>(h)) return -1; }
+    if (nt) {
+        k_fit_dbdr<<<(unsigned)((nt + h->db_threads - 1) / h->db_threads), h->db_threads, 0, h->s>>>(
+            h->dul.as<double2>(), nt, h->fp.pinfo.as<int2>(), h->npairs, h->tabs.as<FitTables>(), h->Z.as<double2>(),
+            h->dbdr.as<double>());
+        count_launches(1);
+    }
+    if (rows) {
+        const long ta = (long)n * FIT_KP, tc = (long)h->nconf * FIT_KP;
+        k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(
+            n, h->tab.ntri, h->poff.as<int>(), h->roff.as<int>(), h->rlist.as<int>(), h->dbdr.as<double>(), nt,
+            h->cfg.as<int>(), h->wf.as<double>(), h->f.as<double>(), nullptr, h->R.as<double>(), h->tgt.as<double>(),
+            h->nconf);
+        k_fit_cfg<<<(unsigned)((tc + 255) / 256), 256, 0, h->s>>>(
+            h->nconf, h->tab.ntri, h->ca0.as<int>(), h->cn.as<int>(), h->poff.as<int>(), h->B.as<double>(), n,
+            h->dbdr.as<double>(), nt, h->fp.prij.as<double4>(), h->we.as<double>(), h->e.as<double>(), nullptr,
+            nullptr, h->R.as<double>(), h->tgt.as<double>(), 0);
+        count_launches(2);
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+static int fit_gram_stages(mdp_fit *h, int mode)
+{
+    const long nr = h->nrows;
+    const int rpc = h->gram_rows;
+    const int nb = (int)((nr + rpc - 1) / rpc);
+    double *out = h->out.as<double>();
+    MDP_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(double) * (FIT_KP * FIT_KP + FIT_KP), h->s));
+    if (mode == 0) {
+        k_fit_gram64<<<nb, FIT_GRAM_THREADS, 0, h->s>>>(h->R.as<double>(), h->tgt.as<double>(), nr, rpc,
+                                                      h->part.as<double>());
+        const int w = FIT_KP * FIT_KP + FIT_KP;
+        k_fit_reduce<double><<<(w + 255) / 256, 256, 0, h->s>>>(h->part.as<double>(), nb, w, w, out);
+        count_launches(2);
+    } else {
+        const long ne = nr * FIT_KP;
+        k_fit_split<<<(unsigned)((ne + 255) / 256), 256, 0, h->s>>>(h->R.as<double>(), ne, h->hi.as<__nv_bfloat16>(),
+                                                                    h->lo.as<__nv_bfloat16>());
+        float *pf = h->part.as<float>();
+        k_fit_gram_bf16<<<nb, 128, 0, h->s>>>(h->hi.as<__nv_bfloat16>(), h->lo.as<__nv_bfloat16>(), nr, rpc, pf);
+        k_fit_reduce<float><<<(FIT_KP * FIT_KP + 255) / 256, 256, 0, h->s>>>(pf, nb, FIT_KP * FIT_KP,
+                                                                           FIT_KP * FIT_KP, out);
+        float *pb = pf + (size_t)nb * FIT_KP * FIT_KP;
+        k_fit_rhs_bf16<<<nb, FIT_KP, 0, h->s>>>(h->hi.as<__nv_bfloat16>(), h->lo.as<__nv_bfloat16>(),
+                                                h->tgt.as<double>(), nr, rpc, pb);
+        k_fit_reduce<float><<<1, FIT_KP, 0, h->s>>>(pb, nb, FIT_KP, FIT_KP, out + FIT_KP * FIT_KP);
+        count_launches(5);
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+static int fit_alloc_work(mdp_fit *h)
+{
+    const int n = h->natoms, tj = h->model.p.twojmax;
+    const long ntiles = (n + 31) / 32;
+    const long nt = std::max(3 * h->npairs, 1L);
+    h->nrows = h->nconf + 3L * n;
+    const int nbmax = (int)((h->nrows + 255) / 256) + 1;   // smallest gram_rows candidate
+    if (h->fp.Ut.ensure(sizeof(double2) * ntiles * idxu_count(tj) * 32) ||
+        h->Z.ensure(sizeof(double2) * ntiles * h->tab.nz * 32) || h->B.ensure(sizeof(double) * h->tab.ntri * n) ||
+        h->dul.ensure(sizeof(double2) * nt * yh_count(tj)) || h->dbdr.ensure(sizeof(double) * nt * h->tab.ntri) ||
+        h->R.ensure(sizeof(double) * h->nrows * FIT_KP) || h->tgt.ensure(sizeof(double) * h->nrows) ||
+        h->hi.ensure(sizeof(__nv_bfloat16) * h->nrows * FIT_KP) || h->lo.ensure(sizeof(__nv_bfloat16) * h->nrows * FIT_KP) ||
+        h->part.ensure(sizeof(double) * (size_t)nbmax * (FIT_KP * FIT_KP + FIT_KP)) ||
+        h->out.ensure(sizeof(double) * (FIT_KP * FIT_KP + FIT_KP)))
+        return -1;
+    return 0;
+}
+
+static void fit_drop_graph(mdp_fit *h)
+{
+    if (h->gexec) cudaGraphExecDestroy(h->gexec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    h->gexec = nullptr;
+    h->graph = nullptr;
+    h->graph_mode = -1;
+}
+
+}  // namespace mdp
+
+extern "C" {
+
+int mdp_fit_create(mdp_fit **hp, const mdp_snap_params *p, int device)
+{
+    if (!hp || !p) { set_error("null argument"); return -1; }
+    *hp = nullptr;
+    if (p->twojmax != 4 && p->twojmax != 6 && p->twojmax != 8) { set_error("twojmax must be 4, 6 or 8"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(device));
+    mdp_snap_params q = *p;
+    std::vector<double> ones(1 + 64, 1.0);
+    if (!q.coeff) { q.coeff = ones.data(); q.ncoeffall = 1 + mdp_snap_ncoeff(p->twojmax); }
+    mdp_fit *h = new mdp_fit();
+    h->device = device;
+    if (model_init(h->model, &q)) { delete h; return -1; }
+    fit_tables(h->tab, p->twojmax, p->bnormflag, p->bzeroflag);
+    if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess || h->tabs.ensure(sizeof(FitTables))) {
+        mdp_fit_destroy(h);
+        set_error("stream / table allocation failed");
+        return -1;
+    }
+    MDP_CUDA_TRY(cudaMemcpy(h->tabs.p, &h->tab, sizeof(FitTables), cudaMemcpyHostToDevice));
+    *hp = h;
+    return 0;
+}
+
+void mdp_fit_destroy(mdp_fit *h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->s) cudaStreamSynchronize(h->s);
+    fit_drop_graph(h);
+    DevBuf *b[] = {&h->x, &h->cfg, &h->ca0, &h->cn, &h->cbox, &h->we, &h->wf, &h->e, &h->f, &h->tabs, &h->pcount,
+                   &h->poff, &h->roff, &h->rcount, &h->cursor, &h->rlist, &h->B, &h->Z, &h->dul, &h->dbdr, &h->G,
+                   &h->R, &h->tgt, &h->hi, &h->lo, &h->part, &h->out, &h->scan_tmp};
+    for (auto x : b) x->release();
+    h->fp.release();
+    if (h->s) cudaStreamDestroy(h->s);
+    delete h;
+}
+
+int mdp_fit_ncoeff(mdp_fit *h) { return h ? h->tab.ntri : -1; }
+
+// Batch of nconf configurations: natoms[c], box[3c..3c+2] (orthogonal box
+// lengths), x (all positions concatenated, 3 per atom, inside [0, L)),
+// targets e[c] and f (3 per atom), weights we[c], wf[c] (any of e, f, we, wf
+// may be NULL: zero targets, unit weights).  Builds the pair lists.
+int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *box, const double *x,
+                      const double *e, const double *f, const double *we, const double *wf)
+{
+    if (!h || nconf < 1 || !natoms || !box || !x) { set_error("bad arguments"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(h->device));
+    const double need = h->model.geom.rcut;
+    long total = 0;
+    h->h_cn.assign(natoms, natoms + nconf);
+    h->h_ca0.resize(nconf);
+    for (int c = 0; c < nconf; c++) {
+        if (natoms[c] < 1) { set_error("configuration %d has no atoms", c); return -1; }
+        for (int d = 0; d < 3; d++)
+            if (!(box[3 * c + d] > need)) {
+                set_error("configuration %d: box length %g must exceed the cutoff %g (one image shell)", c,
+                          box[3 * c + d], need);
+                return -1;
+            }
+        h->h_ca0[c] = (int)total;
+        total += natoms[c];
+    }
+    if (total > (1L << 30)) { set_error("batch too large"); return -1; }
+    fit_drop_graph(h);
+    h->nconf = nconf;
+    h->natoms = (int)total;
+    const int n = h->natoms;
+    std::vector<double> x4(4 * (size_t)n), b4(4 * (size_t)nconf);
+    std::vector<int> cid(n);
+    for (int c = 0; c < nconf; c++) {
+        b4[4 * c] = box[3 * c]; b4[4 * c + 1] = box[3 * c + 1]; b4[4 * c + 2] = box[3 * c + 2]; b4[4 * c + 3] = 0.0;
+        for (int a = 0; a < natoms[c]; a++) cid[h->h_ca0[c] + a] = c;
+    }
+    for (long i = 0; i < n; i++) { x4[4 * i] = x[3 * i]; x4[4 * i + 1] = x[3 * i + 1]; x4[4 * i + 2] = x[3 * i + 2]; x4[4 * i + 3] = 0.0; }
+    if (h->x.ensure(sizeof(double4) * n) || h->cfg.ensure(sizeof(int) * n) || h->ca0.ensure(sizeof(int) * nconf) ||
+        h->cn.ensure(sizeof(int) * nconf) || h->cbox.ensure(sizeof(double4) * nconf) ||
+        h->we.ensure(sizeof(double) * nconf) || h->wf.ensure(sizeof(double) * nconf) ||
+        h->e.ensure(sizeof(double) * nconf) || h->f.ensure(sizeof(double) * 3 * (size_t)n))
+        return -1;
+    std::vector<double> ones(nconf, 1.0), zc(nconf, 0.0), zf(3 * (size_t)n, 0.0);
+    MDP_CUDA_TRY(cudaMemcpy(h->x.p, x4.data(), sizeof(double4) * n, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->cfg.p, cid.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->ca0.p, h->h_ca0.data(), sizeof(int) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->cn.p, natoms, sizeof(int) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->cbox.p, b4.data(), sizeof(double4) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->we.p, we ? we : ones.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->wf.p, wf ? wf : ones.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->e.p, e ? e : zc.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->f.p, f ? f : zf.data(), sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice));
+    if (fit_pairs(h) || fit_alloc_work(h)) return -1;
+    return 0;
+}
+
+long long mdp_fit_npairs(mdp_fit *h) { return h ? h->npairs : -1; }
+
+// Descriptors of the batch (any output may be NULL):
+//   bi [nconf][ncoeff], bd [natoms][3][ncoeff] (= -d(sum B)/dx, the layout
+//   order of cpuSnapTallyBispectrumDeriv per atom), bv [nconf][ncoeff][6],
+//   blist [ncoeff][natoms]
+int mdp_fit_descriptors(mdp_fit *h, double *bi, double *bd, double *bv, double *blist)
+{
+    if (!h || !h->pairs_ready) { set_error("set a batch first"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(h->device));
+    if (fit_descriptor_stages(h, false)) return -1;
+    const int n = h->natoms, nc = h->tab.ntri;
+    const long nt = 3 * h->npairs;
+    DevBuf dbi, dbv, dG;
+    if (dbi.ensure(sizeof(double) * h->nconf * nc) || dbv.ensure(sizeof(double) * h->nconf * nc * 6) ||
+        dG.ensure(sizeof(double) * (size_t)n * 3 * nc))
+        return -1;
+    const long ta = (long)n * FIT_KP, tc = (long)h->nconf * FIT_KP;
+    k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(n, nc, h->poff.as<int>(), h->roff.as<int>(),
+                                                               h->rlist.as<int>(), h->dbdr.as<double>(), nt,
+                                                               h->cfg.as<int>(), nullptr, nullptr, dG.as<double>(),
+                                                               nullptr, nullptr, 0);
+    k_fit_cfg<<<(unsigned)((tc + 255) / 256), 256, 0, h->s>>>(h->nconf, nc, h->ca0.as<int>(), h->cn.as<int>(),
+                                                              h->poff.as<int>(), h->B.as<double>(), n,
+                                                              h->dbdr.as<double>(), nt, h->fp.prij.as<double4>(),
+                                                              nullptr, nullptr, dbi.as<double>(), dbv.as<double>(),
+                                                              nullptr, nullptr, 0);
+    count_launches(2);
+    MDP_CUDA_TRY(cudaGetLastError());
+    MDP_CUDA_TRY(cudaStreamSynchronize(h->s));
+    if (bi) MDP_CUDA_TRY(cudaMemcpy(bi, dbi.p, sizeof(double) * h->nconf * nc, cudaMemcpyDeviceToHost));
+    if (bv) MDP_CUDA_TRY(cudaMemcpy(bv, dbv.p, sizeof(double) * h->nconf * nc * 6, cudaMemcpyDeviceToHost));
+    if (bd) {
+        std::vector<double> g((size_t)n * 3 * nc);
+        MDP_CUDA_TRY(cudaMemcpy(g.data(), dG.p, sizeof(double) * g.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < g.size(); i++) bd[i] = -g[i];
+    }
+    if (blist) MDP_CUDA_TRY(cudaMemcpy(blist, h->B.p, sizeof(double) * (size_t)nc * n, cudaMemcpyDeviceToHost));
+    dbi.release(); dbv.release(); dG.release();
+    return 0;
+}
+
+// Normal equations of the batch: A [64][64] and b [64] (entries beyond
+// 1 + ncoeff are zero), assembled in FP64 (mode 0) or from the BF16 hi/lo
+// split with FP32 sums (mode 1).  The whole pipeline, from U to A, is one CUDA
+// graph, captured on first use per mode and replayed; elapsed_ms (may be NULL)
+// is the CUDA-event time of the graph launch.
+int mdp_fit_run(mdp_fit *h, int mode, double *A, double *b, float *elapsed_ms)
+{
+    if (!h || !h->pairs_ready) { set_error("set a batch first"); return -1; }
+    if (mode != 0 && mode != 1) { set_error("mode must be 0 (FP64) or 1 (BF16 split)"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(h->device));
+    if (h->graph_mode != mode) {
+        fit_drop_graph(h);
+        if (tu_ensure_tables()) return -1;
+        // first call of every launcher outside the capture (attributes, tables)
+        if (fit_descriptor_stages(h, true) || fit_gram_stages(h, mode)) return -1;
+        MDP_CUDA_TRY(cudaStreamSynchronize(h->s));
+        MDP_CUDA_TRY(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+        int rc = fit_descriptor_stages(h, true) || fit_gram_stages(h, mode);
+        cudaGraph_t g = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(h->s, &g);
+        if (rc || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            if (!rc) set_error("graph capture failed: %s", cudaGetErrorString(ce));
+            return -1;
+        }
+        h->graph = g;
+        MDP_CUDA_TRY(cudaGraphInstantiate(&h->gexec, g, 0));
+        h->graph_mode = mode;
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, h->s);
+    MDP_CUDA_TRY(cudaGraphLaunch(h->gexec, h->s));
+    cudaEventRecord(e1, h->s);
+    MDP_CUDA_TRY(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (elapsed_ms) *elapsed_ms = ms;
+    std::vector<double> o(FIT_KP * FIT_KP + FIT_KP);
+    MDP_CUDA_TRY(cudaMemcpy(o.data(), h->out.p, sizeof(double) * o.size(), cudaMemcpyDeviceToHost));
+    if (A) memcpy(A, o.data(), sizeof(double) * FIT_KP * FIT_KP);
+    if (b) memcpy(b, o.data() + FIT_KP * FIT_KP, sizeof(double) * FIT_KP);
+    return 0;
+}
+
+// Autotuner: times the per-pair kernels' block sizes and the Gram kernel's
+// rows per CTA on the current batch (CUDA events, best of 3 each) and keeps
+// the fastest; the captured graph is rebuilt on the next run.  Writes the
+// choice to out3 (du threads, dB/dr threads, Gram rows per CTA) if not NULL.
+int mdp_fit_tune(mdp_fit *h, int *out3)
+{
+    if (!h || !h->pairs_ready) { set_error("set a batch first"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(h->device));
+    fit_drop_graph(h);
+    if (fit_descriptor_stages(h, true)) return -1;   // warm tables and buffers
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    // a candidate that fails to launch is discarded (and its error cleared)
+    auto timeit = [&](auto fn) {
+        float best = 1e30f;
+        for (int r = 0; r < 3; r++) {
+            cudaEventRecord(e0, h->s);
+            if (fn() || cudaPeekAtLastError() != cudaSuccess) { cudaGetLastError(); return -1.0f; }
+            cudaEventRecord(e1, h->s);
+            cudaEventSynchronize(e1);
+            float ms;
+            cudaEventElapsedTime(&ms, e0, e1);
+            best = std::min(best, ms);
+        }
+        return best;
+    };
+    const int tcand[3] = {32, 64, 128};   // within the kernels' launch bounds (128)
+    const int tj = h->model.p.twojmax;
+    float bt = 1e30f;
+    int bsel = h->du_threads;
+    for (int c : tcand) {
+        h->du_threads = c;
+        const float t = timeit([&]() { return tj == 8 ? fit_launch_du<8>(h) : tj == 6 ? fit_launch_du<6>(h) : fit_launch_du<4>(h); });
+        if (t >= 0 && t < bt) { bt = t; bsel = c; }
+    }
+    h->du_threads = bsel;
+    bt = 1e30f;
+    bsel = h->db_threads;
+    const long nt = 3 * h->npairs;
+    for (int c : tcand) {
+        h->db_threads = c;
+        const float t = timeit([&]() {
+            k_fit_dbdr<<<(unsigned)((nt + c - 1) / c), c, 0, h->s>>>(h->dul.as<double2>(), nt, h->fp.pinfo.as<int2>(),
+                                                                    h->npairs, h->tabs.as<FitTables>(),
+                                                                    h->Z.as<double2>(), h->dbdr.as<double>());
+            return 0;
+        });
+        if (t >= 0 && t < bt) { bt = t; bsel = c; }
+    }
+    h->db_threads = bsel;
+    const int rcand[4] = {256, 1024, 4096, 16384};
+    bt = 1e30f;
+    bsel = h->gram_rows;
+    for (int c : rcand) {
+        h->gram_rows = c;
+        const float t = timeit([&]() { return fit_gram_stages(h, 1); });
+        if (t >= 0 && t < bt) { bt = t; bsel = c; }
+    }
+    h->gram_rows = bsel;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    MDP_CUDA_TRY(cudaGetLastError());
+    if (out3) { out3[0] = h->du_threads; out3[1] = h->db_threads; out3[2] = h->gram_rows; }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,170 @@
+"""Batched SNAP descriptors and the linear-fit normal equations on the GPU.
+
+Per configuration this computes what MDP's ComputeSnap computes
+(snappotential.cpp:762-910): the summed bispectrum bi, its derivatives bd with
+respect to every atom coordinate and the virial bv; over a whole batch it
+assembles the normal equations of the linear SNAP fit with the rows of
+Regression.cpp:386-404 (one total-energy row per configuration, one row per
+force component) in FP64 or from a BF16 hi/lo split with FP32 tensor-core sums.
+The whole device pipeline is one CUDA graph (mdp_fit_run).
+
+The synthetic batch (batch_configs) is the fitting workload of the project:
+BCC / FCC / A15 Ta supercells of 16-512 atoms at equal volume per atom, with
+isotropic strain within +-5 % and Gaussian jitter of width U[0.02, 0.3] A; every
+box length is at least rcut + skin = 5.68 A, the single image shell MDP's
+cpuPeriodicImages3D builds.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+
+import numpy as np
+
+from . import _lib
+from .configs import SnapParams, TA_LATTICE, _BASIS
+
+# lattice constants at the BCC volume per atom (a^3 / 2 with a = 3.316 A)
+LATTICE = {"bcc": TA_LATTICE, "fcc": (4 * TA_LATTICE ** 3 / 2) ** (1 / 3), "a15": (8 * TA_LATTICE ** 3 / 2) ** (1 / 3)}
+MIN_WIDTH = 4.67637 + 1.0
+
+
+@dataclasses.dataclass
+class FitConfig:
+    x: np.ndarray      # (N, 3) in [0, L)
+    box: np.ndarray    # (3,)
+    kind: str
+
+    @property
+    def natoms(self):
+        return self.x.shape[0]
+
+
+def supercell(kind: str, target: int, strain: float):
+    """Cells (n1, n2, n3), each >= the count that keeps the strained width above
+    MIN_WIDTH, whose atom count is nearest to target."""
+    m = len(_BASIS[kind])
+    a = LATTICE[kind] * (1.0 + strain)
+    nmin = int(np.ceil(MIN_WIDTH / a))
+    best = None
+    for n1 in range(nmin, 9):
+        for n2 in range(n1, 9):
+            for n3 in range(n2, 9):
+                d = abs(m * n1 * n2 * n3 - target)
+                if best is None or d < best[0]:
+                    best = (d, (n1, n2, n3))
+    return best[1], a
+
+
+def make_config(kind: str, target: int, strain: float, sigma: float, rng) -> FitConfig:
+    (n1, n2, n3), a = supercell(kind, target, strain)
+    basis = _BASIS[kind]
+    ii, jj, kk = np.meshgrid(np.arange(n1), np.arange(n2), np.arange(n3), indexing="ij")
+    cells = np.stack([ii.ravel(), jj.ravel(), kk.ravel()], axis=1).astype(np.float64)
+    x = ((cells[:, None, :] + basis[None, :, :]).reshape(-1, 3)) * a
+    box = np.array([n1 * a, n2 * a, n3 * a])
+    x = x + rng.normal(0.0, sigma, size=x.shape)
+    x = np.mod(x, box)
+    x = np.where(x >= box, x - box, x)
+    return FitConfig(x=x, box=box, kind=kind)
+
+
+def batch_configs(nconf: int = 4096, seed: int = 2024, lo: int = 16, hi: int = 512):
+    """The synthetic fitting batch: kinds, sizes, strains and jitters drawn from
+    seeded distributions; targets y ~ N(0, 1) for every energy and force row."""
+    rng = np.random.default_rng(seed)
+    cfgs = []
+    for _ in range(nconf):
+        kind = ("bcc", "fcc", "a15")[rng.integers(3)]
+        target = int(rng.integers(lo, hi + 1))
+        cfgs.append(make_config(kind, target, rng.uniform(-0.05, 0.05), rng.uniform(0.02, 0.3), rng))
+    e = rng.normal(size=nconf)
+    f = rng.normal(size=(sum(c.natoms for c in cfgs), 3))
+    return cfgs, e, f
+
+
+class BatchFit:
+    """Device state of one batch (ctypes handle over mdp_fit_*)."""
+
+    def __init__(self, params: SnapParams, device: int = 0):
+        L = _lib.lib()
+        self.params = params
+        self._sp, self._keep = _lib.snap_params_c(params)
+        self._h = C.c_void_p()
+        _lib.check(L.mdp_fit_create(C.byref(self._h), C.byref(self._sp), device), "mdp_fit_create")
+        self.ncoeff = L.mdp_fit_ncoeff(self._h)
+        self.nconf = 0
+        self.natoms = 0
+
+    def close(self):
+        if self._h:
+            _lib.lib().mdp_fit_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_batch(self, cfgs, e=None, f=None, we=None, wf=None):
+        n = np.array([c.natoms for c in cfgs], dtype=np.int32)
+        box = np.ascontiguousarray(np.stack([c.box for c in cfgs]), dtype=np.float64)
+        x = np.ascontiguousarray(np.concatenate([c.x for c in cfgs]), dtype=np.float64)
+        keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (e, f, we, wf)]
+        ptr = [None if a is None else a.ctypes.data for a in keep]
+        _lib.check(_lib.lib().mdp_fit_set_batch(self._h, len(cfgs), n, box, x, *ptr), "mdp_fit_set_batch")
+        self.nconf, self.natoms = len(cfgs), int(n.sum())
+        self.counts = n
+
+    def npairs(self) -> int:
+        return int(_lib.lib().mdp_fit_npairs(self._h))
+
+    def descriptors(self):
+        """bi (nconf, k), bd (natoms, 3, k) in the reference's sign, bv (nconf, k, 6), blist (k, natoms)."""
+        k = self.ncoeff
+        bi = np.zeros((self.nconf, k)); bd = np.zeros((self.natoms, 3, k))
+        bv = np.zeros((self.nconf, k, 6)); bl = np.zeros((k, self.natoms))
+        _lib.check(_lib.lib().mdp_fit_descriptors(self._h, bi.ctypes.data, bd.ctypes.data, bv.ctypes.data,
+                                                  bl.ctypes.data), "mdp_fit_descriptors")
+        return bi, bd, bv, bl
+
+    def run(self, mode: str = "fp64"):
+        """Normal equations (A (m, m), b (m,), device ms) with m = 1 + ncoeff."""
+        A = np.zeros(64 * 64); b = np.zeros(64); ms = C.c_float(0.0)
+        _lib.check(_lib.lib().mdp_fit_run(self._h, {"fp64": 0, "bf16": 1}[mode], A, b, C.byref(ms)), "mdp_fit_run")
+        m = 1 + self.ncoeff
+        return A.reshape(64, 64)[:m, :m].copy(), b[:m].copy(), float(ms.value)
+
+    def tune(self):
+        out = np.zeros(3, dtype=np.int32)
+        _lib.check(_lib.lib().mdp_fit_tune(self._h, out), "mdp_fit_tune")
+        return dict(du_threads=int(out[0]), dbdr_threads=int(out[1]), gram_rows=int(out[2]))
+
+
+def solve(A: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """beta of A beta = b by Cholesky in FP64 (Regression.cpp:420-426 inverts A)."""
+    L = np.linalg.cholesky(A)
+    y = np.linalg.solve(L, b)
+    return np.linalg.solve(L.T, y)
+
+
+def rows_numpy(cfgs, bi, bd, e, f, we=None, wf=None):
+    """The same rows in numpy (test reference): R, t."""
+    nc = len(cfgs)
+    k = bi.shape[1]
+    we = np.ones(nc) if we is None else we
+    wf = np.ones(nc) if wf is None else wf
+    n = np.array([c.natoms for c in cfgs])
+    R = np.zeros((nc + 3 * n.sum(), 1 + k))
+    t = np.zeros(R.shape[0])
+    R[:nc, 0] = we * n
+    R[:nc, 1:] = we[:, None] * bi
+    t[:nc] = we * e
+    a0 = np.concatenate([[0], np.cumsum(n)])
+    for c in range(nc):
+        G = -bd[a0[c]:a0[c + 1]]                  # (n, 3, k): d(sum B)/dx
+        rows = slice(nc + 3 * a0[c], nc + 3 * a0[c + 1])
+        R[rows, 1:] = wf[c] * G.reshape(-1, k)
+        t[rows] = -wf[c] * f[a0[c]:a0[c + 1]].reshape(-1)
+    return R, t

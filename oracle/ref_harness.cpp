@@ -208,6 +208,89 @@ void ref_snap_force(double *eatom, double *fatom, double *vatom, const double *x
     }
 }
 
+// Per-configuration SNAP descriptors in the order of ComputeSnap
+// (snappotential.cpp:762-910): bi[ncoeff] = sum_i B_i, bd[3*i + c + 3*inum*k] =
+// d(sum_a B_ak)/dx_ic, bv[6*k + c] (virial), blist[i + inum*k] per-atom B.
+// Outputs are overwritten.  Single element, chemflag = quadraticflag = 0.
+void ref_snap_descriptors(double *bi, double *bd, double *bv, double *blist_out, const double *x,
+                          const int *atomtype, const int *alist, const int *neighlist, const int *neighnum,
+                          int inum, int neighmax, int twojmax, double rcutfac, double rfac0, double rmin0,
+                          double radelem1, double wjelem1, int switchflag, int bzeroflag, int bnormflag,
+                          int wselfallflag)
+{
+    const int dim = 3, ntypes = 1, nelem = 1, chemflag = 0, quadraticflag = 0;
+    int jdim = twojmax + 1;
+    int idxcg_count = 0, idxz_count = 0, idxb_count = 0;
+    for (int j1 = 0; j1 <= twojmax; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= MIN(twojmax, j1 + j2); j += 2) {
+                idxcg_count += (j1 + 1) * (j2 + 1);
+                if (j >= j1) idxb_count++;
+                for (int mb = 0; 2 * mb <= j; mb++) idxz_count += j + 1;
+            }
+    int idx_max[5];
+    std::vector<double> rootpq((jdim + 1) * (jdim + 1)), cglist(idxcg_count), fac(168);
+    std::vector<int> idxz(idxz_count * 10), idxz_block(jdim * jdim * jdim), idxb(idxb_count * 3),
+        idxb_block(jdim * jdim * jdim), idxu_block(jdim), idxcg_block(jdim * jdim * jdim);
+    fac[0] = 1.0;
+    for (int i = 1; i < 168; i++) fac[i] = fac[i - 1] * (double)i;
+    cpuInitSna(rootpq.data(), cglist.data(), fac.data(), idx_max, idxz.data(), idxz_block.data(),
+               idxb.data(), idxb_block.data(), idxu_block.data(), idxcg_block.data(), twojmax);
+    int idxu_max = idx_max[1], idxb_max = idx_max[2], idxz_max = idx_max[3];
+    double radelem[2] = {0.0, radelem1}, wjelem[2] = {0.0, wjelem1};
+    int map[2] = {0, 0};
+    double cut = (radelem1 + radelem1) * rcutfac;
+    double rcutsq[4] = {0, 0, 0, cut * cut};
+    double bzero[64];
+    for (int j = 0; j <= twojmax; j++) bzero[j] = bnormflag ? 1.0 : (double)(j + 1);
+    double wself = 1.0;
+    const int ncoeff = idxb_max, nperdim = ncoeff;
+
+    std::vector<int> pairnum(inum), pairlist((size_t)inum * neighmax), ilist(inum), pairnumsum(inum + 1);
+    for (int i = 0; i < inum; i++) ilist[i] = i;
+    cpuNeighPairList(pairnum.data(), pairlist.data(), (double *)x, rcutsq, ilist.data(), (int *)neighlist,
+                     (int *)neighnum, (int *)atomtype, (int *)alist, inum, neighmax, dim, ntypes);
+    pairnumsum[0] = 0;
+    for (int i = 0; i < inum; i++) pairnumsum[i + 1] = pairnumsum[i] + pairnum[i];
+    int ijnum = pairnumsum[inum];
+    std::vector<int> ai(ijnum + 1), aj(ijnum + 1), ti(ijnum + 1), tj(ijnum + 1), aii(ijnum + 1);
+    std::vector<double> rij((size_t)3 * ijnum + 3);
+    cpuNeighPairs(rij.data(), (double *)x, aii.data(), ai.data(), aj.data(), ti.data(), tj.data(), pairnum.data(),
+                  pairlist.data(), pairnumsum.data(), ilist.data(), (int *)atomtype, (int *)alist, inum, neighmax,
+                  dim);
+    // cpuComputeDbidrj reads direction k of dU at offset k * idxu_max * ijnum
+    const size_t nu = (size_t)idxu_max * ijnum;
+    std::vector<double> ulr(nu + 1), uli(nu + 1), dul((size_t)3 * nu * 2 + 1);
+    double *dulr = dul.data(), *duli = dul.data() + 3 * nu;
+    cpuComputeSij(ulr.data(), uli.data(), dulr, duli, dulr + nu, duli + nu, dulr + 2 * nu, duli + 2 * nu,
+                  rootpq.data(), rij.data(), wjelem, radelem, rmin0, rfac0, rcutfac, idxu_block.data(), ti.data(),
+                  tj.data(), twojmax, idxu_max, ijnum, switchflag);
+    std::vector<double> utr((size_t)idxu_max * inum), uti((size_t)idxu_max * inum);
+    cpuZeroUarraytot2(utr.data(), uti.data(), wself, idxu_block.data(), (int *)atomtype, map, ai.data(),
+                      wselfallflag, chemflag, idxu_max, nelem, twojmax, inum);
+    cpuAddUarraytot(utr.data(), uti.data(), ulr.data(), uli.data(), map, ai.data(), tj.data(), idxu_max, inum, ijnum,
+                    chemflag);
+    std::vector<double> zr((size_t)idxz_max * inum), zi((size_t)idxz_max * inum);
+    cpuComputeZi2(zr.data(), zi.data(), utr.data(), uti.data(), cglist.data(), idxz.data(), idxu_block.data(),
+                  idxcg_block.data(), twojmax, idxu_max, idxz_max, nelem, bnormflag, inum);
+    std::vector<double> blist((size_t)idxb_max * inum);
+    cpuComputeBi2(blist.data(), zr.data(), zi.data(), utr.data(), uti.data(), bzero, ilist.data(), (int *)atomtype,
+                  map, idxb.data(), idxu_block.data(), idxz_block.data(), twojmax, idxb_max, idxu_max, idxz_max,
+                  nelem, bzeroflag, wselfallflag, chemflag, inum);
+    std::vector<double> dblist((size_t)idxb_max * 3 * (ijnum + 1));
+    cpuComputeDbidrj(dblist.data(), zr.data(), zi.data(), dulr, duli, idxb.data(), idxu_block.data(),
+                     idxz_block.data(), map, ai.data(), tj.data(), twojmax, idxb_max, idxu_max, idxz_max, nelem,
+                     bnormflag, chemflag, inum, ijnum);
+    std::vector<int> type1(inum, 1);
+    cpuSnapTallyBispectrum(bi, blist.data(), ilist.data(), type1.data(), inum, ncoeff, nperdim, ntypes,
+                           quadraticflag);
+    cpuSnapTallyBispectrumDeriv(bd, blist.data(), dblist.data(), aii.data(), ai.data(), aj.data(), ti.data(), inum,
+                                ijnum, ncoeff, nperdim, ntypes, quadraticflag);
+    cpuSnapTallyBispectrumVirial(bv, blist.data(), dblist.data(), rij.data(), aii.data(), ai.data(), aj.data(),
+                                 ti.data(), inum, ijnum, ncoeff, nperdim, ntypes, quadraticflag);
+    if (blist_out) std::copy(blist.begin(), blist.end(), blist_out);
+}
+
 void ref_nve_initial(double *x, double *v, const double *f, const double *mass, double dtf,
                      double dtv, const int *type, const int *ilist, int inum)
 {

@@ -42,6 +42,10 @@ def lib():
                                         C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_int, C.c_int]
+        _lib.ref_snap_descriptors.argtypes = [_dp, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _ip, C.c_int, C.c_int,
+                                              C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                              C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
+        _lib.ref_snap_descriptors.restype = None
         _lib.ref_nve_initial.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double, _ip, _ip, C.c_int]
         _lib.ref_nve_final.argtypes = [_dp, _dp, _dp, _dp, C.c_double, _ip, _ip, C.c_int]
         _lib.ref_omp_max_threads.restype = C.c_int
@@ -96,3 +100,20 @@ def snap_force(x_all, alist, neighlist, neighnum, params, nblocks=1, nthreads=1)
                          params.switchflag, params.bzeroflag, params.bnormflag, params.wselfallflag,
                          nblocks, nthreads)
     return e, f.reshape(inum, 3), v.reshape(6, inum)
+
+
+def snap_descriptors(x_all, alist, neighlist, neighnum, params):
+    """Per-configuration descriptors from the reference's ComputeSnap chain
+    (snappotential.cpp:762-910, cpuSnap2.cpp): bi (ncoeff,), bd (ncoeff, inum, 3)
+    with bd[k, i, c] = d(sum_a B_ak)/dx_ic, bv (ncoeff, 6) and per-atom B (ncoeff, inum)."""
+    inum, neighmax = neighlist.shape
+    nc = params.ncoeff
+    bi = np.zeros(nc); bd = np.zeros(3 * inum * nc); bv = np.zeros(6 * nc); bl = np.zeros(inum * nc)
+    atype = np.ones(x_all.shape[0], dtype=np.int32)
+    lib().ref_snap_descriptors(bi, bd, bv, bl, np.ascontiguousarray(x_all).ravel(), atype,
+                               np.ascontiguousarray(alist, dtype=np.int32),
+                               np.ascontiguousarray(neighlist, dtype=np.int32).ravel(),
+                               np.ascontiguousarray(neighnum, dtype=np.int32), inum, neighmax, params.twojmax,
+                               params.rcutfac, params.rfac0, params.rmin0, params.radelem, params.wjelem,
+                               params.switchflag, params.bzeroflag, params.bnormflag, params.wselfallflag)
+    return bi, bd.reshape(nc, inum, 3), bv.reshape(nc, 6), bl.reshape(nc, inum)

@@ -15,6 +15,11 @@ implementation computes for it:
     CIntegration::VelocityVerlet (Integration.cpp:17-139), with thermo rows.
 The inputs are regenerated by the tests from the stored seeds and checked
 against the stored copies, so the fixtures also pin the input generator.
+
+The fit_* fixtures hold single configurations of the batched-fitting workload
+(BCC / FCC / A15 supercells) with the per-configuration descriptors of MDP's
+ComputeSnap chain (snappotential.cpp:762-910, cpuSnap2.cpp): bi, bd, bv and the
+per-atom bispectrum (`--fit-only` regenerates just these).
 """
 from __future__ import annotations
 
@@ -93,8 +98,35 @@ def ref_md(x0, v0, box, p, nsteps, dt, mass):
     return np.array(rows), x, v, f, e, rebuilds
 
 
+# descriptor fixtures (ComputeSnap chain): (name, kind, target atoms, strain, sigma, seed, 2J, flag overrides)
+FIT_CASES = [
+    ("fit_bcc16_2j8", "bcc", 16, 0.03, 0.10, 31, 8, {}),
+    ("fit_fcc32_2j8", "fcc", 32, -0.04, 0.20, 32, 8, {}),
+    ("fit_a15_64_2j8", "a15", 64, 0.00, 0.05, 33, 8, {}),
+    ("fit_bcc54_2j6_flags", "bcc", 54, 0.02, 0.30, 34, 6, {"bnormflag": 1, "bzeroflag": 1}),
+]
+
+
+def fit_fixtures():
+    """Per configuration: positions, box and the reference's bi, bd, bv, blist."""
+    from mdp_b200 import fit
+    for (name, kind, target, strain, sigma, seed, tj, flags) in FIT_CASES:
+        rng = np.random.default_rng(seed)
+        cfg = fit.make_config(kind, target, strain, sigma, rng)
+        p = configs.snap_params(tj, seed=0, **flags)
+        xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+        bi, bd, bv, bl = refpy.snap_descriptors(xa, al, nl, nn, p)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, kind=kind, twojmax=tj, flags=np.array([p.bnormflag, p.bzeroflag, p.switchflag]),
+                            x=cfg.x, box=cfg.box, bi=bi, bd=bd, bv=bv, blist=bl)
+        print(name, cfg.natoms, "atoms", os.path.getsize(path), "bytes")
+
+
 def main():
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    fit_fixtures()
+    if "--fit-only" in sys.argv:
+        return
     for (name, cells, tj, temp, jit, seed, cseed, flags, nsteps, dt) in CASES:
         p = configs.snap_params(tj, seed=cseed, **flags)
         cfg = configs.ta_config(cells, temp=temp, jitter=jit, seed=seed)
