@@ -189,6 +189,10 @@ int mdp_fit_ncoeff(mdp_fit *h);
 int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *box, const double *x,
                       const double *e, const double *f, const double *we, const double *wf);
 long long mdp_fit_npairs(mdp_fit *h);
+/* scratch budget of the chunked stages (default 24e9 bytes; the batch is
+ * processed in configuration-aligned chunks that fit it) and the chunk count */
+int mdp_fit_set_chunk_bytes(mdp_fit *h, double bytes);
+int mdp_fit_nchunks(mdp_fit *h);
 /* bi [nconf][ncoeff]; bd [atom][3][ncoeff] with the reference's sign
  * (cpuSnapTallyBispectrumDeriv: -d(sum_i B_i)/dx); bv [nconf][ncoeff][6];
  * blist [ncoeff][atom].  Any output may be NULL. */

@@ -100,6 +100,8 @@ def lib():
                                     C.c_void_p]
     L.mdp_fit_npairs.argtypes = [C.c_void_p]
     L.mdp_fit_npairs.restype = C.c_longlong
+    L.mdp_fit_set_chunk_bytes.argtypes = [C.c_void_p, C.c_double]
+    L.mdp_fit_nchunks.argtypes = [C.c_void_p]
     L.mdp_fit_descriptors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.mdp_fit_run.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.POINTER(C.c_float)]
     L.mdp_fit_tune.argtypes = [C.c_void_p, _ip32]

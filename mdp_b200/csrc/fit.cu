@@ -93,18 +93,17 @@ constexpr int FIT_ZB_WARPS = 8;
 
 __global__ void __launch_bounds__(FIT_ZB_WARPS * 32)
 k_fit_zb(const double2 *__restrict__ Ut, int natoms, const FitTables *__restrict__ T, double2 *__restrict__ Z,
-         double *__restrict__ B)
+         double *__restrict__ B, int tile_lo, int tile_hi)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *Us = reinterpret_cast<double2 *>(smraw);
     const int tj = T->tj, nu = idxu_count(tj), nz = T->nz;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int ntiles = (natoms + 31) >> 5;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    for (int tile = tile_lo + blockIdx.x; tile < tile_hi; tile += gridDim.x) {
         const double2 *src = Ut + (size_t)tile * nu * 32;
         for (int k = threadIdx.x; k < nu * 32; k += blockDim.x) Us[k] = src[k];
         __syncthreads();
-        double2 *Zt = Z + (size_t)tile * nz * 32 + lane;
+        double2 *Zt = Z + (size_t)(tile - tile_lo) * nz * 32 + lane;
         // work items: (coupling, row mb)
         int item = 0;
         for (int c = 0; c < T->ncoup; c++) {
@@ -280,13 +279,14 @@ k_fit_du(const double4 *__restrict__ prij, long npairs, SnapGeom gp, double2 *__
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(128)
 k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int2 *__restrict__ pinfo, long npairs,
-                           const FitTables *__restrict__ T, const double2 *__restrict__ Z, double *__restrict__ dbdr)
+                           const FitTables *__restrict__ T, const double2 *__restrict__ Z, int tile_lo,
+                           double *__restrict__ dbdr)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 3 * npairs) return;
     const int atom = pinfo[t / 3].x;
     const int nz = T->nz;
-    const double2 *Zi = Z + (size_t)(atom >> 5) * nz * 32 + (atom & 31);
+    const double2 *Zi = Z + (size_t)((atom >> 5) - tile_lo) * nz * 32 + (atom & 31);
     const double2 *d = dul + t;
     for (int k = 0; k < T->ntri; k++) {
         double acc = 0.0;
@@ -341,26 +341,26 @@ __global__ void k_fit_rev_sort(int natoms, const int *__restrict__ roff, int *__
 
 // rows of atom a: G[a][c][k] = sum_(p: j = a) dbdr - sum_(p: i = a) dbdr,
 // written as fit rows [wf * (0, G)] with target -wf * f; row = 3 a + c
-__global__ void k_fit_rows(int natoms, int ntri, const int *__restrict__ poff, const int *__restrict__ roff,
-                           const int *__restrict__ rlist, const double *__restrict__ dbdr, long stride,
+__global__ void k_fit_rows(int a_lo, int a_hi, int ntri, const int *__restrict__ poff, const int *__restrict__ roff,
+                           const int *__restrict__ rlist, const double *__restrict__ dbdr, long stride, long p_lo,
                            const int *__restrict__ cfg, const double *__restrict__ wf, const double *__restrict__ f,
                            double *__restrict__ G, double *__restrict__ R, double *__restrict__ tgt, long row0)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (atom, k)
-    if (t >= (long)natoms * FIT_KP) return;
-    const int a = (int)(t / FIT_KP), k = (int)(t % FIT_KP);
+    if (t >= (long)(a_hi - a_lo) * FIT_KP) return;
+    const int a = a_lo + (int)(t / FIT_KP), k = (int)(t % FIT_KP);
     const double w = wf ? wf[cfg[a]] : 1.0;
     double g[3] = {0.0, 0.0, 0.0};
     if (k >= 1 && k <= ntri) {
         const int kk = k - 1;
         for (int q = roff[a]; q < roff[a + 1]; q++) {
-            const long p = rlist[q];
+            const long p = rlist[q] - p_lo;
 #pragma unroll
             for (int c = 0; c < 3; c++) g[c] += dbdr[(long)kk * stride + 3 * p + c];
         }
-        for (int p = poff[a]; p < poff[a + 1]; p++) {
+        for (long p = poff[a] - p_lo; p < poff[a + 1] - p_lo; p++) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) g[c] -= dbdr[(long)kk * stride + 3 * (long)p + c];
+            for (int c = 0; c < 3; c++) g[c] -= dbdr[(long)kk * stride + 3 * p + c];
         }
         if (G)
             for (int c = 0; c < 3; c++) G[((size_t)a * 3 + c) * ntri + kk] = g[c];
@@ -373,15 +373,15 @@ __global__ void k_fit_rows(int natoms, int ntri, const int *__restrict__ poff, c
 }
 
 // per configuration: bi, the virial, and the energy row [we * (N, bi)] / we * E
-__global__ void k_fit_cfg(int nconf, int ntri, const int *__restrict__ ca0, const int *__restrict__ cn,
+__global__ void k_fit_cfg(int c_lo, int c_hi, int ntri, const int *__restrict__ ca0, const int *__restrict__ cn,
                           const int *__restrict__ poff, const double *__restrict__ B, int natoms,
-                          const double *__restrict__ dbdr, long stride, const double4 *__restrict__ prij,
+                          const double *__restrict__ dbdr, long stride, long p_lo, const double4 *__restrict__ prij,
                           const double *__restrict__ we, const double *__restrict__ e, double *__restrict__ bi,
                           double *__restrict__ bv, double *__restrict__ R, double *__restrict__ tgt, long erow0)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (config, k)
-    if (t >= (long)nconf * FIT_KP) return;
-    const int c = (int)(t / FIT_KP), k = (int)(t % FIT_KP);
+    if (t >= (long)(c_hi - c_lo) * FIT_KP) return;
+    const int c = c_lo + (int)(t / FIT_KP), k = (int)(t % FIT_KP);
     const int a0 = ca0[c], n = cn[c];
     double v = 0.0;
     if (k == 0) v = (double)n;
@@ -393,8 +393,9 @@ __global__ void k_fit_cfg(int nconf, int ntri, const int *__restrict__ ca0, cons
             double s[6] = {0, 0, 0, 0, 0, 0};
             for (long p = poff[a0]; p < poff[a0 + n]; p++) {
                 const double4 r = prij[p];
-                const double bx = dbdr[(long)kk * stride + 3 * p], by = dbdr[(long)kk * stride + 3 * p + 1],
-                             bz = dbdr[(long)kk * stride + 3 * p + 2];
+                const long q = p - p_lo;
+                const double bx = dbdr[(long)kk * stride + 3 * q], by = dbdr[(long)kk * stride + 3 * q + 1],
+                             bz = dbdr[(long)kk * stride + 3 * q + 2];
                 s[0] -= r.x * bx; s[1] -= r.y * by; s[2] -= r.z * bz;
                 s[3] -= r.x * by; s[4] -= r.x * bz; s[5] -= r.y * bz;
             }
@@ -614,6 +615,13 @@ struct mdp_fit {
     ForcePath fp;
     long npairs = 0, nrows = 0;
     bool pairs_ready = false;
+    // the Z / dU / dB/dR stages run over configuration-aligned chunks that fit
+    // the scratch budget; U, B, the rows and the Gram pass span the batch
+    struct Chunk { int c_lo, c_hi, a_lo, a_hi, t_lo, t_hi; long p_lo, p_hi; };
+    std::vector<Chunk> chunks;
+    double chunk_bytes = 24.0e9;   // scratch of the chunked stages (dU rows, dB/dR, Z) per chunk at most
+    long chunk_pairs_max = 0;
+    int chunk_tiles_max = 0;
     // launch shapes (autotuned): threads of the per-pair kernels, rows per Gram CTA
     int du_threads = 128, db_threads = 128, gram_rows = 4096;
     cudaGraph_t graph = nullptr;
@@ -666,60 +674,78 @@ static int fit_pairs(mdp_fit *h)
 }
 
 template <int TJ>
-static int fit_launch_du(mdp_fit *h)
+static int fit_launch_du(mdp_fit *h, const mdp_fit::Chunk &ck)
 {
     if (tu_ensure_tables()) return -1;
-    const long nt = 3 * h->npairs;
+    const long np = ck.p_hi - ck.p_lo, nt = 3 * np;
     if (nt == 0) return 0;
     k_fit_du<TJ><<<(unsigned)((nt + h->du_threads - 1) / h->du_threads), h->du_threads, 0, h->s>>>(
-        h->fp.prij.as<double4>(), h->npairs, h->model.geom, h->dul.as<double2>(), nt);
+        h->fp.prij.as<double4>() + ck.p_lo, np, h->model.geom, h->dul.as<double2>(), nt);
     count_launches(1);
     return 0;
 }
 
-// descriptors of the whole batch: U, Z, B, dU, dB/dR, rows; no host synchronisation
-static int fit_descriptor_stages(mdp_fit *h, bool rows)
+static int fit_du(mdp_fit *h, const mdp_fit::Chunk &ck)
+{
+    const int tj = h->model.p.twojmax;
+    return tj == 8 ? fit_launch_du<8>(h, ck) : tj == 6 ? fit_launch_du<6>(h, ck) : fit_launch_du<4>(h, ck);
+}
+
+static void fit_dbdr(mdp_fit *h, const mdp_fit::Chunk &ck, int threads)
+{
+    const long np = ck.p_hi - ck.p_lo, nt = 3 * np;
+    if (nt == 0) return;
+    k_fit_dbdr<<<(unsigned)((nt + threads - 1) / threads), threads, 0, h->s>>>(
+        h->dul.as<double2>(), nt, h->fp.pinfo.as<int2>() + ck.p_lo, np, h->tabs.as<FitTables>(), h->Z.as<double2>(),
+        ck.t_lo, h->dbdr.as<double>());
+    count_launches(1);
+}
+
+// Z/B, dU, dB/dR of one chunk, then its rows: into R / tgt (rows) and/or the
+// descriptor outputs G [atom][3][k], bi [config][k], bv [config][k][6]
+static int fit_chunk(mdp_fit *h, const mdp_fit::Chunk &ck, bool rows, double *G, double *bi, double *bv)
+{
+    const int n = h->natoms;
+    const size_t zsm = (size_t)idxu_count(h->model.p.twojmax) * 32 * sizeof(double2);
+    k_fit_zb<<<std::max(1, std::min(ck.t_hi - ck.t_lo, num_sms())), FIT_ZB_WARPS * 32, zsm, h->s>>>(
+        h->fp.Ut.as<double2>(), n, h->tabs.as<FitTables>(), h->Z.as<double2>(), h->B.as<double>(), ck.t_lo, ck.t_hi);
+    count_launches(1);
+    if (fit_du(h, ck)) return -1;
+    fit_dbdr(h, ck, h->db_threads);
+    const long nt = 3 * (ck.p_hi - ck.p_lo);
+    const long ta = (long)(ck.a_hi - ck.a_lo) * FIT_KP, tc = (long)(ck.c_hi - ck.c_lo) * FIT_KP;
+    k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(
+        ck.a_lo, ck.a_hi, h->tab.ntri, h->poff.as<int>(), h->roff.as<int>(), h->rlist.as<int>(), h->dbdr.as<double>(),
+        nt, ck.p_lo, h->cfg.as<int>(), h->wf.as<double>(), h->f.as<double>(), G, rows ? h->R.as<double>() : nullptr,
+        rows ? h->tgt.as<double>() : nullptr, h->nconf);
+    k_fit_cfg<<<(unsigned)((tc + 255) / 256), 256, 0, h->s>>>(
+        ck.c_lo, ck.c_hi, h->tab.ntri, h->ca0.as<int>(), h->cn.as<int>(), h->poff.as<int>(), h->B.as<double>(), n,
+        h->dbdr.as<double>(), nt, ck.p_lo, h->fp.prij.as<double4>(), h->we.as<double>(), h->e.as<double>(), bi, bv,
+        rows ? h->R.as<double>() : nullptr, rows ? h->tgt.as<double>() : nullptr, 0);
+    count_launches(2);
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// U over the batch, then every chunk; no host synchronisation
+static int fit_descriptor_stages(mdp_fit *h, bool rows, double *G = nullptr, double *bi = nullptr,
+                                 double *bv = nullptr)
 {
     const int n = h->natoms, tj = h->model.p.twojmax;
-    const int ntiles = (n + 31) / 32;
-    const long nt = 3 * h->npairs;
     if (tu_ensure_tables()) return -1;
     const int urc = tj == 8 ? launch_ui<double, 8>(h->model, h->fp, n, h->s)
                   : tj == 6 ? launch_ui<double, 6>(h->model, h->fp, n, h->s)
                             : launch_ui<double, 4>(h->model, h->fp, n, h->s);
     if (urc) return -1;
     count_launches(1);
-    const size_t zsm = (size_t)idxu_count(tj) * 32 * sizeof(double2);
     static bool attr = false;
     if (!attr) {
         MDP_CUDA_TRY(cudaFuncSetAttribute(k_fit_zb, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)((size_t)idxu_count(TJMAX) * 32 * sizeof(double2))));
         attr = true;
     }
-    k_fit_zb<<<std::min(ntiles, num_sms() * 1), FIT_ZB_WARPS * 32, zsm, h->s>>>(
-        h->fp.Ut.as<double2>(), n, h->tabs.as<FitTables>(), h->Z.as<double2>(), h->B.as<double>());
-    count_launches(1);
-    if (tj == 8) { if (fit_launch_du<8>(h)) return -1; }
-    else if (tj == 6) { if (fit_launch_du<6>(h)) return -1; }
-    else { if (fit_launch_du<4>(h)) return -1; }
-    if (nt) {
-        k_fit_dbdr<<<(unsigned)((nt + h->db_threads - 1) / h->db_threads), h->db_threads, 0, h->s>>>(
-            h->dul.as<double2>(), nt, h->fp.pinfo.as<int2>(), h->npairs, h->tabs.as<FitTables>(), h->Z.as<double2>(),
-            h->dbdr.as<double>());
-        count_launches(1);
-    }
-    if (rows) {
-        const long ta = (long)n * FIT_KP, tc = (long)h->nconf * FIT_KP;
-        k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(
-            n, h->tab.ntri, h->poff.as<int>(), h->roff.as<int>(), h->rlist.as<int>(), h->dbdr.as<double>(), nt,
-            h->cfg.as<int>(), h->wf.as<double>(), h->f.as<double>(), nullptr, h->R.as<double>(), h->tgt.as<double>(),
-            h->nconf);
-        k_fit_cfg<<<(unsigned)((tc + 255) / 256), 256, 0, h->s>>>(
-            h->nconf, h->tab.ntri, h->ca0.as<int>(), h->cn.as<int>(), h->poff.as<int>(), h->B.as<double>(), n,
-            h->dbdr.as<double>(), nt, h->fp.prij.as<double4>(), h->we.as<double>(), h->e.as<double>(), nullptr,
-            nullptr, h->R.as<double>(), h->tgt.as<double>(), 0);
-        count_launches(2);
-    }
+    for (const auto &ck : h->chunks)
+        if (fit_chunk(h, ck, rows, G, bi, bv)) return -1;
     MDP_CUDA_TRY(cudaGetLastError());
     return 0;
 }
@@ -755,16 +781,50 @@ static int fit_gram_stages(mdp_fit *h, int mode)
     return 0;
 }
 
+
 static int fit_alloc_work(mdp_fit *h)
 {
     const int n = h->natoms, tj = h->model.p.twojmax;
     const long ntiles = (n + 31) / 32;
-    const long nt = std::max(3 * h->npairs, 1L);
     h->nrows = h->nconf + 3L * n;
-    const int nbmax = (int)((h->nrows + 255) / 256) + 1;   // smallest gram_rows candidate
+    // chunk plan over whole configurations
+    std::vector<int> poff(n + 1);
+    MDP_CUDA_TRY(cudaMemcpy(poff.data(), h->poff.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+    const double per_pair = 3.0 * (yh_count(tj) * sizeof(double2) + h->tab.ntri * sizeof(double));
+    const double per_tile = (double)h->tab.nz * 32 * sizeof(double2);
+    h->chunks.clear();
+    h->chunk_pairs_max = 1;
+    h->chunk_tiles_max = 1;
+    int c = 0;
+    while (c < h->nconf) {
+        mdp_fit::Chunk ck;
+        ck.c_lo = c;
+        ck.a_lo = h->h_ca0[c];
+        ck.p_lo = poff[ck.a_lo];
+        int c_hi = c;
+        while (c_hi < h->nconf) {
+            const int a_hi = h->h_ca0[c_hi] + h->h_cn[c_hi];
+            const double bytes = per_pair * (poff[a_hi] - ck.p_lo) + per_tile * ((a_hi + 31) / 32 - ck.a_lo / 32);
+            if (c_hi > c && bytes > h->chunk_bytes) break;
+            c_hi++;
+        }
+        ck.c_hi = c_hi;
+        ck.a_hi = h->h_ca0[c_hi - 1] + h->h_cn[c_hi - 1];
+        ck.p_hi = poff[ck.a_hi];
+        ck.t_lo = ck.a_lo / 32;
+        ck.t_hi = (ck.a_hi + 31) / 32;
+        h->chunk_pairs_max = std::max(h->chunk_pairs_max, ck.p_hi - ck.p_lo);
+        h->chunk_tiles_max = std::max(h->chunk_tiles_max, ck.t_hi - ck.t_lo);
+        h->chunks.push_back(ck);
+        c = c_hi;
+    }
+    const long nt = 3 * h->chunk_pairs_max;
+    const int nbmax = (int)((h->nrows + 255) / 256) + 1;   // smallest Gram rows-per-CTA candidate
     if (h->fp.Ut.ensure(sizeof(double2) * ntiles * idxu_count(tj) * 32) ||
-        h->Z.ensure(sizeof(double2) * ntiles * h->tab.nz * 32) || h->B.ensure(sizeof(double) * h->tab.ntri * n) ||
-        h->dul.ensure(sizeof(double2) * nt * yh_count(tj)) || h->dbdr.ensure(sizeof(double) * nt * h->tab.ntri) ||
+        h->Z.ensure(sizeof(double2) * (size_t)h->chunk_tiles_max * h->tab.nz * 32) ||
+        h->B.ensure(sizeof(double) * h->tab.ntri * (size_t)n) ||
+        h->dul.ensure(sizeof(double2) * (size_t)nt * yh_count(tj)) ||
+        h->dbdr.ensure(sizeof(double) * (size_t)nt * h->tab.ntri) ||
         h->R.ensure(sizeof(double) * h->nrows * FIT_KP) || h->tgt.ensure(sizeof(double) * h->nrows) ||
         h->hi.ensure(sizeof(__nv_bfloat16) * h->nrows * FIT_KP) || h->lo.ensure(sizeof(__nv_bfloat16) * h->nrows * FIT_KP) ||
         h->part.ensure(sizeof(double) * (size_t)nbmax * (FIT_KP * FIT_KP + FIT_KP)) ||
@@ -883,6 +943,17 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
 
 long long mdp_fit_npairs(mdp_fit *h) { return h ? h->npairs : -1; }
 
+int mdp_fit_set_chunk_bytes(mdp_fit *h, double bytes)
+{
+    if (!h || !(bytes > 0)) { set_error("bad arguments"); return -1; }
+    h->chunk_bytes = bytes;
+    fit_drop_graph(h);
+    if (h->pairs_ready) return fit_alloc_work(h);
+    return 0;
+}
+
+int mdp_fit_nchunks(mdp_fit *h) { return h ? (int)h->chunks.size() : -1; }
+
 // Descriptors of the batch (any output may be NULL):
 //   bi [nconf][ncoeff], bd [natoms][3][ncoeff] (= -d(sum B)/dx, the layout
 //   order of cpuSnapTallyBispectrumDeriv per atom), bv [nconf][ncoeff][6],
@@ -891,25 +962,12 @@ int mdp_fit_descriptors(mdp_fit *h, double *bi, double *bd, double *bv, double *
 {
     if (!h || !h->pairs_ready) { set_error("set a batch first"); return -1; }
     MDP_CUDA_TRY(cudaSetDevice(h->device));
-    if (fit_descriptor_stages(h, false)) return -1;
     const int n = h->natoms, nc = h->tab.ntri;
-    const long nt = 3 * h->npairs;
     DevBuf dbi, dbv, dG;
     if (dbi.ensure(sizeof(double) * h->nconf * nc) || dbv.ensure(sizeof(double) * h->nconf * nc * 6) ||
         dG.ensure(sizeof(double) * (size_t)n * 3 * nc))
         return -1;
-    const long ta = (long)n * FIT_KP, tc = (long)h->nconf * FIT_KP;
-    k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(n, nc, h->poff.as<int>(), h->roff.as<int>(),
-                                                               h->rlist.as<int>(), h->dbdr.as<double>(), nt,
-                                                               h->cfg.as<int>(), nullptr, nullptr, dG.as<double>(),
-                                                               nullptr, nullptr, 0);
-    k_fit_cfg<<<(unsigned)((tc + 255) / 256), 256, 0, h->s>>>(h->nconf, nc, h->ca0.as<int>(), h->cn.as<int>(),
-                                                              h->poff.as<int>(), h->B.as<double>(), n,
-                                                              h->dbdr.as<double>(), nt, h->fp.prij.as<double4>(),
-                                                              nullptr, nullptr, dbi.as<double>(), dbv.as<double>(),
-                                                              nullptr, nullptr, 0);
-    count_launches(2);
-    MDP_CUDA_TRY(cudaGetLastError());
+    if (fit_descriptor_stages(h, false, dG.as<double>(), dbi.as<double>(), dbv.as<double>())) return -1;
     MDP_CUDA_TRY(cudaStreamSynchronize(h->s));
     if (bi) MDP_CUDA_TRY(cudaMemcpy(bi, dbi.p, sizeof(double) * h->nconf * nc, cudaMemcpyDeviceToHost));
     if (bv) MDP_CUDA_TRY(cudaMemcpy(bv, dbv.p, sizeof(double) * h->nconf * nc * 6, cudaMemcpyDeviceToHost));
@@ -999,26 +1057,18 @@ int mdp_fit_tune(mdp_fit *h, int *out3)
         return best;
     };
     const int tcand[3] = {32, 64, 128};   // within the kernels' launch bounds (128)
-    const int tj = h->model.p.twojmax;
     float bt = 1e30f;
     int bsel = h->du_threads;
     for (int c : tcand) {
         h->du_threads = c;
-        const float t = timeit([&]() { return tj == 8 ? fit_launch_du<8>(h) : tj == 6 ? fit_launch_du<6>(h) : fit_launch_du<4>(h); });
+        const float t = timeit([&]() { return fit_du(h, h->chunks[0]); });
         if (t >= 0 && t < bt) { bt = t; bsel = c; }
     }
     h->du_threads = bsel;
     bt = 1e30f;
     bsel = h->db_threads;
-    const long nt = 3 * h->npairs;
     for (int c : tcand) {
-        h->db_threads = c;
-        const float t = timeit([&]() {
-            k_fit_dbdr<<<(unsigned)((nt + c - 1) / c), c, 0, h->s>>>(h->dul.as<double2>(), nt, h->fp.pinfo.as<int2>(),
-                                                                    h->npairs, h->tabs.as<FitTables>(),
-                                                                    h->Z.as<double2>(), h->dbdr.as<double>());
-            return 0;
-        });
+        const float t = timeit([&]() { fit_dbdr(h, h->chunks[0], c); return 0; });
         if (t >= 0 && t < bt) { bt = t; bsel = c; }
     }
     h->db_threads = bsel;

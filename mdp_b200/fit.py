@@ -117,6 +117,12 @@ class BatchFit:
         self.nconf, self.natoms = len(cfgs), int(n.sum())
         self.counts = n
 
+    def set_chunk_bytes(self, nbytes: float):
+        _lib.check(_lib.lib().mdp_fit_set_chunk_bytes(self._h, float(nbytes)), "mdp_fit_set_chunk_bytes")
+
+    def nchunks(self) -> int:
+        return int(_lib.lib().mdp_fit_nchunks(self._h))
+
     def npairs(self) -> int:
         return int(_lib.lib().mdp_fit_npairs(self._h))
 

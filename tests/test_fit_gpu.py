@@ -79,6 +79,22 @@ def test_fp64_assembly_matches_numpy(small_batch):
     assert np.array_equal(A, A2) and np.array_equal(b, b2)
 
 
+def test_chunked_pipeline_equals_one_chunk(small_batch):
+    bf, cfgs, e, f, we, wf = small_batch
+    A, b, _ = bf.run("fp64")
+    bi, bd, bv, bl = bf.descriptors()
+    assert bf.nchunks() == 1
+    bf.set_chunk_bytes(2e6)          # a few configurations per chunk
+    try:
+        assert bf.nchunks() > 3
+        A2, b2, _ = bf.run("fp64")
+        bi2, bd2, bv2, bl2 = bf.descriptors()
+    finally:
+        bf.set_chunk_bytes(24e9)
+    assert _rel(A2, A) < 1e-13 and _rel(b2, b) < 1e-13
+    assert np.array_equal(bd2, bd) and np.array_equal(bi2, bi) and np.array_equal(bv2, bv)
+
+
 def test_bf16_split_assembly(small_batch):
     bf, cfgs, e, f, we, wf = small_batch
     A, b, _ = bf.run("fp64")
