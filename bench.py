@@ -22,6 +22,12 @@ roofline   the Y kernel (dominant): algorithmic FLOPs / its CUDA-event time,
 cpu_baseline  MDP's own CPU SNAP (oracle/_ref build of src/C++/Core/cpuSnap4.cpp
            chain) on a bounded sample (16,000 atoms, same lattice and model),
            on the host's cores.
+surrogate  MLP on 2J=4 bispectra trained on 20,000 2,000-atom MD snapshots of the
+           plain model, then NVE on the 2M-atom box at 1,000 K with the plain
+           model judging every 50 steps (falls back above 0.05 eV/A force RMSE);
+           also its unjudged rate.
+batched_fit  4,096 fitting configurations: descriptors, dB/dR and the normal
+           equations as one CUDA graph, FP64 and BF16-split assembly.
 
 With --gpus N (torchrun), every rank runs an independent replica of the
 workload (the MD system is not decomposed across GPUs); value sums the ranks'
@@ -347,6 +353,13 @@ def run_ours(args):
     sur_line = None
     if not args.no_surrogate:
         sur_line = surrogate_leg(args, dev, barrier, ws)
+    fit_line = None
+    if not args.no_fit:
+        from mdp_b200 import fit as fitmod
+        fit_line = fitmod.benchmark(args.fit_configs, device=dev, log=lambda m: None)
+        fit_line["workload"] = ("4,096 periodic Ta configurations (BCC/FCC/A15, 16-512 atoms, strain +-5%, "
+                                "jitter U[0.02,0.3] A), 2J=8 bi + dB/dR, normal equations of energy + force rows, "
+                                "targets ~ N(0,1)") if args.fit_configs == 4096 else f"{args.fit_configs} configurations"
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -388,6 +401,7 @@ def run_ours(args):
                      "force_rmse_vs_fp64": fp32_rmse, "force_maxerr_vs_fp64": fp32_max, "unit_err": "eV/A",
                      "fp32_fma_peak_tflops": fp32_peak},
             "surrogate": sur_line,
+            "batched_fit": fit_line,
             "clocks": clk,
             "cpu_baseline": cpu,
         }
@@ -406,6 +420,8 @@ def main():
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate leg")
     ap.add_argument("--sur-snapshots", type=int, default=20000, help="2,000-atom MD snapshots to train on")
     ap.add_argument("--sur-train-steps", type=int, default=20000)
+    ap.add_argument("--no-fit", action="store_true", help="skip the batched-fitting leg")
+    ap.add_argument("--fit-configs", type=int, default=4096)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

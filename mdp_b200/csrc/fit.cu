@@ -413,8 +413,9 @@ __global__ void k_fit_cfg(int c_lo, int c_hi, int ntri, const int *__restrict__ 
 // A = R^T R, b = R^T t over rows [0, nrows)
 // FP64: each CTA sums a slab of rows into a 64 x 64 (+ 64) partial; the
 // partials are added in a fixed order by k_fit_reduce.
-// BF16: R = hi + lo (two BF16 terms); hi^T hi + hi^T lo + lo^T hi with FP32
-// accumulation by warp-level tensor-core MMA (m16n8k16), partials per CTA.
+// BF16: columns equilibrated to unit norm (FP64 pre-pass), R = hi + lo (two
+// BF16 terms), hi^T hi + hi^T lo + lo^T hi with FP32 accumulation by warp-level
+// tensor-core MMA (m16n8k16), partials per CTA summed in FP64, scaling undone.
 // ---------------------------------------------------------------------------
 constexpr int FIT_GRAM_THREADS = 256;
 
@@ -452,13 +453,24 @@ k_fit_gram64(const double *__restrict__ R, const double *__restrict__ tgt, long 
     if ((tid & 3) == 0) o[FIT_KP * FIT_KP + row] = accb;
 }
 
-// hi / lo BF16 split of the rows, [row][64] each
-__global__ void k_fit_split(const double *__restrict__ R, long n, __nv_bfloat16 *__restrict__ hi,
-                            __nv_bfloat16 *__restrict__ lo)
+// column sums of squares of R (one partial per CTA), for the equilibration
+__global__ void k_fit_colsq(const double *__restrict__ R, long nrows, int rows_per_cta, double *__restrict__ part)
+{
+    const int c = threadIdx.x;   // 64 threads
+    const long r0 = (long)blockIdx.x * rows_per_cta, r1 = min(nrows, r0 + rows_per_cta);
+    double s = 0.0;
+    for (long r = r0; r < r1; r++) { const double v = R[r * FIT_KP + c]; s += v * v; }
+    part[(size_t)blockIdx.x * FIT_KP + c] = s;
+}
+
+// hi / lo BF16 split of the column-equilibrated rows R[r][k] / sqrt(sum_r R[r][k]^2)
+__global__ void k_fit_split(const double *__restrict__ R, long n, const double *__restrict__ colsq,
+                            __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo)
 {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double v = R[i];
+    const double q = colsq[i % FIT_KP];
+    const double v = q > 0.0 ? R[i] / sqrt(q) : 0.0;
     const __nv_bfloat16 h = __double2bfloat16(v);
     hi[i] = h;
     lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
@@ -765,8 +777,12 @@ static int fit_gram_stages(mdp_fit *h, int mode)
         count_launches(2);
     } else {
         const long ne = nr * FIT_KP;
-        k_fit_split<<<(unsigned)((ne + 255) / 256), 256, 0, h->s>>>(h->R.as<double>(), ne, h->hi.as<__nv_bfloat16>(),
-                                                                    h->lo.as<__nv_bfloat16>());
+        double *colsq = out + FIT_KP * FIT_KP + FIT_KP;
+        MDP_CUDA_TRY(cudaMemsetAsync(colsq, 0, sizeof(double) * FIT_KP, h->s));
+        k_fit_colsq<<<nb, FIT_KP, 0, h->s>>>(h->R.as<double>(), nr, rpc, h->part.as<double>());
+        k_fit_reduce<double><<<1, FIT_KP, 0, h->s>>>(h->part.as<double>(), nb, FIT_KP, FIT_KP, colsq);
+        k_fit_split<<<(unsigned)((ne + 255) / 256), 256, 0, h->s>>>(h->R.as<double>(), ne, colsq,
+                                                                    h->hi.as<__nv_bfloat16>(), h->lo.as<__nv_bfloat16>());
         float *pf = h->part.as<float>();
         k_fit_gram_bf16<<<nb, 128, 0, h->s>>>(h->hi.as<__nv_bfloat16>(), h->lo.as<__nv_bfloat16>(), nr, rpc, pf);
         k_fit_reduce<float><<<(FIT_KP * FIT_KP + 255) / 256, 256, 0, h->s>>>(pf, nb, FIT_KP * FIT_KP,
@@ -775,7 +791,7 @@ static int fit_gram_stages(mdp_fit *h, int mode)
         k_fit_rhs_bf16<<<nb, FIT_KP, 0, h->s>>>(h->hi.as<__nv_bfloat16>(), h->lo.as<__nv_bfloat16>(),
                                                 h->tgt.as<double>(), nr, rpc, pb);
         k_fit_reduce<float><<<1, FIT_KP, 0, h->s>>>(pb, nb, FIT_KP, FIT_KP, out + FIT_KP * FIT_KP);
-        count_launches(5);
+        count_launches(7);
     }
     MDP_CUDA_TRY(cudaGetLastError());
     return 0;
@@ -828,7 +844,7 @@ static int fit_alloc_work(mdp_fit *h)
         h->R.ensure(sizeof(double) * h->nrows * FIT_KP) || h->tgt.ensure(sizeof(double) * h->nrows) ||
         h->hi.ensure(sizeof(__nv_bfloat16) * h->nrows * FIT_KP) || h->lo.ensure(sizeof(__nv_bfloat16) * h->nrows * FIT_KP) ||
         h->part.ensure(sizeof(double) * (size_t)nbmax * (FIT_KP * FIT_KP + FIT_KP)) ||
-        h->out.ensure(sizeof(double) * (FIT_KP * FIT_KP + FIT_KP)))
+        h->out.ensure(sizeof(double) * (FIT_KP * FIT_KP + 2 * FIT_KP)))
         return -1;
     return 0;
 }
@@ -1022,8 +1038,18 @@ int mdp_fit_run(mdp_fit *h, int mode, double *A, double *b, float *elapsed_ms)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (elapsed_ms) *elapsed_ms = ms;
-    std::vector<double> o(FIT_KP * FIT_KP + FIT_KP);
+    std::vector<double> o(FIT_KP * FIT_KP + 2 * FIT_KP);
     MDP_CUDA_TRY(cudaMemcpy(o.data(), h->out.p, sizeof(double) * o.size(), cudaMemcpyDeviceToHost));
+    if (mode == 1) {
+        // undo the column equilibration: A = D^-1 A' D^-1, b = D^-1 b'
+        const double *q = o.data() + FIT_KP * FIT_KP + FIT_KP;
+        double d[FIT_KP];
+        for (int k = 0; k < FIT_KP; k++) d[k] = q[k] > 0.0 ? sqrt(q[k]) : 0.0;
+        for (int k = 0; k < FIT_KP; k++) {
+            for (int l = 0; l < FIT_KP; l++) o[k * FIT_KP + l] *= d[k] * d[l];
+            o[FIT_KP * FIT_KP + k] *= d[k];
+        }
+    }
     if (A) memcpy(A, o.data(), sizeof(double) * FIT_KP * FIT_KP);
     if (b) memcpy(b, o.data() + FIT_KP * FIT_KP, sizeof(double) * FIT_KP);
     return 0;

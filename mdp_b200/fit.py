@@ -174,3 +174,50 @@ def rows_numpy(cfgs, bi, bd, e, f, we=None, wf=None):
         R[rows, 1:] = wf[c] * G.reshape(-1, k)
         t[rows] = -wf[c] * f[a0[c]:a0[c + 1]].reshape(-1)
     return R, t
+
+
+def benchmark(nconf: int = 4096, seed: int = 2024, coeff_seed: int = 2024, device: int = 0, log=print) -> dict:
+    """The batched-fitting workload end to end: batch set-up (positions to the
+    device, pair lists), autotuning, then one graph launch per assembly mode
+    (timed with CUDA events), and the FP64 vs BF16-split solutions."""
+    import time
+    from .configs import snap_params
+    cfgs, e, f = batch_configs(nconf, seed=seed)
+    p = snap_params(8, seed=coeff_seed)
+    bf = BatchFit(p, device=device)
+    t0 = time.perf_counter()
+    bf.set_batch(cfgs, e, f)
+    t_set = time.perf_counter() - t0
+    tuned = bf.tune()
+    out = {"configs": nconf, "atoms": bf.natoms, "pairs": bf.npairs(), "chunks": bf.nchunks(),
+           "rows": nconf + 3 * bf.natoms, "batch_setup_s": t_set, "tuned": tuned}
+    sol = {}
+    for mode in ("fp64", "bf16"):
+        bf.run(mode)                       # capture and warm
+        A, b, ms = bf.run(mode)            # one graph launch
+        out[f"graph_ms_{mode}"] = ms
+        sol[mode] = (A, b)
+    A64, b64 = sol["fp64"]
+    A16, b16 = sol["bf16"]
+    beta64 = np.linalg.solve(A64, b64)
+    beta16 = np.linalg.solve(A16, b16)
+    out["A_rel_err_bf16"] = float(np.linalg.norm(A16 - A64) / np.linalg.norm(A64))
+    out["b_rel_err_bf16"] = float(np.linalg.norm(b16 - b64) / np.linalg.norm(b64))
+    out["beta_rel_err_bf16"] = float(np.linalg.norm(beta16 - beta64) / np.linalg.norm(beta64))
+    out["cond_A"] = float(np.linalg.cond(A64))
+    dg = 1.0 / np.sqrt(np.diag(A64))
+    out["cond_A_equilibrated"] = float(np.linalg.cond(A64 * dg[:, None] * dg[None, :]))
+    out["configs_per_s_fp64"] = nconf / (out["graph_ms_fp64"] * 1e-3)
+    out["atoms_per_s_fp64"] = bf.natoms / (out["graph_ms_fp64"] * 1e-3)
+    bf.close()
+    log(out)
+    return out
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="batched SNAP descriptors + normal equations benchmark")
+    ap.add_argument("--configs", type=int, default=4096)
+    a = ap.parse_args()
+    print(json.dumps(benchmark(a.configs, log=lambda m: None), indent=1))
