@@ -46,6 +46,10 @@ struct FitTables {
     int ncoup, ntri, nz, tj, bnorm, bzero;
     FitCoupling cp[FIT_NCP];
     FitTriple tr[FIT_NT];
+    // the dB/dR terms grouped by their dU layer: lt_off[L] .. lt_off[L] + lt_n[L]
+    int lt_n[JD], lt_off[JD];
+    int lt_k[3 * FIT_NT], lt_z[3 * FIT_NT];
+    double lt_fac[3 * FIT_NT];
 };
 
 // ---------------------------------------------------------------------------
@@ -277,37 +281,63 @@ k_fit_du(const double4 *__restrict__ prij, long npairs, SnapGeom gp, double2 *__
 // (Z of the centre atom's couplings against the pair's dU rows), half plane
 // with the middle row's centre at 1/2.  dbdr[k * stride + t]
 // ---------------------------------------------------------------------------
+// The pair's dU rows of layer L are loaded once (registers) and every dB/dR
+// term on that layer is applied to them: dU is read once per thread, Z rows
+// come through L1 (all of an atom's pair-directions read the same Z).
+template <int L>
+__device__ __forceinline__ void fdb_layer(const double2 *__restrict__ d, const long stride,
+                                          const double2 *__restrict__ Zi, const FitTables *__restrict__ T,
+                                          double *__restrict__ acc)
+{
+    constexpr int YO = yh_block(L), NR = L / 2 + 1, NE = NR * (L + 1);
+    double2 du[NE];
+#pragma unroll
+    for (int e = 0; e < NE; e++) du[e] = d[(long)(YO + e) * stride];
+    const int q0 = T->lt_off[L], q1 = q0 + T->lt_n[L];
+    for (int q = q0; q < q1; q++) {
+        const double2 *z = Zi + (size_t)T->lt_z[q] * 32;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int e = 0; e < NE; e++) {
+            const int mb = e / (L + 1), ma = e % (L + 1);
+            if (2 * mb == L && ma > mb) continue;   // right of a middle row's centre
+            const double wgt = (2 * mb == L && ma == mb) ? 0.5 : 1.0;
+            const double2 zz = z[(size_t)e * 32];
+            if (e & 1) s1 += wgt * (du[e].x * zz.x + du[e].y * zz.y);
+            else s0 += wgt * (du[e].x * zz.x + du[e].y * zz.y);
+        }
+        acc[T->lt_k[q]] += T->lt_fac[q] * (s0 + s1);
+    }
+}
+
+template <int TJ, int L>
+__device__ __forceinline__ void fdb_layers(const double2 *__restrict__ d, const long stride,
+                                           const double2 *__restrict__ Zi, const FitTables *__restrict__ T,
+                                           double *__restrict__ acc)
+{
+    if constexpr (L <= TJ) {
+        fdb_layer<L>(d, stride, Zi, T, acc);
+        fdb_layers<TJ, L + 1>(d, stride, Zi, T, acc);
+    }
+}
+
+// dB_ik/dr_p along one axis: 2 sum over the three terms of cpuComputeDbidrj
+// (Z of the centre atom's couplings against the pair's dU rows), half plane
+// with the middle row's centre at 1/2.  dbdr[k * stride + t]
+template <int TJ>
 __global__ void __launch_bounds__(128)
 k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int2 *__restrict__ pinfo, long npairs,
-                           const FitTables *__restrict__ T, const double2 *__restrict__ Z, int tile_lo,
-                           double *__restrict__ dbdr)
+           const FitTables *__restrict__ T, const double2 *__restrict__ Z, int tile_lo, double *__restrict__ dbdr)
 {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 3 * npairs) return;
     const int atom = pinfo[t / 3].x;
-    const int nz = T->nz;
+    const int nz = T->nz, ntri = T->ntri;
     const double2 *Zi = Z + (size_t)((atom >> 5) - tile_lo) * nz * 32 + (atom & 31);
-    const double2 *d = dul + t;
-    for (int k = 0; k < T->ntri; k++) {
-        double acc = 0.0;
-        for (int q = 0; q < 3; q++) {
-            const int L = T->tr[k].layer[q];
-            const int zo = T->cp[T->tr[k].coup[q]].zoff, yo = yh_block(L);
-            double s = 0.0;
-            for (int mb = 0; 2 * mb <= L; mb++) {
-                const int mamax = (2 * mb < L) ? L : mb;
-                for (int ma = 0; ma <= mamax; ma++) {
-                    const double wgt = (2 * mb < L || ma < mb) ? 1.0 : 0.5;
-                    const int e = (L + 1) * mb + ma;
-                    const double2 du = d[(long)(yo + e) * stride];
-                    const double2 z = Zi[(size_t)(zo + e) * 32];
-                    s += wgt * (du.x * z.x + du.y * z.y);
-                }
-            }
-            acc += 2.0 * T->tr[k].fac[q] * s;
-        }
-        dbdr[(long)k * stride + t] = acc;
-    }
+    double acc[FIT_NT];
+    for (int k = 0; k < ntri; k++) acc[k] = 0.0;
+    fdb_layers<TJ, 0>(dul + t, stride, Zi, T, acc);
+    for (int k = 0; k < ntri; k++) dbdr[(long)k * stride + t] = acc[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -607,6 +637,19 @@ static void fit_tables(FitTables &T, int tj, int bnorm, int bzero)
                 t.layer[1] = j1; t.coup[1] = idx[j][j2][j1]; t.fac[1] = bnorm ? 1.0 : (j + 1) / (j1 + 1.0);
                 t.layer[2] = j2; t.coup[2] = idx[j][j1][j2]; t.fac[2] = bnorm ? 1.0 : (j + 1) / (j2 + 1.0);
             }
+    int q = 0;
+    for (int L = 0; L < JD; L++) {
+        T.lt_off[L] = q;
+        for (int k = 0; k < T.ntri; k++)
+            for (int r = 0; r < 3; r++)
+                if (T.tr[k].layer[r] == L) {
+                    T.lt_k[q] = k;
+                    T.lt_z[q] = T.cp[T.tr[k].coup[r]].zoff;
+                    T.lt_fac[q] = 2.0 * T.tr[k].fac[r];
+                    q++;
+                }
+        T.lt_n[L] = q - T.lt_off[L];
+    }
 }
 
 }  // namespace mdp
@@ -707,9 +750,15 @@ static void fit_dbdr(mdp_fit *h, const mdp_fit::Chunk &ck, int threads)
 {
     const long np = ck.p_hi - ck.p_lo, nt = 3 * np;
     if (nt == 0) return;
-    k_fit_dbdr<<<(unsigned)((nt + threads - 1) / threads), threads, 0, h->s>>>(
-        h->dul.as<double2>(), nt, h->fp.pinfo.as<int2>() + ck.p_lo, np, h->tabs.as<FitTables>(), h->Z.as<double2>(),
-        ck.t_lo, h->dbdr.as<double>());
+    const unsigned g = (unsigned)((nt + threads - 1) / threads);
+    const double2 *d = h->dul.as<double2>();
+    const int2 *pi = h->fp.pinfo.as<int2>() + ck.p_lo;
+    const FitTables *T = h->tabs.as<FitTables>();
+    switch (h->model.p.twojmax) {
+    case 8: k_fit_dbdr<8><<<g, threads, 0, h->s>>>(d, nt, pi, np, T, h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>()); break;
+    case 6: k_fit_dbdr<6><<<g, threads, 0, h->s>>>(d, nt, pi, np, T, h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>()); break;
+    default: k_fit_dbdr<4><<<g, threads, 0, h->s>>>(d, nt, pi, np, T, h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>()); break;
+    }
     count_launches(1);
 }
 
