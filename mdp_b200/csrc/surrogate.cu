@@ -88,32 +88,191 @@ __global__ void k_sur_round(const float *__restrict__ P, float *__restrict__ Pb)
 }
 
 // ---------------------------------------------------------------------------
-// inference: per-atom energy and G = dE_i/dB_i for B in [k * bstride + atom]
+// inference on tensor cores: each warp takes 16 atoms per tile through
+// mma.sync m16n8k16 (BF16 x BF16 -> FP32).  Weights are BF16 already; every
+// activation operand is split into BF16 hi + lo (two MMAs), so products keep
+// about 16 bits and the energy stays a smooth function of the features, in
+// step with its gradient G.  A layer's FP32 accumulators (C fragments) become
+// the next layer's A fragments in registers.  The backward pass uses
+// transposed weight copies so every B fragment is two adjacent BF16 values.
 // ---------------------------------------------------------------------------
-constexpr int SUR_INF_THREADS = 128;
+constexpr int SUR_TC_WARPS = 4;
 
-__global__ void __launch_bounds__(SUR_INF_THREADS)
-k_sur_infer(const double *__restrict__ B, long bstride, int n, const float *__restrict__ Pb, const SurNorm nrm,
-            double *__restrict__ eatom, float *__restrict__ G)
+__device__ __forceinline__ unsigned sur_bits(__nv_bfloat162 v) { return *reinterpret_cast<unsigned *>(&v); }
+
+// (x0, x1) -> packed BF16 hi and lo parts (x0 in the low half)
+__device__ __forceinline__ void sur_split2(float x0, float x1, unsigned &h, unsigned &l)
 {
-    __shared__ float W[SUR_NPAR];
-    for (int i = threadIdx.x; i < SUR_NPAR; i += blockDim.x) W[i] = Pb[i];
+    const __nv_bfloat162 hv = __floats2bfloat162_rn(x0, x1);
+    const float2 hf = __bfloat1622float2(hv);
+    h = sur_bits(hv);
+    l = sur_bits(__floats2bfloat162_rn(x0 - hf.x, x1 - hf.y));
+}
+
+__device__ __forceinline__ void sur_mma(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                 "{%0,%1,%2,%3};\n"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// A fragments (hi, lo) of k-step kk from C fragments of column tiles 2kk, 2kk+1
+__device__ __forceinline__ void sur_afrag(const float (&c)[8][4], int kk, unsigned (&h)[4], unsigned (&l)[4])
+{
+    sur_split2(c[2 * kk][0], c[2 * kk][1], h[0], l[0]);
+    sur_split2(c[2 * kk][2], c[2 * kk][3], h[1], l[1]);
+    sur_split2(c[2 * kk + 1][0], c[2 * kk + 1][1], h[2], l[2]);
+    sur_split2(c[2 * kk + 1][2], c[2 * kk + 1][3], h[3], l[3]);
+}
+
+__global__ void __launch_bounds__(SUR_TC_WARPS * 32)
+k_sur_infer_tc(const double *__restrict__ B, long bstride, int n, const float *__restrict__ Pb, const SurNorm nrm,
+               double *__restrict__ eatom, float *__restrict__ G)
+{
+    __shared__ __align__(16) __nv_bfloat16 W1s[SUR_H * SUR_KP], W1t[SUR_KP * SUR_H], W2s[SUR_H * SUR_H],
+        W2t[SUR_H * SUR_H];
+    __shared__ float sb1[SUR_H], sb2[SUR_H], sw3[SUR_H];
+    for (int i = threadIdx.x; i < SUR_H * SUR_KP; i += blockDim.x) {
+        const int r = i / SUR_KP, k = i % SUR_KP;
+        const __nv_bfloat16 v = __float2bfloat16_rn(Pb[SUR_OFF_W1 + i]);
+        W1s[i] = v;
+        W1t[k * SUR_H + r] = v;
+    }
+    for (int i = threadIdx.x; i < SUR_H * SUR_H; i += blockDim.x) {
+        const int c = i / SUR_H, r = i % SUR_H;
+        const __nv_bfloat16 v = __float2bfloat16_rn(Pb[SUR_OFF_W2 + i]);
+        W2s[i] = v;
+        W2t[r * SUR_H + c] = v;
+    }
+    for (int i = threadIdx.x; i < SUR_H; i += blockDim.x) {
+        sb1[i] = Pb[SUR_OFF_B1 + i]; sb2[i] = Pb[SUR_OFF_B2 + i]; sw3[i] = Pb[SUR_OFF_W3 + i];
+    }
     __syncthreads();
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
-        float x[SUR_KP];
+    const float b3 = Pb[SUR_OFF_B3];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, tq = lane & 3;
+    const int ntile = (n + 15) / 16;
+    auto wpair = [](const __nv_bfloat16 *p) { return *reinterpret_cast<const unsigned *>(p); };
+    for (int tile = blockIdx.x * SUR_TC_WARPS + w; tile < ntile; tile += gridDim.x * SUR_TC_WARPS) {
+        const int a0 = tile * 16 + g, a1 = a0 + 8;
+        // input fragment: rows g, g+8 (atoms), columns 2tq, 2tq+1, 2tq+8, 2tq+9 (features)
+        float xv[2][4];
 #pragma unroll
-        for (int k = 0; k < SUR_KP; k++) x[k] = k < SUR_NK ? (float)((B[(size_t)k * bstride + a] - nrm.mu[k]) * nrm.sinv[k]) : 0.f;
-        float z1[SUR_H], a1[SUR_H], z2[SUR_H], g1[SUR_H];
-        const float y = mlp_forward(W, x, z1, a1, z2);
-        mlp_backward_z1(W, z1, z2, g1);
-        if (eatom) eatom[a] = (double)nrm.e_mu + (double)nrm.e_sd * (double)y;
+        for (int h = 0; h < 2; h++) {
+            const int a = h ? a1 : a0;
+            const int ks[4] = {2 * tq, 2 * tq + 1, 2 * tq + 8, 2 * tq + 9};
 #pragma unroll
-        for (int k = 0; k < SUR_NK; k++) {
-            float s = 0.f;
-#pragma unroll 8
-            for (int r = 0; r < SUR_H; r++) s += W[SUR_OFF_W1 + r * SUR_KP + k] * g1[r];
-            G[(size_t)k * n + a] = s * (float)(nrm.sinv[k] * nrm.e_sd);
+            for (int q = 0; q < 4; q++) {
+                const int k = ks[q];
+                xv[h][q] = (a < n && k < SUR_NK) ? (float)((B[(size_t)k * bstride + a] - nrm.mu[k]) * nrm.sinv[k]) : 0.f;
+            }
         }
+        unsigned xh[4], xl[4];
+        sur_split2(xv[0][0], xv[0][1], xh[0], xl[0]);
+        sur_split2(xv[1][0], xv[1][1], xh[1], xl[1]);
+        sur_split2(xv[0][2], xv[0][3], xh[2], xl[2]);
+        sur_split2(xv[1][2], xv[1][3], xh[3], xl[3]);
+        // layer 1: z1 = x W1^T + b1
+        float z1[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int nn = 8 * nt + 2 * tq;
+            z1[nt][0] = sb1[nn]; z1[nt][1] = sb1[nn + 1]; z1[nt][2] = sb1[nn]; z1[nt][3] = sb1[nn + 1];
+            const unsigned b0 = wpair(&W1s[(8 * nt + g) * SUR_KP + 2 * tq]), bb1 = wpair(&W1s[(8 * nt + g) * SUR_KP + 2 * tq + 8]);
+            sur_mma(z1[nt], xh, b0, bb1);
+            sur_mma(z1[nt], xl, b0, bb1);
+        }
+        // layer 2: z2 = silu(z1) W2^T + b2
+        float a1f[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) a1f[nt][q] = sur_silu(z1[nt][q]);
+        float z2[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int nn = 8 * nt + 2 * tq;
+            z2[nt][0] = sb2[nn]; z2[nt][1] = sb2[nn + 1]; z2[nt][2] = sb2[nn]; z2[nt][3] = sb2[nn + 1];
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            unsigned ah[4], al[4];
+            sur_afrag(a1f, kk, ah, al);
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const __nv_bfloat16 *wr = &W2s[(8 * nt + g) * SUR_H + 16 * kk + 2 * tq];
+                const unsigned b0 = wpair(wr), bb1 = wpair(wr + 8);
+                sur_mma(z2[nt], ah, b0, bb1);
+                sur_mma(z2[nt], al, b0, bb1);
+            }
+        }
+        // output and dy/dz2 = w3 * silu'(z2)
+        float y0 = 0.f, y1 = 0.f;
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const int nn = 8 * nt + 2 * tq;
+            y0 += sw3[nn] * sur_silu(z2[nt][0]) + sw3[nn + 1] * sur_silu(z2[nt][1]);
+            y1 += sw3[nn] * sur_silu(z2[nt][2]) + sw3[nn + 1] * sur_silu(z2[nt][3]);
+            z2[nt][0] = sw3[nn] * sur_dsilu(z2[nt][0]);
+            z2[nt][1] = sw3[nn + 1] * sur_dsilu(z2[nt][1]);
+            z2[nt][2] = sw3[nn] * sur_dsilu(z2[nt][2]);
+            z2[nt][3] = sw3[nn + 1] * sur_dsilu(z2[nt][3]);
+        }
+        y0 += __shfl_xor_sync(0xffffffffu, y0, 1); y0 += __shfl_xor_sync(0xffffffffu, y0, 2);
+        y1 += __shfl_xor_sync(0xffffffffu, y1, 1); y1 += __shfl_xor_sync(0xffffffffu, y1, 2);
+        if (tq == 0 && eatom) {
+            if (a0 < n) eatom[a0] = (double)nrm.e_mu + (double)nrm.e_sd * (double)(y0 + b3);
+            if (a1 < n) eatom[a1] = (double)nrm.e_mu + (double)nrm.e_sd * (double)(y1 + b3);
+        }
+        // dy/dh1 = (dy/dz2) W2, then dy/dz1 = dy/dh1 * silu'(z1)
+        float g1[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) g1[nt][q] = 0.f;
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            unsigned ah[4], al[4];
+            sur_afrag(z2, kk, ah, al);
+#pragma unroll
+            for (int nt = 0; nt < 8; nt++) {
+                const __nv_bfloat16 *wr = &W2t[(8 * nt + g) * SUR_H + 16 * kk + 2 * tq];
+                const unsigned b0 = wpair(wr), bb1 = wpair(wr + 8);
+                sur_mma(g1[nt], ah, b0, bb1);
+                sur_mma(g1[nt], al, b0, bb1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) g1[nt][q] *= sur_dsilu(z1[nt][q]);
+        // dy/dx = (dy/dz1) W1
+        float gx[2][4];
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) gx[nt][q] = 0.f;
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) {
+            unsigned ah[4], al[4];
+            sur_afrag(g1, kk, ah, al);
+#pragma unroll
+            for (int nt = 0; nt < 2; nt++) {
+                const __nv_bfloat16 *wr = &W1t[(8 * nt + g) * SUR_H + 16 * kk + 2 * tq];
+                const unsigned b0 = wpair(wr), bb1 = wpair(wr + 8);
+                sur_mma(gx[nt], ah, b0, bb1);
+                sur_mma(gx[nt], al, b0, bb1);
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; nt++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int k = 8 * nt + 2 * tq + (q & 1);
+                const int a = (q < 2) ? a0 : a1;
+                if (k < SUR_NK && a < n) G[(size_t)k * n + a] = gx[nt][q] * (float)(nrm.sinv[k] * nrm.e_sd);
+            }
     }
 }
 
@@ -336,8 +495,9 @@ int sur_force(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const int
         for (auto &e : fp.ev) cudaEventCreate(&e);
     if (fp.timing) cudaEventRecord(fp.ev[0], s);
     if (sur_features(S, fp, x, inum, nlist, nnum, nm, s)) return -1;
-    k_sur_infer<<<std::min((inum + SUR_INF_THREADS - 1) / SUR_INF_THREADS, num_sms() * 8), SUR_INF_THREADS, 0, s>>>(
-        S.B.as<double>(), inum, inum, S.Pb.as<float>(), S.norm, eatom, S.G.as<float>());
+    k_sur_infer_tc<<<std::min((inum + 16 * SUR_TC_WARPS - 1) / (16 * SUR_TC_WARPS), num_sms() * 16),
+                     SUR_TC_WARPS * 32, 0, s>>>(S.B.as<double>(), inum, inum, S.Pb.as<float>(), S.norm, eatom,
+                                                S.G.as<float>());
     if (launch_yi_pa_f4(S.model, fp, inum, S.G.as<float>(), s)) return -1;
     if (launch_fi<float, 4>(S.model, fp, inum, nm, s)) return -1;
     const int tb = 256, gb = (inum + tb - 1) / tb;
@@ -578,7 +738,7 @@ int mdp_sur_eval(mdp_sur *S, const double *B, int n, double *E, float *G)
         dg.ensure(sizeof(float) * SUR_NK * (size_t)n))
         return -1;
     MDP_CUDA_TRY(cudaMemcpy(db.p, B, sizeof(double) * SUR_NK * n, cudaMemcpyHostToDevice));
-    k_sur_infer<<<(n + SUR_INF_THREADS - 1) / SUR_INF_THREADS, SUR_INF_THREADS>>>(
+    k_sur_infer_tc<<<(n + 16 * SUR_TC_WARPS - 1) / (16 * SUR_TC_WARPS), SUR_TC_WARPS * 32>>>(
         db.as<double>(), n, n, S->Pb.as<float>(), S->norm, de.as<double>(), dg.as<float>());
     count_launches(1);
     MDP_CUDA_TRY(cudaGetLastError());
