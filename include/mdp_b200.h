@@ -157,6 +157,23 @@ int mdp_sur_grad(mdp_sur *h, const float *X, const float *E, int n, float *grad,
 /* inference on host features B [k * n + atom]: E [n], G = dE_i/dB_ik [k * n + atom] */
 int mdp_sur_eval(mdp_sur *h, const double *B, int n, double *E, float *G);
 
+/* force-matching set from a 2J=4 batch (mdp_fit, declared below) whose
+ * configurations are equal-size snapshots of per atoms: the plain model's
+ * forces (3 per atom) and per-atom energies, host arrays */
+typedef struct mdp_fit mdp_fit;
+int mdp_sur_force_set(mdp_sur *h, mdp_fit *snapshots, const double *forces, const double *energies, int per);
+long long mdp_sur_force_set_npairs(mdp_sur *h);
+/* Adam on windows of snaps_per_batch snapshots: energy loss (as
+ * mdp_sur_train) + alpha * force MSE / var(F); per-step losses out */
+int mdp_sur_train_forces(mdp_sur *h, int steps, int snaps_per_batch, float lr, float alpha, unsigned long long seed,
+                         float *loss_e, float *loss_f);
+/* gradient of that loss over snapshots [snap0, snap0 + snaps) (no update);
+ * losses[2] = (energy, force) parts */
+int mdp_sur_force_grad(mdp_sur *h, int snap0, int snaps, float alpha, float *grad, float *losses);
+/* the force set's features B [k][atom], per-pair dB/dR [pair][3][14], pair
+ * (centre, neighbour) and CSR offsets, for checks */
+int mdp_sur_force_set_copy(mdp_sur *h, double *B, float *db, int *pinfo, int *poff);
+
 /* append the MD engine's current state to the training set: 2J=4 features of
  * the current positions and the per-atom energies of the last force call */
 int mdp_md_sur_sample(mdp_md *md, mdp_sur *s);
@@ -178,8 +195,6 @@ int mdp_md_surrogate_status(mdp_md *md, int *active, long long *fallback_step, i
  * 386-404).  A batch holds configurations of any atom counts, each in an
  * orthogonal periodic box whose lengths exceed the cutoff.
  * ------------------------------------------------------------------------- */
-typedef struct mdp_fit mdp_fit;
-
 /* p: SNAP hyper-parameters (twojmax 4, 6 or 8; coefficients unused) */
 int mdp_fit_create(mdp_fit **h, const mdp_snap_params *p, int device);
 void mdp_fit_destroy(mdp_fit *h);

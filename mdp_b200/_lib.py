@@ -92,6 +92,13 @@ def lib():
     L.mdp_md_sur_features.argtypes = [C.c_void_p, C.c_void_p, _dp]
     L.mdp_md_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
     _ip32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    L.mdp_sur_force_set.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp, C.c_int]
+    L.mdp_sur_force_set_npairs.argtypes = [C.c_void_p]
+    L.mdp_sur_force_set_npairs.restype = C.c_longlong
+    L.mdp_sur_train_forces.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_ulonglong,
+                                       C.c_void_p, C.c_void_p]
+    L.mdp_sur_force_grad.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, _fp, _fp]
+    L.mdp_sur_force_set_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.mdp_fit_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(SnapParamsC), C.c_int]
     L.mdp_fit_destroy.argtypes = [C.c_void_p]
     L.mdp_fit_destroy.restype = None

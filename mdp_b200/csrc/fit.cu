@@ -21,6 +21,7 @@
 //   A, b   (k_fit_gram: FP64, or BF16 hi/lo split with FP32 tensor-core sums)
 #include "common.cuh"
 #include "engine.h"
+#include "fit.h"
 
 #include <cuda_bf16.h>
 #include <math.h>
@@ -29,28 +30,6 @@
 #include <vector>
 
 namespace mdp {
-
-constexpr int FIT_KP = 64;       // row width: 1 + ncoeff (<= 56 at 2J=8) padded to 64
-constexpr int FIT_NCP = 256;     // couplings (j1 >= j2, j) at most (125 at 2J=8)
-constexpr int FIT_NT = 64;       // bispectrum triples at most (55 at 2J=8)
-
-struct FitCoupling {
-    int j1, j2, j, zoff;          // Z rows of this coupling start at zoff (per atom)
-};
-struct FitTriple {
-    int j1, j2, j;
-    int layer[3], coup[3];        // the three dB/dR terms: dU layer and Z coupling
-    double fac[3];
-};
-struct FitTables {
-    int ncoup, ntri, nz, tj, bnorm, bzero;
-    FitCoupling cp[FIT_NCP];
-    FitTriple tr[FIT_NT];
-    // the dB/dR terms grouped by their dU layer: lt_off[L] .. lt_off[L] + lt_n[L]
-    int lt_n[JD], lt_off[JD];
-    int lt_k[3 * FIT_NT], lt_z[3 * FIT_NT];
-    double lt_fac[3 * FIT_NT];
-};
 
 // ---------------------------------------------------------------------------
 // pairs: every atom against every atom of its configuration and the 27 images
@@ -656,33 +635,19 @@ static void fit_tables(FitTables &T, int tj, int bnorm, int bzero)
 
 using namespace mdp;
 
-struct mdp_fit {
-    SnapModel model;
-    FitTables tab;
-    int device = 0;
-    cudaStream_t s = nullptr;
-    // batch
-    int nconf = 0, natoms = 0;
-    std::vector<int> h_cn, h_ca0;
-    DevBuf x, cfg, ca0, cn, cbox, we, wf, e, f;
-    // work (sized for the whole batch)
-    DevBuf tabs, pcount, poff, roff, rcount, cursor, rlist, B, Z, dul, dbdr, G, R, tgt, hi, lo, part, out, scan_tmp;
-    ForcePath fp;
-    long npairs = 0, nrows = 0;
-    bool pairs_ready = false;
-    // the Z / dU / dB/dR stages run over configuration-aligned chunks that fit
-    // the scratch budget; U, B, the rows and the Gram pass span the batch
-    struct Chunk { int c_lo, c_hi, a_lo, a_hi, t_lo, t_hi; long p_lo, p_hi; };
-    std::vector<Chunk> chunks;
-    double chunk_bytes = 24.0e9;   // scratch of the chunked stages (dU rows, dB/dR, Z) per chunk at most
-    long chunk_pairs_max = 0;
-    int chunk_tiles_max = 0;
-    // launch shapes (autotuned): threads of the per-pair kernels, rows per Gram CTA
-    int du_threads = 128, db_threads = 128, gram_rows = 4096;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    int graph_mode = -1;
-};
+namespace mdp {
+// per-pair dB/dR of the whole batch as float [pair][3][k] and the per-atom
+// bispectrum [k][atom] (FP64): the descriptor stages chunk by chunk
+__global__ void k_fit_dbdr_export(const double *__restrict__ dbdr, long np, int ntri, long p_lo,
+                                  float *__restrict__ out)
+{
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;   // (local pair * 3 + dir, k)
+    if (t >= 3 * np * ntri) return;
+    const int k = (int)(t % ntri);
+    const long pd = t / ntri;
+    out[(p_lo * 3 + pd) * ntri + k] = (float)dbdr[(long)k * (3 * np) + pd];
+}
+}  // namespace mdp
 
 namespace mdp {
 
@@ -807,6 +772,42 @@ static int fit_descriptor_stages(mdp_fit *h, bool rows, double *G = nullptr, dou
     }
     for (const auto &ck : h->chunks)
         if (fit_chunk(h, ck, rows, G, bi, bv)) return -1;
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int fit_pair_derivs(mdp_fit *h, float *dbdr_out, double *blist_out)
+{
+    if (!h || !h->pairs_ready) { set_error("set a batch first"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(h->device));
+    const int n = h->natoms, tj = h->model.p.twojmax, nk = h->tab.ntri;
+    if (tu_ensure_tables()) return -1;
+    const int urc = tj == 8 ? launch_ui<double, 8>(h->model, h->fp, n, h->s)
+                  : tj == 6 ? launch_ui<double, 6>(h->model, h->fp, n, h->s)
+                            : launch_ui<double, 4>(h->model, h->fp, n, h->s);
+    if (urc) return -1;
+    static bool attr = false;
+    if (!attr) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_fit_zb, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)((size_t)idxu_count(TJMAX) * 32 * sizeof(double2))));
+        attr = true;
+    }
+    const size_t zsm = (size_t)idxu_count(tj) * 32 * sizeof(double2);
+    for (const auto &ck : h->chunks) {
+        k_fit_zb<<<std::max(1, std::min(ck.t_hi - ck.t_lo, num_sms())), FIT_ZB_WARPS * 32, zsm, h->s>>>(
+            h->fp.Ut.as<double2>(), n, h->tabs.as<FitTables>(), h->Z.as<double2>(), h->B.as<double>(), ck.t_lo,
+            ck.t_hi);
+        if (fit_du(h, ck)) return -1;
+        fit_dbdr(h, ck, h->db_threads);
+        const long np = ck.p_hi - ck.p_lo, ne = 3 * np * nk;
+        if (ne) k_fit_dbdr_export<<<(unsigned)((ne + 255) / 256), 256, 0, h->s>>>(h->dbdr.as<double>(), np, nk,
+                                                                                ck.p_lo, dbdr_out);
+        count_launches(2);
+    }
+    if (blist_out)
+        MDP_CUDA_TRY(cudaMemcpyAsync(blist_out, h->B.p, sizeof(double) * nk * (size_t)n, cudaMemcpyDeviceToDevice,
+                                     h->s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(h->s));
     MDP_CUDA_TRY(cudaGetLastError());
     return 0;
 }

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "engine.h"
 #include "surrogate.h"
+#include "fit.h"
 
 #include <cuda_bf16.h>
 #include <math.h>
@@ -362,6 +363,191 @@ k_sur_grad(const float *__restrict__ X, const float *__restrict__ E, const int *
             atomicAdd(&grad[SUR_OFF_B3], b3);
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// force matching.  With G_i = dE_i/dB_i, F_a = -sum_i G_i . dB_i/dx_a, and for
+// the loss L_F = alpha |F - F_ref|^2 / (3 n var_F) the adjoint of G_i is
+//   lambda_i = dL/dG_i = -sum_(own pairs p of i) dB_i/dr_p . (Q_j(p) - Q_i),
+//   Q_a = dL/dF_a.
+// Since G_ik = e_sd sinv_k dy/dx_k, the weight gradient of the force loss is
+// d(grad_x y . v)/dw with v_k = lambda_ik e_sd sinv_k: forward-over-reverse
+// through the network (tangent pass along v, then adjoints of both passes).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sur_d2silu(float z)
+{
+    const float s = sur_sigmoid(z);
+    return s * (1.0f - s) * (2.0f + z * (1.0f - 2.0f * s));
+}
+
+// per atom a of the batch [a_lo, a_lo + n): predicted force, Q_a and the loss
+__global__ void k_sur_fpred(int a_lo, int n, const int *__restrict__ poff, const int *__restrict__ roff,
+                            const int *__restrict__ rlist, const int2 *__restrict__ pinfo,
+                            const float *__restrict__ db, const float *__restrict__ G, const float *__restrict__ Fref,
+                            float coef, float lw, float *__restrict__ Q, float *__restrict__ loss)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int a = a_lo + t;
+    float de[3] = {0.f, 0.f, 0.f};
+    for (int q = roff[a]; q < roff[a + 1]; q++) {
+        const int p = rlist[q];
+        const int i = pinfo[p].x - a_lo;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < SUR_NK; k++) s += G[(size_t)k * n + i] * db[((size_t)p * 3 + c) * SUR_NK + k];
+            de[c] += s;
+        }
+    }
+    for (int p = poff[a]; p < poff[a + 1]; p++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            float s = 0.f;
+#pragma unroll
+            for (int k = 0; k < SUR_NK; k++) s += G[(size_t)k * n + t] * db[((size_t)p * 3 + c) * SUR_NK + k];
+            de[c] -= s;
+        }
+    float l = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const float r = -de[c] - Fref[3 * (size_t)a + c];
+        Q[3 * t + c] = coef * r;
+        l += r * r;
+    }
+    atomicAdd(loss, lw * l);
+}
+
+// lambda_i, written as the tangent v_ik = lambda_ik e_sd sinv_k ([atom][KP])
+__global__ void k_sur_lambda(int a_lo, int n, const int *__restrict__ poff, const int2 *__restrict__ pinfo,
+                             const float *__restrict__ db, const float *__restrict__ Q, const SurNorm nrm,
+                             float *__restrict__ V)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int a = a_lo + t;
+    float lam[SUR_NK];
+#pragma unroll
+    for (int k = 0; k < SUR_NK; k++) lam[k] = 0.f;
+    const float qi0 = Q[3 * t], qi1 = Q[3 * t + 1], qi2 = Q[3 * t + 2];
+    for (int p = poff[a]; p < poff[a + 1]; p++) {
+        const int j = pinfo[p].y - a_lo;
+        const float d0 = Q[3 * j] - qi0, d1 = Q[3 * j + 1] - qi1, d2 = Q[3 * j + 2] - qi2;
+        const float *b = db + (size_t)p * 3 * SUR_NK;
+#pragma unroll
+        for (int k = 0; k < SUR_NK; k++) lam[k] -= b[k] * d0 + b[SUR_NK + k] * d1 + b[2 * SUR_NK + k] * d2;
+    }
+#pragma unroll
+    for (int k = 0; k < SUR_KP; k++) V[(size_t)t * SUR_KP + k] = k < SUR_NK ? lam[k] * nrm.e_sd * nrm.sinv[k] : 0.f;
+}
+
+// energy + force gradient of the batch: one sample per thread, block-reduced
+// rows of dW1 / dW2 (as k_sur_grad), with the tangent terms of the force part
+constexpr int SUR_TF_THREADS = 64;
+constexpr int SUR_TF_VEC = 8 * (SUR_H + 1) + 2 * (SUR_KP + 1) + 1;   // floats per sample in shared memory
+constexpr size_t SUR_TF_SMEM = sizeof(float) * (SUR_NPAR + (size_t)SUR_TF_THREADS * SUR_TF_VEC);
+
+__global__ void __launch_bounds__(SUR_TF_THREADS)
+k_sur_grad_f(const double *__restrict__ B, long bstride, const float *__restrict__ E, const float *__restrict__ V,
+             int n, float ew, const float *__restrict__ Pb, const SurNorm nrm, float *__restrict__ grad,
+             float *__restrict__ loss)
+{
+    extern __shared__ float sf_sm[];
+    float *W = sf_sm;
+    for (int i = threadIdx.x; i < SUR_NPAR; i += blockDim.x) W[i] = Pb[i];
+    float *base = W + SUR_NPAR;
+    const int t = threadIdx.x, s = blockIdx.x * SUR_TF_THREADS + t;
+    // per-sample vectors: 0 z2bar, 1 a1, 2 zd2bar, 3 ad1, 4 z1bar, 5 zd1bar, 6 a2, 7 ad2 (H+1 each),
+    // then x, v (KP+1 each), then ybar
+    auto vec = [&](int q, int who) { return base + (size_t)who * SUR_TF_VEC + q * (SUR_H + 1); };
+    auto xv = [&](int q, int who) { return base + (size_t)who * SUR_TF_VEC + 8 * (SUR_H + 1) + q * (SUR_KP + 1); };
+    __syncthreads();
+    float *z2b = vec(0, t), *a1s = vec(1, t), *zd2b = vec(2, t), *ad1s = vec(3, t), *z1b = vec(4, t),
+          *zd1b = vec(5, t), *a2s = vec(6, t), *ad2s = vec(7, t), *xs = xv(0, t), *vs = xv(1, t);
+    float *ybs = base + (size_t)t * SUR_TF_VEC + 8 * (SUR_H + 1) + 2 * (SUR_KP + 1);
+    if (s < n) {
+        float x[SUR_KP], v[SUR_KP];
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) {
+            x[k] = k < SUR_NK ? (float)((B[(size_t)k * bstride + s] - nrm.mu[k]) * nrm.sinv[k]) : 0.f;
+            v[k] = V[(size_t)s * SUR_KP + k];
+            xs[k] = x[k];
+            vs[k] = v[k];
+        }
+        // forward and tangent: z1 -> z1b (temporarily), zd1 -> zd1b, a1, ad1
+        for (int r = 0; r < SUR_H; r++) {
+            float z = W[SUR_OFF_B1 + r], zd = 0.f;
+#pragma unroll
+            for (int k = 0; k < SUR_NK; k++) { z += W[SUR_OFF_W1 + r * SUR_KP + k] * x[k]; zd += W[SUR_OFF_W1 + r * SUR_KP + k] * v[k]; }
+            z1b[r] = z;
+            zd1b[r] = zd;
+            a1s[r] = sur_silu(z);
+            ad1s[r] = sur_dsilu(z) * zd;
+        }
+        float y = W[SUR_OFF_B3];
+        for (int c = 0; c < SUR_H; c++) {
+            float z = W[SUR_OFF_B2 + c], zd = 0.f;
+            for (int r = 0; r < SUR_H; r++) { z += W[SUR_OFF_W2 + c * SUR_H + r] * a1s[r]; zd += W[SUR_OFF_W2 + c * SUR_H + r] * ad1s[r]; }
+            z2b[c] = z;      // z2 for now
+            zd2b[c] = zd;    // zd2 for now
+            a2s[c] = sur_silu(z);
+            ad2s[c] = sur_dsilu(z) * zd;
+            y += W[SUR_OFF_W3 + c] * a2s[c];
+        }
+        const float r = y - (E[s] - nrm.e_mu) / nrm.e_sd;
+        const float yb = ew * 2.0f * r / (float)n;
+        atomicAdd(loss, ew * r * r / (float)n);
+        *ybs = yb;
+        // adjoints of layer 2 (the force part has ydot-bar = 1)
+        for (int c = 0; c < SUR_H; c++) {
+            const float w3 = W[SUR_OFF_W3 + c], z = z2b[c], zd = zd2b[c];
+            z2b[c] = yb * w3 * sur_dsilu(z) + w3 * sur_d2silu(z) * zd;
+            zd2b[c] = w3 * sur_dsilu(z);
+        }
+        // adjoints of layer 1
+        for (int r = 0; r < SUR_H; r++) {
+            float ab = 0.f, adb = 0.f;
+            for (int c = 0; c < SUR_H; c++) { ab += W[SUR_OFF_W2 + c * SUR_H + r] * z2b[c]; adb += W[SUR_OFF_W2 + c * SUR_H + r] * zd2b[c]; }
+            const float z = z1b[r], zd = zd1b[r];
+            z1b[r] = ab * sur_dsilu(z) + adb * sur_d2silu(z) * zd;
+            zd1b[r] = adb * sur_dsilu(z);
+        }
+    } else {
+        for (int q = 0; q < 8 * (SUR_H + 1) + 2 * (SUR_KP + 1); q++) base[(size_t)t * SUR_TF_VEC + q] = 0.f;
+        *ybs = 0.f;
+    }
+    __syncthreads();
+    const int ns = min(SUR_TF_THREADS, n - (int)blockIdx.x * SUR_TF_THREADS);
+    // row t of each weight matrix over the block's samples
+    float w2[SUR_H];
+#pragma unroll
+    for (int r = 0; r < SUR_H; r++) w2[r] = 0.f;
+    float w1[SUR_KP];
+#pragma unroll
+    for (int k = 0; k < SUR_KP; k++) w1[k] = 0.f;
+    float b2 = 0.f, b1 = 0.f, w3 = 0.f, b3 = 0.f;
+    for (int q = 0; q < ns; q++) {
+        const float gz2 = vec(0, q)[t], gzd2 = vec(2, q)[t], gz1 = vec(4, q)[t], gzd1 = vec(5, q)[t];
+        const float *qa1 = vec(1, q), *qad1 = vec(3, q), *qx = xv(0, q), *qv = xv(1, q);
+#pragma unroll
+        for (int r = 0; r < SUR_H; r++) w2[r] += gz2 * qa1[r] + gzd2 * qad1[r];
+#pragma unroll
+        for (int k = 0; k < SUR_KP; k++) w1[k] += gz1 * qx[k] + gzd1 * qv[k];
+        b2 += gz2;
+        b1 += gz1;
+        const float yb = base[(size_t)q * SUR_TF_VEC + 8 * (SUR_H + 1) + 2 * (SUR_KP + 1)];
+        w3 += yb * vec(6, q)[t] + vec(7, q)[t];
+        b3 += yb;
+    }
+#pragma unroll
+    for (int r = 0; r < SUR_H; r++) atomicAdd(&grad[SUR_OFF_W2 + t * SUR_H + r], w2[r]);
+#pragma unroll
+    for (int k = 0; k < SUR_NK; k++) atomicAdd(&grad[SUR_OFF_W1 + t * SUR_KP + k], w1[k]);
+    atomicAdd(&grad[SUR_OFF_B2 + t], b2);
+    atomicAdd(&grad[SUR_OFF_B1 + t], b1);
+    atomicAdd(&grad[SUR_OFF_W3 + t], w3);
+    if (t == 0) atomicAdd(&grad[SUR_OFF_B3], b3);
 }
 
 // Adam (Kingma & Ba 2015) on the FP32 master weights; also refreshes the
@@ -747,6 +933,156 @@ int mdp_sur_eval(mdp_sur *S, const double *B, int n, double *E, float *G)
     db.release(); de.release(); dg.release();
     return 0;
 }
+
+// Force-training set from a 2J=4 batch of equal-size snapshots (mdp_fit with
+// the snapshots as configurations): per-pair dB/dR, features, pair structure,
+// and the plain model's forces (3 per atom) and per-atom energies.
+int mdp_sur_force_set(mdp_sur *S, mdp_fit *F, const double *forces, const double *energies, int per)
+{
+    if (!S || !F || !forces || !energies || per < 1) { set_error("bad arguments"); return -1; }
+    if (F->model.p.twojmax != 4 || F->tab.ntri != SUR_NK) { set_error("the force set needs a 2J=4 batch"); return -1; }
+    if (F->natoms % per != 0) { set_error("snapshots must all have %d atoms", per); return -1; }
+    for (int c = 0; c < F->nconf; c++)
+        if (F->h_cn[c] != per) { set_error("snapshot %d has %d atoms, not %d", c, F->h_cn[c], per); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    const long na = F->natoms, np = F->npairs;
+    if (S->fB.ensure(sizeof(double) * SUR_NK * na) || S->fE.ensure(sizeof(float) * na) ||
+        S->fF.ensure(sizeof(float) * 3 * na) || S->fdb.ensure(sizeof(float) * 3 * SUR_NK * std::max(np, 1L)) ||
+        S->fpinfo.ensure(sizeof(int2) * std::max(np, 1L)) || S->fpoff.ensure(sizeof(int) * (na + 1)) ||
+        S->froff.ensure(sizeof(int) * (na + 1)) || S->frlist.ensure(sizeof(int) * std::max(np, 1L)) ||
+        S->fscal.ensure(sizeof(float) * 8))
+        return -1;
+    if (fit_pair_derivs(F, S->fdb.as<float>(), S->fB.as<double>())) return -1;
+    MDP_CUDA_TRY(cudaMemcpy(S->fpinfo.p, F->fp.pinfo.p, sizeof(int2) * np, cudaMemcpyDeviceToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(S->fpoff.p, F->poff.p, sizeof(int) * (na + 1), cudaMemcpyDeviceToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(S->froff.p, F->roff.p, sizeof(int) * (na + 1), cudaMemcpyDeviceToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(S->frlist.p, F->rlist.p, sizeof(int) * np, cudaMemcpyDeviceToDevice));
+    std::vector<float> hf(3 * na), he(na);
+    double var = 0.0;
+    for (long i = 0; i < 3 * na; i++) { hf[i] = (float)forces[i]; var += forces[i] * forces[i]; }
+    for (long i = 0; i < na; i++) he[i] = (float)energies[i];
+    MDP_CUDA_TRY(cudaMemcpy(S->fF.p, hf.data(), sizeof(float) * 3 * na, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(S->fE.p, he.data(), sizeof(float) * na, cudaMemcpyHostToDevice));
+    S->f_atoms = na;
+    S->f_pairs = np;
+    S->f_per = per;
+    S->f_snaps = (int)(na / per);
+    S->f_var = var / (3.0 * na) > 1e-30 ? var / (3.0 * na) : 1.0;
+    return 0;
+}
+
+// Adam steps on windows of snaps_per_batch consecutive snapshots of the force
+// set: loss = mean normalised per-atom energy error^2 + alpha * mean force
+// error^2 / var(F).  loss_e, loss_f (may be NULL): per step.
+int mdp_sur_train_forces(mdp_sur *S, int steps, int snaps_per_batch, float lr, float alpha, unsigned long long seed,
+                         float *loss_e, float *loss_f)
+{
+    if (!S || steps < 1 || snaps_per_batch < 1) { set_error("bad arguments"); return -1; }
+    if (!S->trained) { set_error("set initial parameters first"); return -1; }
+    if (S->f_snaps < snaps_per_batch) { set_error("force set holds %d snapshots", S->f_snaps); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    static bool attr = false;
+    if (!attr) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_sur_grad_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUR_TF_SMEM));
+        attr = true;
+    }
+    const int n = snaps_per_batch * S->f_per;
+    if (S->fG.ensure(sizeof(float) * SUR_NK * (size_t)n) || S->fQ.ensure(sizeof(float) * 3 * (size_t)n) ||
+        S->fV.ensure(sizeof(float) * SUR_KP * (size_t)n))
+        return -1;
+    DevBuf lb;
+    if (lb.ensure(sizeof(float) * 2 * (size_t)steps)) return -1;
+    MDP_CUDA_TRY(cudaMemset(lb.p, 0, sizeof(float) * 2 * steps));
+    const float coef = 2.0f * alpha / (float)(3.0 * n * S->f_var), lw = alpha / (float)(3.0 * n * S->f_var);
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    unsigned long long st = seed * 0x9e3779b97f4a7c15ULL + 1;
+    for (int it = 0; it < steps; it++) {
+        st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+        const int s0 = (int)((st >> 33) % (unsigned long long)(S->f_snaps - snaps_per_batch + 1));
+        const int a_lo = s0 * S->f_per;
+        const double *Bw = S->fB.as<double>() + a_lo;
+        k_sur_infer_tc<<<std::min((n + 16 * SUR_TC_WARPS - 1) / (16 * SUR_TC_WARPS), num_sms() * 16),
+                         SUR_TC_WARPS * 32>>>(Bw, S->f_atoms, n, S->Pb.as<float>(), S->norm, nullptr,
+                                              S->fG.as<float>());
+        k_sur_fpred<<<(n + 127) / 128, 128>>>(a_lo, n, S->fpoff.as<int>(), S->froff.as<int>(), S->frlist.as<int>(),
+                                              S->fpinfo.as<int2>(), S->fdb.as<float>(), S->fG.as<float>(),
+                                              S->fF.as<float>(), coef, lw, S->fQ.as<float>(), lb.as<float>() + 2 * it + 1);
+        k_sur_lambda<<<(n + 127) / 128, 128>>>(a_lo, n, S->fpoff.as<int>(), S->fpinfo.as<int2>(), S->fdb.as<float>(),
+                                               S->fQ.as<float>(), S->norm, S->fV.as<float>());
+        k_sur_grad_f<<<(n + SUR_TF_THREADS - 1) / SUR_TF_THREADS, SUR_TF_THREADS, SUR_TF_SMEM>>>(
+            Bw, S->f_atoms, S->fE.as<float>() + a_lo, S->fV.as<float>(), n, 1.0f, S->Pb.as<float>(), S->norm,
+            S->grad.as<float>(), lb.as<float>() + 2 * it);
+        S->adam_t++;
+        const float c1 = 1.f - powf(b1, (float)S->adam_t), c2 = 1.f - powf(b2, (float)S->adam_t);
+        k_sur_adam<<<(SUR_NPAR + 255) / 256, 256>>>(S->P.as<float>(), S->Pb.as<float>(), S->grad.as<float>(),
+                                                    S->m1.as<float>(), S->m2.as<float>(), lr, b1, b2, eps, c1, c2);
+        count_launches(5);
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    if (loss_e || loss_f) {
+        std::vector<float> h(2 * (size_t)steps);
+        MDP_CUDA_TRY(cudaMemcpy(h.data(), lb.p, sizeof(float) * 2 * steps, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < steps; i++) {
+            if (loss_e) loss_e[i] = h[2 * i];
+            if (loss_f) loss_f[i] = h[2 * i + 1];
+        }
+    }
+    lb.release();
+    return 0;
+}
+
+// gradient of the combined loss over one window (no update), for the oracle
+// check: grad (NPAR), losses (energy, force)
+int mdp_sur_force_grad(mdp_sur *S, int snap0, int snaps, float alpha, float *grad, float *losses)
+{
+    if (!S || !grad || snaps < 1 || snap0 < 0 || snap0 + snaps > S->f_snaps) { set_error("bad arguments"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    static bool attr = false;
+    if (!attr) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_sur_grad_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUR_TF_SMEM));
+        attr = true;
+    }
+    const int n = snaps * S->f_per, a_lo = snap0 * S->f_per;
+    if (S->fG.ensure(sizeof(float) * SUR_NK * (size_t)n) || S->fQ.ensure(sizeof(float) * 3 * (size_t)n) ||
+        S->fV.ensure(sizeof(float) * SUR_KP * (size_t)n))
+        return -1;
+    const float coef = 2.0f * alpha / (float)(3.0 * n * S->f_var), lw = alpha / (float)(3.0 * n * S->f_var);
+    float *lb = S->fscal.as<float>();
+    MDP_CUDA_TRY(cudaMemset(lb, 0, sizeof(float) * 2));
+    MDP_CUDA_TRY(cudaMemset(S->grad.p, 0, sizeof(float) * SUR_NPAR));
+    const double *Bw = S->fB.as<double>() + a_lo;
+    k_sur_infer_tc<<<(n + 16 * SUR_TC_WARPS - 1) / (16 * SUR_TC_WARPS), SUR_TC_WARPS * 32>>>(
+        Bw, S->f_atoms, n, S->Pb.as<float>(), S->norm, nullptr, S->fG.as<float>());
+    k_sur_fpred<<<(n + 127) / 128, 128>>>(a_lo, n, S->fpoff.as<int>(), S->froff.as<int>(), S->frlist.as<int>(),
+                                          S->fpinfo.as<int2>(), S->fdb.as<float>(), S->fG.as<float>(), S->fF.as<float>(),
+                                          coef, lw, S->fQ.as<float>(), lb + 1);
+    k_sur_lambda<<<(n + 127) / 128, 128>>>(a_lo, n, S->fpoff.as<int>(), S->fpinfo.as<int2>(), S->fdb.as<float>(),
+                                           S->fQ.as<float>(), S->norm, S->fV.as<float>());
+    k_sur_grad_f<<<(n + SUR_TF_THREADS - 1) / SUR_TF_THREADS, SUR_TF_THREADS, SUR_TF_SMEM>>>(
+        Bw, S->f_atoms, S->fE.as<float>() + a_lo, S->fV.as<float>(), n, 1.0f, S->Pb.as<float>(), S->norm,
+        S->grad.as<float>(), lb);
+    count_launches(4);
+    MDP_CUDA_TRY(cudaGetLastError());
+    MDP_CUDA_TRY(cudaMemcpy(grad, S->grad.p, sizeof(float) * SUR_NPAR, cudaMemcpyDeviceToHost));
+    if (losses) MDP_CUDA_TRY(cudaMemcpy(losses, lb, sizeof(float) * 2, cudaMemcpyDeviceToHost));
+    MDP_CUDA_TRY(cudaMemset(S->grad.p, 0, sizeof(float) * SUR_NPAR));
+    return 0;
+}
+
+// copy of the force set's features [k][atom] (double) and per-pair dB/dR
+// [pair][3][14] (float), for the oracle check
+int mdp_sur_force_set_copy(mdp_sur *S, double *B, float *db, int *pinfo, int *poff)
+{
+    if (!S) { set_error("null handle"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(S->device));
+    if (B) MDP_CUDA_TRY(cudaMemcpy(B, S->fB.p, sizeof(double) * SUR_NK * S->f_atoms, cudaMemcpyDeviceToHost));
+    if (db) MDP_CUDA_TRY(cudaMemcpy(db, S->fdb.p, sizeof(float) * 3 * SUR_NK * S->f_pairs, cudaMemcpyDeviceToHost));
+    if (pinfo) MDP_CUDA_TRY(cudaMemcpy(pinfo, S->fpinfo.p, sizeof(int2) * S->f_pairs, cudaMemcpyDeviceToHost));
+    if (poff) MDP_CUDA_TRY(cudaMemcpy(poff, S->fpoff.p, sizeof(int) * (S->f_atoms + 1), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+long long mdp_sur_force_set_npairs(mdp_sur *S) { return S ? S->f_pairs : -1; }
 
 int mdp_sur_nparams(void) { return SUR_NPAR; }
 

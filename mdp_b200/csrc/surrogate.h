@@ -35,6 +35,11 @@ struct Surrogate {
     long long adam_t = 0;
     bool trained = false;
     int device = 0;
+    // force-training set: equal-size snapshots, per-pair dB/dR at 2J=4
+    DevBuf fB, fE, fF, fdb, fpinfo, fpoff, froff, frlist, fG, fQ, fV, fscal;
+    long f_atoms = 0, f_pairs = 0;
+    int f_snaps = 0, f_per = 0;
+    double f_var = 1.0;   // variance of the reference force components
 };
 
 // 2J=4 bispectrum of every local atom into S.B (pairs, U and B on fp)

@@ -156,6 +156,52 @@ class Surrogate:
         return E, G.T.copy()
 
 
+def _force_methods():
+    """Force-matching methods of Surrogate (kept together for readability)."""
+
+    def force_set(self, snapshots, forces, energies, per: int):
+        """snapshots: a fit.BatchFit at 2J=4 holding equal-size snapshots (per atoms);
+        forces (natoms, 3), energies (natoms,) of the plain model."""
+        self._fset = snapshots
+        _lib.check(_lib.lib().mdp_sur_force_set(self._h, snapshots._h,
+                                                np.ascontiguousarray(forces, dtype=np.float64).ravel(),
+                                                np.ascontiguousarray(energies, dtype=np.float64), int(per)),
+                   "mdp_sur_force_set")
+        self.f_per = per
+        self.f_snaps = snapshots.natoms // per
+
+    def train_forces(self, steps: int, snaps_per_batch: int = 4, lr: float = 1e-3, alpha: float = 1.0,
+                     seed: int = 0):
+        le = np.zeros(steps, dtype=np.float32)
+        lf = np.zeros(steps, dtype=np.float32)
+        _lib.check(_lib.lib().mdp_sur_train_forces(self._h, int(steps), int(snaps_per_batch), float(lr),
+                                                   float(alpha), int(seed), le.ctypes.data, lf.ctypes.data),
+                   "mdp_sur_train_forces")
+        return le, lf
+
+    def force_grad(self, snap0: int, snaps: int, alpha: float = 1.0):
+        g = np.zeros(NPAR, dtype=np.float32)
+        losses = np.zeros(2, dtype=np.float32)
+        _lib.check(_lib.lib().mdp_sur_force_grad(self._h, int(snap0), int(snaps), float(alpha), g, losses),
+                   "mdp_sur_force_grad")
+        return g, (float(losses[0]), float(losses[1]))
+
+    def force_set_copy(self):
+        n = self._fset.natoms
+        npairs = int(_lib.lib().mdp_sur_force_set_npairs(self._h))
+        B = np.zeros((NK, n)); db = np.zeros((npairs, 3, NK), dtype=np.float32)
+        pinfo = np.zeros((npairs, 2), dtype=np.int32); poff = np.zeros(n + 1, dtype=np.int32)
+        _lib.check(_lib.lib().mdp_sur_force_set_copy(self._h, B.ctypes.data, db.ctypes.data, pinfo.ctypes.data,
+                                                     poff.ctypes.data), "mdp_sur_force_set_copy")
+        return B.T.copy(), db, pinfo, poff
+
+    for f in (force_set, train_forces, force_grad, force_set_copy):
+        setattr(Surrogate, f.__name__, f)
+
+
+_force_methods()
+
+
 def features(md, sur: Surrogate) -> np.ndarray:
     """Per-atom 2J=4 bispectrum (natoms, 14) of md's current positions."""
     B = np.zeros(NK * md.natoms)
@@ -170,20 +216,23 @@ class TrainingSet:
     cells: tuple = (10, 10, 10)     # 2,000 BCC atoms
     every: int = 10                 # MD steps between snapshots
     segment: int = 100              # snapshots per trajectory before a fresh start
+    force_every: int = 10           # every n-th snapshot also keeps positions and forces
     equilibrate: int = 50
     dt: float = 0.001
     seed: int = 7
     neighmax: int = 128             # hot snapshots crowd more atoms into rcut + skin
 
 
-def generate(sur: Surrogate, p8: SnapParams, ts: TrainingSet, precision: str = "fp64", device: int = 0) -> int:
+def generate(sur: Surrogate, p8: SnapParams, ts: TrainingSet, precision: str = "fp64", device: int = 0,
+             forces: list | None = None) -> int:
     """Runs plain 2J=8 SNAP MD at each temperature and appends snapshots to sur's set.
 
     Each temperature's snapshots come from short trajectories (ts.segment
     snapshots each) restarted from a freshly jittered lattice with new
     velocities: the seeded-coefficient potential has no repulsive core, so one
     long hot trajectory drifts into collapsed configurations no deployment
-    visits."""
+    visits.  When forces is a list, every ts.force_every-th snapshot appends
+    (positions, box, forces, per-atom energies) to it."""
     from .snap import SnapMD
     per = max(1, ts.snapshots // len(ts.temps))
     natoms = 2 * int(np.prod(ts.cells))
@@ -203,6 +252,9 @@ def generate(sur: Surrogate, p8: SnapParams, ts: TrainingSet, precision: str = "
             for _ in range(min(ts.segment, per - done)):
                 md.run(ts.every)
                 sur.sample(md)
+                if forces is not None and done % ts.force_every == 0:
+                    x, _, f, e = md.state()
+                    forces.append((x, cfg.box.copy(), f, e))
                 done += 1
             seg += 1
         md.close()
@@ -250,13 +302,16 @@ def force_errors(p8: SnapParams, sur: Surrogate | None, lin_coeff: np.ndarray | 
 
 
 def train_default(p8: SnapParams, ts: TrainingSet, steps: int = 20000, batch: int = 8192, lr: float = 2e-3,
-                  seed: int = 1, device: int = 0, log=print) -> tuple[Surrogate, dict]:
-    """Generate the training set, fit the normalisation and train with Adam
-    (learning rate decayed 10x over the last half of the steps)."""
+                  seed: int = 1, device: int = 0, log=print, force_steps: int = 4000, force_lr: float = 5e-4,
+                  alpha: float = 1.0) -> tuple[Surrogate, dict]:
+    """Generate the training set, fit the normalisation and train with Adam on
+    per-atom energies, then on energies and forces of every force_every-th
+    snapshot (learning rates decayed 10x over the last half of each phase)."""
     import time
     sur = Surrogate(snap_params(4, seed=0), device=device)
     t0 = time.time()
-    n = generate(sur, p8, ts, device=device)
+    fsnaps = [] if force_steps > 0 else None
+    n = generate(sur, p8, ts, device=device, forces=fsnaps)
     t1 = time.time()
     log(f"training set: {n} atoms from {ts.snapshots} snapshots in {t1 - t0:.1f} s")
     sur.set_params(init_params(seed))
@@ -274,7 +329,28 @@ def train_default(p8: SnapParams, ts: TrainingSet, steps: int = 20000, batch: in
     log(f"trained {steps} steps (batch {batch}) in {t2 - t1:.1f} s; loss {loss[:20].mean():.4f} -> {loss[-200:].mean():.4f}")
     X, E = sur.dataset()
     info = dict(rows=n, gen_s=t1 - t0, train_s=t2 - t1, loss_first=float(loss[:20].mean()),
-                loss_last=float(loss[-200:].mean()), lin_coeff=linear_fit(X, E))
+                loss_last=float(loss[-200:].mean()), lin_coeff=linear_fit(X, E), force_steps=0)
+    if force_steps > 0 and fsnaps:
+        from . import fit
+        per = fsnaps[0][0].shape[0]
+        bf = fit.BatchFit(snap_params(4, seed=0), device=device)
+        bf.set_batch([fit.FitConfig(x=np.mod(x, box), box=box, kind="snapshot") for x, box, _, _ in fsnaps])
+        sur.force_set(bf, np.concatenate([f for _, _, f, _ in fsnaps]), np.concatenate([e for *_, e in fsnaps]), per)
+        t3 = time.time()
+        fl, el = [], []
+        chunk = max(1, force_steps // 10)
+        for i in range(0, force_steps, chunk):
+            frac = i / force_steps
+            lri = force_lr if frac < 0.5 else force_lr * 10 ** (-(frac - 0.5) * 2)
+            le, lf = sur.train_forces(min(chunk, force_steps - i), snaps_per_batch=4, lr=lri, alpha=alpha,
+                                      seed=seed + 7 * i)
+            el.append(le); fl.append(lf)
+        el, fl = np.concatenate(el), np.concatenate(fl)
+        t4 = time.time()
+        log(f"force matching: {len(fsnaps)} snapshots, {force_steps} steps in {t4 - t3:.1f} s; "
+            f"energy loss {el[:20].mean():.4f} -> {el[-100:].mean():.4f}, force loss {fl[:20].mean():.4f} -> {fl[-100:].mean():.4f}")
+        info.update(force_steps=force_steps, force_snapshots=len(fsnaps), force_train_s=t4 - t3,
+                    force_loss_first=float(fl[:20].mean()), force_loss_last=float(fl[-100:].mean()))
     return sur, info
 
 

@@ -99,3 +99,67 @@ def loss_grad(P, norm, X, E):
     g[OFF_W1:OFF_B1] = gw1.ravel()
     g[OFF_B1:OFF_W2] = d1.sum(axis=0)
     return g, float(np.mean(r * r))
+
+
+def _d2silu(z):
+    s = _sig(z)
+    return s * (1.0 - s) * (2.0 + z * (1.0 - 2.0 * s))
+
+
+def force_loss_grad(P, norm, B, db, pinfo, F_ref, E_ref, alpha, var):
+    """Combined loss of the force-matching training and its parameter gradient.
+
+    B (n, 14) features, db (npairs, 3, 14) dB_i/dr_p for pair p = (i -> j)
+    (r_p = x_j - x_i), pinfo (npairs, 2) = (i, j), F_ref (n, 3), E_ref (n,).
+    Loss = mean(((y - t))^2) + alpha * sum |F - F_ref|^2 / (3 n var) with
+    F_a = -sum_i G_i . dB_i/dx_a and G_i = dE_i/dB_i.  Returns (grad, (Le, Lf)).
+    """
+    w = forward_params(P)
+    mu, sinv, emu, esd = split_norm(norm)
+    B = np.asarray(B, dtype=np.float64)
+    n = B.shape[0]
+    x = (B - mu) * sinv
+    z1 = x @ w["W1"].T + w["b1"]
+    a1 = _silu(z1)
+    z2 = a1 @ w["W2"].T + w["b2"]
+    a2 = _silu(z2)
+    y = a2 @ w["w3"] + w["b3"]
+    g2 = w["w3"] * _dsilu(z2)
+    g1 = (g2 @ w["W2"]) * _dsilu(z1)
+    G = (g1 @ w["W1"]) * sinv * esd
+    i, j = pinfo[:, 0], pinfo[:, 1]
+    db = np.asarray(db, dtype=np.float64)
+    contrib = np.einsum("pk,pck->pc", G[i], db)
+    dE = np.zeros((n, 3))
+    np.add.at(dE, j, contrib)
+    np.add.at(dE, i, -contrib)
+    r = -dE - F_ref
+    Lf = alpha * np.sum(r * r) / (3.0 * n * var)
+    Q = 2.0 * alpha * r / (3.0 * n * var)
+    lam = np.zeros((n, NK))
+    np.add.at(lam, i, -np.einsum("pck,pc->pk", db, Q[j] - Q[i]))
+    v = lam * esd * sinv
+    t = (np.asarray(E_ref, dtype=np.float64) - emu) / esd
+    re = y - t
+    Le = float(np.mean(re * re))
+    yb = 2.0 * re / n
+    zd1 = v @ w["W1"].T
+    ad1 = _dsilu(z1) * zd1
+    zd2 = ad1 @ w["W2"].T
+    ad2 = _dsilu(z2) * zd2
+    g = np.zeros(NPAR)
+    g[OFF_W3:OFF_B3] = yb @ a2 + ad2.sum(axis=0)
+    g[OFF_B3] = yb.sum()
+    z2b = yb[:, None] * w["w3"] * _dsilu(z2) + w["w3"] * _d2silu(z2) * zd2
+    zd2b = w["w3"] * _dsilu(z2) * np.ones_like(z2)
+    g[OFF_W2:OFF_B2] = (z2b.T @ a1 + zd2b.T @ ad1).ravel()
+    g[OFF_B2:OFF_W3] = z2b.sum(axis=0)
+    a1b = z2b @ w["W2"]
+    ad1b = zd2b @ w["W2"]
+    z1b = a1b * _dsilu(z1) + ad1b * _d2silu(z1) * zd1
+    zd1b = ad1b * _dsilu(z1)
+    gw1 = np.zeros((H, KP))
+    gw1[:, :NK] = z1b.T @ x + zd1b.T @ v
+    g[OFF_W1:OFF_B1] = gw1.ravel()
+    g[OFF_B1:OFF_W2] = z1b.sum(axis=0)
+    return g, (Le, Lf)

@@ -132,3 +132,43 @@ def test_judge_falls_back_to_plain_model(sur):
     assert st["active"] and st["fallback_step"] == -1 and st["judgements"] == 4
     assert np.all(np.diff(st["log"][:, 0]) == 2) and np.all(st["log"][:, 1] > 0)
     md.close()
+
+
+def _force_set(sur, nsnap=3, seed=40):
+    """A small force set: jittered 54-atom cells with plain 2J=8 forces."""
+    from mdp_b200 import fit
+    from mdp_b200.snap import snap_compute
+    p8 = configs.snap_params(8, seed=1)
+    snaps, F, E = [], [], []
+    for s in range(nsnap):
+        cfg = configs.ta_config((3, 3, 3), temp=600.0, jitter=0.12, seed=seed + s)
+        out = snap_compute(p8, cfg.x, cfg.box, 1.0, 96, precision="fp64")
+        snaps.append(fit.FitConfig(x=cfg.x, box=cfg.box, kind="bcc"))
+        F.append(out["fatom"]); E.append(out["eatom"])
+    bf = fit.BatchFit(configs.snap_params(4, seed=0))
+    bf.set_batch(snaps)
+    sur.force_set(bf, np.concatenate(F), np.concatenate(E), 54)
+    return np.concatenate(F), np.concatenate(E)
+
+
+def test_force_matching_gradient_matches_oracle(sur):
+    F, E = _force_set(sur)
+    B, db, pinfo, poff = sur.force_set_copy()
+    norm = np.concatenate([B.mean(0), 1.0 / (B.std(0) + 1e-12), [E.mean(), E.std()]]).astype(np.float32)
+    P = su.init_params(9)
+    sur.set_params(P, norm)
+    var = np.mean(F ** 2)
+    g, (le, lf) = sur.force_grad(0, 3, alpha=0.8)
+    go, (leo, lfo) = mo.force_loss_grad(P, norm, B, db, pinfo, F, E, 0.8, var)
+    assert abs(le - leo) < 1e-4 * max(1.0, leo) and abs(lf - lfo) < 1e-4 * max(1.0, lfo)
+    err = np.linalg.norm(g - go) / np.linalg.norm(go)
+    assert err < 1e-3, err
+
+
+def test_force_matching_lowers_force_loss(sur):
+    F, E = _force_set(sur, nsnap=8, seed=60)
+    B, *_ = sur.force_set_copy()
+    norm = np.concatenate([B.mean(0), 1.0 / (B.std(0) + 1e-12), [E.mean(), E.std()]]).astype(np.float32)
+    sur.set_params(su.init_params(10), norm)
+    le, lf = sur.train_forces(400, snaps_per_batch=2, lr=2e-3, alpha=1.0, seed=3)
+    assert np.all(np.isfinite(lf)) and lf[-40:].mean() < 0.5 * lf[:10].mean()
