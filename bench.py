@@ -228,7 +228,9 @@ def surrogate_leg(args, dev, barrier, ws):
            "training": {"snapshots": ts.snapshots, "atoms_per_snapshot": 2000, "rows": info["rows"],
                         "temps_K": list(ts.temps), "adam_steps": args.sur_train_steps, "batch": 8192,
                         "loss_first": info["loss_first"], "loss_last": info["loss_last"],
-                        "generate_s": info["gen_s"], "train_s": info["train_s"]},
+                        "generate_s": info["gen_s"], "train_s": info["train_s"],
+                        "force_matching": {k: info.get(k) for k in ("force_steps", "force_snapshots", "force_train_s",
+                                                                    "force_loss_first", "force_loss_last")}},
            "heldout_2000_atoms_1000K": errs}
     for mode, judge in (("unjudged", 0), ("judged", 50)):
         md = SnapMD(p8, cfg.box, n, DT, skin=SKIN, neighmax=96, precision="fp64", device=dev)

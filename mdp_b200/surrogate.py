@@ -302,8 +302,8 @@ def force_errors(p8: SnapParams, sur: Surrogate | None, lin_coeff: np.ndarray | 
 
 
 def train_default(p8: SnapParams, ts: TrainingSet, steps: int = 20000, batch: int = 8192, lr: float = 2e-3,
-                  seed: int = 1, device: int = 0, log=print, force_steps: int = 4000, force_lr: float = 5e-4,
-                  alpha: float = 1.0) -> tuple[Surrogate, dict]:
+                  seed: int = 1, device: int = 0, log=print, force_steps: int = 30000, force_lr: float = 5e-4,
+                  alpha: float = 4.0) -> tuple[Surrogate, dict]:
     """Generate the training set, fit the normalisation and train with Adam on
     per-atom energies, then on energies and forces of every force_every-th
     snapshot (learning rates decayed 10x over the last half of each phase)."""
