@@ -596,7 +596,7 @@ int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const doubl
     MDP_CUDA_TRY(cudaMemsetAsync(os.nb.cursor.p, 0, sizeof(int) * inum, s));
     k_rev_fill<<<gb, tb, 0, s>>>(neighlist, neighnum, alist, inum, neighmax, os.nb.roff.as<int>(),
                                  os.nb.cursor.as<int>(), os.nb.rlist.as<long long>());
-    k_rev_sort<<<gb, tb, 0, s>>>(inum, os.nb.roff.as<int>(), os.nb.rlist.as<long long>());
+    k_rev_sort<<<std::min((inum + 7) / 8, num_sms() * 8), 256, 0, s>>>(inum, os.nb.roff.as<int>(), os.nb.rlist.as<long long>());
     if (force_compute(os.fp, os.model, precision, os.x4.as<double4>(), inum, neighlist, neighnum, neighmax,
                       (long)inum * neighmax, os.nb.roff.as<int>(), os.nb.rlist.as<long long>(), eatom,
                       os.f4.as<double4>(), vatom, s))

@@ -285,16 +285,50 @@ __global__ void k_rev_fill(const int *__restrict__ nlist, const int *__restrict_
     }
 }
 
-__global__ void k_rev_sort(int inum, const int *__restrict__ roff, long long *__restrict__ rlist)
+// Each owner's reverse entries ascending, so the tally sums in a fixed order.
+// One warp per owner: the entries go to shared memory, padded to a power of
+// two with the largest key, and a bitonic network sorts them (lists longer
+// than REV_SORT_MAX fall back to an insertion sort in place).
+constexpr int REV_SORT_WARPS = 8, REV_SORT_MAX = 256;
+
+__global__ void __launch_bounds__(REV_SORT_WARPS * 32)
+k_rev_sort(int inum, const int *__restrict__ roff, long long *__restrict__ rlist)
 {
-    int o = blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= inum) return;
-    const int s = roff[o], e = roff[o + 1];
-    for (int a = s + 1; a < e; a++) {
-        long long v = rlist[a];
-        int b = a - 1;
-        while (b >= s && rlist[b] > v) { rlist[b + 1] = rlist[b]; b--; }
-        rlist[b + 1] = v;
+    __shared__ long long keys[REV_SORT_WARPS][REV_SORT_MAX];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long *kw = keys[w];
+    for (int o = blockIdx.x * REV_SORT_WARPS + w; o < inum; o += gridDim.x * REV_SORT_WARPS) {
+        const int s = roff[o], e = roff[o + 1], n = e - s;
+        if (n <= 1) continue;
+        if (n > REV_SORT_MAX) {
+            if (lane == 0)
+                for (int a = s + 1; a < e; a++) {
+                    const long long v = rlist[a];
+                    int b = a - 1;
+                    while (b >= s && rlist[b] > v) { rlist[b + 1] = rlist[b]; b--; }
+                    rlist[b + 1] = v;
+                }
+            __syncwarp();
+            continue;
+        }
+        int P = 2;
+        while (P < n) P <<= 1;
+        for (int i = lane; i < P; i += 32) kw[i] = (i < n) ? rlist[s + i] : 0x7fffffffffffffffLL;
+        __syncwarp();
+        for (int k = 2; k <= P; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < P; i += 32) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const long long a = kw[i], b = kw[l];
+                        const bool up = (i & k) == 0;
+                        if ((a > b) == up) { kw[i] = b; kw[l] = a; }
+                    }
+                }
+                __syncwarp();
+            }
+        for (int i = lane; i < n; i += 32) rlist[s + i] = kw[i];
+        __syncwarp();
     }
 }
 

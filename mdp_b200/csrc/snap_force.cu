@@ -303,7 +303,7 @@ int neighbor_build(Neighbors &nb, const BoxParams &bp, double4 *x, int inum, dou
     MDP_CUDA_TRY(cudaMemsetAsync(nb.cursor.p, 0, sizeof(int) * inum, s));
     k_rev_fill<<<(inum + tb - 1) / tb, tb, 0, s>>>(nb.nlist.as<int>(), nb.nnum.as<int>(), nb.alist.as<int>(), inum, nm,
                                                    nb.roff.as<int>(), nb.cursor.as<int>(), nb.rlist.as<long long>());
-    k_rev_sort<<<(inum + tb - 1) / tb, tb, 0, s>>>(inum, nb.roff.as<int>(), nb.rlist.as<long long>());
+    k_rev_sort<<<std::min((inum + 7) / 8, num_sms() * 8), 256, 0, s>>>(inum, nb.roff.as<int>(), nb.rlist.as<long long>());
     count_launches(8);
     int hs[2] = {0, 0};
     MDP_CUDA_TRY(cudaMemcpyAsync(&hs[0], nb.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
