@@ -363,7 +363,7 @@ def run_ours(args):
     fit_line = None
     if not args.no_fit:
         from mdp_b200 import fit as fitmod
-        fit_line = fitmod.benchmark(args.fit_configs, device=dev, log=lambda m: None)
+        fit_line = fitmod.benchmark(args.fit_configs, device=dev, log=lambda m: None, rank=rank, world=ws)
         fit_line["workload"] = ("4,096 periodic Ta configurations (BCC/FCC/A15, 16-512 atoms, strain +-5%, "
                                 "jitter U[0.02,0.3] A), 2J=8 bi + dB/dR, normal equations of energy + force rows, "
                                 "targets ~ N(0,1)") if args.fit_configs == 4096 else f"{args.fit_configs} configurations"

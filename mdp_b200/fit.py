@@ -176,25 +176,41 @@ def rows_numpy(cfgs, bi, bd, e, f, we=None, wf=None):
     return R, t
 
 
-def benchmark(nconf: int = 4096, seed: int = 2024, coeff_seed: int = 2024, device: int = 0, log=print) -> dict:
+def benchmark(nconf: int = 4096, seed: int = 2024, coeff_seed: int = 2024, device: int = 0, log=print,
+              rank: int = 0, world: int = 1) -> dict:
     """The batched-fitting workload end to end: batch set-up (positions to the
     device, pair lists), autotuning, then one graph launch per assembly mode
-    (timed with CUDA events), and the FP64 vs BF16-split solutions."""
+    (timed with CUDA events), and the FP64 vs BF16-split solutions.  With
+    world > 1 (torch.distributed initialised) every rank takes an atom-balanced
+    share of the configurations and one all-reduce sums A and b; times are the
+    maximum over ranks."""
     import time
+    from . import parallel
     from .configs import snap_params
     cfgs, e, f = batch_configs(nconf, seed=seed)
+    counts = np.array([c.natoms for c in cfgs])
+    lo, hi = parallel.shard_bounds(counts, rank, world) if world > 1 else (0, nconf)
+    a0 = np.concatenate([[0], np.cumsum(counts)])
     p = snap_params(8, seed=coeff_seed)
     bf = BatchFit(p, device=device)
     t0 = time.perf_counter()
-    bf.set_batch(cfgs, e, f)
+    bf.set_batch(cfgs[lo:hi], e[lo:hi], f[a0[lo]:a0[hi]])
     t_set = time.perf_counter() - t0
     tuned = bf.tune()
-    out = {"configs": nconf, "atoms": bf.natoms, "pairs": bf.npairs(), "chunks": bf.nchunks(),
-           "rows": nconf + 3 * bf.natoms, "batch_setup_s": t_set, "tuned": tuned}
+    out = {"configs": nconf, "atoms": int(counts.sum()), "ranks": world, "pairs_rank0": bf.npairs(),
+           "chunks_rank0": bf.nchunks(), "rows": nconf + 3 * int(counts.sum()), "batch_setup_s": t_set,
+           "tuned": tuned}
+    dev = None
+    if world > 1:
+        import torch
+        dev = torch.device("cuda", device)
     sol = {}
     for mode in ("fp64", "bf16"):
         bf.run(mode)                       # capture and warm
         A, b, ms = bf.run(mode)            # one graph launch
+        if world > 1:
+            A, b = parallel.allreduce_sum(A, b, device=dev)
+            ms = parallel.max_over_ranks(ms, device=dev)
         out[f"graph_ms_{mode}"] = ms
         sol[mode] = (A, b)
     A64, b64 = sol["fp64"]
@@ -208,7 +224,7 @@ def benchmark(nconf: int = 4096, seed: int = 2024, coeff_seed: int = 2024, devic
     dg = 1.0 / np.sqrt(np.diag(A64))
     out["cond_A_equilibrated"] = float(np.linalg.cond(A64 * dg[:, None] * dg[None, :]))
     out["configs_per_s_fp64"] = nconf / (out["graph_ms_fp64"] * 1e-3)
-    out["atoms_per_s_fp64"] = bf.natoms / (out["graph_ms_fp64"] * 1e-3)
+    out["atoms_per_s_fp64"] = out["atoms"] / (out["graph_ms_fp64"] * 1e-3)
     bf.close()
     log(out)
     return out
