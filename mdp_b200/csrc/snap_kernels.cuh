@@ -1039,9 +1039,10 @@ __device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__
 }
 
 template <typename T, int TJ>
-__global__ void __launch_bounds__(FR_THREADS)
-k_snap_fr(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
-          SnapGeom gp, const typename cplx<T>::type *__restrict__ Y, double4 *__restrict__ dEslot)
+__device__ __forceinline__ void fr_kernel_body(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo,
+                                               const int *__restrict__ pnum, const SnapGeom &gp,
+                                               const typename cplx<T>::type *__restrict__ Y,
+                                               double4 *__restrict__ dEslot)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double *qg = reinterpret_cast<double *>(smraw) + threadIdx.x;
@@ -1049,6 +1050,24 @@ k_snap_fr(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, cons
     const int npairs = *pnum;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x)
         fr_pair<T, TJ>(p, prij, pinfo, gp, Y, dEslot, qs, qg);
+}
+
+template <typename T, int TJ>
+__global__ void __launch_bounds__(FR_THREADS)
+k_snap_fr(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
+          SnapGeom gp, const typename cplx<T>::type *__restrict__ Y, double4 *__restrict__ dEslot)
+{
+    fr_kernel_body<T, TJ>(prij, pinfo, pnum, gp, Y, dEslot);
+}
+
+// FP32: the state takes half the registers, so the kernel is held to 128 and
+// four CTAs share an SM
+template <int TJ>
+__global__ void __launch_bounds__(FR_THREADS, 4)
+k_snap_fr32(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
+            SnapGeom gp, const float2 *__restrict__ Y, double4 *__restrict__ dEslot)
+{
+    fr_kernel_body<float, TJ>(prij, pinfo, pnum, gp, Y, dEslot);
 }
 
 }  // namespace mdp
