@@ -422,8 +422,10 @@ int mdp_md_counters(mdp_md *m, long long *out)
 {
     if (!m || !out) { set_error("null argument"); return -1; }
     int np = 0;
-    if (m->fp.poff.p)
-        MDP_CUDA_TRY(cudaMemcpy(&np, m->fp.poff.as<int>() + m->cfg.natoms, sizeof(int), cudaMemcpyDeviceToHost));
+    if (m->fp.poff.p) {
+        MDP_CUDA_TRY(cudaMemcpyAsync(&np, m->fp.poff.as<int>() + m->cfg.natoms, sizeof(int), cudaMemcpyDeviceToHost, m->s));
+        MDP_CUDA_TRY(cudaStreamSynchronize(m->s));
+    }
     out[0] = m->step; out[1] = m->rebuilds; out[2] = np; out[3] = m->nb.gnum; out[4] = m->nb.nsum;
     return 0;
 }

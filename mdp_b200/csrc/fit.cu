@@ -855,6 +855,7 @@ static int fit_alloc_work(mdp_fit *h)
     h->nrows = h->nconf + 3L * n;
     // chunk plan over whole configurations
     std::vector<int> poff(n + 1);
+    MDP_CUDA_TRY(cudaStreamSynchronize(h->s));
     MDP_CUDA_TRY(cudaMemcpy(poff.data(), h->poff.p, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
     const double per_pair = 3.0 * (yh_count(tj) * sizeof(double2) + h->tab.ntri * sizeof(double));
     const double per_tile = (double)h->tab.nz * 32 * sizeof(double2);
@@ -1003,6 +1004,9 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
     MDP_CUDA_TRY(cudaMemcpy(h->wf.p, wf ? wf : ones.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->e.p, e ? e : zc.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->f.p, f ? f : zf.data(), sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice));
+    // a copy from pageable memory may return before it lands, and the batch
+    // is read next on the fit's non-blocking stream
+    MDP_CUDA_TRY(cudaDeviceSynchronize());
     if (fit_pairs(h) || fit_alloc_work(h)) return -1;
     return 0;
 }

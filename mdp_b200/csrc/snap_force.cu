@@ -9,20 +9,38 @@
 
 namespace mdp {
 
+// Growth drains the device on both sides.  The old buffer may still be read
+// by work queued on any stream, and the zero fill runs on the legacy stream,
+// which does not order with the engine's non-blocking streams: without the
+// drain, kernels queued right after a growth raced the fill and some of their
+// first results were zeroed.  Growth happens only on a buffer's first use at a
+// larger size, never inside a stream capture.
 int DevBuf::ensure(size_t n)
 {
     if (n <= bytes) return 0;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        set_error("device synchronize before growing a buffer: %s", cudaGetErrorString(e));
+        return -1;
+    }
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
     size_t want = n + n / 8 + 256;
-    cudaError_t e = cudaMalloc(&p, want);
+    e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         set_error("cudaMalloc(%zu bytes): %s", want, cudaGetErrorString(e));
         p = nullptr;
         return -1;
     }
-    cudaMemset(p, 0, want);
+    e = cudaMemset(p, 0, want);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        set_error("zero fill of %zu bytes: %s", want, cudaGetErrorString(e));
+        cudaFree(p);
+        p = nullptr;
+        return -1;
+    }
     bytes = want;
     return 0;
 }

@@ -766,6 +766,8 @@ int mdp_sur_set_params(mdp_sur *S, const float *params, const float *norm)
     MDP_CUDA_TRY(cudaMemset(S->grad.p, 0, sizeof(float) * SUR_NPAR));
     MDP_CUDA_TRY(cudaMemset(S->m1.p, 0, sizeof(float) * SUR_NPAR));
     MDP_CUDA_TRY(cudaMemset(S->m2.p, 0, sizeof(float) * SUR_NPAR));
+    // the MD engine reads the rounded parameters on its own stream
+    MDP_CUDA_TRY(cudaDeviceSynchronize());
     S->adam_t = 0;
     if (norm) {
         for (int k = 0; k < SUR_NK; k++) { S->norm.mu[k] = norm[k]; S->norm.sinv[k] = norm[SUR_NK + k]; }
@@ -810,7 +812,8 @@ int mdp_sur_dataset_add(mdp_sur *S, const double *B_dev, long bstride, const dou
     k_sur_append<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(B_dev, bstride, e_dev, n, S->X.as<float>(),
                                                                   S->E.as<float>(), S->rows);
     count_launches(1);
-    MDP_CUDA_TRY(cudaGetLastError());
+    // the dataset is read next by training kernels on the legacy stream
+    MDP_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
     S->rows += n;
     return 0;
 }
@@ -881,6 +884,8 @@ int mdp_sur_train(mdp_sur *S, int steps, int batch, float lr, unsigned long long
     }
     MDP_CUDA_TRY(cudaGetLastError());
     if (loss) MDP_CUDA_TRY(cudaMemcpy(loss, lbuf.p, sizeof(float) * steps, cudaMemcpyDeviceToHost));
+    // the MD engine reads the parameters on its own stream
+    MDP_CUDA_TRY(cudaDeviceSynchronize());
     lbuf.release();
     return 0;
 }
@@ -1027,6 +1032,8 @@ int mdp_sur_train_forces(mdp_sur *S, int steps, int snaps_per_batch, float lr, f
             if (loss_f) loss_f[i] = h[2 * i + 1];
         }
     }
+    // the MD engine reads the parameters on its own stream
+    MDP_CUDA_TRY(cudaDeviceSynchronize());
     lb.release();
     return 0;
 }

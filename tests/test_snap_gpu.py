@@ -99,6 +99,31 @@ def test_md_energy_conservation_2j8(cuda_lib):
     md.close()
 
 
+def test_md_setup_on_reused_memory_matches_one_shot(cuda_lib):
+    """The MD engine's first evaluation, on buffers freshly grown while the
+    device memory still holds other data, equals the one-shot path on the same
+    positions for every atom (250,000 atoms at 1,000 K, neighmax 96).  A zero
+    fill that was not ordered with the engine's stream once corrupted a few
+    atoms of exactly this evaluation."""
+    import torch
+    from mdp_b200.snap import SnapMD, snap_compute
+    p = configs.snap_params(8, seed=2024)
+    cfg = configs.ta_config((50, 50, 50), temp=1000.0, jitter=0.05 * np.sqrt(1000.0 / 300.0), seed=2025)
+    junk = torch.full((1 << 30,), float("nan"), dtype=torch.float64, device="cuda")   # 8 GB of NaN bytes
+    del junk
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    md = SnapMD(p, cfg.box, cfg.natoms, 0.001, skin=1.0, neighmax=96)
+    md.set_state(cfg.x, cfg.v)
+    md.setup()
+    _, _, f, e = md.state()
+    md.close()
+    ref = snap_compute(p, cfg.x, cfg.box, 1.0, 96)
+    assert np.isfinite(f).all() and np.isfinite(e).all()
+    assert rel_inf(f, ref["fatom"]) < TOL_FP64
+    assert rel_inf(e, ref["eatom"]) < TOL_FP64
+
+
 def test_neighbor_overflow_is_an_error(cuda_lib):
     from mdp_b200 import _lib
     from mdp_b200.snap import snap_compute
