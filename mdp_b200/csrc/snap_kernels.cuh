@@ -45,7 +45,10 @@ struct YParams {
     // betaY[tri] * G[kmap[tri]] (betaY then holds the multiplicity factors)
     unsigned char kmap[NTRI];
 };
-template <typename T> struct YiWarps { static constexpr int n = 8; };
+// warps per Y CTA: FP64 10 (two per row of the costliest layer; 168
+// registers; measured 65 ms at 2M atoms against 70 / 71 / 68 / 68 / 74 ms for
+// 9 / 8 / 11 / 12 / 14 warps), FP32 16
+template <typename T> struct YiWarps { static constexpr int n = 10; };
 template <> struct YiWarps<float> { static constexpr int n = 16; };
 
 __host__ __device__ constexpr bool coupling_ok(int j1, int j2, int j)
