@@ -24,6 +24,17 @@ def bind(path):
         [C.c_int] * 7
     for f in ("idxbcount", "idxcgcount", "idxucount", "idxzcount"):
         getattr(L, f).argtypes = [C.c_int]
+    # descriptor chain (cpuSnap.h:48-84)
+    L.cpuComputeSij.argtypes = [D] * 8 + [D, D, D, D, C.c_double, C.c_double, C.c_double, I, I, I] + [C.c_int] * 4
+    L.cpuComputeUij.argtypes = [D] * 4 + [D, D, D, D, C.c_double, C.c_double, C.c_double, I, I, I] + [C.c_int] * 4
+    L.cpuZeroUarraytot2.argtypes = [D, D, C.c_double, I, I, I, I] + [C.c_int] * 6
+    L.cpuAddUarraytot.argtypes = [D, D, D, D, I, I, I] + [C.c_int] * 4
+    L.cpuComputeZi2.argtypes = [D, D, D, D, D, I, I, I] + [C.c_int] * 6
+    L.cpuComputeBi2.argtypes = [D, D, D, D, D, D, I, I, I, I, I, I] + [C.c_int] * 9
+    L.cpuComputeDbidrj.argtypes = [D, D, D, D, D, I, I, I, I, I, I] + [C.c_int] * 9
+    L.cpuSnapTallyBispectrum.argtypes = [D, D, I, I] + [C.c_int] * 5
+    L.cpuSnapTallyBispectrumDeriv.argtypes = [D, D, D, I, I, I, I] + [C.c_int] * 6
+    L.cpuSnapTallyBispectrumVirial.argtypes = [D, D, D, D, I, I] + [C.c_int] * 6
     return L
 
 
@@ -43,10 +54,8 @@ def tables(L, tj):
     return t
 
 
-def snap_sequence(L, g, p):
-    """Returns every stage's output for the configuration in golden fixture g."""
-    tj = p.twojmax
-    t = tables(L, tj)
+def _pairs(L, g, p):
+    """Pair list and pair arrays of golden fixture g (cpuNeighPairList, cpuNeighPairs)."""
     x = np.ascontiguousarray(g["xall"]).ravel()
     n = g["x"].shape[0]
     nl, nn = g["neighlist"], g["neighnum"]
@@ -67,6 +76,18 @@ def snap_sequence(L, g, p):
     aj = np.zeros(ij, dtype=np.int32); ti = np.zeros(ij, dtype=np.int32); tjv = np.zeros(ij, dtype=np.int32)
     L.cpuNeighPairs(rij, x, aii, ai, aj, ti, tjv, pairlist, pns, ilist, atype, alist, n, 3)
     radelem = np.array([0.0, p.radelem]); wjelem = np.array([0.0, p.wjelem]); mp = np.zeros(2, dtype=np.int32)
+    return dict(n=n, ij=ij, ilist=ilist, atype=atype, pairnum=pairnum, pairlist=pairlist, rij=rij, aii=aii, ai=ai,
+                aj=aj, ti=ti, tjv=tjv, radelem=radelem, wjelem=wjelem, mp=mp)
+
+
+def snap_sequence(L, g, p):
+    """Returns every stage's output for the configuration in golden fixture g."""
+    tj = p.twojmax
+    t = tables(L, tj)
+    q = _pairs(L, g, p)
+    n, ij, ilist, atype, pairnum, pairlist = q["n"], q["ij"], q["ilist"], q["atype"], q["pairnum"], q["pairlist"]
+    rij, aii, ai, aj, ti, tjv = q["rij"], q["aii"], q["ai"], q["aj"], q["ti"], q["tjv"]
+    radelem, wjelem, mp = q["radelem"], q["wjelem"], q["mp"]
     nu = t["nu"]
     ur = np.zeros(n * nu); ui = np.zeros(n * nu)
     L.cpuSnapComputeUi(ur, ui, t["rootpq"], rij, wjelem, radelem, p.rmin0, p.rfac0, p.rcutfac, mp, ai, ti, tjv,
@@ -89,3 +110,43 @@ def snap_sequence(L, g, p):
                        ti, tjv, tj, nu, n, n, ij, p.switchflag, 0)
     return dict(tables=t, pairnum=pairnum, pairlist=pairlist[:ij], rij=rij, aii=aii, ai=ai, aj=aj, u_pairs=u_pairs,
                 u=(ur, ui), eatom=e, blist=b, y=(yr, yi), fatom=f, vatom=v)
+
+
+def descriptor_sequence(L, g, p, quadratic=0):
+    """snapdescriptors' calls after the pair list (src/Julia/Potential/snapcpp.jl:539-665):
+    per-pair U and dU (cpuComputeUij, and cpuComputeSij on the same pairs), U
+    totals, Z, B, dB/dr and the three tallies.  Returns every stage's output."""
+    tj = p.twojmax
+    t = tables(L, tj)
+    q = _pairs(L, g, p)
+    n, ij, ilist, atype = q["n"], q["ij"], q["ilist"], q["atype"]
+    rij, ai, aj, ti, tjv, mp = q["rij"], q["ai"], q["aj"], q["ti"], q["tjv"], q["mp"]
+    nu, nz, nb = t["nu"], t["nz"], t["nb"]
+    geo = (t["rootpq"], rij, q["wjelem"], q["radelem"], p.rmin0, p.rfac0, p.rcutfac, t["idxu_block"], ti, tjv, tj, nu,
+           ij, p.switchflag)
+    ur = np.zeros(nu * ij); ui = np.zeros(nu * ij); dur = np.zeros(3 * nu * ij); dui = np.zeros(3 * nu * ij)
+    L.cpuComputeUij(ur, ui, dur, dui, *geo)
+    s8 = [np.zeros(nu * ij) for _ in range(8)]
+    L.cpuComputeSij(*s8, *geo)
+    utr = np.zeros(n * nu); uti = np.zeros(n * nu)
+    L.cpuZeroUarraytot2(utr, uti, 1.0, t["idxu_block"], atype, mp, ai, p.wselfallflag, 0, nu, 1, tj, n)
+    L.cpuAddUarraytot(utr, uti, ur, ui, mp, ai, tjv, nu, n, ij, 0)
+    zr = np.zeros(nz * n); zi = np.zeros(nz * n)
+    L.cpuComputeZi2(zr, zi, utr, uti, t["cg"], t["idxz"], t["idxu_block"], t["idxcg_block"], tj, nu, nz, 1,
+                    p.bnormflag, n)
+    bzero = np.array([1.0 if p.bnormflag else j + 1.0 for j in range(tj + 1)])
+    bl = np.zeros(nb * n)
+    L.cpuComputeBi2(bl, zr, zi, utr, uti, bzero, ilist, atype, mp, t["idxb"], t["idxu_block"], t["idxz_block"], tj,
+                    nb, nu, nz, 1, p.bzeroflag, p.wselfallflag, 0, n)
+    dbl = np.zeros(nb * 3 * ij)
+    L.cpuComputeDbidrj(dbl, zr, zi, dur, dui, t["idxb"], t["idxu_block"], t["idxz_block"], mp, ai, tjv, tj, nb, nu,
+                       nz, 1, p.bnormflag, 0, n, ij)
+    nper = nb + (nb * (nb + 1) // 2 if quadratic else 0)
+    bi = np.zeros(nper)
+    L.cpuSnapTallyBispectrum(bi, bl, ilist, atype, n, nb, nper, 1, quadratic)
+    bd = np.zeros(nper * 3 * n)
+    L.cpuSnapTallyBispectrumDeriv(bd, bl, dbl, ai, ai, aj, ti, n, ij, nb, nper, 1, quadratic)
+    bv = np.zeros(6 * nper)
+    L.cpuSnapTallyBispectrumVirial(bv, bl, dbl, rij, ai, ti, n, ij, nb, nper, 1, quadratic)
+    return dict(ulist=(ur, ui), dulist=(dur, dui), sij=tuple(s8), utot=(utr, uti), zlist=(zr, zi), blist=bl,
+                dblist=dbl, bi=bi, bd=bd, bv=bv)

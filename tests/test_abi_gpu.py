@@ -38,3 +38,27 @@ def test_julia_abi_matches_reference_library(cuda_lib, name):
     assert rel_inf(b["vatom"], a["vatom"]) < 1e-10
     # and against the golden ComputePairSnap3 forces
     assert rel_inf(b["fatom"].reshape(-1, 3), g["fatom"]) < 1e-10
+
+
+@pytest.mark.parametrize("name,quadratic", [("bcc128_2j6", 0), ("bcc250_2j8", 0), ("bcc128_2j4", 1),
+                                            ("bcc54_2j8_flags", 0), ("bcc250_2j8_hot", 1)])
+def test_descriptor_chain_matches_reference_library(cuda_lib, name, quadratic):
+    """snapdescriptors' calls (pair U and dU, U totals, Z, B, dB/dr, tallies)
+    on the reference CPU library and on ours, stage by stage."""
+    from mdp_b200 import _lib
+    ref = os.path.join(refpy.REF_DIR, "libcpuSnap_ref.so")
+    if not os.path.exists(ref):
+        pytest.fail("oracle/_ref/libcpuSnap_ref.so missing (build with make -C oracle ref)")
+    g = load_golden(name)
+    p = golden_params(g)
+    a = julia_abi.descriptor_sequence(julia_abi.bind(ref), g, p, quadratic)
+    b = julia_abi.descriptor_sequence(julia_abi.bind(_lib.LIB_PATH), g, p, quadratic)
+    for key in ("ulist", "dulist", "sij", "utot", "zlist"):
+        for x, y in zip(b[key], a[key]):
+            assert rel_inf(x, y) < 1e-12, key
+    for key in ("blist", "dblist", "bi", "bd", "bv"):
+        assert rel_inf(b[key], a[key]) < 1e-10, key
+    # entries the reference leaves alone (dU right of the half plane) stay zero
+    dur = a["dulist"][0].reshape(3, -1)
+    assert np.count_nonzero(dur) < dur.size
+    assert np.array_equal(b["dulist"][0] == 0.0, a["dulist"][0] == 0.0)

@@ -55,3 +55,19 @@ def test_init_sna_tables_match_reference(cuda_lib):
             assert np.array_equal(a[k][:4] if k == "idx_max" else a[k], b[k][:4] if k == "idx_max" else b[k]), k
         assert np.abs(a["cg"] - b["cg"]).max() < 1e-14
         assert np.abs(a["rootpq"] - b["rootpq"]).max() < 1e-15
+
+
+# every function of MDP's Julia C ABI (src/Julia/Potential/cpuSnap.h:7-84)
+JULIA_ABI = ["idxbcount", "idxcgcount", "idxucount", "idxzcount", "cpuInitSna", "cpuNeighPairList", "cpuNeighPairs",
+             "cpuSnapComputeUi", "cpuAddWself2Ui", "cpuSnapComputeEi", "cpuSnapComputeBi", "cpuSnapComputeYi",
+             "cpuSnapComputeFi", "cpuComputeSij", "cpuComputeUij", "cpuZeroUarraytot2", "cpuAddUarraytot",
+             "cpuComputeZi2", "cpuComputeBi2", "cpuComputeDbidrj", "cpuSnapTallyBispectrum",
+             "cpuSnapTallyBispectrumDeriv", "cpuSnapTallyBispectrumVirial"]
+
+
+def test_library_exports_the_whole_julia_abi(cuda_lib):
+    from mdp_b200 import _lib
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True, check=True)
+    exported = {line.split()[-1] for line in out.stdout.splitlines() if line.strip()}
+    assert not sorted(set(JULIA_ABI) - exported)
+    assert set(JULIA_ABI) <= declared_functions()
