@@ -1,16 +1,21 @@
 /*
- * Device-pointer SNAP operations with the argument lists of MDP's backend
- * dispatch (src/C++/Common/mdpgpucore.h:516-612, called from the inline
- * wrappers of src/C++/Common/mdpcore.h with backend == 2).
+ * Device-pointer operations with the argument lists of MDP's backend
+ * dispatch (src/C++/Common/mdpgpucore.h, called from the inline wrappers of
+ * src/C++/Common/mdpcore.h with backend == 2): the SNAP stages (:516-612) and
+ * the rest of the MD loop's hot path -- prefix sums, ghost atoms, cell lists,
+ * full neighbour lists, velocity Verlet, periodic wrapping, per-atom kinetic
+ * energy and column sums.
  *
  * The extern "C" functions are exported by libmdp_b200.so.  For C++ builds of
  * MDP (cpuMDP/gpuMDP), defining MDP_B200_GPUCORE_TEMPLATES before including
- * this header also defines the reference's gpu* template entry points for
- * T = double on top of them, replacing src/C++/Core/gpuSnap4.cu and the pair
- * kernels of gpuSnap.cu at link time.  Array layouts are the reference's:
- * U/Y [idxu][inum], rij [ijnum][3], fatom [anum][3], vatom [6][anum].
- * Supported: one element type, 2J = 4, 6, 8, double.  On unsupported input
- * the outputs are untouched and mdp_last_error() says why.
+ * this header also defines the reference's gpu* entry points for T = double on
+ * top of them, replacing src/C++/Core/gpuSnap4.cu, the pair kernels of
+ * gpuSnap.cu, gpuCumsum.cu, gpuNeighborList3D.cu, gpuVelocityIntegration.cu
+ * (modes 0 and 1) and gpuDomain.cu's gpuPBC at link time.  Array layouts are
+ * the reference's: U/Y [idxu][inum], rij [ijnum][3], fatom [anum][3],
+ * vatom [6][anum], x [natom][dim].  Supported: one element type, 2J = 4, 6, 8,
+ * double.  On unsupported input the outputs are untouched and
+ * mdp_last_error() says why.
  */
 #ifndef MDP_B200_GPUCORE_H
 #define MDP_B200_GPUCORE_H
@@ -46,6 +51,12 @@ void mdp_gpu_snap_compute_yi_f64(double *ylist_r, double *ylist_i, const double 
                                  const int *idxz, const int *idxb_block, const int *idxu_block,
                                  const int *idxcg_block, int twojmax, int idxb_max, int idxu_max, int idxz_max,
                                  int nelements, int ncoeffall, int bnorm_flag, int inum);
+/* mdpgpucore.h:599-601, gpuSnapComputeYi (per-atom beta [idxb][inum]) */
+void mdp_gpu_snap_compute_yi_beta_f64(double *ylist_r, double *ylist_i, const double *Utotr, const double *Utoti,
+                                      const double *cglist, const double *beta, const int *idxz,
+                                      const int *idxb_block, const int *idxu_block, const int *idxcg_block,
+                                      int twojmax, int idxb_max, int idxu_max, int idxz_max, int nelements,
+                                      int bnorm_flag, int inum);
 /* mdpgpucore.h:607-609, gpuSnapComputeFi */
 void mdp_gpu_snap_compute_fi_f64(double *fatom, double *vatom, const double *ylist_r, const double *ylist_i,
                                  const double *rootpqarray, const double *rij, const double *wjelem,
@@ -61,6 +72,51 @@ void mdp_gpu_neigh_pair_list_f64(int *pairnum, int *pairlist, const double *x, c
 void mdp_gpu_neigh_pairs_f64(double *xij, const double *x, int *aii, int *ai, int *aj, int *ti, int *tj,
                              const int *pairnum, const int *pairlist, const int *pairnumsum, const int *ilist,
                              const int *atomtype, const int *alist, int inum, int jnum, int dim);
+
+/* ---- the rest of the MD loop (mdp_b200/csrc/abi_md.cu) ---- */
+/* mdpgpucore.h:108, gpuCumsum: out[0] = 0, out[j] = sum of in[0..j-1], j < length */
+void mdp_gpu_cumsum(int *d_out, int *d_in, int *d_sums, int *d_incr, int length);
+/* mdpgpucore.h:132-133, gpuAtomList3D: ghost images appended to x, owners in alist */
+void mdp_gpu_atom_list3d_f64(int *alist, int *inside, int *glistnumsum, int *glistnum, int *d_sums, int *d_incr,
+                             double *x, const double *pimages, const double *wc, const double *s2rmap, int inum,
+                             int pnum, int dim);
+/* mdpgpucore.h:136-137, gpuCellList3D */
+void mdp_gpu_cell_list3d_f64(int *clist, const double *xi, const double *eta1, const double *eta2,
+                             const double *eta3, const double *s2rmap, const int *nc, int inum, int natom, int dim);
+/* mdpgpucore.h:138, gpuCell2AtomList */
+void mdp_gpu_cell2atom_list(int *c2alist, int *c2anumsum, int *c2anum, const int *clist, int *d_temp, int natom,
+                            int ncell);
+/* mdpgpucore.h:145-146, gpuFullNeighborList3D (cell lists) */
+void mdp_gpu_full_neighbor_list3d_cells_f64(int *neighborlist, int *neighbornum, const double *x,
+                                            const double *rcutsq, const int *alist, const int *clist,
+                                            const int *c2alist, const int *c2anumsum, const int *nc, int inum,
+                                            int jnum, int dim);
+/* mdpgpucore.h:141-142, gpuFullNeighborList3D (all pairs) */
+void mdp_gpu_full_neighbor_list3d_f64(int *neighborlist, int *neighbornum, const double *x, const double *rcutsq,
+                                      int anum, int inum, int jnum, int dim);
+/* mdpgpucore.h:309-311, gpuInitialIntegrate (modes 0 NVE, 1 NVE limit; dtarray on the host) */
+void mdp_gpu_initial_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
+                                   const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                   double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
+                                   const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+                                   int mode, int dim, int inum);
+/* mdpgpucore.h:313-315, gpuFinalIntegrate */
+void mdp_gpu_final_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
+                                 const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                 double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
+                                 const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+                                 int mode, int dim, int inum);
+/* mdpgpucore.h:321-322, gpuPBC (orthogonal and tilted boxes) */
+void mdp_gpu_pbc_f64(double *x, double *v, int *image, const double *boxhi, const double *boxlo,
+                     const double *hi_lambda, const double *lo_lambda, const double *h, const double *h_inv,
+                     const double *h_rate, const int *pbc, int vdeform, int triclinic, int dim, int nlocal);
+/* mdpgpucore.h:259-260, gpuComputeKEAtom */
+void mdp_gpu_compute_ke_atom_f64(double *ke, const double *mass, const double *v, double mvv2e, const int *type,
+                                 const int *ilist, int dim, int inum);
+/* mdpgpucore.h:56, gpuArraySumEveryColumn */
+void mdp_gpu_array_sum_every_column_f64(double *b, const double *a, int m, int n);
+/* mdpgpucore.h:49, gpuArrayGetValueAtIndex<int> */
+int mdp_gpu_array_get_value_at_index_int(const int *y, int n);
 
 /* No counterpart in the reference.  The per-atom bispectrum of
  * mdp_gpu_snap_compute_bi_f64 for callers that must not allocate device memory
@@ -165,6 +221,104 @@ template <> inline void gpuNeighPairs<double>(double *xij, double *x, int *aii, 
     mdp_gpu_neigh_pairs_f64(xij, x, aii, ai, aj, ti, tj, pairnum, pairlist, pairnumsum, ilist, atomtype, alist, inum,
                             jnum, dim);
 }
+/* gpuSnapComputeYi, per-atom beta form */
+template <typename T> void gpuSnapComputeYi(T *ylist_r, T *ylist_i, T *Stotr, T *Stoti, T *cglist, T *beta,
+        int *idxz, int *idxb_block, int *idxu_block, int *idxcg_block, int twojmax, int idxb_max, int idxu_max,
+        int idxz_max, int nelements, int bnorm_flag, int inum);
+template <> inline void gpuSnapComputeYi<double>(double *ylist_r, double *ylist_i, double *Stotr, double *Stoti,
+        double *cglist, double *beta, int *idxz, int *idxb_block, int *idxu_block, int *idxcg_block, int twojmax,
+        int idxb_max, int idxu_max, int idxz_max, int nelements, int bnorm_flag, int inum)
+{
+    mdp_gpu_snap_compute_yi_beta_f64(ylist_r, ylist_i, Stotr, Stoti, cglist, beta, idxz, idxb_block, idxu_block,
+                                     idxcg_block, twojmax, idxb_max, idxu_max, idxz_max, nelements, bnorm_flag, inum);
+}
+
+/* the rest of the MD loop: prefix sums, ghosts, cells, neighbour rows,
+ * integrator, wrapping, kinetic energy (replacing gpuCumsum.cu,
+ * gpuNeighborList2D/3D.cu, gpuVelocityIntegration.cu, gpuDomain.cu and the
+ * matching parts of gpuArrayOperations.cu / gpuComputes.cu) */
+inline void gpuCumsum(int *d_out, int *d_in, int *d_sums, int *d_incr, int length)
+{
+    mdp_gpu_cumsum(d_out, d_in, d_sums, d_incr, length);
+}
+template <typename T> void gpuAtomList3D(int *alist, int *inside, int *glistnumsum, int *glistnum, int *d_sums,
+        int *d_incr, T *x, T *pimages, T *wc, T *s2rmap, int inum, int pnum, int dim);
+template <> inline void gpuAtomList3D<double>(int *alist, int *inside, int *glistnumsum, int *glistnum, int *d_sums,
+        int *d_incr, double *x, double *pimages, double *wc, double *s2rmap, int inum, int pnum, int dim)
+{
+    mdp_gpu_atom_list3d_f64(alist, inside, glistnumsum, glistnum, d_sums, d_incr, x, pimages, wc, s2rmap, inum, pnum,
+                            dim);
+}
+template <typename T> void gpuCellList3D(int *clist, T *xi, T *eta1, T *eta2, T *eta3, T *s2rmap, int *nc,
+        int inum, int natom, int dim);
+template <> inline void gpuCellList3D<double>(int *clist, double *xi, double *eta1, double *eta2, double *eta3,
+        double *s2rmap, int *nc, int inum, int natom, int dim)
+{
+    mdp_gpu_cell_list3d_f64(clist, xi, eta1, eta2, eta3, s2rmap, nc, inum, natom, dim);
+}
+inline void gpuCell2AtomList(int *c2alist, int *c2anumsum, int *c2anum, int *clist, int *d_temp, int natom, int ncell)
+{
+    mdp_gpu_cell2atom_list(c2alist, c2anumsum, c2anum, clist, d_temp, natom, ncell);
+}
+template <typename T> void gpuFullNeighborList3D(int *neighborlist, int *neighbornum, T *x, T *rcutsq, int anum,
+        int inum, int jnum, int dim);
+template <> inline void gpuFullNeighborList3D<double>(int *neighborlist, int *neighbornum, double *x, double *rcutsq,
+        int anum, int inum, int jnum, int dim)
+{
+    mdp_gpu_full_neighbor_list3d_f64(neighborlist, neighbornum, x, rcutsq, anum, inum, jnum, dim);
+}
+template <typename T> void gpuFullNeighborList3D(int *neighborlist, int *neighbornum, T *x, T *rcutsq, int *alist,
+        int *clist, int *c2alist, int *c2anumsum, int *nc, int inum, int jnum, int dim);
+template <> inline void gpuFullNeighborList3D<double>(int *neighborlist, int *neighbornum, double *x, double *rcutsq,
+        int *alist, int *clist, int *c2alist, int *c2anumsum, int *nc, int inum, int jnum, int dim)
+{
+    mdp_gpu_full_neighbor_list3d_cells_f64(neighborlist, neighbornum, x, rcutsq, alist, clist, c2alist, c2anumsum,
+                                           nc, inum, jnum, dim);
+}
+template <typename T> void gpuInitialIntegrate(T *x, T *v, T *f, T *mass, T *dtarray, T *tarray, T *eta_mass, T *eta,
+        T *eta_dot, T *eta_dotdot, T *ke, T *tmp, T vlimitsq, int *type, int *ilist, int eta_mass_flag, int biasflag,
+        int mtchain, int nc_tchain, int mode, int dim, int inum);
+template <> inline void gpuInitialIntegrate<double>(double *x, double *v, double *f, double *mass, double *dtarray,
+        double *tarray, double *eta_mass, double *eta, double *eta_dot, double *eta_dotdot, double *ke, double *tmp,
+        double vlimitsq, int *type, int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+        int mode, int dim, int inum)
+{
+    mdp_gpu_initial_integrate_f64(x, v, f, mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, ke, tmp,
+                                  vlimitsq, type, ilist, eta_mass_flag, biasflag, mtchain, nc_tchain, mode, dim, inum);
+}
+template <typename T> void gpuFinalIntegrate(T *x, T *v, T *f, T *mass, T *dtarray, T *tarray, T *eta_mass, T *eta,
+        T *eta_dot, T *eta_dotdot, T *ke, T *tmp, T vlimitsq, int *type, int *ilist, int eta_mass_flag, int biasflag,
+        int mtchain, int nc_tchain, int mode, int dim, int inum);
+template <> inline void gpuFinalIntegrate<double>(double *x, double *v, double *f, double *mass, double *dtarray,
+        double *tarray, double *eta_mass, double *eta, double *eta_dot, double *eta_dotdot, double *ke, double *tmp,
+        double vlimitsq, int *type, int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+        int mode, int dim, int inum)
+{
+    mdp_gpu_final_integrate_f64(x, v, f, mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, ke, tmp,
+                                vlimitsq, type, ilist, eta_mass_flag, biasflag, mtchain, nc_tchain, mode, dim, inum);
+}
+template <typename T> void gpuPBC(T *x, T *v, int *image, T *boxhi, T *boxlo, T *hi_lambda, T *lo_lambda, T *h,
+        T *h_inv, T *h_rate, int *pbc, int vdeform, int triclinic, int dim, int nlocal);
+template <> inline void gpuPBC<double>(double *x, double *v, int *image, double *boxhi, double *boxlo,
+        double *hi_lambda, double *lo_lambda, double *h, double *h_inv, double *h_rate, int *pbc, int vdeform,
+        int triclinic, int dim, int nlocal)
+{
+    mdp_gpu_pbc_f64(x, v, image, boxhi, boxlo, hi_lambda, lo_lambda, h, h_inv, h_rate, pbc, vdeform, triclinic, dim,
+                    nlocal);
+}
+template <typename T> void gpuComputeKEAtom(T *ke, T *mass, T *v, T mvv2e, int *type, int *ilist, int dim, int inum);
+template <> inline void gpuComputeKEAtom<double>(double *ke, double *mass, double *v, double mvv2e, int *type,
+        int *ilist, int dim, int inum)
+{
+    mdp_gpu_compute_ke_atom_f64(ke, mass, v, mvv2e, type, ilist, dim, inum);
+}
+template <typename T> void gpuArraySumEveryColumn(T *b, T *a, int m, int n);
+template <> inline void gpuArraySumEveryColumn<double>(double *b, double *a, int m, int n)
+{
+    mdp_gpu_array_sum_every_column_f64(b, a, m, n);
+}
+template <typename T> T gpuArrayGetValueAtIndex(T *y, int n);
+template <> inline int gpuArrayGetValueAtIndex<int>(int *y, int n) { return mdp_gpu_array_get_value_at_index_int(y, n); }
 #endif /* MDP_B200_GPUCORE_TEMPLATES */
 #endif /* __cplusplus */
 #endif

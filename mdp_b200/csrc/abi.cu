@@ -364,6 +364,28 @@ int ref_snap_yi(double *yr, double *yi, const double *ur, const double *ui, cons
     return 0;
 }
 
+int launch_yi_pa_d(const SnapModel &m, ForcePath &fp, int inum, const double *G, cudaStream_t s);
+
+// Y with per-atom coefficients beta [jjb][inum] (cpuSnap4.cpp:601-691): the
+// model's coefficients are all 1, so its per-triple factors carry only the
+// multiplicities and the bnorm / (j1+1)/(j+1) scalings
+int ref_snap_yi_beta(double *yr, double *yi, const double *ur, const double *ui, const double *beta, int tj,
+                     int bnorm, int inum, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    std::vector<double> ones(mdp_snap_ncoeff(tj) + 1, 1.0);
+    ones[0] = 0.0;
+    if (model_from_args(c.model, tj, ones.data(), (int)ones.size(), bnorm, 0, 0, 1.0, 1.0, 1.0, 0.0, 1)) return -1;
+    if (load_tiles(c, ur, ui, inum, tj, s)) return -1;
+    const long ntiles = (inum + 31) / 32;
+    if (c.fp.Y.ensure(sizeof(double2) * ntiles * 32 * yh_count(tj))) return -1;
+    if (launch_yi_pa_d(c.model, c.fp, inum, beta, s)) return -1;
+    const long n = (long)inum * idxu_count(tj);
+    k_ytiles_to_ref<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(c.fp.Y.as<double2>(), inum, tj, yh_count(tj), yr, yi);
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 int launch_bi_tiles(const double2 *Ut, int natoms, int tj, int bnorm, int bzero, double *bout, long bstride,
                     cudaStream_t s);
 
@@ -535,6 +557,19 @@ void mdp_gpu_snap_compute_yi_f64(double *ylist_r, double *ylist_i, const double 
         return;
     }
     ref_snap_yi(ylist_r, ylist_i, Utotr, Utoti, c.data(), twojmax, ncoeffall, bnorm_flag, inum, 0);
+}
+
+void mdp_gpu_snap_compute_yi_beta_f64(double *ylist_r, double *ylist_i, const double *Utotr, const double *Utoti,
+                                      const double *cglist, const double *beta, const int *idxz,
+                                      const int *idxb_block, const int *idxu_block, const int *idxcg_block,
+                                      int twojmax, int idxb_max, int idxu_max, int idxz_max, int nelements,
+                                      int bnorm_flag, int inum)
+{
+    (void)cglist; (void)idxz; (void)idxb_block; (void)idxu_block; (void)idxcg_block; (void)idxu_max; (void)idxz_max;
+    std::lock_guard<std::mutex> lk(g_ref_mu);
+    if (nelements != 1) { set_error("multi-element SNAP is not supported"); return; }
+    if (idxb_max != mdp_snap_ncoeff(twojmax)) { set_error("idxb_max %d does not match twojmax %d", idxb_max, twojmax); return; }
+    ref_snap_yi_beta(ylist_r, ylist_i, Utotr, Utoti, beta, twojmax, bnorm_flag, inum, 0);
 }
 
 void mdp_gpu_snap_compute_fi_f64(double *fatom, double *vatom, const double *ylist_r, const double *ylist_i,

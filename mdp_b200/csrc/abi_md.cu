@@ -1,0 +1,506 @@
+// The MD-loop operations behind MDP's backend dispatch (src/C++/Common/mdpcore.h
+// with backend == 2) other than the SNAP stages: prefix sums, ghost atoms, cell
+// lists, full neighbour lists, the velocity-Verlet integrator, periodic
+// wrapping, per-atom kinetic energy and column sums.  Argument lists are those
+// of src/C++/Common/mdpgpucore.h; all arrays are device arrays in the
+// reference's layouts (x [natom][dim], neighbour rows [atom][jnum]) except
+// dtarray, which the reference reads on the host.  Positions are mapped to
+// the unit cell and distances formed with the reference CPU code's rounding
+// (products and sums rounded in its order, no fused multiply-add), so ghosts,
+// cells and neighbour sets equal the CPU reference's exactly.  Default stream.
+#include "common.cuh"
+#include "engine.h"
+
+#include <algorithm>
+#include <mutex>
+
+namespace mdp {
+namespace {
+
+std::mutex g_md_mu;
+
+constexpr int TB = 256;
+unsigned blocks_for(long n) { return (unsigned)std::max<long>(1, (n + TB - 1) / TB); }
+
+// s2rmap * (a, b, c): ((m0 a + m3 b) + m6 c), each product rounded
+__device__ __forceinline__ double map0(const double *m, int r, double a, double b, double c)
+{
+    return __dadd_rn(__dadd_rn(__dmul_rn(m[r], a), __dmul_rn(m[3 + r], b)), __dmul_rn(m[6 + r], c));
+}
+
+__device__ __forceinline__ double dist2(double a0, double a1, double a2, double b0, double b1, double b2)
+{
+    const double d0 = __dsub_rn(b0, a0), d1 = __dsub_rn(b1, a1), d2 = __dsub_rn(b2, a2);
+    return __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+}
+
+// ---- ghosts (cpuNeighborList3D.cpp:282-330) --------------------------------
+__global__ void k_md_ghost_flags(int *__restrict__ gnum, int *__restrict__ inside, const double *__restrict__ x,
+                                 const double *__restrict__ pim, const double *__restrict__ wc,
+                                 const double *__restrict__ s2r, int inum, int pnum)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= inum) return;
+    const double x0 = x[3 * (size_t)i], x1 = x[3 * (size_t)i + 1], x2 = x[3 * (size_t)i + 2];
+    int n = 0;
+    for (int j = 1; j < pnum; j++) {
+        const double y0 = __dadd_rn(x0, pim[3 * j]), y1 = __dadd_rn(x1, pim[3 * j + 1]),
+                     y2 = __dadd_rn(x2, pim[3 * j + 2]);
+        const double s0 = map0(s2r, 0, y0, y1, y2), s1 = map0(s2r, 1, y0, y1, y2), s2 = map0(s2r, 2, y0, y1, y2);
+        const int in = (wc[0] <= s0 && s0 <= wc[18] && wc[1] <= s1 && s1 <= wc[19] && wc[2] <= s2 && s2 <= wc[20]);
+        inside[(j - 1) + (size_t)i * (pnum - 1)] = in;
+        n += in;
+    }
+    gnum[i] = n;
+}
+
+__global__ void k_md_ghost_emit(int *__restrict__ alist, const int *__restrict__ inside,
+                                const int *__restrict__ goff, double *__restrict__ x, const double *__restrict__ pim,
+                                int inum, int pnum)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= inum) return;
+    alist[i] = i;
+    const double x0 = x[3 * (size_t)i], x1 = x[3 * (size_t)i + 1], x2 = x[3 * (size_t)i + 2];
+    long q = (long)inum + goff[i];
+    for (int j = 1; j < pnum; j++) {
+        if (!inside[(j - 1) + (size_t)i * (pnum - 1)]) continue;
+        x[3 * q] = __dadd_rn(x0, pim[3 * j]);
+        x[3 * q + 1] = __dadd_rn(x1, pim[3 * j + 1]);
+        x[3 * q + 2] = __dadd_rn(x2, pim[3 * j + 2]);
+        alist[q] = i;
+        q++;
+    }
+}
+
+// ---- cells (cpuNeighborList3D.cpp:334-357, cpuNeighborList2D.cpp:298-307) --
+// the first cell (from m, where m = 1 for local atoms and 0 for ghosts) whose
+// closed interval holds the coordinate; nc - m when none does
+__device__ __forceinline__ int cell_search(const double *__restrict__ eta, int n, int m, double s)
+{
+    int j = m;
+    for (; j < n - m; j++)
+        if (eta[j] <= s && s <= eta[j + 1]) break;
+    return j;
+}
+
+__global__ void k_md_cell_list(int *__restrict__ clist, const double *__restrict__ x, const double *__restrict__ e1,
+                               const double *__restrict__ e2, const double *__restrict__ e3,
+                               const double *__restrict__ s2r, const int *__restrict__ nc, int inum, int natom)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natom) return;
+    const int m = i < inum ? 1 : 0;
+    const double a = x[3 * (size_t)i], b = x[3 * (size_t)i + 1], c = x[3 * (size_t)i + 2];
+    const int n0 = nc[0], n1 = nc[1], n2 = nc[2];
+    const int j1 = cell_search(e1, n0, m, map0(s2r, 0, a, b, c));
+    const int j2 = cell_search(e2, n1, m, map0(s2r, 1, a, b, c));
+    const int j3 = cell_search(e3, n2, m, map0(s2r, 2, a, b, c));
+    clist[i] = j1 + n0 * j2 + n0 * n1 * j3;
+}
+
+// atoms whose cell id lies outside 0..ncell-1 are left out
+__global__ void k_md_cell_count(const int *__restrict__ clist, int natom, int ncell, int *__restrict__ cnt)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < natom && clist[i] >= 0 && clist[i] < ncell) atomicAdd(&cnt[clist[i]], 1);
+}
+
+__global__ void k_md_cell_fill(const int *__restrict__ clist, int natom, int ncell, const int *__restrict__ start,
+                               int *__restrict__ cursor, int *__restrict__ c2alist)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natom) return;
+    const int c = clist[i];
+    if (c < 0 || c >= ncell) return;
+    c2alist[start[c] + atomicAdd(&cursor[c], 1)] = i;
+}
+
+// atoms ascending within each cell (the order of a stable sort by cell), and
+// the sorted cell ids into c2anum
+__global__ void k_md_cell_order(int ncell, const int *__restrict__ start, int *__restrict__ c2alist,
+                                int *__restrict__ c2anum)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    const int s = start[c], e = start[c + 1];
+    for (int a = s + 1; a < e; a++) {
+        const int v = c2alist[a];
+        int b = a - 1;
+        while (b >= s && c2alist[b] > v) { c2alist[b + 1] = c2alist[b]; b--; }
+        c2alist[b + 1] = v;
+    }
+    for (int a = s; a < e; a++) c2anum[a] = c;
+}
+
+// ---- full neighbour lists (cpuNeighborList3D.cpp:361-443) ------------------
+// rows filled in the reference's visiting order, truncated at jnum
+__global__ void k_md_neigh_cells(int *__restrict__ nl, int *__restrict__ nn, const double *__restrict__ x,
+                                 const double *__restrict__ rcutsq, const int *__restrict__ alist,
+                                 const int *__restrict__ clist, const int *__restrict__ c2alist,
+                                 const int *__restrict__ c2anumsum, const int *__restrict__ nc, int inum, int jnum)
+{
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= inum) return;
+    const int i = alist[ii];
+    const double xi0 = x[3 * (size_t)i], xi1 = x[3 * (size_t)i + 1], xi2 = x[3 * (size_t)i + 2];
+    const double rc = rcutsq[0];
+    const int n0 = nc[0], n01 = nc[0] * nc[1];
+    const int ca = clist[i], cb = ca % n01, j3 = (ca - cb) / n01, j1 = cb % n0, j2 = (cb - j1) / n0;
+    int *row = nl + (size_t)jnum * i;
+    int cnt = 0;
+    for (int d1 = -1; d1 <= 1 && cnt < jnum; d1++)
+        for (int d2 = -1; d2 <= 1 && cnt < jnum; d2++)
+            for (int d3 = -1; d3 <= 1 && cnt < jnum; d3++) {
+                // cells off the x/y grid or below it hold no atoms (the reference
+                // reads past its arrays there).  z is left open: MDP passes
+                // nc[2] = 0 (Configuration.cpp:847-848), so locals sit in z layer
+                // 1 and ghosts in layer 0, and the stencil's layer 2 lies within
+                // the ncell = nc0 nc1 (ne2 + 2) cells its prefix sums cover
+                if (j1 + d1 < 0 || j1 + d1 >= n0 || j2 + d2 < 0 || j2 + d2 >= nc[1] || j3 + d3 < 0) continue;
+                const int k = (j1 + d1) + n0 * (j2 + d2) + n01 * (j3 + d3);
+                const int s = c2anumsum[k], e = c2anumsum[k + 1];
+                for (int l = s; l < e && cnt < jnum; l++) {
+                    const int j = c2alist[l];
+                    if (j == i) continue;
+                    if (dist2(xi0, xi1, xi2, x[3 * (size_t)j], x[3 * (size_t)j + 1], x[3 * (size_t)j + 2]) <= rc)
+                        row[cnt++] = j;
+                }
+            }
+    nn[ii] = cnt;
+}
+
+__global__ void k_md_neigh_all(int *__restrict__ nl, int *__restrict__ nn, const double *__restrict__ x,
+                               const double *__restrict__ rcutsq, int anum, int inum, int jnum)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= inum) return;
+    const double xi0 = x[3 * (size_t)i], xi1 = x[3 * (size_t)i + 1], xi2 = x[3 * (size_t)i + 2];
+    const double rc = rcutsq[0];
+    int *row = nl + (size_t)jnum * i;
+    int cnt = 0;
+    for (int j = 0; j < anum && cnt < jnum; j++) {
+        if (j == i) continue;
+        if (dist2(xi0, xi1, xi2, x[3 * (size_t)j], x[3 * (size_t)j + 1], x[3 * (size_t)j + 2]) <= rc) row[cnt++] = j;
+    }
+    nn[i] = cnt;
+}
+
+// ---- velocity Verlet (cpuVelocityIntegration.cpp:307-420) ------------------
+// stage 0: v += dtfm f, [limit], x += dtv v;  stage 1: v += dtfm f, [limit]
+__global__ void k_md_verlet(double *__restrict__ x, double *__restrict__ v, const double *__restrict__ f,
+                            const double *__restrict__ mass, const int *__restrict__ type,
+                            const int *__restrict__ ilist, double dtf, double dtv, double vlimitsq, int limit,
+                            int stage, int dim, int inum)
+{
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= inum) return;
+    const int i = ilist[ii];
+    const double dtfm = __ddiv_rn(dtf, mass[type[i]]);
+    double *vi = v + (size_t)dim * i;
+    const double *fi = f + (size_t)dim * i;
+    for (int d = 0; d < dim; d++) vi[d] = __dadd_rn(vi[d], __dmul_rn(dtfm, fi[d]));
+    if (limit) {
+        double vsq = __dmul_rn(vi[0], vi[0]);
+        for (int d = 1; d < dim; d++) vsq = __dadd_rn(vsq, __dmul_rn(vi[d], vi[d]));
+        if (vsq > vlimitsq) {
+            const double scale = sqrt(__ddiv_rn(vlimitsq, vsq));
+            for (int d = 0; d < dim; d++) vi[d] = __dmul_rn(vi[d], scale);
+        }
+    }
+    if (stage == 0)
+        for (int d = 0; d < dim; d++) x[(size_t)dim * i + d] = __dadd_rn(x[(size_t)dim * i + d], __dmul_rn(dtv, vi[d]));
+}
+
+// ---- periodic wrapping (cpuDomain.cpp:235-385) -----------------------------
+// the velocity shift of a deforming box for crossing boundary d (rates in
+// Voigt order xx yy zz yz xz xy)
+__device__ __forceinline__ void deform_shift(double *v, const double *hr, int d, double sg)
+{
+    if (d == 0) v[0] += sg * hr[0];
+    if (d == 1) { v[0] += sg * hr[5]; v[1] += sg * hr[1]; }
+    if (d == 2) { v[0] += sg * hr[4]; v[1] += sg * hr[3]; v[2] += sg * hr[2]; }
+}
+
+__global__ void k_md_pbc(double *__restrict__ x, double *__restrict__ v, int *__restrict__ image,
+                         const double *__restrict__ hi, const double *__restrict__ lo,
+                         const double *__restrict__ hil, const double *__restrict__ lol, const double *__restrict__ h,
+                         const double *__restrict__ hinv, const double *__restrict__ hr, const int *__restrict__ pbc,
+                         int vdeform, int triclinic, int dim, int nlocal)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nlocal) return;
+    double *xi = x + (size_t)dim * i, *vi = v + (size_t)dim * i;
+    int *im = image + (size_t)dim * i;
+    double c[3] = {0.0, 0.0, 0.0};
+    const double *L = h, *lb = lo, *ub = hi;
+    if (triclinic) {
+        // lambda coordinates
+        const double dx = xi[0] - lo[0], dy = xi[1] - lo[1];
+        c[0] = hinv[0] * dx + hinv[5] * dy;
+        c[1] = hinv[1] * dy;
+        if (dim == 3) {
+            const double dz = xi[2] - lo[2];
+            c[0] += hinv[4] * dz;
+            c[1] += hinv[3] * dz;
+            c[2] = hinv[2] * dz;
+        }
+        L = hil; lb = lol; ub = hil;
+    } else {
+        for (int d = 0; d < dim; d++) c[d] = xi[d];
+    }
+    for (int d = 0; d < dim; d++) {
+        if (!pbc[d]) continue;
+        if (c[d] < lb[d]) {
+            c[d] += L[d];
+            if (vdeform) deform_shift(vi, hr, d, 1.0);
+            im[d] -= 1;
+        }
+        if (c[d] >= ub[d]) {
+            c[d] -= L[d];
+            c[d] = fmax(c[d], lb[d]);
+            if (vdeform) deform_shift(vi, hr, d, -1.0);
+            im[d] += 1;
+        }
+    }
+    if (triclinic) {
+        xi[0] = h[0] * c[0] + h[5] * c[1] + lo[0];
+        xi[1] = h[1] * c[1] + lo[1];
+        if (dim == 3) {
+            xi[0] += h[4] * c[2];
+            xi[1] += h[3] * c[2];
+            xi[2] = h[2] * c[2] + lo[2];
+        }
+    } else {
+        for (int d = 0; d < dim; d++) xi[d] = c[d];
+    }
+}
+
+// ---- kinetic energy and column sums (cpuComputes.cpp:435-451,
+// cpuArrayOperations.cpp:94-103) ---------------------------------------------
+__global__ void k_md_ke(double *__restrict__ ke, const double *__restrict__ mass, const double *__restrict__ v,
+                        double mvv2e, const int *__restrict__ type, const int *__restrict__ ilist, int dim, int inum)
+{
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= inum) return;
+    const int i = ilist[ii];
+    const double *vi = v + (size_t)dim * i;
+    double s = __dadd_rn(__dmul_rn(vi[0], vi[0]), __dmul_rn(vi[1], vi[1]));
+    if (dim == 3) s = __dadd_rn(s, __dmul_rn(vi[2], vi[2]));
+    ke[ii] = __dmul_rn(__dmul_rn(__dmul_rn(0.5, mvv2e), mass[type[i]]), s);
+}
+
+// one CTA per column; a fixed tree over the rows
+__global__ void __launch_bounds__(TB) k_md_colsum(double *__restrict__ b, const double *__restrict__ a, int n)
+{
+    __shared__ double sh[TB];
+    const double *col = a + (size_t)n * blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += TB) s += col[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = TB / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) b[blockIdx.x] = sh[0];
+}
+
+struct CellScratch {
+    DevBuf cnt, cursor, tmp;
+};
+CellScratch &cell_scratch()
+{
+    static CellScratch c;
+    return c;
+}
+
+bool check_launch(const char *fn)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { set_error("%s: %s", fn, cudaGetErrorString(e)); return false; }
+    return true;
+}
+
+}  // namespace
+}  // namespace mdp
+
+using namespace mdp;
+
+extern "C" {
+
+// mdpgpucore.h:108 / gpuCumsum.cu -- out[0] = 0, out[j] = in[0] + ... + in[j-1]
+// for j < length; d_sums is the scratch (length / 4096 + 1 ints are used)
+void mdp_gpu_cumsum(int *d_out, int *d_in, int *d_sums, int *d_incr, int length)
+{
+    (void)d_incr;
+    if (length <= 0) return;
+    if (exclusive_scan(d_in, d_out, (long)length - 1, d_sums, 0)) return;
+    check_launch("gpuCumsum");
+}
+
+// mdpgpucore.h:132-133 -- ghost images inside the bounding box, appended to x
+// after the inum local atoms, owners in alist; glistnumsum gets inum + 1 entries
+void mdp_gpu_atom_list3d_f64(int *alist, int *inside, int *glistnumsum, int *glistnum, int *d_sums, int *d_incr,
+                             double *x, const double *pimages, const double *wc, const double *s2rmap, int inum,
+                             int pnum, int dim)
+{
+    (void)d_incr;
+    if (dim != 3) { set_error("gpuAtomList3D: dim must be 3"); return; }
+    if (inum <= 0) return;
+    k_md_ghost_flags<<<blocks_for(inum), TB>>>(glistnum, inside, x, pimages, wc, s2rmap, inum, pnum);
+    if (exclusive_scan(glistnum, glistnumsum, inum, d_sums, 0)) return;
+    k_md_ghost_emit<<<blocks_for(inum), TB>>>(alist, inside, glistnumsum, x, pimages, inum, pnum);
+    count_launches(5);
+    check_launch("gpuAtomList3D");
+}
+
+// mdpgpucore.h:136-137 -- the cell of every atom (locals among the interior cells)
+void mdp_gpu_cell_list3d_f64(int *clist, const double *xi, const double *eta1, const double *eta2,
+                             const double *eta3, const double *s2rmap, const int *nc, int inum, int natom, int dim)
+{
+    if (dim != 3) { set_error("gpuCellList3D: dim must be 3"); return; }
+    if (natom <= 0) return;
+    k_md_cell_list<<<blocks_for(natom), TB>>>(clist, xi, eta1, eta2, eta3, s2rmap, nc, inum, natom);
+    count_launches(1);
+    check_launch("gpuCellList3D");
+}
+
+// mdpgpucore.h:138 -- atoms grouped by cell (ascending within a cell), cell
+// starts in c2anumsum[0..ncell], sorted cell ids in c2anum
+void mdp_gpu_cell2atom_list(int *c2alist, int *c2anumsum, int *c2anum, const int *clist, int *d_temp, int natom,
+                            int ncell)
+{
+    (void)d_temp;
+    std::lock_guard<std::mutex> lk(g_md_mu);
+    if (natom <= 0 || ncell <= 0) return;
+    CellScratch &s = cell_scratch();
+    if (s.cnt.ensure(sizeof(int) * ncell) || s.cursor.ensure(sizeof(int) * ncell) ||
+        s.tmp.ensure(sizeof(int) * scan_tmp_ints(ncell)))
+        return;
+    if (cudaMemset(s.cnt.p, 0, sizeof(int) * ncell) != cudaSuccess ||
+        cudaMemset(s.cursor.p, 0, sizeof(int) * ncell) != cudaSuccess) {
+        set_error("gpuCell2AtomList: memset failed");
+        return;
+    }
+    k_md_cell_count<<<blocks_for(natom), TB>>>(clist, natom, ncell, s.cnt.as<int>());
+    if (exclusive_scan(s.cnt.as<int>(), c2anumsum, ncell, s.tmp.as<int>(), 0)) return;
+    k_md_cell_fill<<<blocks_for(natom), TB>>>(clist, natom, ncell, c2anumsum, s.cursor.as<int>(), c2alist);
+    k_md_cell_order<<<blocks_for(ncell), TB>>>(ncell, c2anumsum, c2alist, c2anum);
+    count_launches(6);
+    check_launch("gpuCell2AtomList");
+}
+
+// mdpgpucore.h:145-146 -- full neighbour rows from the cell lists
+void mdp_gpu_full_neighbor_list3d_cells_f64(int *neighborlist, int *neighbornum, const double *x,
+                                            const double *rcutsq, const int *alist, const int *clist,
+                                            const int *c2alist, const int *c2anumsum, const int *nc, int inum,
+                                            int jnum, int dim)
+{
+    if (dim != 3) { set_error("gpuFullNeighborList3D: dim must be 3"); return; }
+    if (inum <= 0) return;
+    k_md_neigh_cells<<<blocks_for(inum), TB>>>(neighborlist, neighbornum, x, rcutsq, alist, clist, c2alist,
+                                                c2anumsum, nc, inum, jnum);
+    count_launches(1);
+    check_launch("gpuFullNeighborList3D");
+}
+
+// mdpgpucore.h:141-142 -- full neighbour rows by an O(N^2) search
+void mdp_gpu_full_neighbor_list3d_f64(int *neighborlist, int *neighbornum, const double *x, const double *rcutsq,
+                                      int anum, int inum, int jnum, int dim)
+{
+    if (dim != 3) { set_error("gpuFullNeighborList3D: dim must be 3"); return; }
+    if (inum <= 0) return;
+    k_md_neigh_all<<<blocks_for(inum), TB>>>(neighborlist, neighbornum, x, rcutsq, anum, inum, jnum);
+    count_launches(1);
+    check_launch("gpuFullNeighborList3D");
+}
+
+static void verlet(const char *fn, int stage, double *x, double *v, const double *f, const double *mass,
+                   const double *dtarray, double vlimitsq, const int *type, const int *ilist, int mode, int dim,
+                   int inum)
+{
+    if (mode != 0 && mode != 1) {
+        set_error("%s: mode %d (NVT) is not supported; modes 0 (NVE) and 1 (NVE limit) are", fn, mode);
+        return;
+    }
+    if (dim != 2 && dim != 3) { set_error("%s: dim must be 2 or 3", fn); return; }
+    if (inum <= 0) return;
+    k_md_verlet<<<blocks_for(inum), TB>>>(x, v, f, mass, type, ilist, dtarray[1], dtarray[2], vlimitsq, mode == 1,
+                                           stage, dim, inum);
+    count_launches(1);
+    check_launch(fn);
+}
+
+// mdpgpucore.h:309-311 -- first half of velocity Verlet (dtarray on the host:
+// dtf = dtarray[1], dtv = dtarray[2])
+void mdp_gpu_initial_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
+                                   const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                   double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
+                                   const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+                                   int mode, int dim, int inum)
+{
+    (void)tarray; (void)eta_mass; (void)eta; (void)eta_dot; (void)eta_dotdot; (void)ke; (void)tmp;
+    (void)eta_mass_flag; (void)biasflag; (void)mtchain; (void)nc_tchain;
+    verlet("gpuInitialIntegrate", 0, x, v, f, mass, dtarray, vlimitsq, type, ilist, mode, dim, inum);
+}
+
+// mdpgpucore.h:313-315 -- second half of velocity Verlet
+void mdp_gpu_final_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
+                                 const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                 double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
+                                 const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+                                 int mode, int dim, int inum)
+{
+    (void)tarray; (void)eta_mass; (void)eta; (void)eta_dot; (void)eta_dotdot; (void)ke; (void)tmp;
+    (void)eta_mass_flag; (void)biasflag; (void)mtchain; (void)nc_tchain;
+    verlet("gpuFinalIntegrate", 1, x, v, f, mass, dtarray, vlimitsq, type, ilist, mode, dim, inum);
+}
+
+// mdpgpucore.h:321-322 -- wrap local atoms into the box, counting images
+void mdp_gpu_pbc_f64(double *x, double *v, int *image, const double *boxhi, const double *boxlo,
+                     const double *hi_lambda, const double *lo_lambda, const double *h, const double *h_inv,
+                     const double *h_rate, const int *pbc, int vdeform, int triclinic, int dim, int nlocal)
+{
+    if (dim != 2 && dim != 3) { set_error("gpuPBC: dim must be 2 or 3"); return; }
+    if (nlocal <= 0) return;
+    k_md_pbc<<<blocks_for(nlocal), TB>>>(x, v, image, boxhi, boxlo, hi_lambda, lo_lambda, h, h_inv, h_rate, pbc,
+                                          vdeform, triclinic, dim, nlocal);
+    count_launches(1);
+    check_launch("gpuPBC");
+}
+
+// mdpgpucore.h:259-260 -- ke[ii] = 1/2 mvv2e m v^2
+void mdp_gpu_compute_ke_atom_f64(double *ke, const double *mass, const double *v, double mvv2e, const int *type,
+                                 const int *ilist, int dim, int inum)
+{
+    if (dim != 2 && dim != 3) { set_error("gpuComputeKEAtom: dim must be 2 or 3"); return; }
+    if (inum <= 0) return;
+    k_md_ke<<<blocks_for(inum), TB>>>(ke, mass, v, mvv2e, type, ilist, dim, inum);
+    count_launches(1);
+    check_launch("gpuComputeKEAtom");
+}
+
+// mdpgpucore.h:56 -- b[j] = sum over the n rows of column j of a [m columns][n]
+void mdp_gpu_array_sum_every_column_f64(double *b, const double *a, int m, int n)
+{
+    if (m <= 0) return;
+    if (n <= 0) {
+        cudaMemset(b, 0, sizeof(double) * m);
+        return;
+    }
+    k_md_colsum<<<(unsigned)m, TB>>>(b, a, n);
+    count_launches(1);
+    check_launch("gpuArraySumEveryColumn");
+}
+
+// mdpgpucore.h:49 -- y[n] read back to the host
+int mdp_gpu_array_get_value_at_index_int(const int *y, int n)
+{
+    int v = 0;
+    if (cudaMemcpy(&v, y + n, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        set_error("gpuArrayGetValueAtIndex: copy failed");
+    return v;
+}
+
+}  // extern "C"

@@ -24,6 +24,39 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
     return 0;
 }
 
+// per-atom coefficients G [k][atom] (k over the bispectrum components), FP64:
+// the beta form of the reference's Yi (cpuSnap4.cpp:601-691); no energy
+template <int TJ>
+static int launch_yi_pa_d_tj(const SnapModel &m, ForcePath &fp, int inum, const double *G, cudaStream_t s)
+{
+    if (tu_ensure_tables()) return -1;
+    const size_t sm = yi_smem_bytes<double, TJ, true>();
+    static int per_sm = 0;
+    if (!per_sm) {
+        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<double, TJ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)sm));
+        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<double, TJ, true>,
+                                                                   YiWarps<double>::n * 32, sm));
+        if (per_sm < 1) { set_error("k_snap_yi (per-atom, FP64) does not fit on an SM (%zu B shared)", sm); return -1; }
+    }
+    const int ntiles = (inum + 31) / 32;
+    const int blocks = std::min(ntiles, num_sms() * per_sm);
+    k_snap_yi<double, TJ, true><<<blocks, YiWarps<double>::n * 32, sm, s>>>(fp.Ut.as<double2>(), inum, m.yd,
+                                                                            fp.Y.as<double2>(), nullptr, G);
+    return 0;
+}
+
+int launch_yi_pa_d(const SnapModel &m, ForcePath &fp, int inum, const double *G, cudaStream_t s)
+{
+    switch (m.p.twojmax) {
+    case 4: return launch_yi_pa_d_tj<4>(m, fp, inum, G, s);
+    case 6: return launch_yi_pa_d_tj<6>(m, fp, inum, G, s);
+    case 8: return launch_yi_pa_d_tj<8>(m, fp, inum, G, s);
+    }
+    set_error("twojmax %d not supported", m.p.twojmax);
+    return -1;
+}
+
 #define MDP_INST(T, TJ) \
     template int launch_yi<T, TJ>(const SnapModel &, const YParams<T> &, ForcePath &, int, double *, cudaStream_t);
 MDP_INST(double, 4) MDP_INST(double, 6) MDP_INST(double, 8)
