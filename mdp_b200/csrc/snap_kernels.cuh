@@ -18,6 +18,8 @@
 
 #include "common.cuh"
 
+#include <type_traits>
+
 namespace mdp {
 
 struct SnapGeom {
@@ -479,13 +481,86 @@ __host__ __device__ constexpr int items_of(int j1, int j2, int j)
     return n;
 }
 
+// One warp's partial output row of a layer, in registers: separate real and
+// imaginary parts in FP64; {re, im} pairs in FP32, where the packed two-lane
+// instructions of sm_100 do the complex arithmetic.
+template <typename T> struct YRow {
+    T r[JD], i[JD];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int m = 0; m < JD; m++) { r[m] = T(0); i[m] = T(0); }
+    }
+    __device__ __forceinline__ typename cplx<T>::type get(int m) const { return {r[m], i[m]}; }
+};
+template <> struct YRow<float> {
+    float2 v[JD];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int m = 0; m < JD; m++) v[m] = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ float2 get(int m) const { return v[m]; }
+};
+
+// FP32 rows: for every (ma1, ma2) the product p = (s u1[ma1]) u2[ma2] takes a
+// packed multiply and a packed fused multiply-add ({ar, ai} * {br, br}, then
+// {-ai, ar} * {bi, bi} added), and y[ma] += c p one more packed FMA, with
+// ma = ma1 + ma2 - (J1 + J2 - J)/2.  u2 stays in registers as {re, re} and
+// {im, im}; u1 streams from shared memory one entry at a time.
+template <int J1, int J2, int J>
+__device__ __forceinline__ void z_rows_f32(const int mb, const int o, const int st, const float2 *__restrict__ Us,
+                                           const int lane, const float beta, YRow<float> &acc)
+{
+    constexpr int N1 = J1 + 1, N2 = J2 + 1;
+    constexpr int CGB = cg_block(J1, J2, J);
+    constexpr int OFF = (J1 + J2 - J) / 2;
+    const int mb1min = max(0, (2 * mb - J - J2 + J1) / 2);
+    const int mb2max = (2 * mb - J - (2 * mb1min - J1) + J2) / 2;
+    const int nb = min(J1, (2 * mb - J + J2 + J1) / 2) - mb1min + 1;
+    for (int ib = o; ib < nb; ib += st) {
+        const int mb1 = mb1min + ib, mb2 = mb2max - ib;
+        const float s = beta * cgc<float>(CGB + mb1 * N2 + mb2);
+        const float2 *r1 = Us + (idxu_block(J1) + N1 * mb1) * 32 + lane;
+        const float2 *r2 = Us + (idxu_block(J2) + N2 * mb2) * 32 + lane;
+        float2 br[N2], bi[N2];
+#pragma unroll
+        for (int a = 0; a < N2; a++) {
+            const float2 v = r2[a * 32];
+            br[a] = make_float2(v.x, v.x);
+            bi[a] = make_float2(v.y, v.y);
+        }
+#pragma unroll
+        for (int ma1 = 0; ma1 < N1; ma1++) {
+            const float2 v = r1[ma1 * 32];
+            const float2 a = __fmul2_rn(make_float2(s, s), v);
+            const float2 an = make_float2(-a.y, a.x);
+#pragma unroll
+            for (int ma2 = 0; ma2 < N2; ma2++) {
+                const int ma = ma1 + ma2 - OFF;
+                if (ma < 0 || ma > J) continue;
+                float2 p = __fmul2_rn(a, br[ma2]);
+                p = __ffma2_rn(an, bi[ma2], p);
+                const float c = cgc<float>(CGB + ma1 * N2 + ma2);
+                acc.v[ma] = __ffma2_rn(make_float2(c, c), p, acc.v[ma]);
+            }
+        }
+    }
+}
+
 // Row mb of beta' Z_{J1 J2 J}, restricted to the row pairs ib = o, o+st, ...,
-// accumulated into yr/yi (registers).
+// accumulated into the warp's row (registers).
 template <typename T, int J1, int J2, int J>
 __device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
                                        const typename cplx<T>::type *__restrict__ Us, const int lane, const T beta,
-                                       T (&yr)[JD], T (&yi)[JD])
+                                       YRow<T> &acc)
 {
+    if constexpr (std::is_same<T, float>::value) {
+        z_rows_f32<J1, J2, J>(mb, o, st, Us, lane, beta, acc);
+        return;
+    } else {
+    T(&yr)[JD] = acc.r;
+    T(&yi)[JD] = acc.i;
     typedef typename cplx<T>::type T2;
     constexpr int N1 = J1 + 1, N2 = J2 + 1;
     constexpr int CGB = cg_block(J1, J2, J);
@@ -517,6 +592,7 @@ __device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
             }
         }
     }
+    }
 }
 
 // all couplings of output layer J, in enumeration order (every warp walks the
@@ -524,7 +600,7 @@ __device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
 template <typename T, int TJ, bool PA, int J, int J1, int J2>
 __device__ __forceinline__ void z_layer(const int mb, const int o, const int st,
                                         const typename cplx<T>::type *__restrict__ Us, const int lane,
-                                        const YParams<T> &P, const T *__restrict__ Gs, T (&yr)[JD], T (&yi)[JD])
+                                        const YParams<T> &P, const T *__restrict__ Gs, YRow<T> &acc)
 {
     if constexpr (J1 <= TJ) {
         if constexpr (J2 <= J1) {
@@ -532,11 +608,11 @@ __device__ __forceinline__ void z_layer(const int mb, const int o, const int st,
                 constexpr int TRI = tri_index(J1, J2, J);
                 T beta = P.betaY[TRI];
                 if constexpr (PA) beta *= Gs[P.kmap[TRI] * 32 + lane];
-                z_rows<T, J1, J2, J>(mb, o, st, Us, lane, beta, yr, yi);
+                z_rows<T, J1, J2, J>(mb, o, st, Us, lane, beta, acc);
             }
-            z_layer<T, TJ, PA, J, J1, J2 + 1>(mb, o, st, Us, lane, P, Gs, yr, yi);
+            z_layer<T, TJ, PA, J, J1, J2 + 1>(mb, o, st, Us, lane, P, Gs, acc);
         } else {
-            z_layer<T, TJ, PA, J, J1 + 1, 0>(mb, o, st, Us, lane, P, Gs, yr, yi);
+            z_layer<T, TJ, PA, J, J1 + 1, 0>(mb, o, st, Us, lane, P, Gs, acc);
         }
     }
 }
@@ -552,12 +628,11 @@ __device__ __forceinline__ void y_layer(const typename cplx<T>::type *__restrict
     typedef typename cplx<T>::type T2;
     const int mb = P.lay_mb[J][w];
     if (mb != 255) {
-        T yr[JD], yi[JD];
+        YRow<T> acc;
+        acc.zero();
+        z_layer<T, TJ, PA, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w], Us, lane, P, Gs, acc);
 #pragma unroll
-        for (int ma = 0; ma < JD; ma++) { yr[ma] = T(0); yi[ma] = T(0); }
-        z_layer<T, TJ, PA, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w], Us, lane, P, Gs, yr, yi);
-#pragma unroll
-        for (int ma = 0; ma <= J; ma++) red[(w * JD + ma) * 32 + lane] = T2{yr[ma], yi[ma]};
+        for (int ma = 0; ma <= J; ma++) red[(w * JD + ma) * 32 + lane] = acc.get(ma);
     }
     __syncthreads();
     constexpr int NE = (J / 2 + 1) * (J + 1);
@@ -680,16 +755,15 @@ __device__ __forceinline__ void b_triples(const typename cplx<T>::type *__restri
                     if (C % BI_WARPS == w) {
                         double sum = 0.0;
                         for (int mb = 0; 2 * mb <= J; mb++) {
-                            T zr[JD], zi[JD];
-#pragma unroll
-                            for (int ma = 0; ma < JD; ma++) { zr[ma] = T(0); zi[ma] = T(0); }
-                            z_rows<T, J1, J2, J>(mb, 0, 1, Us, lane, T(1), zr, zi);
+                            YRow<T> z;
+                            z.zero();
+                            z_rows<T, J1, J2, J>(mb, 0, 1, Us, lane, T(1), z);
                             const T2 *urow = Us + (idxu_block(J) + (J + 1) * mb) * 32 + lane;
 #pragma unroll
                             for (int ma = 0; ma <= J; ma++) {
                                 const double wgt = (2 * mb < J) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
-                                const T2 u = urow[ma * 32];
-                                sum += wgt * ((double)u.x * (double)zr[ma] + (double)u.y * (double)zi[ma]);
+                                const T2 u = urow[ma * 32], zm = z.get(ma);
+                                sum += wgt * ((double)u.x * (double)zm.x + (double)u.y * (double)zm.y);
                             }
                         }
                         double b = 2.0 * sum;
