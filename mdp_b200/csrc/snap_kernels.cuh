@@ -34,7 +34,7 @@ struct SnapGeom {
 // one output row mb of the layer and a residue class of the row-pair index ib,
 // accumulates its share of that row in registers across all couplings, and the
 // warps' partial rows are summed once per layer through shared memory.
-constexpr int YI_MAXW = 16;
+constexpr int YI_MAXW = 24;
 template <typename T>
 struct YParams {
     T betaY[NTRI];          // beta' of each coupling triple (bnorm 1/(j+1) folded in)
@@ -49,9 +49,11 @@ struct YParams {
 };
 // warps per Y CTA: FP64 10 (two per row of the costliest layer; 168
 // registers; measured 65 ms at 2M atoms against 70 / 71 / 68 / 68 / 74 ms for
-// 9 / 8 / 11 / 12 / 14 warps), FP32 16
+// 9 / 8 / 11 / 12 / 14 warps); FP32 20 (packed rows, 92 registers; the FP32
+// form measured 34.9 M atom-steps/s against 33.6 / 34.1 / 34.2 at 12 / 16 /
+// 24 warps)
 template <typename T> struct YiWarps { static constexpr int n = 10; };
-template <> struct YiWarps<float> { static constexpr int n = 16; };
+template <> struct YiWarps<float> { static constexpr int n = 20; };
 
 __host__ __device__ constexpr bool coupling_ok(int j1, int j2, int j)
 {
