@@ -268,6 +268,29 @@ template <typename T, int TJ, int J, int MB>
 __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const T bi, T (&pr)[TJ + 1],
                                        T (&pi)[TJ + 1])
 {
+    if constexpr (std::is_same<T, float>::value) {
+        // packed {re, im} pairs: conj(a) u = {ar, ar} u + {ai, -ai} swap(u),
+        // -conj(b) v = {-br, -br} v + {-bi, bi} swap(v)
+        const float2 A = make_float2(ar, ar), An = make_float2(ai, -ai);
+        const float2 B = make_float2(-br, -br), Bn = make_float2(-bi, bi);
+        {
+            float2 t = __fmul2_rn(B, make_float2(pr[J - 1], pi[J - 1]));
+            t = __ffma2_rn(Bn, make_float2(pi[J - 1], pr[J - 1]), t);
+            pr[J] = t.x;
+            pi[J] = t.y;
+        }
+#pragma unroll
+        for (int ma = J - 1; ma >= 0; ma--) {
+            float2 t = __fmul2_rn(A, make_float2(pr[ma], pi[ma]));
+            t = __ffma2_rn(An, make_float2(pi[ma], pr[ma]), t);
+            if (ma >= 1) {
+                t = __ffma2_rn(B, make_float2(pr[ma - 1], pi[ma - 1]), t);
+                t = __ffma2_rn(Bn, make_float2(pi[ma - 1], pr[ma - 1]), t);
+            }
+            pr[ma] = t.x;
+            pi[ma] = t.y;
+        }
+    } else {
     {
         const T vr = pr[J - 1], vi = pi[J - 1];
         pr[J] = -br * vr - bi * vi;
@@ -283,6 +306,7 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
         const T ur = pr[0], ui = pi[0];
         pr[0] = ar * ur + ai * ui;
         pi[0] = ar * ui - ai * ur;
+    }
     }
     if constexpr (MB > 0 && J == 2 * MB) {
 #pragma unroll
@@ -365,7 +389,11 @@ __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::t
             const T nu = unorm<T>(J, MB, ma);
             T2 v = row[ma * 32];
 #pragma unroll
-            for (int q = 0; q < UC_PB; q++) { v.x += nu * s.pr[q][ma]; v.y += nu * s.pi[q][ma]; }
+            for (int q = 0; q < UC_PB; q++) {
+                if constexpr (std::is_same<T, float>::value)
+                    v = __ffma2_rn(make_float2(nu, nu), make_float2(s.pr[q][ma], s.pi[q][ma]), v);
+                else { v.x += nu * s.pr[q][ma]; v.y += nu * s.pi[q][ma]; }
+            }
             row[ma * 32] = v;
         }
         uc_column<T, TJ, MB, J + 1, JEND>(s, acc);
