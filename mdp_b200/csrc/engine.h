@@ -30,11 +30,11 @@ __global__ void k_neigh_build(const double4 *, int, const __grid_constant__ BoxP
 __global__ void k_rev_count(const int *, const int *, const int *, int, int, int *);
 __global__ void k_rev_fill(const int *, const int *, const int *, int, int, const int *, int *, long long *);
 __global__ void k_rev_sort(int, const int *, long long *);
-__global__ void k_pair_count(const double4 *, const int *, const int *, int, int, double, double4 *, int *);
-__global__ void k_pair_emit(const double4 *, const int *, int, int, const int *, SnapGeom, double4 *, int2 *,
-                            double4 *);
-__global__ void k_tally(const double4 *, const double4 *, const int *, int, int, const int *, const long long *,
-                        double4 *, double *);
+__global__ void k_pair_count(const double4 *, const int *, const int *, int, int, double, int *);
+__global__ void k_pair_emit(const double4 *, const int *, const int *, int, int, const int *, SnapGeom, double4 *,
+                            int2 *, double4 *, int *);
+__global__ void k_tally(const double4 *, const double4 *, const int *, const int *, int, const int *,
+                        const long long *, double4 *, double *);
 __global__ void k_nve_initial(double4 *, double4 *, const double4 *, double4 *, int, double, double);
 __global__ void k_nve_final(double4 *, const double4 *, int, double);
 __global__ void k_maxdisp(const double4 *, const double4 *, int, unsigned long long *);
@@ -63,7 +63,7 @@ struct DevBuf {
 };
 
 struct ForcePath {
-    DevBuf pcount, poff, prij, pinfo, pab, rslot, dE, Ut, Y, scan_tmp;
+    DevBuf pcount, poff, prij, pinfo, pab, smap, dE, Ut, Y, scan_tmp;
     int natoms_cap = 0, nm_cap = 0;
     // per-stage timing (CUDA events on the launching stream), enabled on demand
     bool timing = false;

@@ -335,9 +335,20 @@ k_rev_sort(int inum, const int *__restrict__ roff, long long *__restrict__ rlist
 // ---------------------------------------------------------------------------
 // per-step pairs
 // ---------------------------------------------------------------------------
+// the pair test of slot l of atom i: r < rcut and r > 0 (cpuSnap.cpp:1883-1906),
+// with r^2 rounded in the CPU code's order
+__device__ __forceinline__ bool slot_pair(const double4 &xi, const double4 &xj, double rcutsq, double &d0,
+                                          double &d1, double &d2)
+{
+    d0 = xj.x - xi.x;
+    d1 = xj.y - xi.y;
+    d2 = xj.z - xi.z;
+    const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+    return rsq < rcutsq && rsq > 1e-20;
+}
+
 __global__ void k_pair_count(const double4 *__restrict__ x, const int *__restrict__ nlist,
-                             const int *__restrict__ nnum, int inum, int nm, double rcutsq,
-                             double4 *__restrict__ rslot, int *__restrict__ pcount)
+                             const int *__restrict__ nnum, int inum, int nm, double rcutsq, int *__restrict__ pcount)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= inum) return;
@@ -345,65 +356,65 @@ __global__ void k_pair_count(const double4 *__restrict__ x, const int *__restric
     const int n = nnum[i];
     int cnt = 0;
     for (int l = 0; l < n; l++) {
-        const int j = nlist[(size_t)i * nm + l];
-        const double4 xj = x[j];
-        const double d0 = xj.x - xi.x, d1 = xj.y - xi.y, d2 = xj.z - xi.z;
-        const double rsq = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-        const bool pair = rsq < rcutsq && rsq > 1e-20;
-        rslot[(size_t)i * nm + l] = make_double4(d0, d1, d2, pair ? 1.0 : 0.0);
-        cnt += pair;
+        double d0, d1, d2;
+        cnt += slot_pair(xi, x[nlist[(size_t)i * nm + l]], rcutsq, d0, d1, d2);
     }
     pcount[i] = cnt;
 }
 
-// compact pair list of the atoms' slots in order; each pair also gets its
-// Cayley-Klein parameters (a, b) in pab and its sfac in prij.w
-__global__ void k_pair_emit(const double4 *__restrict__ rslot, const int *__restrict__ nnum, int inum, int nm,
-                            const int *__restrict__ poff, SnapGeom gp, double4 *__restrict__ prij,
-                            int2 *__restrict__ pinfo, double4 *__restrict__ pab)
+// compact pair list of the atoms' slots in order: r and sfac in prij, the
+// Cayley-Klein parameters (a, b) in pab, (atom, pair) in pinfo; smap maps
+// every slot to its pair (-1 for slots beyond rcut)
+__global__ void k_pair_emit(const double4 *__restrict__ x, const int *__restrict__ nlist,
+                            const int *__restrict__ nnum, int inum, int nm, const int *__restrict__ poff, SnapGeom gp,
+                            double4 *__restrict__ prij, int2 *__restrict__ pinfo, double4 *__restrict__ pab,
+                            int *__restrict__ smap)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= inum) return;
+    const double4 xi = x[i];
     const int n = nnum[i];
     int p = poff[i];
     for (int l = 0; l < n; l++) {
-        const double4 r = rslot[(size_t)i * nm + l];
-        if (r.w != 0.0) {
+        const size_t s = (size_t)i * nm + l;
+        double d0, d1, d2;
+        if (slot_pair(xi, x[nlist[s]], gp.rcutsq, d0, d1, d2)) {
             PairGeo g;
-            pair_geometry<false>(g, r.x, r.y, r.z, gp);
-            prij[p] = make_double4(r.x, r.y, r.z, g.sfac);
+            pair_geometry<false>(g, d0, d1, d2, gp);
+            prij[p] = make_double4(d0, d1, d2, g.sfac);
             pab[p] = make_double4(g.ar, g.ai, g.br, g.bi);
-            pinfo[p] = make_int2(i, (int)((size_t)i * nm + l));
+            pinfo[p] = make_int2(i, p);
+            smap[s] = p;
             p++;
+        } else {
+            smap[s] = -1;
         }
     }
 }
 
 // f_o = sum_{own pairs} dE - sum_{pairs whose neighbour is an image of o} dE;
-// per-atom virial -1/2 r (x) dE on both atoms (cpuSnap4.cpp:1177-1209)
-__global__ void k_tally(const double4 *__restrict__ rslot, const double4 *__restrict__ dE,
-                        const int *__restrict__ nnum, int inum, int nm, const int *__restrict__ roff,
-                        const long long *__restrict__ rlist, double4 *__restrict__ f, double *__restrict__ vatom)
+// per-atom virial -1/2 r (x) dE on both atoms (cpuSnap4.cpp:1177-1209).  Own
+// pairs in slot order, then the reverse entries in ascending slot order: a
+// fixed summation order without atomics.
+__global__ void k_tally(const double4 *__restrict__ prij, const double4 *__restrict__ dE,
+                        const int *__restrict__ poff, const int *__restrict__ smap, int inum,
+                        const int *__restrict__ roff, const long long *__restrict__ rlist, double4 *__restrict__ f,
+                        double *__restrict__ vatom)
 {
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= inum) return;
     double fx = 0, fy = 0, fz = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-    const int n = nnum[o];
-    for (int l = 0; l < n; l++) {
-        const size_t s = (size_t)o * nm + l;
-        const double4 r = rslot[s];
-        if (r.w == 0.0) continue;
-        const double4 d = dE[s];
+    for (int p = poff[o]; p < poff[o + 1]; p++) {
+        const double4 r = prij[p], d = dE[p];
         fx += d.x; fy += d.y; fz += d.z;
         v0 += -0.5 * r.x * d.x; v1 += -0.5 * r.y * d.y; v2 += -0.5 * r.z * d.z;
         v3 += -0.5 * r.x * d.y; v4 += -0.5 * r.x * d.z; v5 += -0.5 * r.y * d.z;
     }
     const int s0 = roff[o], s1 = roff[o + 1];
     for (int t = s0; t < s1; t++) {
-        const long long s = rlist[t];
-        const double4 r = rslot[s];
-        if (r.w == 0.0) continue;
-        const double4 d = dE[s];
+        const int p = smap[rlist[t]];
+        if (p < 0) continue;
+        const double4 r = prij[p], d = dE[p];
         fx -= d.x; fy -= d.y; fz -= d.z;
         v0 += -0.5 * r.x * d.x; v1 += -0.5 * r.y * d.y; v2 += -0.5 * r.z * d.z;
         v3 += -0.5 * r.x * d.y; v4 += -0.5 * r.x * d.z; v5 += -0.5 * r.y * d.z;

@@ -53,7 +53,7 @@ void DevBuf::release()
 
 void ForcePath::release()
 {
-    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &rslot, &dE, &Ut, &Y, &scan_tmp};
+    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &smap, &dE, &Ut, &Y, &scan_tmp};
     for (auto x : b) x->release();
     for (auto &e : ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
@@ -240,7 +240,7 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (fp.pcount.ensure(sizeof(int) * (size_t)inum) || fp.poff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
         fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
         fp.pab.ensure(sizeof(double4) * (size_t)pair_cap) ||
-        fp.rslot.ensure(sizeof(double4) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)inum * nm) ||
+        fp.smap.ensure(sizeof(int) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)pair_cap) ||
         fp.Ut.ensure(tsz * (size_t)ntiles * m.nu * 32) || fp.Y.ensure(tsz * (size_t)ntiles * 32 * m.nyh) ||
         fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(inum)))
         return -1;
@@ -249,15 +249,16 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     const int tb = 256;
     const int gb = (inum + tb - 1) / tb;
     if (fp.timing) cudaEventRecord(fp.ev[0], s);
-    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.rslot.as<double4>(), fp.pcount.as<int>());
+    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.pcount.as<int>());
     if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
-    k_pair_emit<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), nnum, inum, nm, fp.poff.as<int>(), m.geom,
-                                  fp.prij.as<double4>(), fp.pinfo.as<int2>(), fp.pab.as<double4>());
+    k_pair_emit<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
+                                  fp.pinfo.as<int2>(), fp.pab.as<double4>(), fp.smap.as<int>());
     int rc = (precision == MDP_PREC_FP32) ? launch_snap_tj<float>(m, m.yf, fp, inum, nm, eatom, s)
                                            : launch_snap_tj<double>(m, m.yd, fp, inum, nm, eatom, s);
     if (rc) return rc;
     if (fp.timing) cudaEventRecord(fp.ev[4], s);
-    k_tally<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), fp.dE.as<double4>(), nnum, inum, nm, roff, rlist, f, vatom);
+    k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,
+                              roff, rlist, f, vatom);
     count_launches(6);   // pair_count, pair_emit, ui, yi, fi, tally (+ the scan counts itself)
     if (fp.timing) {
         cudaEventRecord(fp.ev[5], s);

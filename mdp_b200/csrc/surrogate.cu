@@ -656,17 +656,17 @@ int sur_features(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const 
     if (fp.pcount.ensure(sizeof(int) * (size_t)inum) || fp.poff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
         fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
         fp.pab.ensure(sizeof(double4) * (size_t)pair_cap) ||
-        fp.rslot.ensure(sizeof(double4) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)inum * nm) ||
+        fp.smap.ensure(sizeof(int) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)pair_cap) ||
         fp.Ut.ensure(sizeof(float2) * (size_t)ntiles * m.nu * 32) ||
         fp.Y.ensure(sizeof(float2) * (size_t)ntiles * 32 * m.nyh) ||
         fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(inum)) || S.B.ensure(sizeof(double) * SUR_NK * (size_t)inum) ||
         S.G.ensure(sizeof(float) * SUR_NK * (size_t)inum))
         return -1;
     const int tb = 256, gb = (inum + tb - 1) / tb;
-    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.rslot.as<double4>(), fp.pcount.as<int>());
+    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.pcount.as<int>());
     if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
-    k_pair_emit<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), nnum, inum, nm, fp.poff.as<int>(), m.geom,
-                                  fp.prij.as<double4>(), fp.pinfo.as<int2>(), fp.pab.as<double4>());
+    k_pair_emit<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
+                                  fp.pinfo.as<int2>(), fp.pab.as<double4>(), fp.smap.as<int>());
     count_launches(2);
     if (launch_ui<float, 4>(m, fp, inum, s)) return -1;
     count_launches(1);
@@ -688,7 +688,8 @@ int sur_force(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const int
     if (launch_fi<float, 4>(S.model, fp, inum, nm, s)) return -1;
     const int tb = 256, gb = (inum + tb - 1) / tb;
     if (fp.timing) cudaEventRecord(fp.ev[4], s);
-    k_tally<<<gb, tb, 0, s>>>(fp.rslot.as<double4>(), fp.dE.as<double4>(), nnum, inum, nm, roff, rlist, f, vatom);
+    k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,
+                              roff, rlist, f, vatom);
     count_launches(4);
     if (fp.timing) {
         cudaEventRecord(fp.ev[5], s);
