@@ -14,13 +14,13 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
     static int per_sm = 0;
     if (!per_sm) {
         MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<T, TJ>, YiWarps<T>::n * 32, sm));
+        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<T, TJ>, YiWarps<T, TJ>::n * 32, sm));
         if (per_sm < 1) { set_error("k_snap_yi does not fit on an SM (%zu B shared)", sm); return -1; }
     }
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[2], s);
-    k_snap_yi<T, TJ><<<blocks, YiWarps<T>::n * 32, sm, s>>>(fp.Ut.as<T2>(), inum, yp, fp.Y.as<T2>(), eatom);
+    k_snap_yi<T, TJ><<<blocks, YiWarps<T, TJ>::n * 32, sm, s>>>(fp.Ut.as<T2>(), inum, yp, fp.Y.as<T2>(), eatom);
     return 0;
 }
 
@@ -33,13 +33,13 @@ int launch_yi_pa_f4(const SnapModel &m, ForcePath &fp, int inum, const float *G,
     if (!per_sm) {
         MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<float, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<float, 4, true>,
-                                                                   YiWarps<float>::n * 32, sm));
+                                                                   YiWarps<float, 4>::n * 32, sm));
         if (per_sm < 1) { set_error("k_snap_yi (per-atom) does not fit on an SM"); return -1; }
     }
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[2], s);
-    k_snap_yi<float, 4, true><<<blocks, YiWarps<float>::n * 32, sm, s>>>(fp.Ut.as<float2>(), inum, m.yf,
+    k_snap_yi<float, 4, true><<<blocks, YiWarps<float, 4>::n * 32, sm, s>>>(fp.Ut.as<float2>(), inum, m.yf,
                                                                          fp.Y.as<float2>(), nullptr, G);
     return 0;
 }

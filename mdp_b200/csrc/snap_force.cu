@@ -195,8 +195,8 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
         }
         return 0;
     };
-    if (assign(YiWarps<double>::n, m.yd.lay_mb, m.yd.lay_o, m.yd.lay_st) ||
-        assign(YiWarps<float>::n, m.yf.lay_mb, m.yf.lay_o, m.yf.lay_st)) {
+    if (assign(yi_warps(false, tj), m.yd.lay_mb, m.yd.lay_o, m.yd.lay_st) ||
+        assign(yi_warps(true, tj), m.yf.lay_mb, m.yf.lay_o, m.yf.lay_st)) {
         set_error("Y-kernel warp assignment failed");
         return -1;
     }

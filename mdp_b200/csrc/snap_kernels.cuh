@@ -51,9 +51,23 @@ struct YParams {
 // registers; measured 65 ms at 2M atoms against 70 / 71 / 68 / 68 / 74 ms for
 // 9 / 8 / 11 / 12 / 14 warps); FP32 20 (packed rows, 92 registers; the FP32
 // form measured 34.9 M atom-steps/s against 33.6 / 34.1 / 34.2 at 12 / 16 /
-// 24 warps)
-template <typename T> struct YiWarps { static constexpr int n = 10; };
-template <> struct YiWarps<float> { static constexpr int n = 20; };
+// 24 warps).  At 2J <= 4 no layer has more than three rows and the extra
+// warps only wait at the barriers: the FP32 per-atom-coefficient kernel of the
+// surrogate takes 4 (surrogate steps at 2M atoms: 14.8 ms against 14.9 / 15.2
+// / 15.8 / 17.6 / 16.9 ms at 3 / 6 / 8 / 12 / 20 warps; 2 cannot cover the
+// three rows).
+#ifndef YI_W4_D
+#define YI_W4_D 10
+#endif
+#ifndef YI_W4_F
+#define YI_W4_F 4
+#endif
+__host__ __device__ constexpr int yi_warps(bool fp32, int tj)
+{
+    return fp32 ? (tj <= 4 ? YI_W4_F : 20) : (tj <= 4 ? YI_W4_D : 10);
+}
+template <typename T, int TJ> struct YiWarps { static constexpr int n = yi_warps(false, TJ); };
+template <int TJ> struct YiWarps<float, TJ> { static constexpr int n = yi_warps(true, TJ); };
 
 __host__ __device__ constexpr bool coupling_ok(int j1, int j2, int j)
 {
@@ -712,7 +726,7 @@ template <typename T, int TJ, bool PA = false>
 constexpr size_t yi_smem_bytes()
 {
     return (size_t)idxu_count(TJ) * 32 * sizeof(typename cplx<T>::type) +
-           (size_t)YiWarps<T>::n * JD * 32 * sizeof(typename cplx<T>::type) + YiWarps<T>::n * 32 * sizeof(double) +
+           (size_t)YiWarps<T, TJ>::n * JD * 32 * sizeof(typename cplx<T>::type) + YiWarps<T, TJ>::n * 32 * sizeof(double) +
            (PA ? (size_t)nbispec(TJ) * 32 * sizeof(T) : 0);
 }
 
@@ -720,12 +734,12 @@ constexpr size_t yi_smem_bytes()
 // PA: per-atom coefficients G[k * natoms + atom] (k over the nbispec(TJ)
 // components) instead of the model's; no energy is written.
 template <typename T, int TJ, bool PA = false>
-__global__ void __launch_bounds__(YiWarps<T>::n * 32, 1)
+__global__ void __launch_bounds__(YiWarps<T, TJ>::n * 32, 1)
 k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __grid_constant__ YParams<T> P,
           typename cplx<T>::type *__restrict__ Y, double *__restrict__ eatom, const T *__restrict__ G = nullptr)
 {
     typedef typename cplx<T>::type T2;
-    constexpr int NW = YiWarps<T>::n;
+    constexpr int NW = YiWarps<T, TJ>::n;
     constexpr int NU = idxu_count(TJ);
     constexpr int NYH = yh_count(TJ);
     constexpr int NK = nbispec(TJ);
