@@ -347,48 +347,64 @@ __device__ __forceinline__ bool slot_pair(const double4 &xi, const double4 &xj, 
     return rsq < rcutsq && rsq > 1e-20;
 }
 
+// One warp per atom: the lanes test 32 of the atom's slots at a time, and a
+// ballot ranks each lane's pair among the atom's pairs in slot order.
 __global__ void k_pair_count(const double4 *__restrict__ x, const int *__restrict__ nlist,
                              const int *__restrict__ nnum, int inum, int nm, double rcutsq, int *__restrict__ pcount)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= inum) return;
+    const int lane = threadIdx.x & 31;
+    const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= inum) return;   // whole warps leave together
     const double4 xi = x[i];
     const int n = nnum[i];
     int cnt = 0;
-    for (int l = 0; l < n; l++) {
-        double d0, d1, d2;
-        cnt += slot_pair(xi, x[nlist[(size_t)i * nm + l]], rcutsq, d0, d1, d2);
+    for (int l0 = 0; l0 < n; l0 += 32) {
+        const int l = l0 + lane;
+        bool pair = false;
+        if (l < n) {
+            double d0, d1, d2;
+            pair = slot_pair(xi, x[nlist[(size_t)i * nm + l]], rcutsq, d0, d1, d2);
+        }
+        cnt += __popc(__ballot_sync(0xffffffffu, pair));
     }
-    pcount[i] = cnt;
+    if (lane == 0) pcount[i] = cnt;
 }
 
 // compact pair list of the atoms' slots in order: r and sfac in prij, the
 // Cayley-Klein parameters (a, b) in pab, (atom, pair) in pinfo; smap maps
-// every slot to its pair (-1 for slots beyond rcut)
+// every slot to its pair (-1 for slots beyond rcut).  One warp per atom.
 __global__ void k_pair_emit(const double4 *__restrict__ x, const int *__restrict__ nlist,
                             const int *__restrict__ nnum, int inum, int nm, const int *__restrict__ poff, SnapGeom gp,
                             double4 *__restrict__ prij, int2 *__restrict__ pinfo, double4 *__restrict__ pab,
                             int *__restrict__ smap)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= inum) return;
+    const int lane = threadIdx.x & 31;
+    const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= inum) return;   // whole warps leave together
     const double4 xi = x[i];
     const int n = nnum[i];
     int p = poff[i];
-    for (int l = 0; l < n; l++) {
+    for (int l0 = 0; l0 < n; l0 += 32) {
+        const int l = l0 + lane;
         const size_t s = (size_t)i * nm + l;
-        double d0, d1, d2;
-        if (slot_pair(xi, x[nlist[s]], gp.rcutsq, d0, d1, d2)) {
-            PairGeo g;
-            pair_geometry<false>(g, d0, d1, d2, gp);
-            prij[p] = make_double4(d0, d1, d2, g.sfac);
-            pab[p] = make_double4(g.ar, g.ai, g.br, g.bi);
-            pinfo[p] = make_int2(i, p);
-            smap[s] = p;
-            p++;
-        } else {
-            smap[s] = -1;
+        bool pair = false;
+        double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+        if (l < n) pair = slot_pair(xi, x[nlist[s]], gp.rcutsq, d0, d1, d2);
+        const unsigned m = __ballot_sync(0xffffffffu, pair);
+        if (l < n) {
+            if (pair) {
+                const int q = p + __popc(m & ((1u << lane) - 1u));
+                PairGeo g;
+                pair_geometry<false>(g, d0, d1, d2, gp);
+                prij[q] = make_double4(d0, d1, d2, g.sfac);
+                pab[q] = make_double4(g.ar, g.ai, g.br, g.bi);
+                pinfo[q] = make_int2((int)i, q);
+                smap[s] = q;
+            } else {
+                smap[s] = -1;
+            }
         }
+        p += __popc(m);
     }
 }
 

@@ -249,9 +249,10 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     const int tb = 256;
     const int gb = (inum + tb - 1) / tb;
     if (fp.timing) cudaEventRecord(fp.ev[0], s);
-    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.pcount.as<int>());
+    const unsigned gw = (unsigned)(((long)inum * 32 + tb - 1) / tb);   // one warp per atom
+    k_pair_count<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.pcount.as<int>());
     if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
-    k_pair_emit<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
+    k_pair_emit<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
                                   fp.pinfo.as<int2>(), fp.pab.as<double4>(), fp.smap.as<int>());
     int rc = (precision == MDP_PREC_FP32) ? launch_snap_tj<float>(m, m.yf, fp, inum, nm, eatom, s)
                                            : launch_snap_tj<double>(m, m.yd, fp, inum, nm, eatom, s);

@@ -663,9 +663,10 @@ int sur_features(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const 
         S.G.ensure(sizeof(float) * SUR_NK * (size_t)inum))
         return -1;
     const int tb = 256, gb = (inum + tb - 1) / tb;
-    k_pair_count<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.pcount.as<int>());
+    const unsigned gw = (unsigned)(((long)inum * 32 + tb - 1) / tb);   // one warp per atom
+    k_pair_count<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.geom.rcutsq, fp.pcount.as<int>());
     if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
-    k_pair_emit<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
+    k_pair_emit<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
                                   fp.pinfo.as<int2>(), fp.pab.as<double4>(), fp.smap.as<int>());
     count_launches(2);
     if (launch_ui<float, 4>(m, fp, inum, s)) return -1;
