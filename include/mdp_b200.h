@@ -184,6 +184,14 @@ int mdp_md_sur_features(mdp_md *md, mdp_sur *s, double *B_host);
  * same positions; its forces replace the surrogate's for that step and, when
  * the force RMSE (over the 3N components) exceeds tol, the engine falls back
  * to the plain model for the rest of its life. */
+/* ZBL pair term added to SNAP, as MDP's snapTA06A example pairs them
+ * (simulating/snap/snapTA06A.jl:62-69, potential simulating/snap/ZBLpotential.jl,
+ * tallied as src/C++/Potentials/cpuPotentials.cpp:1587-1650 does for full
+ * neighbour lists): screened Coulomb for nuclear charge z between all atom
+ * pairs closer than `outer`, switched to zero between `inner` and `outer`.
+ * z <= 0 turns it off.  `outer` must not exceed the SNAP cutoff + skin.
+ * Call mdp_md_setup afterwards. */
+int mdp_md_set_zbl(mdp_md *md, double inner, double outer, double z);
 int mdp_md_set_surrogate(mdp_md *md, mdp_sur *s, int judge_every, double tol);
 /* active (1 while the surrogate drives), fallback step (-1: none), number of
  * judgements, and up to cap (step, rmse) pairs */

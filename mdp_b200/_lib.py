@@ -91,6 +91,7 @@ def lib():
     L.mdp_md_sur_sample.argtypes = [C.c_void_p, C.c_void_p]
     L.mdp_md_sur_features.argtypes = [C.c_void_p, C.c_void_p, _dp]
     L.mdp_md_set_surrogate.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_double]
+    L.mdp_md_set_zbl.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
     _ip32 = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
     L.mdp_sur_force_set.argtypes = [C.c_void_p, C.c_void_p, _dp, _dp, C.c_int]
     L.mdp_sur_force_set_npairs.argtypes = [C.c_void_p]

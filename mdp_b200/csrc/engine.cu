@@ -458,6 +458,19 @@ int mdp_md_sur_features(mdp_md *m, mdp_sur *S, double *B_host)
     return 0;
 }
 
+int mdp_md_set_zbl(mdp_md *m, double inner, double outer, double z)
+{
+    if (!m) { set_error("null handle"); return -1; }
+    const double reach = m->model.geom.rcut + m->cfg.skin;
+    if (z > 0.0 && outer > reach) {
+        set_error("ZBL cutoff %g A exceeds the neighbour-list reach %g A (SNAP cutoff + skin)", outer, reach);
+        return -1;
+    }
+    if (zbl_setup(m->model.zbl, inner, outer, z)) return -1;
+    m->ready = false;   // forces must be recomputed by mdp_md_setup
+    return 0;
+}
+
 int mdp_md_set_surrogate(mdp_md *m, mdp_sur *S, int judge_every, double tol)
 {
     if (!m) { set_error("null handle"); return -1; }

@@ -43,6 +43,17 @@ __global__ void k_ghost_shift(double4 *, const double4 *, const int *, int, int)
 __global__ void k_thermo(const double *, const double *, const double4 *, int, double *);
 
 // SNAP model: validated parameters plus the derived kernel parameter blocks
+// ZBL pair potential added to SNAP (the snapTA06A example's Paira term,
+// simulating/snap/ZBLpotential.jl): screening exponents d_k / a, prefactors
+// c_k Z^2 qqr2e, inner switch radius, outer cutoff^2 and the switch
+// polynomial's coefficients
+struct ZblParams {
+    int on = 0;
+    double dk[4], ck[4], inner, rcsq, sw3, sw4, sw5;
+};
+int zbl_setup(ZblParams &zp, double inner, double outer, double z);
+__global__ void k_zbl(const double4 *, const int *, const int *, int, int, ZblParams, double *, double4 *, double *);
+
 struct SnapModel {
     mdp_snap_params p;
     std::vector<double> coeff;
@@ -50,6 +61,7 @@ struct SnapModel {
     YParams<double> yd;
     YParams<float> yf;
     int nu, nyh, ncoeff;
+    ZblParams zbl;
 };
 int model_init(SnapModel &m, const mdp_snap_params *p);
 

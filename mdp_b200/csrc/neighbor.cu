@@ -442,6 +442,53 @@ __global__ void k_tally(const double4 *__restrict__ prij, const double4 *__restr
     }
 }
 
+// ZBL pair term over each atom's full neighbour row (cpuPotentials.cpp:1587-1650
+// with the potential of ZBLpotential.jl): pairs with |x_ij|^2 <= rcut^2 add
+// u/2 to the atom's energy, du/dx_ij to its force and -x_ij (x) du/dx_ij / 2 to
+// its virial, on top of what SNAP wrote.  Thread per atom, no atomics.
+__global__ void k_zbl(const double4 *__restrict__ x, const int *__restrict__ nlist, const int *__restrict__ nnum,
+                      int inum, int nm, ZblParams zp, double *__restrict__ eatom, double4 *__restrict__ f,
+                      double *__restrict__ vatom)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= inum) return;
+    const double4 xi = x[i];
+    const int n = nnum[i];
+    double e = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
+    for (int l = 0; l < n; l++) {
+        const double4 xj = x[nlist[(size_t)i * nm + l]];
+        const double d0 = xj.x - xi.x, d1 = xj.y - xi.y, d2 = xj.z - xi.z;
+        const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+        if (!(r2 <= zp.rcsq)) continue;
+        const double r = sqrt(r2), rinv = 1.0 / r;
+        // screened Coulomb part and its radial derivative
+        double s = 0.0, sp = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const double ek = zp.ck[k] * exp(-zp.dk[k] * r);
+            s += ek;
+            sp -= zp.dk[k] * ek;
+        }
+        const double ez = s * rinv, ezp = (sp - s * rinv) * rinv;
+        // smoothed switch: A(t) t^3 (sw3 + sw4 t) with A = 1/2 + tanh(100 t)/2
+        const double t = r - zp.inner, t2 = t * t, t3 = t2 * t;
+        const double th = tanh(100.0 * t), a = 0.5 + 0.5 * th, da = 50.0 * (1.0 - th * th);
+        const double poly = zp.sw3 + zp.sw4 * t;
+        const double u = ez + zp.sw5 + a * t3 * poly;
+        const double g = (ezp + da * t3 * poly + a * (3.0 * t2 * poly + t3 * zp.sw4)) * rinv;
+        const double ux = g * d0, uy = g * d1, uz = g * d2;
+        e += 0.5 * u;
+        fx += ux; fy += uy; fz += uz;
+        v[0] -= 0.5 * d0 * ux; v[1] -= 0.5 * d1 * uy; v[2] -= 0.5 * d2 * uz;
+        v[3] -= 0.5 * d0 * uy; v[4] -= 0.5 * d0 * uz; v[5] -= 0.5 * d1 * uz;
+    }
+    eatom[i] += e;
+    const double4 fo = f[i];
+    f[i] = make_double4(fo.x + fx, fo.y + fy, fo.z + fz, 0.0);
+    if (vatom)
+        for (int k = 0; k < 6; k++) vatom[k * (size_t)inum + i] += v[k];
+}
+
 // ---------------------------------------------------------------------------
 // integrator, PBC, rebuild check, ghost shift, thermo sums
 // ---------------------------------------------------------------------------

@@ -15,6 +15,45 @@ namespace mdp {
 // drain, kernels queued right after a growth raced the fill and some of their
 // first results were zeroed.  Growth happens only on a buffer's first use at a
 // larger size, never inside a stream capture.
+// ZBL parameters as ZBLpotential.jl:14-99 defines them: 1/a = (Z^0.23 +
+// Z^0.23) / 0.4685, prefactors c_k Z^2 qqr2e, and the switch polynomial that
+// takes E, E' and E'' to zero at the outer cutoff
+int zbl_setup(ZblParams &zp, double inner, double outer, double z)
+{
+    zp.on = 0;
+    if (z <= 0.0) return 0;
+    if (!(inner > 0.0 && outer > inner)) {
+        set_error("ZBL radii must satisfy 0 < inner < outer (got %g, %g)", inner, outer);
+        return -1;
+    }
+    static const double c[4] = {0.02817, 0.28022, 0.50986, 0.18175};
+    static const double d[4] = {0.20162, 0.40290, 0.94229, 3.19980};
+    const double ainv = 2.0 * pow(z, 0.23) / 0.46850, zze = z * z * 14.399645;
+    for (int k = 0; k < 4; k++) {
+        zp.dk[k] = d[k] * ainv;
+        zp.ck[k] = c[k] * zze;
+    }
+    // E and its first two derivatives at the outer cutoff
+    double s = 0.0, sp = 0.0, spp = 0.0;
+    for (int k = 0; k < 4; k++) {
+        const double ek = zp.ck[k] * exp(-zp.dk[k] * outer);
+        s += ek;
+        sp -= zp.dk[k] * ek;
+        spp += zp.dk[k] * zp.dk[k] * ek;
+    }
+    const double ri = 1.0 / outer;
+    const double fc = s * ri, fcp = (sp - s * ri) * ri, fcpp = (spp - 2.0 * sp * ri + 2.0 * s * ri * ri) * ri;
+    const double tc = outer - inner;
+    const double swa = (-3.0 * fcp + tc * fcpp) / (tc * tc), swb = (2.0 * fcp - tc * fcpp) / (tc * tc * tc);
+    zp.sw3 = swa / 3.0;
+    zp.sw4 = swb / 4.0;
+    zp.sw5 = -fc + 0.5 * tc * fcp - tc * tc / 12.0 * fcpp;
+    zp.inner = inner;
+    zp.rcsq = outer * outer;
+    zp.on = 1;
+    return 0;
+}
+
 int DevBuf::ensure(size_t n)
 {
     if (n <= bytes) return 0;
@@ -261,6 +300,10 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,
                               roff, rlist, f, vatom);
     count_launches(6);   // pair_count, pair_emit, ui, yi, fi, tally (+ the scan counts itself)
+    if (m.zbl.on) {
+        k_zbl<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.zbl, eatom, f, vatom);
+        count_launches(1);
+    }
     if (fp.timing) {
         cudaEventRecord(fp.ev[5], s);
         cudaEventSynchronize(fp.ev[5]);

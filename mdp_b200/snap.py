@@ -141,6 +141,11 @@ class SnapMD:
         return dict(steps=int(out[0]), rebuilds=int(out[1]), pairs=int(out[2]), ghosts=int(out[3]),
                     neighbors=int(out[4]))
 
+    def set_zbl(self, inner: float = 4.0, outer: float = 4.8, z: float = 73.0):
+        """Add the ZBL pair term of MDP's snapTA06A example (defaults: its Ta
+        parameters); z <= 0 removes it.  Call setup() afterwards."""
+        _lib.check(_lib.lib().mdp_md_set_zbl(self._h, float(inner), float(outer), float(z)), "mdp_md_set_zbl")
+
     def set_surrogate(self, sur, judge_every: int = 50, tol: float = 0.05):
         """Drive the forces by a trained surrogate (None: the plain model), judged
         every judge_every steps against the plain model with force-RMSE tolerance tol."""

@@ -15,6 +15,9 @@
 // blocks one after another; per-block results are independent, forces are
 // summed from per-thread buffers).
 #include "cpuCore.cpp"
+// MDP's generated code for the Ta ZBL pair potential of its snapTA06A example
+// (src/C++/Potentials/cpuPairaGradient.cpp, from simulating/snap/ZBLpotential.jl)
+#include "cpuPairaGradient.cpp"
 
 #include <stdlib.h>
 #include <string.h>
@@ -310,6 +313,14 @@ int ref_omp_max_threads(void)
 #else
     return 1;
 #endif
+}
+
+// u and du/dx_ij of the ZBL pair potential for n pair vectors xij [n][3]
+// (the reference's generated cpuPairaGradient, potential 1)
+void ref_zbl_pairs(double *u, double *u_xij, const double *xij, int n)
+{
+    cpuPairaGradient<double>(u, u_xij, (double *)xij, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                             nullptr, nullptr, 3, 0, 0, 0, 0, n, 1);
 }
 
 }  // extern "C"

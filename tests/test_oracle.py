@@ -102,3 +102,23 @@ def test_tables_match_reference_counts():
     for tj, (ncg, nu, nb, nz) in {4: (305, 55, 14, 185), 6: (1321, 140, 30, 779), 8: (4098, 285, 55, 2386)}.items():
         s = oracle.table_sizes(tj)
         assert (s["idxcg"], s["idxu"], s["idxb"], s["idxz"]) == (ncg, nu, nb, nz)
+
+
+def test_zbl_restatement_matches_reference_generated_code():
+    """The numpy ZBL restatement against MDP's own generated code for the Ta
+    potential of its snapTA06A example (inner 4, outer 4.8, Z 73)."""
+    from oracle import refpy, zbl
+    if not refpy.available():
+        pytest.skip("oracle/_ref not built")
+    import ctypes as C
+    L = refpy.lib()
+    L.ref_zbl_pairs.argtypes = [C.c_void_p] * 3 + [C.c_int]
+    rng = np.random.default_rng(3)
+    r = np.concatenate([rng.uniform(1.5, 4.8, 4000), np.linspace(3.9, 4.1, 101)])
+    u_dir = rng.normal(size=(r.size, 3))
+    xij = np.ascontiguousarray(u_dir / np.linalg.norm(u_dir, axis=1)[:, None] * r[:, None])
+    u_ref, ux_ref = np.zeros(r.size), np.zeros((r.size, 3))
+    L.ref_zbl_pairs(u_ref.ctypes.data, ux_ref.ctypes.data, xij.ctypes.data, r.size)
+    u, ux = zbl.zbl_pair(xij)
+    assert np.abs(u - u_ref).max() <= 1e-12 * np.abs(u_ref).max()
+    assert np.abs(ux - ux_ref).max() <= 1e-11 * np.abs(ux_ref).max()
