@@ -11,7 +11,7 @@
  * this header also defines the reference's gpu* entry points for T = double on
  * top of them, replacing src/C++/Core/gpuSnap4.cu, the pair kernels of
  * gpuSnap.cu, gpuCumsum.cu, gpuNeighborList3D.cu, gpuVelocityIntegration.cu
- * (modes 0 and 1) and gpuDomain.cu's gpuPBC at link time.  Array layouts are
+ * (modes 0, 1 and 2) and gpuDomain.cu's gpuPBC at link time.  Array layouts are
  * the reference's: U/Y [idxu][inum], rij [ijnum][3], fatom [anum][3],
  * vatom [6][anum], x [natom][dim].  Supported: one element type, 2J = 4, 6, 8,
  * double.  On unsupported input the outputs are untouched and
@@ -94,15 +94,16 @@ void mdp_gpu_full_neighbor_list3d_cells_f64(int *neighborlist, int *neighbornum,
 /* mdpgpucore.h:141-142, gpuFullNeighborList3D (all pairs) */
 void mdp_gpu_full_neighbor_list3d_f64(int *neighborlist, int *neighbornum, const double *x, const double *rcutsq,
                                       int anum, int inum, int jnum, int dim);
-/* mdpgpucore.h:309-311, gpuInitialIntegrate (modes 0 NVE, 1 NVE limit; dtarray on the host) */
+/* mdpgpucore.h:309-311, gpuInitialIntegrate (modes 0 NVE, 1 NVE limit, 2 NVT Nose-Hoover chain;
+ * dtarray, tarray and the eta arrays on the host, ke and tmp device scratch) */
 void mdp_gpu_initial_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
-                                   const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                   double *tarray, double *eta_mass, double *eta, double *eta_dot,
                                    double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
                                    const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
                                    int mode, int dim, int inum);
 /* mdpgpucore.h:313-315, gpuFinalIntegrate */
 void mdp_gpu_final_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
-                                 const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                 double *tarray, double *eta_mass, double *eta, double *eta_dot,
                                  double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
                                  const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
                                  int mode, int dim, int inum);

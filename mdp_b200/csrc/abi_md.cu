@@ -212,6 +212,16 @@ __global__ void k_md_verlet(double *__restrict__ x, double *__restrict__ v, cons
         for (int d = 0; d < dim; d++) x[(size_t)dim * i + d] = __dadd_rn(x[(size_t)dim * i + d], __dmul_rn(dtv, vi[d]));
 }
 
+// velocity scaling of the thermostat (cpuVelocityIntegration.cpp:465-503; the
+// reference's bias flag changes nothing there)
+__global__ void k_md_vscale(double *__restrict__ v, double factor, const int *__restrict__ ilist, int dim, int inum)
+{
+    const int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= inum) return;
+    double *vi = v + (size_t)dim * ilist[ii];
+    for (int d = 0; d < dim; d++) vi[d] *= factor;
+}
+
 // ---- periodic wrapping (cpuDomain.cpp:235-385) -----------------------------
 // the velocity shift of a deforming box for crossing boundary d (rates in
 // Voigt order xx yy zz yz xz xy)
@@ -416,45 +426,126 @@ void mdp_gpu_full_neighbor_list3d_f64(int *neighborlist, int *neighbornum, const
     check_launch("gpuFullNeighborList3D");
 }
 
-static void verlet(const char *fn, int stage, double *x, double *v, const double *f, const double *mass,
-                   const double *dtarray, double vlimitsq, const int *type, const int *ilist, int mode, int dim,
-                   int inum)
+// temperature tfactor * sum m v^2 over the listed atoms (cpuComputes.cpp:276-296):
+// per-atom terms into ke, a fixed-tree sum into tmp[0] (both the caller's
+// device scratch, as gpuComputeTempScalar uses them), read on the host
+static int temperature(double &t, double *ke, double *tmp, const double *mass, const double *v, double tfactor,
+                       const int *type, const int *ilist, int dim, int inum)
 {
-    if (mode != 0 && mode != 1) {
-        set_error("%s: mode %d (NVT) is not supported; modes 0 (NVE) and 1 (NVE limit) are", fn, mode);
+    k_md_ke<<<blocks_for(inum), TB>>>(ke, mass, v, 2.0 * tfactor, type, ilist, dim, inum);
+    k_md_colsum<<<1, TB>>>(tmp, ke, inum);
+    count_launches(2);
+    if (cudaMemcpy(&t, tmp, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error("temperature read-back failed");
+        return -1;
+    }
+    return 0;
+}
+
+// Nose-Hoover chain half step (cpuVelocityIntegration.cpp:505-600): the chain
+// lives on the host (eta arrays of mtchain + 1 entries, tarray[4] the current
+// temperature on entry); each sub-step scales the listed atoms' velocities.
+static void nose_hoover(double *v, const int *ilist, int dim, int inum, const double *dtarray, double *tarray,
+                        double *eta_mass, double *eta, double *eta_dot, double *eta_dotdot, int eta_mass_flag,
+                        int mtchain, int nc_tchain)
+{
+    const double dt = dtarray[0], half = 0.5 * dt, quarter = 0.25 * dt, eighth = 0.125 * dt;
+    const double t_freq = tarray[2], t_target = tarray[3], tdof = tarray[5], boltz = tarray[6], drag = tarray[7];
+    const double drag_f = 1.0 - (dt * t_freq * drag / nc_tchain), nc = 1.0 / nc_tchain;
+    const double ke_target = tdof * boltz * t_target;
+    double ke_now = tdof * boltz * tarray[4];
+    if (eta_mass_flag) {
+        eta_mass[0] = tdof * boltz * t_target / (t_freq * t_freq);
+        for (int c = 1; c < mtchain; c++) eta_mass[c] = boltz * t_target / (t_freq * t_freq);
+    }
+    eta_dotdot[0] = eta_mass[0] > 0.0 ? (ke_now - ke_target) / eta_mass[0] : 0.0;
+    for (int loop = 0; loop < nc_tchain; loop++) {
+        for (int c = mtchain - 1; c > 0; c--) {
+            const double ex = exp(-nc * eighth * eta_dot[c + 1]);
+            eta_dot[c] = (eta_dot[c] * ex + eta_dotdot[c] * nc * quarter) * drag_f * ex;
+        }
+        double ex = exp(-nc * eighth * eta_dot[1]);
+        eta_dot[0] = (eta_dot[0] * ex + eta_dotdot[0] * nc * quarter) * drag_f * ex;
+        const double scale = exp(-nc * half * eta_dot[0]);
+        k_md_vscale<<<blocks_for(inum), TB>>>(v, scale, ilist, dim, inum);
+        count_launches(1);
+        tarray[4] *= scale * scale;
+        ke_now = tdof * boltz * tarray[4];
+        eta_dotdot[0] = eta_mass[0] > 0.0 ? (ke_now - ke_target) / eta_mass[0] : 0.0;
+        for (int c = 0; c < mtchain; c++) eta[c] += nc * half * eta_dot[c];
+        eta_dot[0] = (eta_dot[0] * ex + eta_dotdot[0] * nc * quarter) * ex;
+        for (int c = 1; c < mtchain; c++) {
+            ex = exp(-nc * eighth * eta_dot[c + 1]);
+            eta_dotdot[c] = (eta_mass[c - 1] * eta_dot[c - 1] * eta_dot[c - 1] - boltz * t_target) / eta_mass[c];
+            eta_dot[c] = (eta_dot[c] * ex + eta_dotdot[c] * nc * quarter) * ex;
+        }
+    }
+}
+
+static void verlet(const char *fn, int stage, double *x, double *v, const double *f, const double *mass,
+                   const double *dtarray, double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                   double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type, const int *ilist,
+                   int eta_mass_flag, int mtchain, int nc_tchain, int mode, int dim, int inum)
+{
+    if (mode < 0 || mode > 2) {
+        set_error("%s: mode %d is not supported; modes 0 (NVE), 1 (NVE limit) and 2 (NVT) are", fn, mode);
         return;
     }
     if (dim != 2 && dim != 3) { set_error("%s: dim must be 2 or 3", fn); return; }
     if (inum <= 0) return;
+    if (mode == 2 && (!tarray || !eta_mass || !eta || !eta_dot || !eta_dotdot || !ke || !tmp || mtchain < 1 ||
+                      nc_tchain < 1)) {
+        set_error("%s: NVT needs tarray, the eta arrays (mtchain + 1 entries), ke and tmp", fn);
+        return;
+    }
+    auto thermostat = [&]() -> int {
+        const double tfactor = tarray[8] / (tarray[5] * tarray[6]);   // mvv2e / (tdof boltz)
+        double t = 0.0;
+        if (temperature(t, ke, tmp, mass, v, tfactor, type, ilist, dim, inum)) return -1;
+        tarray[4] = t;
+        nose_hoover(v, ilist, dim, inum, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, eta_mass_flag, mtchain,
+                    nc_tchain);
+        return 0;
+    };
+    if (mode == 2 && stage == 0) {
+        // target temperature ramped over the run (cpuVelocityIntegration.cpp:602-628)
+        const double delta = (dtarray[5] - dtarray[3]) / (dtarray[4] - dtarray[3]);
+        tarray[3] = tarray[0] + delta * (tarray[1] - tarray[0]);
+        if (thermostat()) return;
+    }
     k_md_verlet<<<blocks_for(inum), TB>>>(x, v, f, mass, type, ilist, dtarray[1], dtarray[2], vlimitsq, mode == 1,
                                            stage, dim, inum);
     count_launches(1);
+    if (mode == 2 && stage == 1 && thermostat()) return;
     check_launch(fn);
 }
 
-// mdpgpucore.h:309-311 -- first half of velocity Verlet (dtarray on the host:
-// dtf = dtarray[1], dtv = dtarray[2])
+// mdpgpucore.h:309-311 -- first half of velocity Verlet.  dtarray (dt, dtf, dtv,
+// begin, end, current step), tarray (t_start, t_stop, t_freq, t_target,
+// t_current, tdof, boltz, drag, mvv2e) and the eta arrays live on the host, as
+// the reference reads them there; ke and tmp are device scratch of inum and 1
+// doubles, used by mode 2 (NVT, Nose-Hoover chain)
 void mdp_gpu_initial_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
-                                   const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                   double *tarray, double *eta_mass, double *eta, double *eta_dot,
                                    double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
                                    const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
                                    int mode, int dim, int inum)
 {
-    (void)tarray; (void)eta_mass; (void)eta; (void)eta_dot; (void)eta_dotdot; (void)ke; (void)tmp;
-    (void)eta_mass_flag; (void)biasflag; (void)mtchain; (void)nc_tchain;
-    verlet("gpuInitialIntegrate", 0, x, v, f, mass, dtarray, vlimitsq, type, ilist, mode, dim, inum);
+    (void)biasflag;
+    verlet("gpuInitialIntegrate", 0, x, v, f, mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, ke, tmp,
+           vlimitsq, type, ilist, eta_mass_flag, mtchain, nc_tchain, mode, dim, inum);
 }
 
 // mdpgpucore.h:313-315 -- second half of velocity Verlet
 void mdp_gpu_final_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *dtarray,
-                                 const double *tarray, double *eta_mass, double *eta, double *eta_dot,
+                                 double *tarray, double *eta_mass, double *eta, double *eta_dot,
                                  double *eta_dotdot, double *ke, double *tmp, double vlimitsq, const int *type,
                                  const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
                                  int mode, int dim, int inum)
 {
-    (void)tarray; (void)eta_mass; (void)eta; (void)eta_dot; (void)eta_dotdot; (void)ke; (void)tmp;
-    (void)eta_mass_flag; (void)biasflag; (void)mtchain; (void)nc_tchain;
-    verlet("gpuFinalIntegrate", 1, x, v, f, mass, dtarray, vlimitsq, type, ilist, mode, dim, inum);
+    (void)biasflag;
+    verlet("gpuFinalIntegrate", 1, x, v, f, mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, ke, tmp,
+           vlimitsq, type, ilist, eta_mass_flag, mtchain, nc_tchain, mode, dim, inum);
 }
 
 // mdpgpucore.h:321-322 -- wrap local atoms into the box, counting images

@@ -323,4 +323,20 @@ void ref_zbl_pairs(double *u, double *u_xij, const double *xij, int n)
                              nullptr, nullptr, 3, 0, 0, 0, 0, n, 1);
 }
 
+// MDP's NVT (Nose-Hoover chain) half steps, cpuVelocityIntegration.cpp:602-648
+void ref_nvt_initial(double *x, double *v, const double *f, const double *mass, double *dtarray, double *tarray,
+                     double *eta_mass, double *eta, double *eta_dot, double *eta_dotdot, const int *type,
+                     const int *ilist, int eta_mass_flag, int mtchain, int nc_tchain, int inum)
+{
+    cpuNVTInitialIntegrate(x, v, (double *)f, (double *)mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot,
+                           (int *)type, (int *)ilist, eta_mass_flag, 0, mtchain, nc_tchain, 3, inum);
+}
+void ref_nvt_final(double *x, double *v, const double *f, const double *mass, double *dtarray, double *tarray,
+                   double *eta_mass, double *eta, double *eta_dot, double *eta_dotdot, const int *type,
+                   const int *ilist, int eta_mass_flag, int mtchain, int nc_tchain, int inum)
+{
+    cpuNVTFinalIntegrate(x, v, (double *)f, (double *)mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot,
+                         (int *)type, (int *)ilist, eta_mass_flag, 0, mtchain, nc_tchain, 3, inum);
+}
+
 }  // extern "C"

@@ -298,3 +298,51 @@ def test_yi_per_atom_beta(cuda_lib, name):
         for k in (0, 1):
             scale = max(np.abs(want[k]).max(), 1e-300)
             assert np.abs(got[k][:, cols] - want[k][:, cols]).max() / scale < 1e-13
+
+
+def test_nvt_matches_reference(cuda_lib):
+    """Mode 2 (Nose-Hoover chain NVT) of the integrator entry points against
+    MDP's own cpuNVTInitialIntegrate / cpuNVTFinalIntegrate: five steps with a
+    ramped target temperature, a 3-link chain and two sub-steps, positions,
+    velocities, chain state and temperatures compared after every half step."""
+    L = lib()
+    R = refpy.lib()
+    R.ref_nvt_initial.argtypes = [P] * 12 + [C.c_int] * 4
+    R.ref_nvt_final.argtypes = [P] * 12 + [C.c_int] * 4
+    rng = np.random.default_rng(17)
+    n = 3000
+    x, v, f = rng.normal(size=(n, 3)) * 10, rng.normal(size=(n, 3)) * 4, rng.normal(size=(n, 3)) * 5
+    mass = np.array([0.0, 180.88, 92.9]); typ = rng.integers(1, 3, n).astype(np.int32)
+    ilist = rng.permutation(n).astype(np.int32)[: n - 50]
+    dt = 0.001
+    dtarray = np.array([dt, 0.5 * dt / 1.0364269e-4, dt, 0.0, 100.0, 0.0])
+    tarray = np.array([300.0, 600.0, 10.0, 0.0, 0.0, 3.0 * len(ilist) - 3.0, 8.617343e-5, 0.2, 1.0364269e-4])
+    mt, nc = 3, 2
+    chains = [np.zeros(mt + 1) for _ in range(4)]        # eta_mass, eta, eta_dot, eta_dotdot
+    ref = dict(x=x.copy(), v=v.copy(), d=dtarray.copy(), t=tarray.copy(), c=[a.copy() for a in chains])
+    ours = dict(d=dtarray.copy(), t=tarray.copy(), c=[a.copy() for a in chains])
+    dx, dv, df, dm, dt_, di = dev(x), dev(v), dev(f), dev(mass), dev(typ), dev(ilist)
+    ke, tmp = dev(np.zeros(n)), dev(np.zeros(8))
+    hp = lambda a: C.c_void_p(a.ctypes.data)
+
+    def ours_half(fn):
+        fn(ptr(dx), ptr(dv), ptr(df), ptr(dm), hp(ours["d"]), hp(ours["t"]), *[hp(a) for a in ours["c"]],
+           ptr(ke), ptr(tmp), 0.0, ptr(dt_), ptr(di), 1, 0, mt, nc, 2, 3, len(ilist))
+        sync()
+
+    def ref_half(fn):
+        fn(hp(ref["x"]), hp(ref["v"]), hp(f), hp(mass), hp(ref["d"]), hp(ref["t"]), *[hp(a) for a in ref["c"]],
+           hp(typ), hp(ilist), 1, mt, nc, len(ilist))
+
+    for step in range(1, 6):
+        ours["d"][5] = ref["d"][5] = float(step)
+        for mine, theirs in ((L.mdp_gpu_initial_integrate_f64, R.ref_nvt_initial),
+                             (L.mdp_gpu_final_integrate_f64, R.ref_nvt_final)):
+            ours_half(mine)
+            ref_half(theirs)
+            assert np.abs(dv.cpu().numpy() - ref["v"]).max() <= 1e-12 * np.abs(ref["v"]).max()
+            assert np.abs(dx.cpu().numpy() - ref["x"]).max() <= 1e-12 * np.abs(ref["x"]).max()
+            assert np.allclose(ours["t"], ref["t"], rtol=1e-12, atol=0)
+            for a, b in zip(ours["c"], ref["c"]):
+                assert np.allclose(a, b, rtol=1e-10, atol=1e-14)
+    assert ref["c"][2][0] != 0.0          # the chain moved
