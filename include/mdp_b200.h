@@ -211,6 +211,13 @@ int mdp_fit_ncoeff(mdp_fit *h);
  * targets e[c], f (3 per atom) and weights we[c], wf[c] may be NULL */
 int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *box, const double *x,
                       const double *e, const double *f, const double *we, const double *wf);
+/* the same for general (triclinic) periodic cells: lattice[9c..9c+8] holds the
+ * cell vectors a, b, c of configuration c as rows, and x lies inside the cell;
+ * every perpendicular cell width must exceed the cutoff.  Serves the real-data
+ * fits of MDP's fitting/snap/Ta/fitsnap.jl:107-159, whose configurations
+ * (readJSON.jl "Lattice") are sheared and surface cells. */
+int mdp_fit_set_batch_lattice(mdp_fit *h, int nconf, const int *natoms, const double *lattice, const double *x,
+                              const double *e, const double *f, const double *we, const double *wf);
 long long mdp_fit_npairs(mdp_fit *h);
 /* scratch budget of the chunked stages (default 24e9 bytes; the batch is
  * processed in configuration-aligned chunks that fit it) and the chunk count */

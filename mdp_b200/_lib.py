@@ -106,6 +106,8 @@ def lib():
     L.mdp_fit_ncoeff.argtypes = [C.c_void_p]
     L.mdp_fit_set_batch.argtypes = [C.c_void_p, C.c_int, _ip32, _dp, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p]
+    L.mdp_fit_set_batch_lattice.argtypes = [C.c_void_p, C.c_int, _ip32, _dp, _dp, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, C.c_void_p]
     L.mdp_fit_npairs.argtypes = [C.c_void_p]
     L.mdp_fit_npairs.restype = C.c_longlong
     L.mdp_fit_set_chunk_bytes.argtypes = [C.c_void_p, C.c_double]

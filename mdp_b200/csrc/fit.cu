@@ -1,8 +1,9 @@
 // Batched SNAP descriptors, dB/dR and the linear-fit normal equations.
 //
-// For a batch of periodic configurations (orthogonal boxes, every width at
-// least rcut + skin so that one shell of images holds every pair, as MDP's
-// cpuPeriodicImages3D assumes) this computes what MDP's ComputeSnap
+// For a batch of periodic configurations (general triclinic cells given by
+// three lattice vectors, every perpendicular width above rcut so that one
+// shell of images holds every pair, as MDP's cpuPeriodicImages3D assumes)
+// this computes what MDP's ComputeSnap
 // (snappotential.cpp:762-910, cpuSnap2.cpp) computes per configuration:
 //   bi[k]          = sum_i B_ik
 //   G[i][c][k]     = d(sum_a B_ak)/dx_ic  (= -bd of cpuSnapTallyBispectrumDeriv)
@@ -43,12 +44,15 @@ __global__ void k_fit_pairs(const double4 *__restrict__ x, const int *__restrict
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= natoms) return;
     const int c = cfg[i], a0 = ca0[c], n = cn[c];
-    const double4 L = cbox[c], xi = x[i];
+    // lattice vectors a, b, c of the configuration's cell (rows of cbox)
+    const double4 la = cbox[3 * c], lb = cbox[3 * c + 1], lc = cbox[3 * c + 2], xi = x[i];
     int cnt = 0, p = EMIT ? poff[i] : 0;
     for (int jj = 0; jj < n; jj++) {
         const double4 xj = x[a0 + jj];
         for (int im = 0; im < 27; im++) {
-            const double sx = (im % 3 - 1) * L.x, sy = ((im / 3) % 3 - 1) * L.y, sz = (im / 9 - 1) * L.z;
+            const double u = im % 3 - 1, v = (im / 3) % 3 - 1, w = im / 9 - 1;
+            const double sx = u * la.x + v * lb.x + w * lc.x, sy = u * la.y + v * lb.y + w * lc.y,
+                         sz = u * la.z + v * lb.z + w * lc.z;
             const double d0 = xj.x + sx - xi.x, d1 = xj.y + sy - xi.y, d2 = xj.z + sz - xi.z;
             const double rsq = d0 * d0 + d1 * d1 + d2 * d2;
             if (rsq < gp.rcutsq && rsq > 1e-20) {
@@ -953,14 +957,14 @@ void mdp_fit_destroy(mdp_fit *h)
 
 int mdp_fit_ncoeff(mdp_fit *h) { return h ? h->tab.ntri : -1; }
 
-// Batch of nconf configurations: natoms[c], box[3c..3c+2] (orthogonal box
-// lengths), x (all positions concatenated, 3 per atom, inside [0, L)),
-// targets e[c] and f (3 per atom), weights we[c], wf[c] (any of e, f, we, wf
-// may be NULL: zero targets, unit weights).  Builds the pair lists.
-int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *box, const double *x,
-                      const double *e, const double *f, const double *we, const double *wf)
+// Batch of nconf configurations: natoms[c], lattice[9c..9c+8] (the cell's
+// vectors a, b, c as rows), x (all positions concatenated, 3 per atom, inside
+// the cell), targets e[c] and f (3 per atom), weights we[c], wf[c] (any of e,
+// f, we, wf may be NULL: zero targets, unit weights).  Builds the pair lists.
+int mdp_fit_set_batch_lattice(mdp_fit *h, int nconf, const int *natoms, const double *lattice, const double *x,
+                              const double *e, const double *f, const double *we, const double *wf)
 {
-    if (!h || nconf < 1 || !natoms || !box || !x) { set_error("bad arguments"); return -1; }
+    if (!h || nconf < 1 || !natoms || !lattice || !x) { set_error("bad arguments"); return -1; }
     MDP_CUDA_TRY(cudaSetDevice(h->device));
     const double need = h->model.geom.rcut;
     long total = 0;
@@ -968,12 +972,18 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
     h->h_ca0.resize(nconf);
     for (int c = 0; c < nconf; c++) {
         if (natoms[c] < 1) { set_error("configuration %d has no atoms", c); return -1; }
-        for (int d = 0; d < 3; d++)
-            if (!(box[3 * c + d] > need)) {
-                set_error("configuration %d: box length %g must exceed the cutoff %g (one image shell)", c,
-                          box[3 * c + d], need);
+        // perpendicular width of the cell across each lattice vector: |volume| / |cross of the other two|
+        const double *L = lattice + 9 * (size_t)c;
+        for (int d = 0; d < 3; d++) {
+            const double *p = L + 3 * ((d + 1) % 3), *q = L + 3 * ((d + 2) % 3), *r = L + 3 * d;
+            const double cx = p[1] * q[2] - p[2] * q[1], cy = p[2] * q[0] - p[0] * q[2], cz = p[0] * q[1] - p[1] * q[0];
+            const double width = fabs(r[0] * cx + r[1] * cy + r[2] * cz) / sqrt(cx * cx + cy * cy + cz * cz);
+            if (!(width > need)) {
+                set_error("configuration %d: cell width %g across lattice vector %d must exceed the cutoff %g "
+                          "(one image shell)", c, width, d, need);
                 return -1;
             }
+        }
         h->h_ca0[c] = (int)total;
         total += natoms[c];
     }
@@ -982,15 +992,16 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
     h->nconf = nconf;
     h->natoms = (int)total;
     const int n = h->natoms;
-    std::vector<double> x4(4 * (size_t)n), b4(4 * (size_t)nconf);
+    std::vector<double> x4(4 * (size_t)n), b4(12 * (size_t)nconf, 0.0);
     std::vector<int> cid(n);
     for (int c = 0; c < nconf; c++) {
-        b4[4 * c] = box[3 * c]; b4[4 * c + 1] = box[3 * c + 1]; b4[4 * c + 2] = box[3 * c + 2]; b4[4 * c + 3] = 0.0;
+        for (int r = 0; r < 3; r++)
+            for (int d = 0; d < 3; d++) b4[12 * c + 4 * r + d] = lattice[9 * c + 3 * r + d];
         for (int a = 0; a < natoms[c]; a++) cid[h->h_ca0[c] + a] = c;
     }
     for (long i = 0; i < n; i++) { x4[4 * i] = x[3 * i]; x4[4 * i + 1] = x[3 * i + 1]; x4[4 * i + 2] = x[3 * i + 2]; x4[4 * i + 3] = 0.0; }
     if (h->x.ensure(sizeof(double4) * n) || h->cfg.ensure(sizeof(int) * n) || h->ca0.ensure(sizeof(int) * nconf) ||
-        h->cn.ensure(sizeof(int) * nconf) || h->cbox.ensure(sizeof(double4) * nconf) ||
+        h->cn.ensure(sizeof(int) * nconf) || h->cbox.ensure(3 * sizeof(double4) * nconf) ||
         h->we.ensure(sizeof(double) * nconf) || h->wf.ensure(sizeof(double) * nconf) ||
         h->e.ensure(sizeof(double) * nconf) || h->f.ensure(sizeof(double) * 3 * (size_t)n))
         return -1;
@@ -999,7 +1010,7 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
     MDP_CUDA_TRY(cudaMemcpy(h->cfg.p, cid.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->ca0.p, h->h_ca0.data(), sizeof(int) * nconf, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->cn.p, natoms, sizeof(int) * nconf, cudaMemcpyHostToDevice));
-    MDP_CUDA_TRY(cudaMemcpy(h->cbox.p, b4.data(), sizeof(double4) * nconf, cudaMemcpyHostToDevice));
+    MDP_CUDA_TRY(cudaMemcpy(h->cbox.p, b4.data(), 3 * sizeof(double4) * nconf, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->we.p, we ? we : ones.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->wf.p, wf ? wf : ones.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
     MDP_CUDA_TRY(cudaMemcpy(h->e.p, e ? e : zc.data(), sizeof(double) * nconf, cudaMemcpyHostToDevice));
@@ -1009,6 +1020,17 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
     MDP_CUDA_TRY(cudaDeviceSynchronize());
     if (fit_pairs(h) || fit_alloc_work(h)) return -1;
     return 0;
+}
+
+// Orthogonal cells: box[3c..3c+2] are the edge lengths, x inside [0, L).
+int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *box, const double *x,
+                      const double *e, const double *f, const double *we, const double *wf)
+{
+    if (!h || nconf < 1 || !natoms || !box || !x) { set_error("bad arguments"); return -1; }
+    std::vector<double> lat(9 * (size_t)nconf, 0.0);
+    for (int c = 0; c < nconf; c++)
+        for (int d = 0; d < 3; d++) lat[9 * c + 4 * d] = box[3 * c + d];
+    return mdp_fit_set_batch_lattice(h, nconf, natoms, lat.data(), x, e, f, we, wf);
 }
 
 long long mdp_fit_npairs(mdp_fit *h) { return h ? h->npairs : -1; }

@@ -1,0 +1,192 @@
+"""Training data of MDP's SNAP fits and the weighted linear fit over it.
+
+Readers:
+  read_json          one file of MDP's JSON training format (readJSON.jl:8-165):
+                     text before the first '{' is skipped, frames are
+                     Dataset.Data[*] with NumAtoms, Lattice (cell vectors as
+                     rows), Positions, Forces, Energy, Stress and AtomTypes
+                     (mapped to 1-based indices of `species`; unknown types
+                     keep type 1, as the reference does)
+  read_json_folder   every file of a folder in name order, frames appended
+                     (readJSONfromFolder.jl:8-190)
+
+Fit (fit_groups) follows MDP's fitting/snap/Ta/fitsnap.jl:107-159 with the
+"lsq" method of linearfit2 (Optimization/linearfit.jl:355-470): each group of
+frames (one data folder) carries an energy weight and a force weight that
+multiply its rows (applyweight); energies are divided by the atom count when
+normalize_energy is set; the normal equations of all groups are summed and
+solved.  The rows are the batched GPU pipeline's (mdp_fit_run): per frame one
+energy row [N, sum_i B_i] and one row per force component [0, d(sum B)/dx],
+with the one-body column N standing in for the reference's "single"
+descriptor.  Not included: stress rows and the ZBL reference potential that
+fitsnap.jl subtracts from the targets.
+
+Cells narrower than the cutoff (the 2- and 4-atom Elastic / Volume cells)
+are replicated along each short cell vector until every perpendicular width
+exceeds the cutoff, which is what the batched pipeline's single image shell
+needs; the copies reproduce every neighbour of the original cell, so each
+atom's descriptors are unchanged.  A frame replicated m times enters with
+its energy row per atom (the same row as the original) and its force rows
+scaled by 1/sqrt(m), so it adds exactly what the original frame would.
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+
+import numpy as np
+
+from . import fit as _fit
+from .configs import SnapParams
+
+
+@dataclasses.dataclass
+class Frame:
+    natoms: int
+    lattice: np.ndarray            # (3, 3) cell vectors as rows
+    x: np.ndarray                  # (N, 3)
+    e: float | None = None         # total energy (eV)
+    f: np.ndarray | None = None    # (N, 3) forces (eV/A)
+    stress: np.ndarray | None = None
+    types: np.ndarray | None = None  # (N,) 1-based species index
+    source: str = ""
+
+
+def _frames_of(text: str, species, source: str):
+    i1 = text.find("{")
+    if i1 < 0:
+        raise ValueError(f"{source}: no JSON object")
+    data = json.loads(text[i1:])["Dataset"]["Data"]
+    out = []
+    for d in data:
+        x = np.asarray(d["Positions"], dtype=np.float64).reshape(-1, 3)
+        n = int(d.get("NumAtoms", x.shape[0]))
+        if n != x.shape[0]:
+            raise ValueError(f"{source}: NumAtoms {n} but {x.shape[0]} positions")
+        lat = np.asarray(d["Lattice"], dtype=np.float64).reshape(3, 3)
+        e = d.get("Energy")
+        e = None if e is None else float(np.asarray(e, dtype=np.float64).ravel()[0])
+        f = d.get("Forces")
+        f = None if f is None else np.asarray(f, dtype=np.float64).reshape(n, 3)
+        st = d.get("Stress")
+        st = None if st is None else np.asarray(st, dtype=np.float64).reshape(3, 3)
+        types = np.ones(n, dtype=np.int32)
+        if "AtomTypes" in d:
+            names = list(d["AtomTypes"])
+            for k, s in enumerate(species):
+                types[[i for i, t in enumerate(names) if t == s]] = k + 1
+        out.append(Frame(natoms=n, lattice=lat, x=x, e=e, f=f, stress=st, types=types, source=source))
+    return out
+
+
+def read_json(path: str, species=("Ta",)) -> list[Frame]:
+    """Frames of one JSON training file (readJSON.jl:8-165)."""
+    with open(path) as fh:
+        return _frames_of(fh.read(), species, path)
+
+
+def read_json_folder(folder: str, species=("Ta",), extension: str = "json") -> list[Frame]:
+    """Frames of every file of `folder` with the extension, in name order
+    (readJSONfromFolder.jl:8-190 walks readdir, which sorts)."""
+    out = []
+    for name in sorted(os.listdir(folder)):
+        if name.endswith("." + extension):
+            out.extend(read_json(os.path.join(folder, name), species))
+    if not out:
+        raise ValueError(f"{folder}: no .{extension} files")
+    return out
+
+
+def cell_widths(lattice: np.ndarray) -> np.ndarray:
+    """Perpendicular width of the cell across each of its vectors."""
+    H = np.asarray(lattice, dtype=np.float64)
+    vol = abs(np.linalg.det(H))
+    return np.array([vol / np.linalg.norm(np.cross(H[(k + 1) % 3], H[(k + 2) % 3])) for k in range(3)])
+
+
+def wrap(x: np.ndarray, lattice: np.ndarray) -> np.ndarray:
+    """Positions mapped into the cell (fractional coordinates in [0, 1))."""
+    H = np.asarray(lattice, dtype=np.float64)
+    s = x @ np.linalg.inv(H)
+    s -= np.floor(s)
+    s[s >= 1.0] = 0.0
+    return s @ H
+
+
+def replicate(frame: Frame, rcut: float):
+    """(FitConfig, copies): the frame's cell repeated along each vector until
+    every perpendicular width exceeds rcut, the original atoms first."""
+    H = np.asarray(frame.lattice, dtype=np.float64)
+    reps = np.maximum(1, np.floor(rcut / cell_widths(H)).astype(int) + 1)
+    x0 = wrap(frame.x, H)
+    shifts = [i * H[0] + j * H[1] + k * H[2]
+              for k in range(reps[2]) for j in range(reps[1]) for i in range(reps[0])]
+    x = np.concatenate([x0 + s for s in shifts])
+    big = H * reps[:, None]
+    return _fit.FitConfig(x=x, box=big, kind=frame.source), int(np.prod(reps))
+
+
+@dataclasses.dataclass
+class Group:
+    """One data folder: its frames and the weights of its energy and force rows."""
+    name: str
+    frames: list
+    we: float = 1.0
+    wf: float = 1.0
+
+
+def batch_of(groups, rcut: float, normalize_energy: bool = True):
+    """(configs, e, f, we, wf, copies, group index) for set_batch."""
+    cfgs, e, f, we, wf, copies, gid = [], [], [], [], [], [], []
+    for g, grp in enumerate(groups):
+        for fr in grp.frames:
+            cfg, m = replicate(fr, rcut)
+            cfgs.append(cfg)
+            copies.append(m)
+            gid.append(g)
+            e.append(m * (fr.e if fr.e is not None else 0.0))
+            ff = fr.f if fr.f is not None else np.zeros((fr.natoms, 3))
+            f.append(np.tile(ff, (m, 1)))
+            we.append(grp.we / (cfg.natoms if normalize_energy else m))
+            wf.append(grp.wf / np.sqrt(m))
+    return (cfgs, np.array(e), np.concatenate(f), np.array(we), np.array(wf), np.array(copies),
+            np.array(gid))
+
+
+def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, mode: str = "fp64", device: int = 0):
+    """Solve the weighted linear SNAP fit over the groups on the GPU.
+
+    Returns beta (1 + ncoeff: the one-body term, then the bispectrum
+    coefficients), the normal equations, and per group the unweighted energy
+    (per atom) and force MAE / RMSE of the fitted model, as
+    validate2 reports them (maespace.jl:210)."""
+    cfgs, e, f, we, wf, copies, gid = batch_of(groups, params.rcut, normalize_energy)
+    bf = _fit.BatchFit(params, device)
+    try:
+        bf.set_batch(cfgs, e, f, we, wf)
+        A, b, ms = bf.run(mode)
+        bi, bd, _, _ = bf.descriptors()
+    finally:
+        bf.close()
+    try:
+        beta = _fit.solve(A, b)
+    except np.linalg.LinAlgError:
+        beta = np.linalg.lstsq(A, b, rcond=None)[0]
+    counts = np.array([c.natoms for c in cfgs])
+    a0 = np.concatenate([[0], np.cumsum(counts)])
+    e_pred = beta[0] * counts + bi @ beta[1:]
+    errors = []
+    for g, grp in enumerate(groups):
+        de, dfs = [], []
+        for c in np.nonzero(gid == g)[0]:
+            n0 = counts[c] // copies[c]
+            de.append((e_pred[c] - e[c]) / counts[c])
+            fp = bd[a0[c]:a0[c] + n0] @ beta[1:]
+            dfs.append((fp - f[a0[c]:a0[c] + n0]).ravel())
+        de, dfs = np.array(de), np.concatenate(dfs)
+        errors.append(dict(group=grp.name, frames=len(de),
+                           energy_mae=float(np.abs(de).mean()), energy_rmse=float(np.sqrt((de ** 2).mean())),
+                           force_mae=float(np.abs(dfs).mean()), force_rmse=float(np.sqrt((dfs ** 2).mean()))))
+    return dict(beta=beta, A=A, b=b, graph_ms=ms, errors=errors, configs=len(cfgs),
+                atoms=int(counts.sum()), replicated=int((copies > 1).sum()))

@@ -31,8 +31,8 @@ MIN_WIDTH = 4.67637 + 1.0
 
 @dataclasses.dataclass
 class FitConfig:
-    x: np.ndarray      # (N, 3) in [0, L)
-    box: np.ndarray    # (3,)
+    x: np.ndarray      # (N, 3) inside the cell
+    box: np.ndarray    # (3,) edge lengths of an orthogonal cell, or (3, 3) cell vectors a, b, c as rows
     kind: str
 
     @property
@@ -83,6 +83,12 @@ def batch_configs(nconf: int = 4096, seed: int = 2024, lo: int = 16, hi: int = 5
     return cfgs, e, f
 
 
+def cell_vectors(box) -> np.ndarray:
+    """(3, 3) cell vectors as rows, from edge lengths (3,) or vectors (3, 3)."""
+    b = np.asarray(box, dtype=np.float64)
+    return np.diag(b) if b.shape == (3,) else b.reshape(3, 3)
+
+
 class BatchFit:
     """Device state of one batch (ctypes handle over mdp_fit_*)."""
 
@@ -109,11 +115,16 @@ class BatchFit:
 
     def set_batch(self, cfgs, e=None, f=None, we=None, wf=None):
         n = np.array([c.natoms for c in cfgs], dtype=np.int32)
-        box = np.ascontiguousarray(np.stack([c.box for c in cfgs]), dtype=np.float64)
         x = np.ascontiguousarray(np.concatenate([c.x for c in cfgs]), dtype=np.float64)
         keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (e, f, we, wf)]
         ptr = [None if a is None else a.ctypes.data for a in keep]
-        _lib.check(_lib.lib().mdp_fit_set_batch(self._h, len(cfgs), n, box, x, *ptr), "mdp_fit_set_batch")
+        if all(np.shape(c.box) == (3,) for c in cfgs):
+            box = np.ascontiguousarray(np.stack([c.box for c in cfgs]), dtype=np.float64)
+            _lib.check(_lib.lib().mdp_fit_set_batch(self._h, len(cfgs), n, box, x, *ptr), "mdp_fit_set_batch")
+        else:
+            lat = np.ascontiguousarray(np.stack([cell_vectors(c.box) for c in cfgs]), dtype=np.float64)
+            _lib.check(_lib.lib().mdp_fit_set_batch_lattice(self._h, len(cfgs), n, lat, x, *ptr),
+                       "mdp_fit_set_batch_lattice")
         self.nconf, self.natoms = len(cfgs), int(n.sum())
         self.counts = n
 

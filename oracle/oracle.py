@@ -67,7 +67,10 @@ def neighbor_list(x_local, box, rcut, skin, neighmax=64):
     alist = np.zeros(anummax, dtype=np.int32)
     nl = np.zeros(inum * neighmax, dtype=np.int32)
     nn = np.zeros(inum, dtype=np.int32)
-    a = np.array([box[0], 0.0, 0.0]); b = np.array([0.0, box[1], 0.0]); c = np.array([0.0, 0.0, box[2]])
+    B = np.asarray(box, dtype=np.float64)
+    if B.shape == (3,):
+        B = np.diag(B)
+    a, b, c = (np.ascontiguousarray(B[k]) for k in range(3))   # cell vectors as rows
     anum = lib().orc_neighbor_list(x, alist, nl, nn, a, b, c, rcut + skin, inum, neighmax, anummax)
     if anum == -1:
         raise RuntimeError("ghost capacity exceeded")

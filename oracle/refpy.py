@@ -53,7 +53,10 @@ def lib():
 
 
 def box_setup(box, rcut_skin):
-    a = np.array([box[0], 0.0, 0.0]); b = np.array([0.0, box[1], 0.0]); c = np.array([0.0, 0.0, box[2]])
+    B = np.asarray(box, dtype=np.float64)
+    if B.shape == (3,):
+        B = np.diag(B)
+    a, b, c = (np.ascontiguousarray(B[k]) for k in range(3))   # cell vectors as rows
     off = np.full(3, float(rcut_skin))
     pbc = np.ones(3, dtype=np.int32)
     s2r = np.zeros(9); rbv = np.zeros(24); pim = np.zeros(81)

@@ -107,12 +107,34 @@ FIT_CASES = [
 ]
 
 
-def fit_fixtures():
-    """Per configuration: positions, box and the reference's bi, bd, bv, blist."""
+# triclinic descriptor fixtures: as FIT_CASES plus the tilts (xy, xz, yz) as
+# fractions of the edge lengths; the cell vectors are a = (Lx, 0, 0),
+# b = (xy Lx, Ly, 0), c = (xz Lx, yz Ly, Lz) and the atoms keep their
+# fractional coordinates
+TRI_FIT_CASES = [
+    ("fit_bcc54_tri_2j8", "bcc", 54, 0.02, 0.10, 35, 8, {}, (0.12, -0.08, 0.05)),
+    ("fit_fcc108_tri_2j6", "fcc", 108, -0.03, 0.25, 36, 6, {"bnormflag": 1}, (-0.10, 0.06, 0.15)),
+]
+
+
+def sheared(cfg, tilt):
+    """The configuration in the sheared cell of the tilts (xy, xz, yz)."""
     from mdp_b200 import fit
-    for (name, kind, target, strain, sigma, seed, tj, flags) in FIT_CASES:
+    L = np.asarray(cfg.box, dtype=np.float64)
+    H = np.array([[L[0], 0.0, 0.0], [tilt[0] * L[0], L[1], 0.0], [tilt[1] * L[0], tilt[2] * L[1], L[2]]])
+    return fit.FitConfig(x=(cfg.x / L) @ H, box=H, kind=cfg.kind)
+
+
+def fit_fixtures():
+    """Per configuration: positions, box (edge lengths or cell vectors as rows)
+    and the reference's bi, bd, bv, blist."""
+    from mdp_b200 import fit
+    cases = [c + ((0.0, 0.0, 0.0),) for c in FIT_CASES] + TRI_FIT_CASES
+    for (name, kind, target, strain, sigma, seed, tj, flags, tilt) in cases:
         rng = np.random.default_rng(seed)
         cfg = fit.make_config(kind, target, strain, sigma, rng)
+        if any(tilt):
+            cfg = sheared(cfg, tilt)
         p = configs.snap_params(tj, seed=0, **flags)
         xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
         bi, bd, bv, bl = refpy.snap_descriptors(xa, al, nl, nn, p)

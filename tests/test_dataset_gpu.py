@@ -1,0 +1,58 @@
+"""GPU: the real-data linear fit (mdp_b200.dataset.fit_groups) end to end.
+
+Training files in MDP's JSON format are written for two groups of frames --
+narrow sheared 2-atom BCC cells (replicated to cover the cutoff) and sheared
+16-54 atom supercells -- with energies and forces of a known linear SNAP
+model from the oracle.  Reading them back and fitting on the GPU must
+recover the model: the fitted energies and forces match the targets and the
+coefficients match the known ones."""
+import numpy as np
+import pytest
+
+from mdp_b200 import configs, dataset, fit
+from oracle import oracle
+from test_dataset_cpu import bcc2, write_json
+
+pytestmark = pytest.mark.gpu
+
+
+def _targets(fr, p):
+    cfg, m = dataset.replicate(fr, p.rcut)
+    xa, al, nl, nn = oracle.neighbor_list(cfg.x, cfg.box, p.rcut, 1.0, 96)
+    e, f, _ = oracle.snap_force(xa, al, nl, nn, p)
+    fr.e, fr.f = float(e.sum() / m), f[:fr.natoms].copy()
+    return fr
+
+
+def _frames(p):
+    rng = np.random.default_rng(11)
+    narrow = [_targets(bcc2(a=3.316 * (1 + rng.uniform(-0.04, 0.04)), tilt=tuple(rng.uniform(-0.1, 0.1, 3)),
+                            jitter=0.08, seed=s), p) for s in range(6)]
+    bulk = []
+    for s, (kind, n) in enumerate([("bcc", 16), ("fcc", 32), ("a15", 64), ("bcc", 54), ("fcc", 32), ("bcc", 16)]):
+        cfg = fit.make_config(kind, n, rng.uniform(-0.04, 0.04), rng.uniform(0.05, 0.25), rng)
+        L = np.asarray(cfg.box)
+        t = rng.uniform(-0.1, 0.1, 3)
+        H = np.array([[L[0], 0, 0], [t[0] * L[0], L[1], 0], [t[1] * L[0], t[2] * L[1], L[2]]])
+        bulk.append(_targets(dataset.Frame(natoms=cfg.natoms, lattice=H, x=(cfg.x / L) @ H), p))
+    return narrow, bulk
+
+
+def test_fit_recovers_known_model_from_json(tmp_path):
+    p = configs.snap_params(6, seed=21)
+    narrow, bulk = _frames(p)
+    (tmp_path / "Narrow").mkdir()
+    (tmp_path / "Bulk").mkdir()
+    for i, fr in enumerate(narrow):
+        write_json(tmp_path / "Narrow" / f"N_{i}.json", [fr])
+    write_json(tmp_path / "Bulk" / "B.json", bulk)
+    groups = [dataset.Group("Narrow", dataset.read_json_folder(str(tmp_path / "Narrow")), we=100.0, wf=1.0),
+              dataset.Group("Bulk", dataset.read_json_folder(str(tmp_path / "Bulk")), we=1.0, wf=1.0)]
+    out = dataset.fit_groups(groups, p)
+    assert out["replicated"] == 6
+    for err in out["errors"]:
+        assert err["energy_rmse"] < 1e-6, err        # eV/atom
+        assert err["force_rmse"] < 1e-6, err         # eV/A
+    beta = out["beta"]
+    assert abs(beta[0] - p.coeff[0]) < 1e-6 * abs(p.coeff[0])
+    assert np.max(np.abs(beta[1:] - p.coeff[1:])) < 1e-4 * np.max(np.abs(p.coeff[1:]))

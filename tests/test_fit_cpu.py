@@ -15,9 +15,13 @@ import make_golden  # noqa: E402
 
 @pytest.mark.parametrize("name", fit_names())
 def test_fixture_inputs_regenerate(name):
-    case = {c[0]: c for c in make_golden.FIT_CASES}[name]
-    _, kind, target, strain, sigma, seed, tj, flags = case
+    cases = {c[0]: c + ((0.0, 0.0, 0.0),) for c in make_golden.FIT_CASES}
+    cases.update({c[0]: c for c in make_golden.TRI_FIT_CASES})
+    _, kind, target, strain, sigma, seed, tj, flags, tilt = cases[name]
     cfg = fit.make_config(kind, target, strain, sigma, np.random.default_rng(seed))
+    if any(tilt):
+        cfg = make_golden.sheared(cfg, tilt)
+        assert cfg.box.shape == (3, 3)
     d = np.load(os.path.join(GOLDEN, name + ".npz"))
     assert np.array_equal(cfg.x, d["x"]) and np.array_equal(cfg.box, d["box"])
 
