@@ -9,6 +9,11 @@ Readers:
                      keep type 1, as the reference does)
   read_json_folder   every file of a folder in name order, frames appended
                      (readJSONfromFolder.jl:8-190)
+  read_extxyz        extended-XYZ files (readEXTXYZ.jl): per frame an atom
+                     count, a comment line of key=value pairs (Lattice as
+                     nine numbers, a, b, c in turn; energy; stress; pbc;
+                     Properties=name:type:columns...) and one line per atom
+                     with the Properties columns (species, pos, forces used)
 
 Fit (fit_groups) follows MDP's fitting/snap/Ta/fitsnap.jl:107-159 with the
 "lsq" method of linearfit2 (Optimization/linearfit.jl:355-470): each group of
@@ -34,6 +39,7 @@ from __future__ import annotations
 import dataclasses
 import json
 import os
+import re
 
 import numpy as np
 
@@ -89,10 +95,64 @@ def read_json(path: str, species=("Ta",)) -> list[Frame]:
 def read_json_folder(folder: str, species=("Ta",), extension: str = "json") -> list[Frame]:
     """Frames of every file of `folder` with the extension, in name order
     (readJSONfromFolder.jl:8-190 walks readdir, which sorts)."""
+    return read_folder(folder, species, extension)
+
+
+_KV = re.compile(r'([A-Za-z_][\w-]*)\s*=\s*("([^"]*)"|\S+)')
+
+
+def _comment_fields(line: str) -> dict:
+    return {m.group(1).lower(): (m.group(3) if m.group(3) is not None else m.group(2))
+            for m in _KV.finditer(line)}
+
+
+def read_extxyz(path: str, species=("Ta",)) -> list[Frame]:
+    """Frames of one extended-XYZ file (readEXTXYZ.jl)."""
+    with open(path) as fh:
+        lines = [ln for ln in fh.read().splitlines()]
+    out, m = [], 0
+    while m < len(lines):
+        if not lines[m].strip():
+            m += 1
+            continue
+        n = int(lines[m].split()[0])
+        kv = _comment_fields(lines[m + 1])
+        if "lattice" not in kv or "properties" not in kv:
+            raise ValueError(f"{path}: frame at line {m + 1} lacks Lattice or Properties")
+        lat = np.array(kv["lattice"].split(), dtype=np.float64).reshape(3, 3)
+        props = kv["properties"].split(":")
+        if len(props) % 3:
+            raise ValueError(f"{path}: bad Properties {kv['properties']}")
+        if m + 2 + n > len(lines):
+            raise ValueError(f"{path}: frame at line {m + 1} is truncated")
+        rows = [lines[m + 2 + i].split() for i in range(n)]
+        cols, c0 = {}, 0
+        for k in range(0, len(props), 3):
+            name, typ, width = props[k].lower(), props[k + 1].upper(), int(props[k + 2])
+            cols[name] = (typ, [r[c0:c0 + width] for r in rows])
+            c0 += width
+        x = np.array(cols["pos"][1], dtype=np.float64).reshape(n, 3)
+        f = np.array(cols["forces"][1], dtype=np.float64).reshape(n, 3) if "forces" in cols else None
+        types = np.ones(n, dtype=np.int32)
+        if "species" in cols:
+            names = [r[0] for r in cols["species"][1]]
+            for k, sp in enumerate(species):
+                types[[i for i, t in enumerate(names) if t == sp]] = k + 1
+        e = float(kv["energy"]) if "energy" in kv else None
+        st = np.array(kv["stress"].split(), dtype=np.float64).reshape(3, 3) if "stress" in kv else None
+        out.append(Frame(natoms=n, lattice=lat, x=x, e=e, f=f, stress=st, types=types, source=path))
+        m += 2 + n
+    return out
+
+
+def read_folder(folder: str, species=("Ta",), extension: str = "json") -> list[Frame]:
+    """Frames of every file of `folder` with the extension, in name order;
+    "json" files go through read_json, "xyz" / "extxyz" through read_extxyz."""
+    reader = read_json if extension == "json" else read_extxyz
     out = []
     for name in sorted(os.listdir(folder)):
         if name.endswith("." + extension):
-            out.extend(read_json(os.path.join(folder, name), species))
+            out.extend(reader(os.path.join(folder, name), species))
     if not out:
         raise ValueError(f"{folder}: no .{extension} files")
     return out

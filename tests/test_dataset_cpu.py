@@ -78,14 +78,14 @@ def test_replication_covers_cutoff_and_keeps_atoms_first():
 
 def test_replicated_energy_per_atom_is_invariant():
     """The replicated cell reproduces the narrow cell's physics: energy per atom
-    and the original atoms' forces are the same for m and 2m copies."""
+    and the original atoms' forces are the same for m and 27m copies."""
     p = configs.snap_params(4, seed=5)
     fr = bcc2(tilt=(0.07, 0.0, -0.04), jitter=0.08, seed=4)
     res = []
     for scale in (1, 2):
         cfg, m = dataset.replicate(fr, p.rcut)
         H = cfg.box
-        if scale == 2:                                    # one more copy along a
+        if scale == 2:                                    # three copies along each vector
             cfg = dataset.replicate(dataset.Frame(natoms=cfg.natoms, lattice=H, x=cfg.x), 2.0 * np.linalg.norm(H[0]))[0]
         xa, al, nl, nn = oracle.neighbor_list(cfg.x, cfg.box, p.rcut, 1.0, 64)
         e, f, _ = oracle.snap_force(xa, al, nl, nn, p)
@@ -119,3 +119,33 @@ def test_reads_the_reference_ta_training_set():
             assert np.all(dataset.cell_widths(cfg.box) > 4.67637)
         sizes[folder] = len(frames)
     assert len(sizes) == 12 and sum(sizes.values()) == 363
+
+
+def write_extxyz(path, frames):
+    """Frames in extended-XYZ form (readEXTXYZ.jl)."""
+    with open(path, "w") as fh:
+        for fr in frames:
+            fh.write(f"{fr.natoms}\n")
+            lat = " ".join(f"{v:.17g}" for v in fr.lattice.ravel())
+            st = " ".join(f"{v:.17g}" for v in fr.stress.ravel())
+            fh.write(f'Lattice="{lat}" Properties=species:S:1:pos:R:3:forces:R:3 energy={fr.e:.17g} '
+                     f'stress="{st}" pbc="T T T"\n')
+            for i in range(fr.natoms):
+                row = " ".join(f"{v:.17g}" for v in np.concatenate([fr.x[i], fr.f[i]]))
+                fh.write(f"Ta {row}\n")
+
+
+def test_extxyz_reader_matches_json_reader(tmp_path):
+    rng = np.random.default_rng(7)
+    frames = [dataset.Frame(natoms=n, lattice=np.diag(rng.uniform(5, 9, 3)) + rng.normal(0, 0.3, (3, 3)),
+                            x=rng.uniform(0, 5, (n, 3)), e=float(rng.normal(-20, 3)), f=rng.normal(size=(n, 3)),
+                            stress=rng.normal(size=(3, 3))) for n in (3, 1, 4)]
+    write_json(tmp_path / "t.json", frames)
+    write_extxyz(tmp_path / "t.xyz", frames)
+    a = dataset.read_folder(str(tmp_path), extension="json")
+    b = dataset.read_folder(str(tmp_path), extension="xyz")
+    assert len(a) == len(b) == 3
+    for fa, fb in zip(a, b):
+        assert fa.natoms == fb.natoms and fa.e == fb.e
+        for k in ("lattice", "x", "f", "stress", "types"):
+            np.testing.assert_array_equal(getattr(fa, k), getattr(fb, k))
