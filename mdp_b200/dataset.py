@@ -23,8 +23,13 @@ normalize_energy is set; the normal equations of all groups are summed and
 solved.  The rows are the batched GPU pipeline's (mdp_fit_run): per frame one
 energy row [N, sum_i B_i] and one row per force component [0, d(sum B)/dx],
 with the one-body column N standing in for the reference's "single"
-descriptor.  Not included: stress rows and the ZBL reference potential that
-fitsnap.jl subtracts from the targets.
+descriptor.  Stress rows (emldescriptors.jl:199-259, the "energyforcestress"
+loss) are six per frame: the GPU's virial descriptors bv times
+1.6021765e6 / cell volume (eV/A^3 to bar, normalizestress) against the
+frame's stress in Voigt order xx, yy, zz, yz, xz, xy; being six rows of
+1 + ncoeff numbers per frame, their outer products are added to the GPU's
+normal equations on the host.  Not included: the ZBL reference potential
+that fitsnap.jl subtracts from the targets.
 
 Cells narrower than the cutoff (the 2- and 4-atom Elastic / Volume cells)
 are replicated along each short cell vector until every perpendicular width
@@ -189,11 +194,25 @@ def replicate(frame: Frame, rcut: float):
 
 @dataclasses.dataclass
 class Group:
-    """One data folder: its frames and the weights of its energy and force rows."""
+    """One data folder: its frames and the weights of its energy, force and stress rows."""
     name: str
     frames: list
     we: float = 1.0
     wf: float = 1.0
+    ws: float = 0.0
+
+
+EV_PER_A3_IN_BAR = 1.6021765e6
+VOIGT = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))   # emldescriptors.jl: ind = [1, 5, 9, 6, 3, 2]
+
+
+def stress_rows(bv: np.ndarray, cell: np.ndarray, copies: int, normalize_stress: bool = True) -> np.ndarray:
+    """(6, 1 + k) stress rows of one frame from the virial descriptors bv
+    (k, 6) of its (possibly replicated) cell; the one-body column is zero."""
+    scale = EV_PER_A3_IN_BAR / abs(np.linalg.det(cell)) if normalize_stress else 1.0 / copies
+    R = np.zeros((6, 1 + bv.shape[0]))
+    R[:, 1:] = scale * bv.T
+    return R
 
 
 def batch_of(groups, rcut: float, normalize_energy: bool = True):
@@ -214,21 +233,33 @@ def batch_of(groups, rcut: float, normalize_energy: bool = True):
             np.array(gid))
 
 
-def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, mode: str = "fp64", device: int = 0):
+def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, normalize_stress: bool = True,
+               mode: str = "fp64", device: int = 0):
     """Solve the weighted linear SNAP fit over the groups on the GPU.
 
     Returns beta (1 + ncoeff: the one-body term, then the bispectrum
     coefficients), the normal equations, and per group the unweighted energy
-    (per atom) and force MAE / RMSE of the fitted model, as
+    (per atom), force and stress MAE / RMSE of the fitted model, as
     validate2 reports them (maespace.jl:210)."""
     cfgs, e, f, we, wf, copies, gid = batch_of(groups, params.rcut, normalize_energy)
     bf = _fit.BatchFit(params, device)
     try:
         bf.set_batch(cfgs, e, f, we, wf)
         A, b, ms = bf.run(mode)
-        bi, bd, _, _ = bf.descriptors()
+        bi, bd, bv, _ = bf.descriptors()
     finally:
         bf.close()
+    frames = [fr for grp in groups for fr in grp.frames]
+    srows = [None] * len(cfgs)
+    for c, fr in enumerate(frames):
+        if fr.stress is None:
+            continue
+        srows[c] = stress_rows(bv[c], cfgs[c].box, copies[c], normalize_stress)
+        ws = groups[gid[c]].ws
+        if ws:
+            t = np.array([fr.stress[i, j] for i, j in VOIGT])
+            A = A + ws * ws * (srows[c].T @ srows[c])
+            b = b + ws * ws * (srows[c].T @ t)
     try:
         beta = _fit.solve(A, b)
     except np.linalg.LinAlgError:
@@ -238,15 +269,21 @@ def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, mode: 
     e_pred = beta[0] * counts + bi @ beta[1:]
     errors = []
     for g, grp in enumerate(groups):
-        de, dfs = [], []
+        de, dfs, dss = [], [], []
         for c in np.nonzero(gid == g)[0]:
             n0 = counts[c] // copies[c]
             de.append((e_pred[c] - e[c]) / counts[c])
             fp = bd[a0[c]:a0[c] + n0] @ beta[1:]
             dfs.append((fp - f[a0[c]:a0[c] + n0]).ravel())
+            if srows[c] is not None:
+                dss.append(srows[c] @ beta - np.array([frames[c].stress[i, j] for i, j in VOIGT]))
         de, dfs = np.array(de), np.concatenate(dfs)
-        errors.append(dict(group=grp.name, frames=len(de),
-                           energy_mae=float(np.abs(de).mean()), energy_rmse=float(np.sqrt((de ** 2).mean())),
-                           force_mae=float(np.abs(dfs).mean()), force_rmse=float(np.sqrt((dfs ** 2).mean()))))
+        err = dict(group=grp.name, frames=len(de),
+                   energy_mae=float(np.abs(de).mean()), energy_rmse=float(np.sqrt((de ** 2).mean())),
+                   force_mae=float(np.abs(dfs).mean()), force_rmse=float(np.sqrt((dfs ** 2).mean())))
+        if dss:
+            dss = np.concatenate(dss)
+            err.update(stress_mae=float(np.abs(dss).mean()), stress_rmse=float(np.sqrt((dss ** 2).mean())))
+        errors.append(err)
     return dict(beta=beta, A=A, b=b, graph_ms=ms, errors=errors, configs=len(cfgs),
                 atoms=int(counts.sum()), replicated=int((copies > 1).sum()))

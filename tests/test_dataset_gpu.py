@@ -4,8 +4,8 @@ Training files in MDP's JSON format are written for two groups of frames --
 narrow sheared 2-atom BCC cells (replicated to cover the cutoff) and sheared
 16-54 atom supercells -- with energies and forces of a known linear SNAP
 model from the oracle.  Reading them back and fitting on the GPU must
-recover the model: the fitted energies and forces match the targets and the
-coefficients match the known ones."""
+recover the model: the fitted energies, forces and stresses match the
+targets and the coefficients match the known ones."""
 import numpy as np
 import pytest
 
@@ -17,10 +17,15 @@ pytestmark = pytest.mark.gpu
 
 
 def _targets(fr, p):
+    """Energy, forces and stress (bar) of the known model on the frame."""
     cfg, m = dataset.replicate(fr, p.rcut)
     xa, al, nl, nn = oracle.neighbor_list(cfg.x, cfg.box, p.rcut, 1.0, 96)
-    e, f, _ = oracle.snap_force(xa, al, nl, nn, p)
+    e, f, v = oracle.snap_force(xa, al, nl, nn, p)
     fr.e, fr.f = float(e.sum() / m), f[:fr.natoms].copy()
+    w = v.sum(axis=1) * dataset.EV_PER_A3_IN_BAR / abs(np.linalg.det(cfg.box))
+    fr.stress = np.zeros((3, 3))
+    for k, (i, j) in enumerate(dataset.VOIGT):
+        fr.stress[i, j] = fr.stress[j, i] = w[k]
     return fr
 
 
@@ -46,13 +51,16 @@ def test_fit_recovers_known_model_from_json(tmp_path):
     for i, fr in enumerate(narrow):
         write_json(tmp_path / "Narrow" / f"N_{i}.json", [fr])
     write_json(tmp_path / "Bulk" / "B.json", bulk)
-    groups = [dataset.Group("Narrow", dataset.read_json_folder(str(tmp_path / "Narrow")), we=100.0, wf=1.0),
-              dataset.Group("Bulk", dataset.read_json_folder(str(tmp_path / "Bulk")), we=1.0, wf=1.0)]
+    groups = [dataset.Group("Narrow", dataset.read_json_folder(str(tmp_path / "Narrow")), we=100.0, wf=1.0,
+                            ws=1e-5),
+              dataset.Group("Bulk", dataset.read_json_folder(str(tmp_path / "Bulk")), we=1.0, wf=1.0, ws=1e-4)]
     out = dataset.fit_groups(groups, p)
     assert out["replicated"] == 6
+    smax = max(np.abs(fr.stress).max() for fr in narrow + bulk)
     for err in out["errors"]:
         assert err["energy_rmse"] < 1e-6, err        # eV/atom
         assert err["force_rmse"] < 1e-6, err         # eV/A
+        assert err["stress_rmse"] < 1e-6 * smax, err  # bar
     beta = out["beta"]
     assert abs(beta[0] - p.coeff[0]) < 1e-6 * abs(p.coeff[0])
     assert np.max(np.abs(beta[1:] - p.coeff[1:])) < 1e-4 * np.max(np.abs(p.coeff[1:]))
