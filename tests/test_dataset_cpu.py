@@ -149,3 +149,15 @@ def test_extxyz_reader_matches_json_reader(tmp_path):
         assert fa.natoms == fb.natoms and fa.e == fb.e
         for k in ("lattice", "x", "f", "stress", "types"):
             np.testing.assert_array_equal(getattr(fa, k), getattr(fb, k))
+
+
+def test_fitsnap_folder_table_and_loading(tmp_path):
+    from mdp_b200 import fitsnap
+    assert len(fitsnap.TA_FOLDERS) == 12
+    for k, (name, *_) in enumerate(fitsnap.TA_FOLDERS):
+        (tmp_path / name).mkdir()
+        write_json(tmp_path / name / "x.json", [bcc2(seed=k)])
+    groups = fitsnap.load_groups(str(tmp_path))
+    assert [g.name for g in groups] == [f[0] for f in fitsnap.TA_FOLDERS]
+    assert groups[3].ws == 1e-4 and groups[7].we == 467.0
+    assert all(len(g.frames) == 1 for g in groups)

@@ -64,3 +64,18 @@ def test_fit_recovers_known_model_from_json(tmp_path):
     beta = out["beta"]
     assert abs(beta[0] - p.coeff[0]) < 1e-6 * abs(p.coeff[0])
     assert np.max(np.abs(beta[1:] - p.coeff[1:])) < 1e-4 * np.max(np.abs(p.coeff[1:]))
+
+
+def test_fitsnap_cli_on_a_folder_tree(tmp_path):
+    """fitsnap.jl's twelve folders and weights through the command-line entry."""
+    from mdp_b200 import fitsnap
+    p = configs.snap_params(6, seed=21)
+    narrow, bulk = _frames(p)
+    for (name, *_), fr in zip(fitsnap.TA_FOLDERS, narrow + bulk):
+        (tmp_path / name).mkdir()
+        write_json(tmp_path / name / "a.json", [fr])
+    res = fitsnap.main(["--data", str(tmp_path)])
+    assert len(res["errors"]) == 12 and res["configs"] == 12
+    assert len(res["coefficients"]) == 1 + p.ncoeff and np.all(np.isfinite(res["coefficients"]))
+    for err in res["errors"]:                            # the data come from one linear model
+        assert err["force_rmse"] < 1e-4, err
