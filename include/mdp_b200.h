@@ -218,6 +218,12 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
  * (readJSON.jl "Lattice") are sheared and surface cells. */
 int mdp_fit_set_batch_lattice(mdp_fit *h, int nconf, const int *natoms, const double *lattice, const double *x,
                               const double *e, const double *f, const double *we, const double *wf);
+/* ZBL reference potential (inner, outer radii, atomic number z) of every atom
+ * of the current batch, into host arrays: eatom[natoms], fatom[3 natoms],
+ * vatom[6][natoms] (xx, yy, zz, xy, xz, yz).  The fit of MDP's
+ * fitting/snap/Ta/fitsnap.jl:81 subtracts this pair term from the targets
+ * (emldescriptors.jl:199-259). */
+int mdp_fit_zbl(mdp_fit *h, double inner, double outer, double z, double *eatom, double *fatom, double *vatom);
 long long mdp_fit_npairs(mdp_fit *h);
 /* scratch budget of the chunked stages (default 24e9 bytes; the batch is
  * processed in configuration-aligned chunks that fit it) and the chunk count */

@@ -108,6 +108,7 @@ def lib():
                                     C.c_void_p]
     L.mdp_fit_set_batch_lattice.argtypes = [C.c_void_p, C.c_int, _ip32, _dp, _dp, C.c_void_p, C.c_void_p,
                                             C.c_void_p, C.c_void_p]
+    L.mdp_fit_zbl.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
     L.mdp_fit_npairs.argtypes = [C.c_void_p]
     L.mdp_fit_npairs.restype = C.c_longlong
     L.mdp_fit_set_chunk_bytes.argtypes = [C.c_void_p, C.c_double]

@@ -52,6 +52,27 @@ struct ZblParams {
     double dk[4], ck[4], inner, rcsq, sw3, sw4, sw5;
 };
 int zbl_setup(ZblParams &zp, double inner, double outer, double z);
+
+// ZBL pair energy u(r) and g = u'(r) / r of the switched potential
+// (ZBLpotential.jl): screened Coulomb plus A(t) t^3 (sw3 + sw4 t) + sw5 with
+// t = r - inner and A = 1/2 + tanh(100 t)/2
+__device__ __forceinline__ void zbl_pair(const ZblParams &zp, double r, double &u, double &g)
+{
+    const double rinv = 1.0 / r;
+    double s = 0.0, sp = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double ek = zp.ck[k] * exp(-zp.dk[k] * r);
+        s += ek;
+        sp -= zp.dk[k] * ek;
+    }
+    const double ez = s * rinv, ezp = (sp - s * rinv) * rinv;
+    const double t = r - zp.inner, t2 = t * t, t3 = t2 * t;
+    const double th = tanh(100.0 * t), a = 0.5 + 0.5 * th, da = 50.0 * (1.0 - th * th);
+    const double poly = zp.sw3 + zp.sw4 * t;
+    u = ez + zp.sw5 + a * t3 * poly;
+    g = (ezp + da * t3 * poly + a * (3.0 * t2 * poly + t3 * zp.sw4)) * rinv;
+}
 __global__ void k_zbl(const double4 *, const int *, const int *, int, int, ZblParams, double *, double4 *, double *);
 
 struct SnapModel {

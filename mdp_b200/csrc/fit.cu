@@ -72,6 +72,43 @@ __global__ void k_fit_pairs(const double4 *__restrict__ x, const int *__restrict
     if (!EMIT) pcount[i] = cnt;
 }
 
+// ZBL reference potential of every atom of the batch (the pair term that MDP's
+// fitsnap.jl subtracts from the training targets): brute force over the
+// atom's configuration and 27 images as k_fit_pairs, pairs within the ZBL
+// outer cutoff.  Per atom: energy u/2 per pair, force du/dx_ij, virial
+// -x_ij (x) du/dx_ij / 2 in the order xx, yy, zz, xy, xz, yz ([6][natoms]).
+__global__ void k_fit_zbl(const double4 *__restrict__ x, const int *__restrict__ cfg, const int *__restrict__ ca0,
+                          const int *__restrict__ cn, const double4 *__restrict__ cbox, int natoms, ZblParams zp,
+                          double *__restrict__ eatom, double *__restrict__ fatom, double *__restrict__ vatom)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= natoms) return;
+    const int c = cfg[i], a0 = ca0[c], n = cn[c];
+    const double4 la = cbox[3 * c], lb = cbox[3 * c + 1], lc = cbox[3 * c + 2], xi = x[i];
+    double e = 0.0, fx = 0.0, fy = 0.0, fz = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
+    for (int jj = 0; jj < n; jj++) {
+        const double4 xj = x[a0 + jj];
+        for (int im = 0; im < 27; im++) {
+            const double u0 = im % 3 - 1, u1 = (im / 3) % 3 - 1, u2 = im / 9 - 1;
+            const double d0 = xj.x + (u0 * la.x + u1 * lb.x + u2 * lc.x) - xi.x;
+            const double d1 = xj.y + (u0 * la.y + u1 * lb.y + u2 * lc.y) - xi.y;
+            const double d2 = xj.z + (u0 * la.z + u1 * lb.z + u2 * lc.z) - xi.z;
+            const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+            if (!(r2 <= zp.rcsq && r2 > 1e-20)) continue;
+            double u, g;
+            zbl_pair(zp, sqrt(r2), u, g);
+            const double ux = g * d0, uy = g * d1, uz = g * d2;
+            e += 0.5 * u;
+            fx += ux; fy += uy; fz += uz;
+            v[0] -= 0.5 * d0 * ux; v[1] -= 0.5 * d1 * uy; v[2] -= 0.5 * d2 * uz;
+            v[3] -= 0.5 * d0 * uy; v[4] -= 0.5 * d0 * uz; v[5] -= 0.5 * d1 * uz;
+        }
+    }
+    eatom[i] = e;
+    fatom[3 * (size_t)i] = fx; fatom[3 * (size_t)i + 1] = fy; fatom[3 * (size_t)i + 2] = fz;
+    for (int k = 0; k < 6; k++) vatom[k * (size_t)natoms + i] = v[k];
+}
+
 // ---------------------------------------------------------------------------
 // Z rows of every coupling and B for j >= j1, per 32-atom tile (lane = atom)
 // Z layout [tile][zoff + (j+1) mb + ma][lane]; B layout [k][atom]
@@ -988,6 +1025,7 @@ int mdp_fit_set_batch_lattice(mdp_fit *h, int nconf, const int *natoms, const do
         total += natoms[c];
     }
     if (total > (1L << 30)) { set_error("batch too large"); return -1; }
+    h->h_lat.assign(lattice, lattice + 9 * (size_t)nconf);
     fit_drop_graph(h);
     h->nconf = nconf;
     h->natoms = (int)total;
@@ -1031,6 +1069,49 @@ int mdp_fit_set_batch(mdp_fit *h, int nconf, const int *natoms, const double *bo
     for (int c = 0; c < nconf; c++)
         for (int d = 0; d < 3; d++) lat[9 * c + 4 * d] = box[3 * c + d];
     return mdp_fit_set_batch_lattice(h, nconf, natoms, lat.data(), x, e, f, we, wf);
+}
+
+// ZBL reference potential (inner, outer, z) of every atom of the current
+// batch into host arrays: eatom[natoms], fatom[3 natoms], vatom[6][natoms]
+// (xx, yy, zz, xy, xz, yz).  Every cell width must exceed the outer cutoff.
+int mdp_fit_zbl(mdp_fit *h, double inner, double outer, double z, double *eatom, double *fatom, double *vatom)
+{
+    if (!h || h->natoms < 1 || !eatom || !fatom || !vatom) { set_error("bad arguments"); return -1; }
+    ZblParams zp;
+    if (zbl_setup(zp, inner, outer, z)) return -1;
+    if (!zp.on) { set_error("ZBL atomic number must be positive (got %g)", z); return -1; }
+    for (int c = 0; c < h->nconf; c++) {
+        const double *L = h->h_lat.data() + 9 * (size_t)c;
+        for (int d = 0; d < 3; d++) {
+            const double *p = L + 3 * ((d + 1) % 3), *q = L + 3 * ((d + 2) % 3), *r = L + 3 * d;
+            const double cx = p[1] * q[2] - p[2] * q[1], cy = p[2] * q[0] - p[0] * q[2], cz = p[0] * q[1] - p[1] * q[0];
+            const double width = fabs(r[0] * cx + r[1] * cy + r[2] * cz) / sqrt(cx * cx + cy * cy + cz * cz);
+            if (!(width > outer)) {
+                set_error("configuration %d: cell width %g must exceed the ZBL cutoff %g", c, width, outer);
+                return -1;
+            }
+        }
+    }
+    MDP_CUDA_TRY(cudaSetDevice(h->device));
+    const int n = h->natoms;
+    const size_t bytes = sizeof(double) * 10 * (size_t)n;
+    double *buf = nullptr;
+    MDP_CUDA_TRY(cudaMalloc(&buf, bytes));
+    k_fit_zbl<<<(n + 127) / 128, 128, 0, h->s>>>(h->x.as<double4>(), h->cfg.as<int>(), h->ca0.as<int>(),
+                                                 h->cn.as<int>(), h->cbox.as<double4>(), n, zp, buf, buf + n,
+                                                 buf + 4 * (size_t)n);
+    count_launches(1);
+    cudaError_t err = cudaGetLastError();
+    if (err == cudaSuccess) err = cudaMemcpyAsync(eatom, buf, sizeof(double) * n, cudaMemcpyDeviceToHost, h->s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(fatom, buf + n, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToHost, h->s);
+    if (err == cudaSuccess)
+        err = cudaMemcpyAsync(vatom, buf + 4 * (size_t)n, sizeof(double) * 6 * (size_t)n, cudaMemcpyDeviceToHost,
+                              h->s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(h->s);
+    cudaFree(buf);
+    if (err != cudaSuccess) { set_error("mdp_fit_zbl: %s", cudaGetErrorString(err)); return -1; }
+    return 0;
 }
 
 long long mdp_fit_npairs(mdp_fit *h) { return h ? h->npairs : -1; }

@@ -40,6 +40,7 @@ struct mdp_fit {
     // batch
     int nconf = 0, natoms = 0;
     std::vector<int> h_cn, h_ca0;
+    std::vector<double> h_lat;   // cell vectors (9 per configuration) of the current batch
     mdp::DevBuf x, cfg, ca0, cn, cbox, we, wf, e, f;
     // work (sized for the whole batch)
     mdp::DevBuf tabs, pcount, poff, roff, rcount, cursor, rlist, B, Z, dul, dbdr, G, R, tgt, hi, lo, part, out, scan_tmp;

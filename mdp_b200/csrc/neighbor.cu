@@ -460,22 +460,8 @@ __global__ void k_zbl(const double4 *__restrict__ x, const int *__restrict__ nli
         const double d0 = xj.x - xi.x, d1 = xj.y - xi.y, d2 = xj.z - xi.z;
         const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
         if (!(r2 <= zp.rcsq)) continue;
-        const double r = sqrt(r2), rinv = 1.0 / r;
-        // screened Coulomb part and its radial derivative
-        double s = 0.0, sp = 0.0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-            const double ek = zp.ck[k] * exp(-zp.dk[k] * r);
-            s += ek;
-            sp -= zp.dk[k] * ek;
-        }
-        const double ez = s * rinv, ezp = (sp - s * rinv) * rinv;
-        // smoothed switch: A(t) t^3 (sw3 + sw4 t) with A = 1/2 + tanh(100 t)/2
-        const double t = r - zp.inner, t2 = t * t, t3 = t2 * t;
-        const double th = tanh(100.0 * t), a = 0.5 + 0.5 * th, da = 50.0 * (1.0 - th * th);
-        const double poly = zp.sw3 + zp.sw4 * t;
-        const double u = ez + zp.sw5 + a * t3 * poly;
-        const double g = (ezp + da * t3 * poly + a * (3.0 * t2 * poly + t3 * zp.sw4)) * rinv;
+        double u, g;
+        zbl_pair(zp, sqrt(r2), u, g);
         const double ux = g * d0, uy = g * d1, uz = g * d2;
         e += 0.5 * u;
         fx += ux; fy += uy; fz += uz;

@@ -25,11 +25,14 @@ energy row [N, sum_i B_i] and one row per force component [0, d(sum B)/dx],
 with the one-body column N standing in for the reference's "single"
 descriptor.  Stress rows (emldescriptors.jl:199-259, the "energyforcestress"
 loss) are six per frame: the GPU's virial descriptors bv times
-1.6021765e6 / cell volume (eV/A^3 to bar, normalizestress) against the
-frame's stress in Voigt order xx, yy, zz, yz, xz, xy; being six rows of
+1.6021765e6 / cell volume (eV/A^3 to bar, normalizestress), reordered as
+snapcpp.jl:662 does, against the frame's stress in the order xx, yy, zz, yz,
+xz, xy; being six rows of
 1 + ncoeff numbers per frame, their outer products are added to the GPU's
-normal equations on the host.  Not included: the ZBL reference potential
-that fitsnap.jl subtracts from the targets.
+normal equations on the host.  With `zbl` = (inner, outer, Z), the ZBL
+reference potential of fitsnap.jl:81 is evaluated on the GPU
+(mdp_fit_zbl) and its energy, forces and stress are subtracted from the
+targets first (emldescriptors.jl:199-259: e - eref, f - fref, s - sref).
 
 Cells narrower than the cutoff (the 2- and 4-atom Elastic / Volume cells)
 are replicated along each short cell vector until every perpendicular width
@@ -203,7 +206,11 @@ class Group:
 
 
 EV_PER_A3_IN_BAR = 1.6021765e6
-VOIGT = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))   # emldescriptors.jl: ind = [1, 5, 9, 6, 3, 2]
+# stress components of the rows, in emldescriptors.jl's order (ind = [1, 5, 9, 6, 3, 2]): xx, yy, zz, yz, xz, xy
+VOIGT = ((0, 0), (1, 1), (2, 2), (1, 2), (0, 2), (0, 1))
+# the virial descriptors bv come as xx, yy, zz, xy, xz, yz (cpuSnap virial tally); snapcpp.jl:662 reorders
+# them to the stress order with bv[[1; 2; 3; 6; 5; 4], :]
+BV_TO_VOIGT = (0, 1, 2, 5, 4, 3)
 
 
 def stress_rows(bv: np.ndarray, cell: np.ndarray, copies: int, normalize_stress: bool = True) -> np.ndarray:
@@ -211,7 +218,7 @@ def stress_rows(bv: np.ndarray, cell: np.ndarray, copies: int, normalize_stress:
     (k, 6) of its (possibly replicated) cell; the one-body column is zero."""
     scale = EV_PER_A3_IN_BAR / abs(np.linalg.det(cell)) if normalize_stress else 1.0 / copies
     R = np.zeros((6, 1 + bv.shape[0]))
-    R[:, 1:] = scale * bv.T
+    R[:, 1:] = scale * bv.T[list(BV_TO_VOIGT)]
     return R
 
 
@@ -233,15 +240,39 @@ def batch_of(groups, rcut: float, normalize_energy: bool = True):
             np.array(gid))
 
 
+def zbl_reference(cfgs, params: SnapParams, zbl, device: int = 0):
+    """Per configuration: ZBL energy, forces (all atoms, concatenated) and
+    summed virial (6,) in the order xx, yy, zz, xy, xz, yz."""
+    bf = _fit.BatchFit(params, device)
+    try:
+        bf.set_batch(cfgs)
+        ea, fa, va = bf.zbl(*zbl)
+    finally:
+        bf.close()
+    a0 = np.concatenate([[0], np.cumsum([c.natoms for c in cfgs])])
+    e = np.array([ea[a0[c]:a0[c + 1]].sum() for c in range(len(cfgs))])
+    w = np.stack([va[:, a0[c]:a0[c + 1]].sum(axis=1) for c in range(len(cfgs))])
+    return e, fa, w
+
+
 def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, normalize_stress: bool = True,
-               mode: str = "fp64", device: int = 0):
+               mode: str = "fp64", device: int = 0, zbl=None):
     """Solve the weighted linear SNAP fit over the groups on the GPU.
 
     Returns beta (1 + ncoeff: the one-body term, then the bispectrum
     coefficients), the normal equations, and per group the unweighted energy
     (per atom), force and stress MAE / RMSE of the fitted model, as
     validate2 reports them (maespace.jl:210)."""
-    cfgs, e, f, we, wf, copies, gid = batch_of(groups, params.rcut, normalize_energy)
+    rcut = max(params.rcut, zbl[1]) if zbl is not None else params.rcut
+    cfgs, e, f, we, wf, copies, gid = batch_of(groups, rcut, normalize_energy)
+    sref = [np.zeros(6)] * len(cfgs)
+    if zbl is not None:
+        ez, fz, wz = zbl_reference(cfgs, params, zbl, device)
+        e = e - ez
+        f = f - fz
+        for c, cfg in enumerate(cfgs):
+            scale = EV_PER_A3_IN_BAR / abs(np.linalg.det(cfg.box)) if normalize_stress else 1.0 / copies[c]
+            sref[c] = scale * wz[c][list(BV_TO_VOIGT)]
     bf = _fit.BatchFit(params, device)
     try:
         bf.set_batch(cfgs, e, f, we, wf)
@@ -257,7 +288,7 @@ def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, normal
         srows[c] = stress_rows(bv[c], cfgs[c].box, copies[c], normalize_stress)
         ws = groups[gid[c]].ws
         if ws:
-            t = np.array([fr.stress[i, j] for i, j in VOIGT])
+            t = np.array([fr.stress[i, j] for i, j in VOIGT]) - sref[c]
             A = A + ws * ws * (srows[c].T @ srows[c])
             b = b + ws * ws * (srows[c].T @ t)
     try:
@@ -276,7 +307,7 @@ def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, normal
             fp = bd[a0[c]:a0[c] + n0] @ beta[1:]
             dfs.append((fp - f[a0[c]:a0[c] + n0]).ravel())
             if srows[c] is not None:
-                dss.append(srows[c] @ beta - np.array([frames[c].stress[i, j] for i, j in VOIGT]))
+                dss.append(srows[c] @ beta + sref[c] - np.array([frames[c].stress[i, j] for i, j in VOIGT]))
         de, dfs = np.array(de), np.concatenate(dfs)
         err = dict(group=grp.name, frames=len(de),
                    energy_mae=float(np.abs(de).mean()), energy_rmse=float(np.sqrt((de ** 2).mean())),

@@ -146,6 +146,13 @@ class BatchFit:
                                                   bl.ctypes.data), "mdp_fit_descriptors")
         return bi, bd, bv, bl
 
+    def zbl(self, inner: float = 4.0, outer: float = 4.8, z: float = 73.0):
+        """ZBL reference potential of every atom: energy (natoms,), forces
+        (natoms, 3), virial (6, natoms) in the order xx, yy, zz, xy, xz, yz."""
+        e = np.zeros(self.natoms); f = np.zeros((self.natoms, 3)); v = np.zeros((6, self.natoms))
+        _lib.check(_lib.lib().mdp_fit_zbl(self._h, float(inner), float(outer), float(z), e, f, v), "mdp_fit_zbl")
+        return e, f, v
+
     def run(self, mode: str = "fp64"):
         """Normal equations (A (m, m), b (m,), device ms) with m = 1 + ncoeff."""
         A = np.zeros(64 * 64); b = np.zeros(64); ms = C.c_float(0.0)

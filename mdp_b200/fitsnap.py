@@ -6,9 +6,10 @@ fitting/snap/Ta/fitsnap.jl:1-159.
 The defaults are fitsnap.jl's: the 12 Ta folders and their (energy, force,
 stress) weights, species Ta, rcut 4.67637, rfac0 0.99363, rmin0 0,
 switching on, bzero / bnorm / wselfall off, 2J = 6, energies per atom and
-stresses per volume.  Prints the coefficients and the per-folder unweighted
-errors (printerrors) as one JSON object.  The ZBL reference potential that
-fitsnap.jl subtracts from the targets is not applied.
+stresses per volume, and the ZBL reference potential (inner 4.0, outer 4.8,
+Z 73) subtracted from the targets (--no-zbl leaves it out).  Prints the
+coefficients and the per-folder unweighted errors (printerrors) as one JSON
+object.
 """
 from __future__ import annotations
 
@@ -18,7 +19,7 @@ import os
 
 from . import configs, dataset
 
-# fitsnap.jl:12-30: folders and their (energy, force, stress) weights
+# fitsnap.jl:14-30: folders and their (energy, force, stress) weights
 TA_FOLDERS = (
     ("Displaced_A15", 100.0, 1.0, 1e-8),
     ("Displaced_BCC", 100.0, 1.0, 1e-8),
@@ -35,6 +36,10 @@ TA_FOLDERS = (
 )
 
 
+# fitsnap.jl:81: addpotential("pair", "nonbonded", [1, 1], "zbl", [4.0, 4.8, 73], 4.8)
+TA_ZBL = (4.0, 4.8, 73.0)
+
+
 def load_groups(root: str, folders=TA_FOLDERS, species=("Ta",), extension: str = "json"):
     return [dataset.Group(name, dataset.read_folder(os.path.join(root, name), species, extension), we, wf, ws)
             for name, we, wf, ws in folders]
@@ -47,10 +52,12 @@ def main(argv=None) -> dict:
     ap.add_argument("--mode", choices=("fp64", "bf16"), default="fp64")
     ap.add_argument("--extension", default="json")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--no-zbl", action="store_true", help="fit without the ZBL reference potential")
     a = ap.parse_args(argv)
     p = configs.snap_params(a.twojmax, seed=0, rcutfac=4.67637, radelem=0.5, rfac0=0.99363, rmin0=0.0,
                             switchflag=1, bzeroflag=0, bnormflag=0, wselfallflag=0)
-    out = dataset.fit_groups(load_groups(a.data, extension=a.extension), p, mode=a.mode, device=a.device)
+    out = dataset.fit_groups(load_groups(a.data, extension=a.extension), p, mode=a.mode, device=a.device,
+                             zbl=None if a.no_zbl else TA_ZBL)
     res = dict(coefficients=out["beta"].tolist(), errors=out["errors"], configs=out["configs"],
                atoms=out["atoms"], replicated=out["replicated"], graph_ms=out["graph_ms"])
     print(json.dumps(res))

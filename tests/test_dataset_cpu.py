@@ -161,3 +161,15 @@ def test_fitsnap_folder_table_and_loading(tmp_path):
     assert [g.name for g in groups] == [f[0] for f in fitsnap.TA_FOLDERS]
     assert groups[3].ws == 1e-4 and groups[7].we == 467.0
     assert all(len(g.frames) == 1 for g in groups)
+
+
+def test_stress_rows_use_the_reference_component_order():
+    """bv arrives as xx, yy, zz, xy, xz, yz; the rows are xx, yy, zz, yz, xz, xy
+    (snapcpp.jl:662 with emldescriptors.jl's stress index [1, 5, 9, 6, 3, 2])."""
+    bv = np.arange(12.0).reshape(2, 6)                  # (k, 6)
+    cell = np.diag([2.0, 3.0, 4.0])
+    R = dataset.stress_rows(bv, cell, 1)
+    s = dataset.EV_PER_A3_IN_BAR / 24.0
+    np.testing.assert_allclose(R[:, 0], 0.0)
+    np.testing.assert_allclose(R[:, 1:], s * bv.T[[0, 1, 2, 5, 4, 3]])
+    assert dataset.VOIGT[3] == (1, 2) and dataset.VOIGT[5] == (0, 1)

@@ -24,7 +24,7 @@ def _targets(fr, p):
     fr.e, fr.f = float(e.sum() / m), f[:fr.natoms].copy()
     w = v.sum(axis=1) * dataset.EV_PER_A3_IN_BAR / abs(np.linalg.det(cfg.box))
     fr.stress = np.zeros((3, 3))
-    for k, (i, j) in enumerate(dataset.VOIGT):
+    for k, (i, j) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))):   # the oracle's virial order
         fr.stress[i, j] = fr.stress[j, i] = w[k]
     return fr
 
@@ -74,8 +74,57 @@ def test_fitsnap_cli_on_a_folder_tree(tmp_path):
     for (name, *_), fr in zip(fitsnap.TA_FOLDERS, narrow + bulk):
         (tmp_path / name).mkdir()
         write_json(tmp_path / name / "a.json", [fr])
-    res = fitsnap.main(["--data", str(tmp_path)])
+    res = fitsnap.main(["--data", str(tmp_path), "--no-zbl"])
     assert len(res["errors"]) == 12 and res["configs"] == 12
     assert len(res["coefficients"]) == 1 + p.ncoeff and np.all(np.isfinite(res["coefficients"]))
     for err in res["errors"]:                            # the data come from one linear model
         assert err["force_rmse"] < 1e-4, err
+
+
+def test_zbl_reference_matches_oracle():
+    """mdp_fit_zbl on a sheared cell and a replicated narrow cell against the
+    oracle's full-list ZBL tally (oracle/zbl.py)."""
+    from oracle import zbl
+    p = configs.snap_params(6, seed=21)
+    narrow, bulk = _frames(p)
+    cfgs = [dataset.replicate(fr, 4.8)[0] for fr in (narrow[0], bulk[1], bulk[2])]
+    e, f, w = dataset.zbl_reference(cfgs, p, (4.0, 4.8, 73.0))
+    a0 = 0
+    for c, cfg in enumerate(cfgs):
+        xa, al, nl, nn = oracle.neighbor_list(cfg.x, cfg.box, 4.8, 0.5, 160)
+        ez, fz, vz = zbl.zbl_tally(xa, nl, nn, 4.8)
+        n = cfg.natoms
+        assert abs(e[c] - ez.sum()) <= 1e-10 * abs(ez).sum()
+        np.testing.assert_allclose(f[a0:a0 + n], fz, rtol=0, atol=1e-10 * np.abs(fz).max())
+        np.testing.assert_allclose(w[c], vz.sum(axis=1), rtol=0, atol=1e-10 * np.abs(vz).sum())
+        a0 += n
+
+
+def test_fit_with_zbl_recovers_snap_part():
+    """Targets = known linear SNAP + ZBL: fitting with the ZBL reference
+    subtracted recovers the SNAP coefficients."""
+    from oracle import zbl
+    p = configs.snap_params(6, seed=21)
+    narrow, bulk = _frames(p)
+    for fr in narrow + bulk:
+        cfg, m = dataset.replicate(fr, 4.8 + 0.5)
+        xa, al, nl, nn = oracle.neighbor_list(cfg.x, cfg.box, 4.8, 0.5, 160)
+        ez, fz, vz = zbl.zbl_tally(xa, nl, nn, 4.8)
+        fr.e += ez.sum() / m
+        fr.f = fr.f + fz[:fr.natoms]
+        w = vz.sum(axis=1) * dataset.EV_PER_A3_IN_BAR / abs(np.linalg.det(cfg.box))
+        for k, (i, j) in enumerate(((0, 0), (1, 1), (2, 2), (0, 1), (0, 2), (1, 2))):
+            fr.stress[i, j] += w[k]
+            if i != j:
+                fr.stress[j, i] += w[k]
+    groups = [dataset.Group("Narrow", narrow, we=100.0, wf=1.0, ws=1e-5),
+              dataset.Group("Bulk", bulk, we=1.0, wf=1.0, ws=1e-4)]
+    out = dataset.fit_groups(groups, p, zbl=(4.0, 4.8, 73.0))
+    smax = max(np.abs(fr.stress).max() for fr in narrow + bulk)
+    for err in out["errors"]:
+        assert err["energy_rmse"] < 1e-6, err
+        assert err["force_rmse"] < 1e-6, err
+        assert err["stress_rmse"] < 1e-6 * smax, err
+    beta = out["beta"]
+    assert abs(beta[0] - p.coeff[0]) < 1e-6 * abs(p.coeff[0])
+    assert np.max(np.abs(beta[1:] - p.coeff[1:])) < 1e-4 * np.max(np.abs(p.coeff[1:]))
