@@ -350,7 +350,12 @@ def run_ours(args):
     barrier()
     _, ms32 = md32.run(args.steps)
     barrier()
+    md32.stage_timing(True)              # per-stage CUDA events, after the timed steps
+    md32.run(2)
+    st32 = md32.stage_times()
+    md32.stage_timing(False)
     md32.close()
+    stages32 = {k: v / max(st32["calls"], 1) for k, v in st32.items() if k != "calls"}
     if ws > 1:
         t = torch.tensor([ms32], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -406,7 +411,7 @@ def run_ours(args):
             "ui_tflops": FLOP_U_PER_PAIR * pairs / (ui_ms * 1e-3) / 1e12,
             "fp32": {"value": value32, "unit": "atom-steps/s", "speedup_vs_fp64": value32 / value,
                      "force_rmse_vs_fp64": fp32_rmse, "force_maxerr_vs_fp64": fp32_max, "unit_err": "eV/A",
-                     "fp32_fma_peak_tflops": fp32_peak},
+                     "fp32_fma_peak_tflops": fp32_peak, "stages_ms": stages32},
             "surrogate": sur_line,
             "batched_fit": fit_line,
             "clocks": clk,
