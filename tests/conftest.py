@@ -19,7 +19,12 @@ def pytest_configure(config):
 def golden_names():
     """Force / MD fixtures (the fit_* fixtures hold descriptors and are listed by fit_names)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith("fit_"))
+                  if not os.path.basename(p).startswith(("fit_", "tri_")))
+
+
+def tri_names():
+    """Sheared-cell force fixtures."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "tri_*.npz")))
 
 
 def fit_names():

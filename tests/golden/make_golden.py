@@ -16,6 +16,10 @@ implementation computes for it:
 The inputs are regenerated by the tests from the stored seeds and checked
 against the stored copies, so the fixtures also pin the input generator.
 
+The tri_* fixtures hold sheared (triclinic) cells with the reference's ghosts,
+neighbour lists and per-atom energy, forces and virial (`--tri-only` stops
+after them).
+
 The fit_* fixtures hold single configurations of the batched-fitting workload
 (BCC / FCC / A15 supercells) with the per-configuration descriptors of MDP's
 ComputeSnap chain (snappotential.cpp:762-910, cpuSnap2.cpp): bi, bd, bv and the
@@ -144,10 +148,51 @@ def fit_fixtures():
         print(name, cfg.natoms, "atoms", os.path.getsize(path), "bytes")
 
 
+# sheared-cell force fixtures: (name, cells, 2J, temp, jitter, seed, coeff seed, tilts (xy, xz, yz)); the
+# atoms of the orthogonal lattice keep their fractional coordinates in the cell a = (Lx, 0, 0),
+# b = (xy Lx, Ly, 0), c = (xz Lx, yz Ly, Lz)
+TRI_CASES = [
+    ("tri_bcc128_2j8", (4, 4, 4), 8, 300.0, 0.05, 16, 106, (0.10, -0.05, 0.08)),
+    ("tri_bcc250_2j6", (5, 5, 5), 6, 1000.0, 0.10, 17, 107, (-0.15, 0.12, 0.0)),
+]
+
+
+def tri_config(cells, temp, jit, seed, tilt):
+    """Positions and cell vectors (rows) of a sheared case."""
+    cfg = configs.ta_config(cells, temp=temp, jitter=jit, seed=seed)
+    L = np.asarray(cfg.box, dtype=np.float64)
+    H = np.array([[L[0], 0.0, 0.0], [tilt[0] * L[0], L[1], 0.0], [tilt[1] * L[0], tilt[2] * L[1], L[2]]])
+    s = cfg.x / L
+    s -= np.floor(s)
+    return s @ H, H
+
+
+def tri_fixtures():
+    """Sheared cells: the reference's ghosts, both neighbour-list forms and
+    per-atom energy, forces and virial."""
+    for (name, cells, tj, temp, jit, seed, cseed, tilt) in TRI_CASES:
+        p = configs.snap_params(tj, seed=cseed)
+        x, H = tri_config(cells, temp, jit, seed, tilt)
+        xa0, al0, nl0, nn0 = refpy.neighbor_list(x, H, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+        xa1, al1, nl1, nn1 = refpy.neighbor_list(x, H, p.rcut, SKIN, NEIGHMAX, neighcell=1)
+        e, f, va = refpy.snap_force(xa0, al0, nl0, nn0, p)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, cells=np.array(cells), twojmax=tj, temp=temp, jitter=jit, seed=seed,
+                            coeff_seed=cseed, tilt=np.array(tilt), flags=np.array([p.bnormflag, p.bzeroflag,
+                                                                                   p.switchflag]),
+                            skin=SKIN, neighmax=NEIGHMAX, x=x, box=H, coeff=p.coeff, xall=xa0, alist=al0,
+                            neighlist=nl0, neighnum=nn0, neighlist_cell=nl1, neighnum_cell=nn1,
+                            xall_cell=xa1, alist_cell=al1, eatom=e, fatom=f, vatom=va)
+        print(name, x.shape[0], "atoms", xa0.shape[0] - x.shape[0], "ghosts", os.path.getsize(path), "bytes")
+
+
 def main():
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
     fit_fixtures()
     if "--fit-only" in sys.argv:
+        return
+    tri_fixtures()
+    if "--tri-only" in sys.argv:
         return
     for (name, cells, tj, temp, jit, seed, cseed, flags, nsteps, dt) in CASES:
         p = configs.snap_params(tj, seed=cseed, **flags)
