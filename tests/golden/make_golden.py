@@ -121,6 +121,20 @@ TRI_FIT_CASES = [
 ]
 
 
+# sparse descriptor fixtures: (name, atoms, box edge, seed, 2J); one isolated atom, or atoms uniform in
+# the box (many with no neighbour inside the cutoff)
+SPARSE_FIT_CASES = [
+    ("fit_isolated1_2j8", 1, 20.0, 41, 8),
+    ("fit_gas40_2j8", 40, 32.0, 42, 8),
+]
+
+
+def sparse_config(n, edge, seed):
+    from mdp_b200 import fit
+    x = np.array([[3.0, 4.0, 5.0]]) if n == 1 else np.random.default_rng(seed).uniform(0.0, edge, (n, 3))
+    return fit.FitConfig(x=x, box=np.array([edge, edge, edge]), kind="sparse")
+
+
 def sheared(cfg, tilt):
     """The configuration in the sheared cell of the tilts (xy, xz, yz)."""
     from mdp_b200 import fit
@@ -144,6 +158,16 @@ def fit_fixtures():
         bi, bd, bv, bl = refpy.snap_descriptors(xa, al, nl, nn, p)
         path = os.path.join(HERE, f"{name}.npz")
         np.savez_compressed(path, kind=kind, twojmax=tj, flags=np.array([p.bnormflag, p.bzeroflag, p.switchflag]),
+                            x=cfg.x, box=cfg.box, bi=bi, bd=bd, bv=bv, blist=bl)
+        print(name, cfg.natoms, "atoms", os.path.getsize(path), "bytes")
+    for (name, n, edge, seed, tj) in SPARSE_FIT_CASES:
+        cfg = sparse_config(n, edge, seed)
+        p = configs.snap_params(tj, seed=0)
+        xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+        bi, bd, bv, bl = refpy.snap_descriptors(xa, al, nl, nn, p)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, kind=cfg.kind, twojmax=tj, flags=np.array([p.bnormflag, p.bzeroflag,
+                                                                             p.switchflag]),
                             x=cfg.x, box=cfg.box, bi=bi, bd=bd, bv=bv, blist=bl)
         print(name, cfg.natoms, "atoms", os.path.getsize(path), "bytes")
 
