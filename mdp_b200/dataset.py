@@ -65,6 +65,7 @@ class Frame:
     stress: np.ndarray | None = None
     types: np.ndarray | None = None  # (N,) 1-based species index
     source: str = ""
+    pbc: tuple = (True, True, True)  # periodic along a, b, c
 
 
 def _frames_of(text: str, species, source: str):
@@ -148,7 +149,8 @@ def read_extxyz(path: str, species=("Ta",)) -> list[Frame]:
                 types[[i for i, t in enumerate(names) if t == sp]] = k + 1
         e = float(kv["energy"]) if "energy" in kv else None
         st = np.array(kv["stress"].split(), dtype=np.float64).reshape(3, 3) if "stress" in kv else None
-        out.append(Frame(natoms=n, lattice=lat, x=x, e=e, f=f, stress=st, types=types, source=path))
+        pbc = tuple(t.upper() in ("T", "TRUE", "1") for t in kv["pbc"].split()) if "pbc" in kv else (True,) * 3
+        out.append(Frame(natoms=n, lattice=lat, x=x, e=e, f=f, stress=st, types=types, source=path, pbc=pbc))
         m += 2 + n
     return out
 
@@ -223,10 +225,13 @@ def stress_rows(bv: np.ndarray, cell: np.ndarray, copies: int, normalize_stress:
 
 
 def batch_of(groups, rcut: float, normalize_energy: bool = True):
-    """(configs, e, f, we, wf, copies, group index) for set_batch."""
+    """(configs, e, f, we, wf, copies, group index) for set_batch.  Every
+    frame must be periodic along all three cell vectors."""
     cfgs, e, f, we, wf, copies, gid = [], [], [], [], [], [], []
     for g, grp in enumerate(groups):
         for fr in grp.frames:
+            if not all(fr.pbc):
+                raise ValueError(f"{fr.source or grp.name}: pbc {fr.pbc}; the batched fit needs periodic cells")
             cfg, m = replicate(fr, rcut)
             cfgs.append(cfg)
             copies.append(m)

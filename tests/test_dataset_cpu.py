@@ -173,3 +173,15 @@ def test_stress_rows_use_the_reference_component_order():
     np.testing.assert_allclose(R[:, 0], 0.0)
     np.testing.assert_allclose(R[:, 1:], s * bv.T[[0, 1, 2, 5, 4, 3]])
     assert dataset.VOIGT[3] == (1, 2) and dataset.VOIGT[5] == (0, 1)
+
+
+def test_non_periodic_frames_are_refused(tmp_path):
+    fr = bcc2(seed=1)
+    fr.e, fr.f, fr.stress = -20.0, np.zeros((2, 3)), np.zeros((3, 3))
+    write_extxyz(tmp_path / "a.xyz", [fr])
+    text = (tmp_path / "a.xyz").read_text().replace('pbc="T T T"', 'pbc="T T F"')
+    (tmp_path / "a.xyz").write_text(text)
+    got = dataset.read_extxyz(str(tmp_path / "a.xyz"))
+    assert got[0].pbc == (True, True, False)
+    with pytest.raises(ValueError, match="periodic"):
+        dataset.batch_of([dataset.Group("slab", got)], 4.67637)
