@@ -928,6 +928,12 @@ static int fit_alloc_work(mdp_fit *h)
     }
     const long nt = 3 * h->chunk_pairs_max;
     const int nbmax = (int)((h->nrows + 255) / 256) + 1;   // smallest Gram rows-per-CTA candidate
+    if (!h->gram_tuned) {
+        // rows per Gram CTA: the largest candidate that still gives two CTAs per SM
+        h->gram_rows = 256;
+        for (int c : {1024, 4096})
+            if (h->nrows / c >= 2L * num_sms()) h->gram_rows = c;
+    }
     if (h->fp.Ut.ensure(sizeof(double2) * ntiles * idxu_count(tj) * 32) ||
         h->Z.ensure(sizeof(double2) * (size_t)h->chunk_tiles_max * h->tab.nz * 32) ||
         h->B.ensure(sizeof(double) * h->tab.ntri * (size_t)n) ||
@@ -1264,6 +1270,7 @@ int mdp_fit_tune(mdp_fit *h, int *out3)
         if (t >= 0 && t < bt) { bt = t; bsel = c; }
     }
     h->gram_rows = bsel;
+    h->gram_tuned = true;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     MDP_CUDA_TRY(cudaGetLastError());

@@ -56,6 +56,7 @@ struct mdp_fit {
     int chunk_tiles_max = 0;
     // launch shapes (autotuned): threads of the per-pair kernels, rows per Gram CTA
     int du_threads = 128, db_threads = 128, gram_rows = 4096;
+    bool gram_tuned = false;   // gram_rows chosen by mdp_fit_tune (else sized from the row count)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     int graph_mode = -1;
