@@ -239,8 +239,10 @@ def batch_of(groups, rcut: float, normalize_energy: bool = True):
             e.append(m * (fr.e if fr.e is not None else 0.0))
             ff = fr.f if fr.f is not None else np.zeros((fr.natoms, 3))
             f.append(np.tile(ff, (m, 1)))
-            we.append(grp.we / (cfg.natoms if normalize_energy else m))
-            wf.append(grp.wf / np.sqrt(m))
+            # rows of data a frame does not carry get zero weight (emldescriptors.jl adds rows only for
+            # energies / forces that are present)
+            we.append(0.0 if fr.e is None else grp.we / (cfg.natoms if normalize_energy else m))
+            wf.append(0.0 if fr.f is None else grp.wf / np.sqrt(m))
     return (cfgs, np.array(e), np.concatenate(f), np.array(we), np.array(wf), np.array(copies),
             np.array(gid))
 
@@ -308,15 +310,20 @@ def fit_groups(groups, params: SnapParams, normalize_energy: bool = True, normal
         de, dfs, dss = [], [], []
         for c in np.nonzero(gid == g)[0]:
             n0 = counts[c] // copies[c]
-            de.append((e_pred[c] - e[c]) / counts[c])
-            fp = bd[a0[c]:a0[c] + n0] @ beta[1:]
-            dfs.append((fp - f[a0[c]:a0[c] + n0]).ravel())
+            if frames[c].e is not None:
+                de.append((e_pred[c] - e[c]) / counts[c])
+            if frames[c].f is not None:
+                fp = bd[a0[c]:a0[c] + n0] @ beta[1:]
+                dfs.append((fp - f[a0[c]:a0[c] + n0]).ravel())
             if srows[c] is not None:
                 dss.append(srows[c] @ beta + sref[c] - np.array([frames[c].stress[i, j] for i, j in VOIGT]))
-        de, dfs = np.array(de), np.concatenate(dfs)
-        err = dict(group=grp.name, frames=len(de),
-                   energy_mae=float(np.abs(de).mean()), energy_rmse=float(np.sqrt((de ** 2).mean())),
-                   force_mae=float(np.abs(dfs).mean()), force_rmse=float(np.sqrt((dfs ** 2).mean())))
+        err = dict(group=grp.name, frames=int((gid == g).sum()))
+        if de:
+            de = np.array(de)
+            err.update(energy_mae=float(np.abs(de).mean()), energy_rmse=float(np.sqrt((de ** 2).mean())))
+        if dfs:
+            dfs = np.concatenate(dfs)
+            err.update(force_mae=float(np.abs(dfs).mean()), force_rmse=float(np.sqrt((dfs ** 2).mean())))
         if dss:
             dss = np.concatenate(dss)
             err.update(stress_mae=float(np.abs(dss).mean()), stress_rmse=float(np.sqrt((dss ** 2).mean())))

@@ -185,3 +185,12 @@ def test_non_periodic_frames_are_refused(tmp_path):
     assert got[0].pbc == (True, True, False)
     with pytest.raises(ValueError, match="periodic"):
         dataset.batch_of([dataset.Group("slab", got)], 4.67637)
+
+
+def test_missing_energy_or_forces_get_zero_weight():
+    a, b = bcc2(seed=1), bcc2(seed=2)
+    a.e = -20.0                                         # a: energy only; b: forces only
+    b.f = np.ones((2, 3))
+    cfgs, e, f, we, wf, copies, gid = dataset.batch_of([dataset.Group("g", [a, b], we=3.0, wf=2.0)], 4.67637)
+    assert we[0] > 0 and wf[0] == 0.0
+    assert we[1] == 0.0 and wf[1] > 0
