@@ -54,6 +54,7 @@ TWOJ = 8
 DT = 0.001
 SKIN = 1.0
 NEIGHMAX = 64
+GLOBALFREQ = 10                    # thermo output every 10 steps, as simulating/snap/snapTA06A.jl sets it
 SAMPLE_CELLS = (20, 20, 20)        # CPU-baseline sample: 16,000 atoms
 
 
@@ -150,7 +151,9 @@ class CpuSample:
         from mdp_b200 import configs
         from oracle import refpy
         if not refpy.available():
-            subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "oracle"), "ref"])
+            from oracle.refroot import reference_root
+            subprocess.check_call(["make", "-s", "-C", os.path.join(HERE, "oracle"), "ref",
+                                   f"REFROOT={reference_root() or ''}"])
         self.refpy = refpy
         self.p = configs.snap_params(TWOJ, seed=2024)
         self.cfg = configs.ta_config(SAMPLE_CELLS, temp=300.0, jitter=0.05, seed=2024)
@@ -244,7 +247,7 @@ def surrogate_leg(args, dev, barrier, ws):
         md.setup()
         md.run(args.warmup)
         barrier()
-        _, ms = md.run(args.steps)
+        _, ms = md.run(args.steps, thermo_every=GLOBALFREQ)
         barrier()
         st = md.surrogate_status()
         md.close()
@@ -291,7 +294,7 @@ def run_ours(args):
     barrier()
     clocks.start()
     l0 = launch_count()
-    _, ms = md.run(args.steps)
+    _, ms = md.run(args.steps, thermo_every=GLOBALFREQ)
     l1 = launch_count()
     barrier()
     clk = clocks.stop()
@@ -348,7 +351,7 @@ def run_ours(args):
     md32.setup()
     md32.run(args.warmup)
     barrier()
-    _, ms32 = md32.run(args.steps)
+    _, ms32 = md32.run(args.steps, thermo_every=GLOBALFREQ)
     barrier()
     md32.stage_timing(True)              # per-stage CUDA events, after the timed steps
     md32.run(2)
@@ -396,7 +399,8 @@ def run_ours(args):
                                    "SNAP 2J=8 (55 components), seeded beta, dt 1 fs, skin 1 A",
                        "atoms": n, "twojmax": TWOJ, "pairs_per_atom": pairs / n,
                        "l2": "inputs larger than L2 (U 9 GB, Y 5 GB per step)",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU"},
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "1 GPU",
+                       "thermo": f"every {GLOBALFREQ} steps inside the timed window (reference globalfreq)"},
             "e2e": {"value": e2e_value, "unit": "atom-steps/s", "h2d_bytes_per_step": int(hx.nbytes + hv.nbytes),
                     "d2h_bytes_per_step": int(hf.nbytes + he.nbytes)},
             "gpu_launches": int(launches),

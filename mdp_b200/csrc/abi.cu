@@ -316,8 +316,9 @@ int ref_snap_ui(double *ur, double *ui, const double *rij, double rcut, double w
 #define MDP_UIREF(TJ)                                                                                              \
     {                                                                                                              \
         const size_t sm = (size_t)UI_WARPS * (idxu_count(TJ) + 32 * (TJ + 1)) * sizeof(double2);                  \
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_ui<double, TJ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                          (int)sm));                                                               \
+        int per_sm = 0;                                                                                            \
+        if (kernel_setup((const void *)k_snap_ui<double, TJ, true>, UI_WARPS * 32, sm, &per_sm, "k_snap_ui"))      \
+            return -1;                                                                                             \
         k_snap_ui<double, TJ, true><<<blocks, UI_WARPS * 32, sm, s>>>(c.off.as<int>(), c.fp.prij.as<double4>(),    \
                                                                       inum, c.model.geom, nullptr, ur, ui);        \
     }

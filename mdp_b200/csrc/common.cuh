@@ -14,6 +14,8 @@
 #include <stdio.h>
 #include <mutex>
 
+#include "device_cache.h"
+
 namespace mdp {
 
 constexpr int TJMAX = 8;
@@ -103,17 +105,16 @@ static inline int tu_ensure_tables()
     return 0;
 }
 
-static inline int num_sms()
-{
-    static int n = 0;
-    if (!n) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-        if (n <= 0) n = 148;
-    }
-    return n;
-}
+// SM count of the current device (cached per device).
+int num_sms();
+
+// Launch set-up of a kernel on the current device: raises its dynamic
+// shared-memory limit to smem bytes and returns in *per_sm how many CTAs of
+// `threads` threads fit on one SM.  Done once per (kernel, device) under a
+// lock; cudaFuncSetAttribute is per device, so a second GPU in the same
+// process gets its own set-up.  Returns -1 (error set) if the kernel cannot
+// launch with that much shared memory.
+int kernel_setup(const void *fn, int threads, size_t smem, int *per_sm, const char *name);
 
 template <typename T> struct cplx;
 template <> struct cplx<double> { typedef double2 type; };

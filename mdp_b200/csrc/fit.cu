@@ -805,12 +805,10 @@ static int fit_descriptor_stages(mdp_fit *h, bool rows, double *G = nullptr, dou
                             : launch_ui<double, 4>(h->model, h->fp, n, h->s);
     if (urc) return -1;
     count_launches(1);
-    static bool attr = false;
-    if (!attr) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_fit_zb, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)((size_t)idxu_count(TJMAX) * 32 * sizeof(double2))));
-        attr = true;
-    }
+    int zb_per_sm = 0;
+    if (kernel_setup((const void *)k_fit_zb, FIT_ZB_WARPS * 32, (size_t)idxu_count(TJMAX) * 32 * sizeof(double2),
+                     &zb_per_sm, "k_fit_zb"))
+        return -1;
     for (const auto &ck : h->chunks)
         if (fit_chunk(h, ck, rows, G, bi, bv)) return -1;
     MDP_CUDA_TRY(cudaGetLastError());
@@ -827,12 +825,10 @@ int fit_pair_derivs(mdp_fit *h, float *dbdr_out, double *blist_out)
                   : tj == 6 ? launch_ui<double, 6>(h->model, h->fp, n, h->s)
                             : launch_ui<double, 4>(h->model, h->fp, n, h->s);
     if (urc) return -1;
-    static bool attr = false;
-    if (!attr) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_fit_zb, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)((size_t)idxu_count(TJMAX) * 32 * sizeof(double2))));
-        attr = true;
-    }
+    int zb_per_sm = 0;
+    if (kernel_setup((const void *)k_fit_zb, FIT_ZB_WARPS * 32, (size_t)idxu_count(TJMAX) * 32 * sizeof(double2),
+                     &zb_per_sm, "k_fit_zb"))
+        return -1;
     const size_t zsm = (size_t)idxu_count(tj) * 32 * sizeof(double2);
     for (const auto &ck : h->chunks) {
         k_fit_zb<<<std::max(1, std::min(ck.t_hi - ck.t_lo, num_sms())), FIT_ZB_WARPS * 32, zsm, h->s>>>(

@@ -11,12 +11,8 @@ static int launch_bi(const typename cplx<T>::type *Ut, int natoms, int bnorm, in
 {
     if (tu_ensure_tables()) return -1;
     const size_t sm = (size_t)idxu_count(TJ) * 32 * sizeof(typename cplx<T>::type);
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_bi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_bi<T, TJ>, BI_WARPS * 32, sm));
-        if (per_sm < 1) { set_error("k_snap_bi does not fit"); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_bi<T, TJ>, BI_WARPS * 32, sm, &per_sm, "k_snap_bi")) return -1;
     const int blocks = std::min((natoms + 31) / 32, num_sms() * per_sm);
     k_snap_bi<T, TJ><<<blocks, BI_WARPS * 32, sm, s>>>(Ut, natoms, bnorm, bzero, bout, bstride);
     count_launches(1);

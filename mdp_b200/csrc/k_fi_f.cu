@@ -12,12 +12,8 @@ int launch_fi(const SnapModel &m, ForcePath &fp, int inum, int /*nm*/, cudaStrea
     if (tu_ensure_tables()) return -1;
     if (fp.timing) cudaEventRecord(fp.ev[3], s);
     const size_t sm = fr_smem_bytes<T, TJ>();
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_fr32<TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_fr32<TJ>, FR_THREADS, sm));
-        if (per_sm < 1) { set_error("k_snap_fr does not fit on an SM"); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_fr32<TJ>, FR_THREADS, sm, &per_sm, "k_snap_fr")) return -1;
     const int blocks = num_sms() * per_sm;
     k_snap_fr32<TJ><<<blocks, FR_THREADS, sm, s>>>(fp.prij.as<double4>(), fp.pinfo.as<int2>(),
                                                     fp.poff.as<int>() + inum, m.geom, fp.Y.as<T2>(),

@@ -11,12 +11,8 @@ int launch_ui(const SnapModel &m, ForcePath &fp, int inum, cudaStream_t s)
     typedef typename cplx<T>::type T2;
     if (tu_ensure_tables()) return -1;
     const size_t sm = uc_smem_bytes<T, TJ>();
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_uc<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_uc<T, TJ>, uc_warps<TJ>() * 32, sm));
-        if (per_sm < 1) { set_error("k_snap_uc does not fit on an SM"); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_uc<T, TJ>, uc_warps<TJ>() * 32, sm, &per_sm, "k_snap_uc")) return -1;
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[1], s);

@@ -11,12 +11,8 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
     typedef typename cplx<T>::type T2;
     if (tu_ensure_tables()) return -1;
     const size_t sm = yi_smem_bytes<T, TJ>();
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<T, TJ>, YiWarps<T, TJ>::n * 32, sm));
-        if (per_sm < 1) { set_error("k_snap_yi does not fit on an SM (%zu B shared)", sm); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_yi<T, TJ>, YiWarps<T, TJ>::n * 32, sm, &per_sm, "k_snap_yi")) return -1;
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[2], s);
@@ -31,14 +27,10 @@ static int launch_yi_pa_d_tj(const SnapModel &m, ForcePath &fp, int inum, const 
 {
     if (tu_ensure_tables()) return -1;
     const size_t sm = yi_smem_bytes<double, TJ, true>();
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<double, TJ, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<double, TJ, true>,
-                                                                   YiWarps<double, TJ>::n * 32, sm));
-        if (per_sm < 1) { set_error("k_snap_yi (per-atom, FP64) does not fit on an SM (%zu B shared)", sm); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_yi<double, TJ, true>, YiWarps<double, TJ>::n * 32, sm, &per_sm,
+                     "k_snap_yi (per-atom, FP64)"))
+        return -1;
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     k_snap_yi<double, TJ, true><<<blocks, YiWarps<double, TJ>::n * 32, sm, s>>>(fp.Ut.as<double2>(), inum, m.yd,

@@ -11,12 +11,8 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
     typedef typename cplx<T>::type T2;
     if (tu_ensure_tables()) return -1;
     const size_t sm = yi_smem_bytes<T, TJ>();
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<T, TJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<T, TJ>, YiWarps<T, TJ>::n * 32, sm));
-        if (per_sm < 1) { set_error("k_snap_yi does not fit on an SM (%zu B shared)", sm); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_yi<T, TJ>, YiWarps<T, TJ>::n * 32, sm, &per_sm, "k_snap_yi")) return -1;
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[2], s);
@@ -29,13 +25,10 @@ int launch_yi_pa_f4(const SnapModel &m, ForcePath &fp, int inum, const float *G,
 {
     if (tu_ensure_tables()) return -1;
     const size_t sm = yi_smem_bytes<float, 4, true>();
-    static int per_sm = 0;
-    if (!per_sm) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_snap_yi<float, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        MDP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_snap_yi<float, 4, true>,
-                                                                   YiWarps<float, 4>::n * 32, sm));
-        if (per_sm < 1) { set_error("k_snap_yi (per-atom) does not fit on an SM"); return -1; }
-    }
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_yi<float, 4, true>, YiWarps<float, 4>::n * 32, sm, &per_sm,
+                     "k_snap_yi (per-atom)"))
+        return -1;
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[2], s);

@@ -735,8 +735,8 @@ int mdp_sur_create(mdp_sur **h, const mdp_snap_params *p4, int device)
         mdp_sur_destroy(S);
         return -1;
     }
-    if (cudaFuncSetAttribute(k_sur_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUR_TR_SMEM) != cudaSuccess) {
-        set_error("k_sur_grad shared memory (%zu B) not available", SUR_TR_SMEM);
+    int tr_per_sm = 0;
+    if (kernel_setup((const void *)k_sur_grad, SUR_TR_THREADS, SUR_TR_SMEM, &tr_per_sm, "k_sur_grad")) {
         mdp_sur_destroy(S);
         return -1;
     }
@@ -988,11 +988,8 @@ int mdp_sur_train_forces(mdp_sur *S, int steps, int snaps_per_batch, float lr, f
     if (!S->trained) { set_error("set initial parameters first"); return -1; }
     if (S->f_snaps < snaps_per_batch) { set_error("force set holds %d snapshots", S->f_snaps); return -1; }
     MDP_CUDA_TRY(cudaSetDevice(S->device));
-    static bool attr = false;
-    if (!attr) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_sur_grad_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUR_TF_SMEM));
-        attr = true;
-    }
+    int tf_per_sm = 0;
+    if (kernel_setup((const void *)k_sur_grad_f, SUR_TF_THREADS, SUR_TF_SMEM, &tf_per_sm, "k_sur_grad_f")) return -1;
     const int n = snaps_per_batch * S->f_per;
     if (S->fG.ensure(sizeof(float) * SUR_NK * (size_t)n) || S->fQ.ensure(sizeof(float) * 3 * (size_t)n) ||
         S->fV.ensure(sizeof(float) * SUR_KP * (size_t)n))
@@ -1046,11 +1043,8 @@ int mdp_sur_force_grad(mdp_sur *S, int snap0, int snaps, float alpha, float *gra
 {
     if (!S || !grad || snaps < 1 || snap0 < 0 || snap0 + snaps > S->f_snaps) { set_error("bad arguments"); return -1; }
     MDP_CUDA_TRY(cudaSetDevice(S->device));
-    static bool attr = false;
-    if (!attr) {
-        MDP_CUDA_TRY(cudaFuncSetAttribute(k_sur_grad_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SUR_TF_SMEM));
-        attr = true;
-    }
+    int tf_per_sm = 0;
+    if (kernel_setup((const void *)k_sur_grad_f, SUR_TF_THREADS, SUR_TF_SMEM, &tf_per_sm, "k_sur_grad_f")) return -1;
     const int n = snaps * S->f_per, a_lo = snap0 * S->f_per;
     if (S->fG.ensure(sizeof(float) * SUR_NK * (size_t)n) || S->fQ.ensure(sizeof(float) * 3 * (size_t)n) ||
         S->fV.ensure(sizeof(float) * SUR_KP * (size_t)n))

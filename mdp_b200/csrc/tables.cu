@@ -25,6 +25,50 @@ void set_error(const char *fmt, ...)
 }
 const char *get_error() { return g_err; }
 
+static int current_device(int *dev)
+{
+    if (cudaGetDevice(dev) != cudaSuccess || *dev < 0) {
+        set_error("no current CUDA device");
+        return -1;
+    }
+    return 0;
+}
+
+static PerDeviceMemo g_sms, g_kernels;
+
+int num_sms()
+{
+    int dev = 0, n = 0;
+    if (current_device(&dev)) return 148;
+    auto setup = [dev](int *v) {
+        if (cudaDeviceGetAttribute(v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || *v <= 0) return -1;
+        return 0;
+    };
+    if (g_sms.get(nullptr, 0, dev, setup, &n)) return 148;
+    return n;
+}
+
+int kernel_setup(const void *fn, int threads, size_t smem, int *per_sm, const char *name)
+{
+    int dev = 0;
+    if (current_device(&dev)) return -1;
+    auto setup = [&](int *v) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(v, fn, threads, smem);
+        if (e != cudaSuccess) {
+            set_error("%s: launch set-up with %zu B shared memory failed on device %d: %s", name, smem, dev,
+                      cudaGetErrorString(e));
+            return -1;
+        }
+        if (*v < 1) {
+            set_error("%s does not fit on an SM of device %d (%zu B shared, %d threads)", name, dev, smem, threads);
+            return -1;
+        }
+        return 0;
+    };
+    return g_kernels.get(fn, ((long)smem << 16) | threads, dev, setup, per_sm);
+}
+
 // Clebsch-Gordan coefficients by the Racah formula, in the block order of
 // src/C++/Core/cpuSnap.cpp:137-193 (aa2, bb2, cc2 are doubled m values).
 void host_cg_table(double *cg)

@@ -1,12 +1,12 @@
 """Small, fixed workloads for kernel profiling.
 
-    python -m mdp_b200.profile_case fp64|fp32 CELLS [REPEAT]
+    python profile_case.py fp64|fp32 CELLS [REPEAT]
         REPEAT (default 2) SNAP force evaluations (snap_compute) on a
         CELLS^3-cell BCC Ta lattice (2*CELLS^3 atoms, jitter 0.05 A, 2J=8).
-    python -m mdp_b200.profile_case sur CELLS [REPEAT]
+    python profile_case.py sur CELLS [REPEAT]
         the surrogate force path (random network, normalised on the lattice's
         own features) for REPEAT steps of NVE on the same lattice.
-    python -m mdp_b200.profile_case fit NCONF [REPEAT]
+    python profile_case.py fit NCONF [REPEAT]
         REPEAT runs of the batched descriptors + FP64 normal equations over
         NCONF configurations of the fitting workload.
 
@@ -16,11 +16,13 @@ configurations) so profiler replays finish quickly.
 """
 from __future__ import annotations
 
+import os
 import sys
 
 import numpy as np
 
-from . import configs
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+from mdp_b200 import configs  # noqa: E402
 
 
 def main(argv=None):
@@ -29,7 +31,7 @@ def main(argv=None):
     n = int(argv[1]) if len(argv) > 1 else 20
     rep = int(argv[2]) if len(argv) > 2 else 2
     if kind in ("fp64", "fp32"):
-        from .snap import snap_compute
+        from mdp_b200.snap import snap_compute
         p = configs.snap_params(8, seed=1)
         cfg = configs.ta_config((n, n, n), temp=300, jitter=0.05, seed=1)
         out = None
@@ -37,8 +39,8 @@ def main(argv=None):
             out = snap_compute(p, cfg.x, cfg.box, 1.0, 64, precision=kind)
         print("ok", cfg.natoms, float(out["eatom"].sum()))
     elif kind == "sur":
-        from . import surrogate as su
-        from .snap import SnapMD
+        from mdp_b200 import surrogate as su
+        from mdp_b200.snap import SnapMD
         p = configs.snap_params(8, seed=1)
         cfg = configs.ta_config((n, n, n), temp=1000, jitter=0.09, seed=1)
         sur = su.Surrogate(configs.snap_params(4, seed=0))
@@ -52,7 +54,7 @@ def main(argv=None):
         md.run(rep)
         print("ok", cfg.natoms, float(md.state()[3].sum()))
     elif kind == "fit":
-        from . import fit
+        from mdp_b200 import fit
         cfgs, e, f = fit.batch_configs(n, seed=3)
         bf = fit.BatchFit(configs.snap_params(8, seed=0))
         bf.set_batch(cfgs, e, f)

@@ -19,7 +19,7 @@ def pytest_configure(config):
 def golden_names():
     """Force / MD fixtures (the fit_* fixtures hold descriptors and are listed by fit_names)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("fit_", "tri_")))
+                  if not os.path.basename(p).startswith(("fit_", "tri_", "c2_", "chem_")))
 
 
 def tri_names():
@@ -29,6 +29,20 @@ def tri_names():
 
 def fit_names():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "fit_*.npz")))
+
+
+def row_hashes(nl, nn):
+    """One 64-bit hash per neighbour row of its sorted index set: the rows of
+    a 16,000-atom list are pinned by 128 KB instead of the list itself."""
+    nl = np.asarray(nl)
+    nn = np.asarray(nn).astype(np.int64)
+    cols = np.arange(nl.shape[1])[None, :]
+    srt = np.sort(np.where(cols < nn[:, None], nl, np.iinfo(np.int32).max), axis=1).astype(np.uint64)
+    h = nn.astype(np.uint64)
+    with np.errstate(over="ignore"):
+        for k in range(nl.shape[1]):
+            h = h * np.uint64(1000003) + np.where(k < nn, srt[:, k] + np.uint64(1), np.uint64(0))
+    return h
 
 
 def load_golden(name):

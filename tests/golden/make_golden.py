@@ -36,6 +36,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
 
 from mdp_b200 import configs  # noqa: E402
 from oracle import refpy  # noqa: E402
@@ -64,16 +65,19 @@ def thermo_row(step, e, v, vatom, box, mass):
     return [step, temp, pe, pe + ke, pres]
 
 
-def ref_md(x0, v0, box, p, nsteps, dt, mass):
-    """NVE in the reference's step order using the reference's own kernels."""
+def ref_md(x0, v0, box, p, nsteps, dt, mass, neighmax=NEIGHMAX, nthreads=1, snap_steps=(), snap_atoms=None):
+    """NVE in the reference's step order using the reference's own kernels.
+    With snap_steps, also returns {step: (x, v)} of the atoms snap_atoms at those steps."""
     dtf = 0.5 * dt * configs.FTM2V
     ilist = np.arange(x0.shape[0], dtype=np.int32)
     typ = np.ones(x0.shape[0] + 1, dtype=np.int32)
     massarr = np.array([0.0, mass])
     x = x0.copy(); v = v0.copy()
-    xa, al, nl, nn = refpy.neighbor_list(x, box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+    nb = dict(nblocks=8 * nthreads, nthreads=nthreads) if nthreads > 1 else {}
+    snaps = {}
+    xa, al, nl, nn = refpy.neighbor_list(x, box, p.rcut, SKIN, neighmax, neighcell=0)
     xhold = x.copy()
-    e, f, va = refpy.snap_force(xa, al, nl, nn, p)
+    e, f, va = refpy.snap_force(xa, al, nl, nn, p, **nb)
     rows = [thermo_row(0, e, v, va, box, mass)]
     rebuilds = 1
     n = x.shape[0]
@@ -86,19 +90,25 @@ def ref_md(x0, v0, box, p, nsteps, dt, mass):
         if np.max(np.sum((x - xhold) ** 2, axis=1)) > 0.25 * SKIN * SKIN:
             x = np.where(x < 0.0, x + box, x)
             x = np.where(x >= box, np.maximum(x - box, 0.0), x)
-            xa, al, nl, nn = refpy.neighbor_list(x, box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+            xa, al, nl, nn = refpy.neighbor_list(x, box, p.rcut, SKIN, neighmax, neighcell=0)
+            if nn.max() >= neighmax:
+                raise RuntimeError("neighmax too small for the reference trajectory")
             xhold = x.copy()
             rebuilds += 1
         else:
             xa = xa.copy()
             xa[:n] = x
             xa[n:] += (x - xstart)[al[n:]]
-        e, f, va = refpy.snap_force(xa, al, nl, nn, p)
+        e, f, va = refpy.snap_force(xa, al, nl, nn, p, **nb)
         vf = np.ascontiguousarray(v).ravel()
         lib.ref_nve_final(np.ascontiguousarray(x).ravel(), vf, np.ascontiguousarray(f).ravel(), massarr, dtf, typ,
                           ilist, n)
         v = vf.reshape(n, 3)
         rows.append(thermo_row(step, e, v, va, box, mass))
+        if step in snap_steps:
+            snaps[step] = (x[snap_atoms].copy(), v[snap_atoms].copy())
+    if snap_steps:
+        return np.array(rows), x, v, f, e, rebuilds, snaps
     return np.array(rows), x, v, f, e, rebuilds
 
 
@@ -210,8 +220,58 @@ def tri_fixtures():
         print(name, x.shape[0], "atoms", xa0.shape[0] - x.shape[0], "ghosts", os.path.getsize(path), "bytes")
 
 
+# The 16,000-atom configuration of the benchmark's FP64-vs-reference check: 20x20x20 BCC Ta cells at
+# 600 K, jitter 0.05 A, 2J=8 with seeded coefficients, 1,000 NVE steps of 1 fs.
+C2 = dict(name="c2_bcc16000_2j8", cells=(20, 20, 20), twojmax=8, temp=600.0, jitter=0.05, seed=2016,
+          coeff_seed=2017, dt=0.001, steps=1000, neighmax=80, snap_steps=(100, 1000), atom_stride=8)
+
+
+def row_hashes(nl, nn):
+    """One 64-bit hash per neighbour row, of its sorted index set (tests/conftest.py restates it)."""
+    from conftest import row_hashes as rh
+    return rh(nl, nn)
+
+
+def c2_fixture(nthreads):
+    """The reference's neighbour rows (as per-row hashes), ghosts, per-atom energy/force/virial sums
+    and a 1,000-step NVE run (thermo every step; positions and velocities of every 8th atom at steps
+    100 and 1,000) for the 16,000-atom configuration."""
+    c = C2
+    p = configs.snap_params(c["twojmax"], seed=c["coeff_seed"])
+    cfg = configs.ta_config(c["cells"], temp=c["temp"], jitter=c["jitter"], seed=c["seed"])
+    nm = c["neighmax"]
+    xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, nm, neighcell=0)
+    xa1, al1, nl1, nn1 = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, nm, neighcell=1)
+    e, f, va = refpy.snap_force(xa, al, nl, nn, p, nblocks=8 * nthreads, nthreads=nthreads)
+    atoms = np.arange(0, cfg.natoms, c["atom_stride"])
+    th, x, v, ff, ee, nreb, snaps = ref_md(cfg.x, cfg.v, cfg.box, p, c["steps"], c["dt"], configs.TA_MASS,
+                                           neighmax=nm, nthreads=nthreads, snap_steps=c["snap_steps"],
+                                           snap_atoms=atoms)
+    out = dict(cells=np.array(c["cells"]), twojmax=c["twojmax"], temp=c["temp"], jitter=c["jitter"],
+               seed=c["seed"], coeff_seed=c["coeff_seed"], skin=SKIN, neighmax=nm, md_dt=c["dt"],
+               md_steps=c["steps"], box=cfg.box, coeff=p.coeff,
+               x_check=np.array([cfg.x.sum(), (cfg.x ** 2).sum()]), v_check=np.array([cfg.v.sum(), (cfg.v ** 2).sum()]),
+               ghosts=xa.shape[0] - cfg.natoms, xall_check=np.array([xa.sum(), (xa ** 2).sum()]),
+               alist_check=np.array([int(al.astype(np.int64).sum()), int((al.astype(np.int64) ** 2).sum())]),
+               neighnum=nn.astype(np.int8), row_hash=row_hashes(nl, nn), cell_rows_equal=np.array(
+                   [tuple(sorted(nl[i, :nn[i]])) == tuple(sorted(nl1[i, :nn1[i]])) for i in range(cfg.natoms)]).all(),
+               e_check=np.array([e.sum(), (e ** 2).sum()]), f_check=np.array([f.sum(), (f ** 2).sum()]),
+               v_virial_check=np.array([va.sum(), (va ** 2).sum()]),
+               md_thermo=th, md_rebuilds=nreb, md_atoms=atoms)
+    for st, (xs, vs) in snaps.items():
+        out[f"md_x_{st}"] = xs
+        out[f"md_v_{st}"] = vs
+    path = os.path.join(HERE, f"{c['name']}.npz")
+    np.savez_compressed(path, **out)
+    print(c["name"], cfg.natoms, "atoms", nreb, "list builds", os.path.getsize(path), "bytes")
+
+
 def main():
-    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"])
+    from oracle.refroot import reference_root
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REFROOT={reference_root() or ''}"])
+    if "--c2" in sys.argv:
+        c2_fixture(os.cpu_count() or 1)
+        return
     fit_fixtures()
     if "--fit-only" in sys.argv:
         return

@@ -8,8 +8,10 @@ import pytest
 
 from mdp_b200 import configs, dataset
 from oracle import oracle
+from oracle.refroot import reference_root
 
-TA_JSON = "/root/reference/fitting/snap/Ta/JSON"
+_REF = reference_root()
+TA_JSON = os.path.join(_REF, "fitting", "snap", "Ta", "JSON") if _REF else ""
 
 
 def write_json(path, frames, header="# A test JSON file for QM data\n"):

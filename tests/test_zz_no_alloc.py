@@ -5,9 +5,13 @@ device memory (a host application whose memory pool owns the device, or a loop
 that cannot take cudaMalloc/cudaFree's implicit synchronisation).  It keeps its
 scratch in a fixed array inside the library.  This test calls it through the C
 ABI twice in a row, on two different configurations, and checks each result
-against the existing entry point mdp_gpu_snap_compute_bi_f64; it also checks
-that a size beyond the fixed scratch is refused.  The file is named so pytest
-collects it last."""
+against the existing entry point mdp_gpu_snap_compute_bi_f64 and against the
+per-atom bispectrum of the reference's own library (cpuSnapComputeBi of
+oracle/_ref/libcpuSnap_ref.so, MDP's src/Julia/Potential/cpuSnap.cpp).  On the
+second call it also checks the property the entry point exists for: the free
+device memory is the same before and after the call.  A size beyond the fixed
+scratch is refused.  The file is named so pytest collects it last."""
+import os
 import ctypes as C
 
 import numpy as np
@@ -25,13 +29,21 @@ def rel_inf(a, b):
     return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
 
 
+REF_LIB = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref",
+                       "libcpuSnap_ref.so")
+
+
 def _u_of(name, lib_path):
     """U (wself added, mirrored) of a golden configuration in MDP's layout,
-    computed through this library's Julia-ABI entry points."""
+    computed through this library's Julia-ABI entry points, and the
+    reference library's per-atom bispectrum of the same configuration."""
     g = load_golden(name)
     p = golden_params(g)
     seq = julia_abi.snap_sequence(julia_abi.bind(lib_path), g, p)
-    return p, g["x"].shape[0], seq["u"], seq["tables"]
+    if not os.path.exists(REF_LIB):
+        pytest.fail("oracle/_ref/libcpuSnap_ref.so missing (build with make -C oracle ref)")
+    ref = julia_abi.snap_sequence(julia_abi.bind(REF_LIB), g, p)
+    return p, g["x"].shape[0], seq["u"], seq["tables"], ref["blist"]
 
 
 def test_no_alloc_bispectrum_matches_existing_entry(cuda_lib):
@@ -45,8 +57,8 @@ def test_no_alloc_bispectrum_matches_existing_entry(cuda_lib):
     L.mdp_gpu_snap_compute_bi_f64.restype = None
     dev = torch.device("cuda:0")
     stream = torch.cuda.current_stream().cuda_stream
-    for name in ("bcc250_2j8", "bcc54_2j8_flags"):   # two calls in a row, the second smaller
-        p, n, (ur, ui), t = _u_of(name, _lib.LIB_PATH)
+    for call, name in enumerate(("bcc250_2j8", "bcc54_2j8_flags")):   # two calls in a row, the second smaller
+        p, n, (ur, ui), t, bref = _u_of(name, _lib.LIB_PATH)
         ur_d = torch.tensor(ur, dtype=torch.float64, device=dev)
         ui_d = torch.tensor(ui, dtype=torch.float64, device=dev)
         nb = t["nb"]
@@ -56,13 +68,18 @@ def test_no_alloc_bispectrum_matches_existing_entry(cuda_lib):
                                       p.bzeroflag, p.wselfallflag, n)
         torch.cuda.synchronize()
         out = torch.full((nb * n,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         rc = L.mdp_gpu_snap_compute_bi_noalloc_f64(out.data_ptr(), ur_d.data_ptr(), ui_d.data_ptr(), p.twojmax,
                                                    p.bnormflag, p.bzeroflag, n, stream)
         assert rc == 0, L.mdp_last_error()
         torch.cuda.synchronize()
+        if call > 0:   # after the first call (which loads the kernels), nothing is allocated
+            assert torch.cuda.mem_get_info()[0] == free0
         a, b = out.cpu().numpy(), existing.cpu().numpy()
         assert np.all(np.isfinite(a))
         assert rel_inf(a, b) < TOL_FP64, name
+        assert rel_inf(a, np.asarray(bref).ravel()) < TOL_FP64, name
 
 
 def test_no_alloc_rejects_sizes_beyond_its_scratch(cuda_lib):
