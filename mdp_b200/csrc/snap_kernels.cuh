@@ -335,7 +335,7 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
 // ---------------------------------------------------------------------------
 // k_snap_uc: U of a 32-atom tile, one warp per column of the half plane.
 //
-// Lane = atom.  Each lane walks its own atom's pairs, UC_PB per iteration, and
+// Lane = atom.  Each lane walks its own atom's pairs, uc_pb<T>() per pass, and
 // per pair recomputes the recursion path that reaches its warp's column: the
 // seed chain (rows 1, 2c..2c+1 of the columns c below, each mirrored into the
 // next column's seed) and then the column's own rows, which it adds into a
@@ -347,7 +347,10 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
 // rows mb > j/2 by inversion symmetry (cpuSnap4.cpp:11-244, cpuAddWself2Ui).
 // (a, b, sfac) of each pair come from the pair stage.
 // ---------------------------------------------------------------------------
-constexpr int UC_PB = 1;
+// pairs per lane per pass: FP32 takes two (independent chains, half the tile
+// updates; 8.1 against 8.2 ms at 2M atoms); FP64 one (two measured 18.1
+// against 15.7 ms: twice the unrolled code per warp path)
+template <typename T> __host__ __device__ constexpr int uc_pb() { return std::is_same<T, float>::value ? 2 : 1; }
 template <int TJ> __host__ __device__ constexpr int uc_warps() { return TJ / 2; }
 template <typename T, int TJ> constexpr size_t uc_smem_bytes()
 {
@@ -358,8 +361,9 @@ template <typename T, int TJ> constexpr size_t uc_smem_bytes()
 // out weighted by sfac (the recursion is linear in its root)
 template <typename T, int TJ>
 struct UcPairs {
-    T ar[UC_PB], ai[UC_PB], br[UC_PB], bi[UC_PB];
-    T pr[UC_PB][TJ + 1], pi[UC_PB][TJ + 1];
+    static constexpr int PB = uc_pb<T>();
+    T ar[PB], ai[PB], br[PB], bi[PB];
+    T pr[PB][TJ + 1], pi[PB][TJ + 1];
 };
 
 // seed chain up to column MB: column C's last chain row (2C+1) mirrored into
@@ -370,7 +374,7 @@ __device__ __forceinline__ void uc_chain(UcPairs<T, TJ> &s)
     if constexpr (C < MB) {
         constexpr int J = 2 * C + 1;
 #pragma unroll
-        for (int q = 0; q < UC_PB; q++) {
+        for (int q = 0; q < UcPairs<T, TJ>::PB; q++) {
             if constexpr (C > 0) cf_fwd<T, TJ, 2 * C, C>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
             cf_fwd<T, TJ, J, C>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
             T nr[J + 1], ni[J + 1];
@@ -394,7 +398,7 @@ __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::t
     if constexpr (J <= JEND) {
         if constexpr (J > 0) {
 #pragma unroll
-            for (int q = 0; q < UC_PB; q++)
+            for (int q = 0; q < UcPairs<T, TJ>::PB; q++)
                 cf_fwd<T, TJ, J, MB>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
         }
         T2 *row = acc + (yh_block(J) + (J + 1) * MB) * 32;
@@ -403,7 +407,7 @@ __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::t
             const T nu = unorm<T>(J, MB, ma);
             T2 v = row[ma * 32];
 #pragma unroll
-            for (int q = 0; q < UC_PB; q++) {
+            for (int q = 0; q < UcPairs<T, TJ>::PB; q++) {
                 if constexpr (std::is_same<T, float>::value)
                     v = __ffma2_rn(make_float2(nu, nu), make_float2(s.pr[q][ma], s.pi[q][ma]), v);
                 else { v.x += nu * s.pr[q][ma]; v.y += nu * s.pi[q][ma]; }
@@ -427,14 +431,14 @@ __device__ __forceinline__ void uc_path(UcPairs<T, TJ> &s, typename cplx<T>::typ
         // copy while column TJ/2 takes its single row TJ
         constexpr int MT = MB + 1;
         uc_column<T, TJ, MB, (MB == 0 ? 0 : 2 * MB), 2 * MB + 1>(s, acc);
-        T kr[UC_PB][TJ + 1], ki[UC_PB][TJ + 1];
+        T kr[UcPairs<T, TJ>::PB][TJ + 1], ki[UcPairs<T, TJ>::PB][TJ + 1];
 #pragma unroll
-        for (int q = 0; q < UC_PB; q++)
+        for (int q = 0; q < UcPairs<T, TJ>::PB; q++)
 #pragma unroll
             for (int ma = 0; ma <= 2 * MB + 1; ma++) { kr[q][ma] = s.pr[q][ma]; ki[q][ma] = s.pi[q][ma]; }
         uc_column<T, TJ, MB, 2 * MB + 2, TJ>(s, acc);
 #pragma unroll
-        for (int q = 0; q < UC_PB; q++) {
+        for (int q = 0; q < UcPairs<T, TJ>::PB; q++) {
             constexpr int J = 2 * MB + 1;
 #pragma unroll
             for (int ma = 0; ma <= J; ma++) {
@@ -473,10 +477,10 @@ k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const 
         const int i = tile * 32 + lane;
         int p = 0, pend = 0;
         if (i < natoms) { p = poff[i]; pend = poff[i + 1]; }
-        for (; p < pend; p += UC_PB) {
+        for (; p < pend; p += UcPairs<T, TJ>::PB) {
             UcPairs<T, TJ> s;
 #pragma unroll
-            for (int q = 0; q < UC_PB; q++) {
+            for (int q = 0; q < UcPairs<T, TJ>::PB; q++) {
                 const bool ok = p + q < pend;
                 const double4 g = ok ? pab[p + q] : make_double4(1.0, 0.0, 0.0, 0.0);
                 s.ar[q] = (T)g.x; s.ai[q] = (T)g.y; s.br[q] = (T)g.z; s.bi[q] = (T)g.w;
@@ -885,10 +889,12 @@ template <> struct FAccSel<float> { typedef FAccComp type; };
 //     l'[k] = A_k a l[k] - B_(k+1) b l[k+1]           (parent row's adjoint)
 //     dF/d(ar + i ai) += A_ma conj(l[ma]) p[ma]        (as (re, im) pairs)
 //     dF/d(br + i bi) -= B_ma conj(l[ma]) p[ma-1]
-// and F itself is the real part of the adjoint of the root u_0 = 1.  This is
-// about 5,100 operations per pair at 2J=8 against about 14,000 for carrying
-// the three derivative directions forward through the recursion, which is how
-// cpuSnap4.cpp:798-1175 computes dU/dr.
+// and F itself is the real part of the adjoint of the root u_0 = 1.  In FP32
+// the rows are instead the coefficient-free ones of k_snap_uc (u = unorm v,
+// A = B = 1, adjoint seeded with unorm Y), which saves the rootpq products.
+// This is about 5,100 operations per pair at 2J=8 against about 14,000 for
+// carrying the three derivative directions forward through the recursion,
+// which is how cpuSnap4.cpp:798-1175 computes dU/dr.
 //
 // Columns mb depend on each other only through the seed rows (the parent of
 // row (2mb, mb) is the mirror of row (2mb-1, mb-1)), so the pass is:
@@ -918,7 +924,7 @@ struct FrState {
     T lr[TJ + 1], li[TJ + 1];                   // adjoint row
 };
 
-// row J-1 -> row J of column MB, in place (entries 0..J), as u_rows does
+// row J-1 -> row J of column MB, in place (entries 0..J), as u_rows does (u-space, rootpq factors)
 template <typename T, int TJ, int J, int MB>
 __device__ __forceinline__ void fr_fwd(const T ar, const T ai, const T br, const T bi, T (&pr)[TJ + 1],
                                        T (&pi)[TJ + 1])
@@ -952,6 +958,19 @@ __device__ __forceinline__ void fr_fwd(const T ar, const T ai, const T br, const
     }
 }
 
+// FP64 runs the recursion in u-space (rootpq factors), FP32 in the
+// coefficient-free v-space of k_snap_uc (u = unorm v).  Both give the same
+// gradient; in FP64 the coefficient-free form issues fewer instructions but,
+// at 254 registers, measured twice as slow (its memory latency is exposed).
+template <typename T> __host__ __device__ constexpr bool fr_cf() { return std::is_same<T, float>::value; }
+template <typename T, int TJ, int J, int MB>
+__device__ __forceinline__ void fr_row(const T ar, const T ai, const T br, const T bi, T (&pr)[TJ + 1],
+                                       T (&pi)[TJ + 1])
+{
+    if constexpr (fr_cf<T>()) cf_fwd<T, TJ, J, MB>(ar, ai, br, bi, pr, pi);
+    else fr_fwd<T, TJ, J, MB>(ar, ai, br, bi, pr, pi);
+}
+
 // seed S_(MB+1)[J - ma] = (-1)^(MB+ma) conj(row (J = 2MB+1, MB)[ma])
 template <typename T, int TJ, int MB>
 __device__ __forceinline__ void fr_put_seed(const T (&pr)[TJ + 1], const T (&pi)[TJ + 1], T *__restrict__ qs)
@@ -973,11 +992,11 @@ __device__ __forceinline__ void fr_seeds(const T ar, const T ai, const T br, con
     if constexpr (2 * (MB + 1) <= TJ) {
         if constexpr (MB == 0) {
             pr[0] = T(1); pi[0] = T(0);
-            fr_fwd<T, TJ, 1, 0>(ar, ai, br, bi, pr, pi);
+            fr_row<T, TJ, 1, 0>(ar, ai, br, bi, pr, pi);
         } else {
             // pr/pi hold S_MB (entries 0..2MB-1)
-            fr_fwd<T, TJ, 2 * MB, MB>(ar, ai, br, bi, pr, pi);
-            fr_fwd<T, TJ, 2 * MB + 1, MB>(ar, ai, br, bi, pr, pi);
+            fr_row<T, TJ, 2 * MB, MB>(ar, ai, br, bi, pr, pi);
+            fr_row<T, TJ, 2 * MB + 1, MB>(ar, ai, br, bi, pr, pi);
         }
         fr_put_seed<T, TJ, MB>(pr, pi, qs);
         // the next column starts from the seed just written
@@ -999,7 +1018,7 @@ template <typename T, int TJ, int J, int MB>
 __device__ __forceinline__ void fr_col_fwd(FrState<T, TJ> &st, T (&pr)[TJ + 1], T (&pi)[TJ + 1])
 {
     if constexpr (J < TJ) {
-        fr_fwd<T, TJ, J, MB>(st.ar, st.ai, st.br, st.bi, pr, pi);
+        fr_row<T, TJ, J, MB>(st.ar, st.ai, st.br, st.bi, pr, pi);
 #pragma unroll
         for (int ma = 0; ma <= J; ma++) { st.ur[fr_row_off(J) + ma] = pr[ma]; st.ui[fr_row_off(J) + ma] = pi[ma]; }
         fr_col_fwd<T, TJ, J + 1, MB>(st, pr, pi);
@@ -1015,9 +1034,11 @@ __device__ __forceinline__ void fr_add_y(FrState<T, TJ> &st, const typename cplx
     constexpr int MAMAX = (2 * MB == J) ? MB : J;
 #pragma unroll
     for (int ma = 0; ma <= MAMAX; ma++) {
-        T2 y = yrow[ma * 32];
-        if (2 * MB == J && ma == MB) { y.x *= T(0.5); y.y *= T(0.5); }
-        st.lr[ma] += y.x; st.li[ma] += y.y;
+        const T2 y = yrow[ma * 32];
+        // v-space (FP32): u = unorm v, so the adjoint of the row v is unorm Y
+        const T un = fr_cf<T>() ? unorm<T>(J, MB, ma) : T(1);
+        const T nu = (2 * MB == J && ma == MB) ? T(0.5) * un : un;
+        st.lr[ma] += nu * y.x; st.li[ma] += nu * y.y;
     }
 }
 
@@ -1028,32 +1049,47 @@ __device__ __forceinline__ void fr_col_bwd(FrState<T, TJ> &st, const typename cp
 {
     constexpr int PO = fr_row_off(J - 1);
     const T ar = st.ar, ai = st.ai, br = st.br, bi = st.bi;
-    // gradient of this layer
+    // gradient of this layer (coefficient-free rows: n[ma] = conj(a) p[ma] - conj(b) p[ma-1])
     T gar = T(0), gai = T(0), gbr = T(0), gbi = T(0);
 #pragma unroll
     for (int ma = 0; ma <= J; ma++) {
         const T lr = st.lr[ma], li = st.li[ma];
         if (ma < J) {
-            const T A = rootpq<T>(J - ma, J - MB);
             const T pr = st.ur[PO + ma], pi = st.ui[PO + ma];
-            gar += A * (lr * pr + li * pi);
-            gai += A * (lr * pi - li * pr);
+            if constexpr (fr_cf<T>()) {
+                gar += lr * pr + li * pi;
+                gai += lr * pi - li * pr;
+            } else {
+                const T A = rootpq<T>(J - ma, J - MB);
+                gar += A * (lr * pr + li * pi);
+                gai += A * (lr * pi - li * pr);
+            }
         }
         if (ma >= 1) {
-            const T B = rootpq<T>(ma, J - MB);
             const T pr = st.ur[PO + ma - 1], pi = st.ui[PO + ma - 1];
-            gbr -= B * (lr * pr + li * pi);
-            gbi -= B * (lr * pi - li * pr);
+            if constexpr (fr_cf<T>()) {
+                gbr -= lr * pr + li * pi;
+                gbi -= lr * pi - li * pr;
+            } else {
+                const T B = rootpq<T>(ma, J - MB);
+                gbr -= B * (lr * pr + li * pi);
+                gbi -= B * (lr * pi - li * pr);
+            }
         }
     }
     G[0].add(gar); G[1].add(gai); G[2].add(gbr); G[3].add(gbi);
     // adjoint of the parent row, in place (ascending k reads l[k+1] before it changes)
 #pragma unroll
     for (int k = 0; k < J; k++) {
-        const T A = rootpq<T>(J - k, J - MB), B = rootpq<T>(k + 1, J - MB);
         const T lr = st.lr[k], li = st.li[k], mr = st.lr[k + 1], mi = st.li[k + 1];
-        st.lr[k] = A * (ar * lr - ai * li) - B * (br * mr - bi * mi);
-        st.li[k] = A * (ar * li + ai * lr) - B * (br * mi + bi * mr);
+        if constexpr (fr_cf<T>()) {
+            st.lr[k] = (ar * lr - ai * li) - (br * mr - bi * mi);
+            st.li[k] = (ar * li + ai * lr) - (br * mi + bi * mr);
+        } else {
+            const T A = rootpq<T>(J - k, J - MB), B = rootpq<T>(k + 1, J - MB);
+            st.lr[k] = A * (ar * lr - ai * li) - B * (br * mr - bi * mi);
+            st.li[k] = A * (ar * li + ai * lr) - B * (br * mi + bi * mr);
+        }
     }
     if constexpr (J - 1 >= 2 * MB) {
         // parent is row (J-1, MB) of this column

@@ -221,9 +221,12 @@ def tri_fixtures():
 
 
 # The 16,000-atom configuration of the benchmark's FP64-vs-reference check: 20x20x20 BCC Ta cells at
-# 600 K, jitter 0.05 A, 2J=8 with seeded coefficients, 1,000 NVE steps of 1 fs.
+# 600 K, jitter 0.05 A, 2J=8 with seeded coefficients beta_k ~ N(0, 0.01), 1,000 NVE steps of 1 fs.
+# Coefficients drawn at random need not hold a BCC crystal together: of the seeds 2017-2096, run for
+# 1,000 steps at 600 K, most heat up or collapse (one reached 1.8 million K).  Seed 2022 keeps the
+# temperature near 570 K and the potential energy flat, and rebuilds the neighbour list a dozen times.
 C2 = dict(name="c2_bcc16000_2j8", cells=(20, 20, 20), twojmax=8, temp=600.0, jitter=0.05, seed=2016,
-          coeff_seed=2017, dt=0.001, steps=1000, neighmax=80, snap_steps=(100, 1000), atom_stride=8)
+          coeff_seed=2022, dt=0.001, steps=1000, neighmax=80, snap_steps=(100, 1000), atom_stride=8)
 
 
 def row_hashes(nl, nn):
