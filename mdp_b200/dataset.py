@@ -155,6 +155,35 @@ def read_extxyz(path: str, species=("Ta",)) -> list[Frame]:
     return out
 
 
+def reference_orientation(frame: Frame, transpose_lattice: bool = False) -> Frame:
+    """The frame as MDP's training-data reader leaves it (readconfigfile.jl:28-58).
+
+    With transpose_lattice (the `transposelattice` flag of adddata, which
+    fitting/snap/Ta/fitsnap.jl sets) the cell vectors are the COLUMNS of the
+    file's Lattice array.  The cell is then rotated to the standard
+    orientation -- a along x, b in the xy plane (rotatelattice.jl) -- and the
+    positions with it (transformcoords.jl: x = [a b c] [A B C]^-1 X).  Forces
+    and stresses stay as read, as the reference leaves them.  For a file whose
+    rows are already in that orientation the rotation is the identity.
+
+    Files that store the cell vectors as rows (every frame of MDP's Ta set:
+    the positions of its 2-atom BCC cells sit exactly at the body centre of the
+    row cell) are distorted by the transposition wherever the cell has
+    off-diagonal terms; the reference's published force errors of the Elastic
+    folders come from exactly that distortion."""
+    L = np.asarray(frame.lattice, dtype=np.float64)
+    A, B, C = (L.T if transpose_lattice else L)
+    An, Bn, Cn = np.linalg.norm(A), np.linalg.norm(B), np.linalg.norm(C)
+    bx = B @ A / An
+    by = np.sqrt(Bn * Bn - bx * bx)
+    cx = C @ A / An
+    cy = (B @ C - bx * cx) / by
+    cz = np.sqrt(Cn * Cn - cx * cx - cy * cy)
+    new = np.array([[An, 0.0, 0.0], [bx, by, 0.0], [cx, cy, cz]])
+    R = new.T @ np.linalg.inv(np.stack([A, B, C]).T)
+    return dataclasses.replace(frame, lattice=new, x=np.asarray(frame.x) @ R.T)
+
+
 def read_folder(folder: str, species=("Ta",), extension: str = "json") -> list[Frame]:
     """Frames of every file of `folder` with the extension, in name order;
     "json" files go through read_json, "xyz" / "extxyz" through read_extxyz."""

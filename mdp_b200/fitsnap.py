@@ -9,7 +9,11 @@ switching on, bzero / bnorm / wselfall off, 2J = 6, energies per atom and
 stresses per volume, and the ZBL reference potential (inner 4.0, outer 4.8,
 Z 73) subtracted from the targets (--no-zbl leaves it out).  Prints the
 coefficients and the per-folder unweighted errors (printerrors) as one JSON
-object.
+object.  fitsnap.jl also sets transposelattice = true, which reads the cell
+vectors as the columns of each file's Lattice array; --transpose-lattice does
+the same (dataset.reference_orientation) and reproduces the reference's
+published errors, while the default reads them as rows, the reading under
+which the Ta files' atoms sit at their crystal positions.
 """
 from __future__ import annotations
 
@@ -40,9 +44,17 @@ TA_FOLDERS = (
 TA_ZBL = (4.0, 4.8, 73.0)
 
 
-def load_groups(root: str, folders=TA_FOLDERS, species=("Ta",), extension: str = "json"):
-    return [dataset.Group(name, dataset.read_folder(os.path.join(root, name), species, extension), we, wf, ws)
-            for name, we, wf, ws in folders]
+def load_groups(root: str, folders=TA_FOLDERS, species=("Ta",), extension: str = "json",
+                transpose_lattice: bool = False):
+    """One Group per folder; transpose_lattice reads the cells as fitsnap.jl
+    does (dataset.reference_orientation)."""
+    groups = []
+    for name, we, wf, ws in folders:
+        frames = dataset.read_folder(os.path.join(root, name), species, extension)
+        if transpose_lattice:
+            frames = [dataset.reference_orientation(fr, True) for fr in frames]
+        groups.append(dataset.Group(name, frames, we, wf, ws))
+    return groups
 
 
 def main(argv=None) -> dict:
@@ -53,11 +65,13 @@ def main(argv=None) -> dict:
     ap.add_argument("--extension", default="json")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--no-zbl", action="store_true", help="fit without the ZBL reference potential")
+    ap.add_argument("--transpose-lattice", action="store_true",
+                    help="read the cell vectors as the columns of Lattice, as fitsnap.jl's transposelattice = true")
     a = ap.parse_args(argv)
     p = configs.snap_params(a.twojmax, seed=0, rcutfac=4.67637, radelem=0.5, rfac0=0.99363, rmin0=0.0,
                             switchflag=1, bzeroflag=0, bnormflag=0, wselfallflag=0)
-    out = dataset.fit_groups(load_groups(a.data, extension=a.extension), p, mode=a.mode, device=a.device,
-                             zbl=None if a.no_zbl else TA_ZBL)
+    out = dataset.fit_groups(load_groups(a.data, extension=a.extension, transpose_lattice=a.transpose_lattice), p,
+                             mode=a.mode, device=a.device, zbl=None if a.no_zbl else TA_ZBL)
     res = dict(coefficients=out["beta"].tolist(), errors=out["errors"], configs=out["configs"],
                atoms=out["atoms"], replicated=out["replicated"], graph_ms=out["graph_ms"])
     print(json.dumps(res))
