@@ -160,10 +160,11 @@ class CpuSample:
         self.threads = os.cpu_count() or 1
         self.nb = refpy.neighbor_list(self.cfg.x, self.cfg.box, self.p.rcut, SKIN, NEIGHMAX, neighcell=1)
 
-    def step(self) -> float:
+    def step(self, nthreads: int | None = None) -> float:
         xa, al, nl, nn = self.nb
+        th = nthreads or self.threads
         t0 = time.perf_counter()
-        self.refpy.snap_force(xa, al, nl, nn, self.p, nblocks=4 * self.threads, nthreads=self.threads)
+        self.refpy.snap_force(xa, al, nl, nn, self.p, nblocks=4 * th if th > 1 else 1, nthreads=th)
         return time.perf_counter() - t0
 
     def describe(self, seconds: float, steps: int) -> str:
@@ -172,17 +173,74 @@ class CpuSample:
                 f"threads over atom blocks, {seconds:.2f} s")
 
 
+def c1_full_run(repeats: int = 3) -> dict:
+    """The reference's CPU code on the small configuration of its own benchmark
+    set, run in full on one core: 4x4x4 BCC Ta cells (128 atoms), 300 K, SNAP
+    2J=6, 100 velocity-Verlet steps of 0.5 fs, in cpuMDP's step order
+    (nve_initial, rebuild check or ghost shift, SNAP force, nve_final) with the
+    reference build's kernels; the median of `repeats` runs."""
+    from mdp_b200 import configs
+    from oracle import refpy
+    p = configs.snap_params(6, seed=2024)
+    cfg = configs.ta_config((4, 4, 4), temp=300.0, jitter=0.05, seed=2024)
+    n, dt, skin, nm = cfg.natoms, 0.0005, SKIN, NEIGHMAX
+    dtf = 0.5 * dt * configs.FTM2V
+    ilist = np.arange(n, dtype=np.int32)
+    typ = np.ones(n + 1, dtype=np.int32)
+    mass = np.array([0.0, configs.TA_MASS])
+    box = np.asarray(cfg.box, dtype=np.float64)
+    lib = refpy.lib()
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        x, v = cfg.x.copy().ravel(), cfg.v.copy().ravel()
+        xa, al, nl, nn = refpy.neighbor_list(x.reshape(n, 3), box, p.rcut, skin, nm)
+        xhold = x.copy()
+        _, f, _ = refpy.snap_force(xa, al, nl, nn, p)
+        f = f.ravel().copy()
+        for _ in range(100):
+            xs = x.copy()
+            lib.ref_nve_initial(x, v, f, mass, dtf, dt, typ, ilist, n)
+            if np.max(np.sum((x - xhold).reshape(n, 3) ** 2, axis=1)) > 0.25 * skin * skin:
+                xw = x.reshape(n, 3)
+                xw = np.where(xw < 0.0, xw + box, xw)
+                xw = np.where(xw >= box, np.maximum(xw - box, 0.0), xw)
+                x = np.ascontiguousarray(xw).ravel()
+                xa, al, nl, nn = refpy.neighbor_list(x.reshape(n, 3), box, p.rcut, skin, nm)
+                xhold = x.copy()
+            else:
+                xa = xa.copy()
+                xa[:n] = x.reshape(n, 3)
+                xa[n:] += (x - xs).reshape(n, 3)[al[n:]]
+            _, f, _ = refpy.snap_force(xa, al, nl, nn, p)
+            f = f.ravel().copy()
+            lib.ref_nve_final(x, v, f, mass, dtf, typ, ilist, n)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    return {"value": n * 100 / t, "unit": "atom-steps/s", "cores": 1, "seconds": t, "runs": repeats,
+            "workload": "128-atom BCC Ta, 2J=6, 100 NVE steps of 0.5 fs (full run, median of 3)"}
+
+
 def cpu_baseline(min_seconds: float = 10.0, max_evals: int = 200) -> dict:
     """MDP's CPU SNAP on the 16,000-atom sample: one untimed evaluation, then
-    evaluations until at least min_seconds of CPU work have been timed."""
+    evaluations until at least min_seconds of CPU work have been timed, on all
+    host threads over atom blocks; beside it the same sample on one core (the
+    reference code is single-threaded; median of 3 evaluations) and a full run
+    of the 128-atom configuration on one core."""
     s = CpuSample()
     s.step()
     el, k = 0.0, 0
     while el < min_seconds and k < max_evals:
         el += s.step()
         k += 1
-    return {"value": s.cfg.natoms * k / el, "unit": "atom-steps/s", "cores": s.threads, "kind": "reference",
-            "sample": s.describe(el, k)}
+    out = {"value": s.cfg.natoms * k / el, "unit": "atom-steps/s", "cores": s.threads, "kind": "reference",
+           "sample": s.describe(el, k)}
+    one = sorted(s.step(nthreads=1) for _ in range(3))[1]
+    out["one_core"] = {"value": s.cfg.natoms / one, "unit": "atom-steps/s", "cores": 1,
+                       "sample": f"{s.cfg.natoms} atoms, one SNAP force evaluation on one thread, median of 3 "
+                                 f"({one:.2f} s)"}
+    out["c1_full_run_one_core"] = c1_full_run()
+    return out
 
 
 def run_reference(args):

@@ -128,3 +128,42 @@ def test_fit_with_zbl_recovers_snap_part():
     beta = out["beta"]
     assert abs(beta[0] - p.coeff[0]) < 1e-6 * abs(p.coeff[0])
     assert np.max(np.abs(beta[1:] - p.coeff[1:])) < 1e-4 * np.max(np.abs(p.coeff[1:]))
+
+
+def test_frames_missing_energies_or_forces_add_only_their_rows():
+    """A group mixing energy-only, force-only and complete frames: the GPU
+    fit's coefficients equal a NumPy least-squares solve over exactly the rows
+    that are present (descriptors from the reference's ComputeSnap chain),
+    with random targets so that every row matters."""
+    from oracle import refpy
+    p = configs.snap_params(6, seed=5)
+    rng = np.random.default_rng(17)
+    frames = []
+    for s, (kind, n) in enumerate([("bcc", 54), ("fcc", 32), ("a15", 64), ("bcc", 16), ("fcc", 108), ("bcc", 54),
+                                   ("a15", 64), ("fcc", 32)]):
+        cfg = fit.make_config(kind, n, rng.uniform(-0.04, 0.04), rng.uniform(0.05, 0.25), rng)
+        fr = dataset.Frame(natoms=cfg.natoms, lattice=np.diag(np.asarray(cfg.box, dtype=np.float64)), x=cfg.x)
+        has_e, has_f = (s % 3 != 1), (s % 3 != 0)
+        fr.e = float(rng.normal() * cfg.natoms) if has_e else None
+        fr.f = rng.normal(size=(cfg.natoms, 3)) if has_f else None
+        frames.append(fr)
+    we, wf = 3.0, 0.7
+    out = dataset.fit_groups([dataset.Group("Mixed", frames, we=we, wf=wf, ws=0.0)], p)
+    rows, ys = [], []
+    for fr in frames:
+        cfg, m = dataset.replicate(fr, p.rcut)
+        assert m == 1
+        xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, 0.0, 128, neighcell=0)
+        bi, bd, _, _ = refpy.snap_descriptors(xa, al, nl, nn, p)
+        if fr.e is not None:
+            rows.append(we / fr.natoms * np.concatenate([[fr.natoms], bi]))
+            ys.append(we / fr.natoms * fr.e)
+        if fr.f is not None:
+            F = np.zeros((3 * fr.natoms, 1 + p.ncoeff))
+            F[:, 1:] = bd.reshape(p.ncoeff, -1).T
+            rows.extend(wf * F)
+            ys.extend(wf * fr.f.ravel())
+    beta = np.linalg.lstsq(np.array(rows), np.array(ys), rcond=None)[0]
+    assert np.abs(out["beta"] - beta).max() < 1e-6 * np.abs(beta).max()
+    err = out["errors"][0]
+    assert err["frames"] == len(frames) and "energy_rmse" in err and "force_rmse" in err
