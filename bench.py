@@ -221,6 +221,51 @@ def c1_full_run(repeats: int = 3) -> dict:
             "workload": "128-atom BCC Ta, 2J=6, 100 NVE steps of 0.5 fs (full run, median of 3)"}
 
 
+REF_GPU_CELLS = (60, 60, 60)        # 432,000 atoms: within the reference GPU kernels' 32-bit indexing at 2J=8
+
+
+def reference_gpu_baseline(device: int) -> dict:
+    """MDP's own GPU SNAP kernels (gpuSnap4.cu, compiled unchanged for sm_100a)
+    against this repository's stages on the same 432,000-atom configuration
+    of the workload (60^3 BCC Ta cells, 2J=8, the bench's seeds).  The
+    reference's launchers index with 32-bit ints (idxz_max * inum reaches 2^31
+    near 900,000 atoms at 2J=8), so the 2M-atom workload cannot be run through
+    them.  Times are CUDA-event medians per stage; the reference's pair arrays
+    are built on the host and not timed, so the totals compare the SNAP stages
+    (U, energy, Y, dE/dr and the force/virial tally) without the pair build."""
+    from mdp_b200 import configs
+    from mdp_b200.snap import SnapMD
+    from oracle import refgpu
+    if not refgpu.available():
+        return {"unavailable": "oracle/_ref/libmdp_ref_gpusnap.so not built"}
+    p = configs.snap_params(TWOJ, seed=2024)
+    cfg = configs.ta_config(REF_GPU_CELLS, temp=300.0, jitter=0.05, seed=2024)
+    ref = refgpu.stage_times(p, cfg.x, cfg.box, SKIN, NEIGHMAX, repeats=3, device=device)
+    if ref is None:
+        return {"unavailable": "size exceeds the reference kernels' 32-bit indexing"}
+    md = SnapMD(p, cfg.box, cfg.natoms, DT, skin=SKIN, neighmax=NEIGHMAX, precision="fp64", device=device)
+    md.set_state(cfg.x, cfg.v)
+    md.setup()
+    md.run(3)
+    md.stage_timing(True)
+    md.run(4)
+    st = md.stage_times()
+    md.stage_timing(False)
+    md.close()
+    ours = {k: v / max(st["calls"], 1) for k, v in st.items() if k != "calls"}
+    ref_tot = ref["ui"] + ref["ei"] + ref["yi"] + ref["fi"]
+    our_tot = ours["ui"] + ours["yi"] + ours["fi"] + ours["tally"]
+    return {"atoms": cfg.natoms, "pairs": ref["pairs"], "twojmax": TWOJ, "dtype": "f64",
+            "reference_ms": {"ui_wself": ref["ui"], "ei": ref["ei"], "yi": ref["yi"], "fi": ref["fi"],
+                             "total": ref_tot},
+            "ours_ms": {"pairs": ours["pairs"], "ui": ours["ui"], "yi_with_energy": ours["yi"], "dedr": ours["fi"],
+                        "tally": ours["tally"], "total_without_pairs": our_tot},
+            "speedup": {"u": ref["ui"] / ours["ui"], "energy_and_y": (ref["ei"] + ref["yi"]) / ours["yi"],
+                        "forces": ref["fi"] / (ours["fi"] + ours["tally"]), "total": ref_tot / our_tot},
+            "source": "src/C++/Core/gpuSnap4.cu launchers gpuSnapComputeUi, gpuAddWself2Ui, gpuSnapComputeEi, "
+                      "gpuSnapComputeYi, gpuSnapComputeFi; one atom block"}
+
+
 def cpu_baseline(min_seconds: float = 10.0, max_evals: int = 200) -> dict:
     """MDP's CPU SNAP on the 16,000-atom sample: one untimed evaluation, then
     evaluations until at least min_seconds of CPU work have been timed, on all
@@ -435,11 +480,16 @@ def run_ours(args):
                                 "targets ~ N(0,1)") if args.fit_configs == 4096 else f"{args.fit_configs} configurations"
 
     cpu = None
+    ref_gpu = None
     if rank == 0 and not args.no_cpu:
         try:
             cpu = cpu_baseline()
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "error": str(ex)[:200]}
+        try:
+            ref_gpu = reference_gpu_baseline(dev)
+        except Exception as ex:
+            ref_gpu = {"error": str(ex)[:200]}
 
     traffic = None
     prof = os.path.join(HERE, "profiles", "k_snap_yi_fp64_traffic.json")
@@ -478,6 +528,7 @@ def run_ours(args):
             "batched_fit": fit_line,
             "clocks": clk,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
