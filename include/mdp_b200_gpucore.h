@@ -119,6 +119,78 @@ void mdp_gpu_array_sum_every_column_f64(double *b, const double *a, int m, int n
 /* mdpgpucore.h:49, gpuArrayGetValueAtIndex<int> */
 int mdp_gpu_array_get_value_at_index_int(const int *y, int n);
 
+/* PREC_FLOAT builds of MDP (dstype = float): the same entry points on float
+ * device arrays.  The MD-loop operations and the pair list/pairs compute in
+ * float with the reference float build's rounding; the SNAP stages widen the
+ * float arrays into library-owned double scratch, run the double path and
+ * narrow the results back into the caller's arrays. */
+void mdp_gpu_snap_compute_ui_f32(float *Utotr, float *Utoti, const float *rootpqarray, const float *rij,
+                                 const float *wjelem, const float *radelem, float rmin0, float rfac0,
+                                 float rcutfac, const int *idxu_block, const int *map, const int *aii,
+                                 const int *ti, const int *tj, int twojmax, int idxu_max, int inum, int ijnum,
+                                 int switchflag, int chemflag);
+void mdp_gpu_add_wself2ui_f32(float *Utotr, float *Utoti, float wself, const int *idxu_block, const int *type,
+                              const int *map, const int *ai, int wselfall_flag, int chemflag, int idxu_max,
+                              int nelements, int twojmax, int inum);
+void mdp_gpu_snap_compute_ei_f32(float *eatom, const float *Utotr, const float *Utoti, const float *cglist,
+                                 const float *bzero, const float *coeffelem, const int *ilist, const int *map,
+                                 const int *type, const int *idxb, const int *idxcg_block, const int *idxu_block,
+                                 int twojmax, int idxb_max, int idxu_max, int nelements, int ncoeffall,
+                                 int bnorm_flag, int bzero_flag, int wselfall_flag, int quadraticflag, int inum);
+void mdp_gpu_snap_compute_bi_f32(float *blist, const float *Utotr, const float *Utoti, const float *cglist,
+                                 const float *bzero, const int *idxb, const int *idxcg_block, const int *idxu_block,
+                                 const int *idxz_block, int twojmax, int idxb_max, int idxu_max, int idxz_max,
+                                 int nelements, int bnorm_flag, int bzero_flag, int wselfall_flag, int inum);
+void mdp_gpu_snap_compute_yi_f32(float *ylist_r, float *ylist_i, const float *Utotr, const float *Utoti,
+                                 const float *cglist, const float *coeffelem, const int *map, const int *type,
+                                 const int *idxz, const int *idxb_block, const int *idxu_block,
+                                 const int *idxcg_block, int twojmax, int idxb_max, int idxu_max, int idxz_max,
+                                 int nelements, int ncoeffall, int bnorm_flag, int inum);
+void mdp_gpu_snap_compute_yi_beta_f32(float *ylist_r, float *ylist_i, const float *Utotr, const float *Utoti,
+                                      const float *cglist, const float *beta, const int *idxz,
+                                      const int *idxb_block, const int *idxu_block, const int *idxcg_block,
+                                      int twojmax, int idxb_max, int idxu_max, int idxz_max, int nelements,
+                                      int bnorm_flag, int inum);
+void mdp_gpu_snap_compute_fi_f32(float *fatom, float *vatom, const float *ylist_r, const float *ylist_i,
+                                 const float *rootpqarray, const float *rij, const float *wjelem,
+                                 const float *radelem, float rmin0, float rfac0, float rcutfac,
+                                 const int *idxu_block, const int *map, const int *aii, const int *ai, const int *aj,
+                                 const int *ti, const int *tj, int twojmax, int idxu_max, int inum, int anum,
+                                 int ijnum, int switchflag, int chemflag);
+void mdp_gpu_neigh_pair_list_f32(int *pairnum, int *pairlist, const float *x, const float *rcutsq, const int *ilist,
+                                 const int *neighlist, const int *neighnum, const int *atomtype, const int *alist,
+                                 int inum, int jnum, int dim, int ntypes);
+void mdp_gpu_neigh_pairs_f32(float *xij, const float *x, int *aii, int *ai, int *aj, int *ti, int *tj,
+                             const int *pairnum, const int *pairlist, const int *pairnumsum, const int *ilist,
+                             const int *atomtype, const int *alist, int inum, int jnum, int dim);
+void mdp_gpu_atom_list3d_f32(int *alist, int *inside, int *glistnumsum, int *glistnum, int *d_sums, int *d_incr,
+                             float *x, const float *pimages, const float *wc, const float *s2rmap, int inum,
+                             int pnum, int dim);
+void mdp_gpu_cell_list3d_f32(int *clist, const float *xi, const float *eta1, const float *eta2,
+                             const float *eta3, const float *s2rmap, const int *nc, int inum, int natom, int dim);
+void mdp_gpu_full_neighbor_list3d_cells_f32(int *neighborlist, int *neighbornum, const float *x,
+                                            const float *rcutsq, const int *alist, const int *clist,
+                                            const int *c2alist, const int *c2anumsum, const int *nc, int inum,
+                                            int jnum, int dim);
+void mdp_gpu_full_neighbor_list3d_f32(int *neighborlist, int *neighbornum, const float *x, const float *rcutsq,
+                                      int anum, int inum, int jnum, int dim);
+void mdp_gpu_initial_integrate_f32(float *x, float *v, const float *f, const float *mass, const float *dtarray,
+                                   float *tarray, float *eta_mass, float *eta, float *eta_dot,
+                                   float *eta_dotdot, float *ke, float *tmp, float vlimitsq, const int *type,
+                                   const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+                                   int mode, int dim, int inum);
+void mdp_gpu_final_integrate_f32(float *x, float *v, const float *f, const float *mass, const float *dtarray,
+                                 float *tarray, float *eta_mass, float *eta, float *eta_dot,
+                                 float *eta_dotdot, float *ke, float *tmp, float vlimitsq, const int *type,
+                                 const int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+                                 int mode, int dim, int inum);
+void mdp_gpu_pbc_f32(float *x, float *v, int *image, const float *boxhi, const float *boxlo,
+                     const float *hi_lambda, const float *lo_lambda, const float *h, const float *h_inv,
+                     const float *h_rate, const int *pbc, int vdeform, int triclinic, int dim, int nlocal);
+void mdp_gpu_compute_ke_atom_f32(float *ke, const float *mass, const float *v, float mvv2e, const int *type,
+                                 const int *ilist, int dim, int inum);
+void mdp_gpu_array_sum_every_column_f32(float *b, const float *a, int m, int n);
+
 /* No counterpart in the reference.  The per-atom bispectrum of
  * mdp_gpu_snap_compute_bi_f64 for callers that must not allocate device memory
  * (a host application whose memory pool owns the device, or a loop that cannot
@@ -320,6 +392,130 @@ template <> inline void gpuArraySumEveryColumn<double>(double *b, double *a, int
 }
 template <typename T> T gpuArrayGetValueAtIndex(T *y, int n);
 template <> inline int gpuArrayGetValueAtIndex<int>(int *y, int n) { return mdp_gpu_array_get_value_at_index_int(y, n); }
+/* float (PREC_FLOAT) instantiations */
+template <> inline void gpuSnapComputeUi<float>(float *Stotr, float *Stoti, float *rootpqarray, float *rij,
+        float *wjelem, float *radelem, float rmin0, float rfac0, float rcutfac, int *idxu_block, int *map,
+        int *ai, int *ti, int *tj, int twojmax, int idxu_max, int inum, int ijnum, int switchflag, int chemflag)
+{
+    mdp_gpu_snap_compute_ui_f32(Stotr, Stoti, rootpqarray, rij, wjelem, radelem, rmin0, rfac0, rcutfac, idxu_block,
+                                map, ai, ti, tj, twojmax, idxu_max, inum, ijnum, switchflag, chemflag);
+}
+template <> inline void gpuAddWself2Ui<float>(float *Stotr, float *Stoti, float wself, int *idxu_block,
+        int *type, int *map, int *ai, int wselfall_flag, int chemflag, int idxu_max, int nelements, int twojmax,
+        int inum)
+{
+    mdp_gpu_add_wself2ui_f32(Stotr, Stoti, wself, idxu_block, type, map, ai, wselfall_flag, chemflag, idxu_max,
+                             nelements, twojmax, inum);
+}
+template <> inline void gpuSnapComputeEi<float>(float *eatom, float *Stotr, float *Stoti, float *cglist,
+        float *bzero, float *coeffelem, int *ilist, int *map, int *type, int *idxb, int *idxcg_block,
+        int *idxu_block, int twojmax, int idxb_max, int idxu_max, int nelements, int ncoeffall, int bnorm_flag,
+        int bzero_flag, int wselfall_flag, int quadraticflag, int inum)
+{
+    mdp_gpu_snap_compute_ei_f32(eatom, Stotr, Stoti, cglist, bzero, coeffelem, ilist, map, type, idxb, idxcg_block,
+                                idxu_block, twojmax, idxb_max, idxu_max, nelements, ncoeffall, bnorm_flag,
+                                bzero_flag, wselfall_flag, quadraticflag, inum);
+}
+template <> inline void gpuSnapComputeBi<float>(float *blist, float *Stotr, float *Stoti, float *cglist,
+        float *bzero, int *idxb, int *idxcg_block, int *idxu_block, int *idxz_block, int twojmax, int idxb_max,
+        int idxu_max, int idxz_max, int nelements, int bnorm_flag, int bzero_flag, int wselfall_flag, int inum)
+{
+    mdp_gpu_snap_compute_bi_f32(blist, Stotr, Stoti, cglist, bzero, idxb, idxcg_block, idxu_block, idxz_block,
+                                twojmax, idxb_max, idxu_max, idxz_max, nelements, bnorm_flag, bzero_flag,
+                                wselfall_flag, inum);
+}
+template <> inline void gpuSnapComputeYi<float>(float *ylist_r, float *ylist_i, float *Stotr, float *Stoti,
+        float *cglist, float *coeffelem, int *map, int *type, int *idxz, int *idxb_block, int *idxu_block,
+        int *idxcg_block, int twojmax, int idxb_max, int idxu_max, int idxz_max, int nelements, int ncoeffall,
+        int bnorm_flag, int inum)
+{
+    mdp_gpu_snap_compute_yi_f32(ylist_r, ylist_i, Stotr, Stoti, cglist, coeffelem, map, type, idxz, idxb_block,
+                                idxu_block, idxcg_block, twojmax, idxb_max, idxu_max, idxz_max, nelements,
+                                ncoeffall, bnorm_flag, inum);
+}
+template <> inline void gpuSnapComputeFi<float>(float *fatom, float *vatom, float *ylist_r, float *ylist_i,
+        float *rootpqarray, float *rij, float *wjelem, float *radelem, float rmin0, float rfac0,
+        float rcutfac, int *idxu_block, int *map, int *aii, int *ai, int *aj, int *ti, int *tj, int twojmax,
+        int idxu_max, int inum, int anum, int ijnum, int switchflag, int chemflag)
+{
+    mdp_gpu_snap_compute_fi_f32(fatom, vatom, ylist_r, ylist_i, rootpqarray, rij, wjelem, radelem, rmin0, rfac0,
+                                rcutfac, idxu_block, map, aii, ai, aj, ti, tj, twojmax, idxu_max, inum, anum, ijnum,
+                                switchflag, chemflag);
+}
+template <> inline void gpuNeighPairList<float>(int *pairnum, int *pairlist, float *x, float *rcutsq, int *ilist,
+        int *neighlist, int *neighnum, int *atomtype, int *alist, int inum, int jnum, int dim, int ntypes)
+{
+    mdp_gpu_neigh_pair_list_f32(pairnum, pairlist, x, rcutsq, ilist, neighlist, neighnum, atomtype, alist, inum,
+                                jnum, dim, ntypes);
+}
+template <> inline void gpuNeighPairs<float>(float *xij, float *x, int *aii, int *ai, int *aj, int *ti, int *tj,
+        int *pairnum, int *pairlist, int *pairnumsum, int *ilist, int *atomtype, int *alist, int inum, int jnum,
+        int dim)
+{
+    mdp_gpu_neigh_pairs_f32(xij, x, aii, ai, aj, ti, tj, pairnum, pairlist, pairnumsum, ilist, atomtype, alist, inum,
+                            jnum, dim);
+}
+template <> inline void gpuSnapComputeYi<float>(float *ylist_r, float *ylist_i, float *Stotr, float *Stoti,
+        float *cglist, float *beta, int *idxz, int *idxb_block, int *idxu_block, int *idxcg_block, int twojmax,
+        int idxb_max, int idxu_max, int idxz_max, int nelements, int bnorm_flag, int inum)
+{
+    mdp_gpu_snap_compute_yi_beta_f32(ylist_r, ylist_i, Stotr, Stoti, cglist, beta, idxz, idxb_block, idxu_block,
+                                     idxcg_block, twojmax, idxb_max, idxu_max, idxz_max, nelements, bnorm_flag, inum);
+}
+template <> inline void gpuAtomList3D<float>(int *alist, int *inside, int *glistnumsum, int *glistnum, int *d_sums,
+        int *d_incr, float *x, float *pimages, float *wc, float *s2rmap, int inum, int pnum, int dim)
+{
+    mdp_gpu_atom_list3d_f32(alist, inside, glistnumsum, glistnum, d_sums, d_incr, x, pimages, wc, s2rmap, inum, pnum,
+                            dim);
+}
+template <> inline void gpuCellList3D<float>(int *clist, float *xi, float *eta1, float *eta2, float *eta3,
+        float *s2rmap, int *nc, int inum, int natom, int dim)
+{
+    mdp_gpu_cell_list3d_f32(clist, xi, eta1, eta2, eta3, s2rmap, nc, inum, natom, dim);
+}
+template <> inline void gpuFullNeighborList3D<float>(int *neighborlist, int *neighbornum, float *x, float *rcutsq,
+        int anum, int inum, int jnum, int dim)
+{
+    mdp_gpu_full_neighbor_list3d_f32(neighborlist, neighbornum, x, rcutsq, anum, inum, jnum, dim);
+}
+template <> inline void gpuFullNeighborList3D<float>(int *neighborlist, int *neighbornum, float *x, float *rcutsq,
+        int *alist, int *clist, int *c2alist, int *c2anumsum, int *nc, int inum, int jnum, int dim)
+{
+    mdp_gpu_full_neighbor_list3d_cells_f32(neighborlist, neighbornum, x, rcutsq, alist, clist, c2alist, c2anumsum,
+                                           nc, inum, jnum, dim);
+}
+template <> inline void gpuInitialIntegrate<float>(float *x, float *v, float *f, float *mass, float *dtarray,
+        float *tarray, float *eta_mass, float *eta, float *eta_dot, float *eta_dotdot, float *ke, float *tmp,
+        float vlimitsq, int *type, int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+        int mode, int dim, int inum)
+{
+    mdp_gpu_initial_integrate_f32(x, v, f, mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, ke, tmp,
+                                  vlimitsq, type, ilist, eta_mass_flag, biasflag, mtchain, nc_tchain, mode, dim, inum);
+}
+template <> inline void gpuFinalIntegrate<float>(float *x, float *v, float *f, float *mass, float *dtarray,
+        float *tarray, float *eta_mass, float *eta, float *eta_dot, float *eta_dotdot, float *ke, float *tmp,
+        float vlimitsq, int *type, int *ilist, int eta_mass_flag, int biasflag, int mtchain, int nc_tchain,
+        int mode, int dim, int inum)
+{
+    mdp_gpu_final_integrate_f32(x, v, f, mass, dtarray, tarray, eta_mass, eta, eta_dot, eta_dotdot, ke, tmp,
+                                vlimitsq, type, ilist, eta_mass_flag, biasflag, mtchain, nc_tchain, mode, dim, inum);
+}
+template <> inline void gpuPBC<float>(float *x, float *v, int *image, float *boxhi, float *boxlo,
+        float *hi_lambda, float *lo_lambda, float *h, float *h_inv, float *h_rate, int *pbc, int vdeform,
+        int triclinic, int dim, int nlocal)
+{
+    mdp_gpu_pbc_f32(x, v, image, boxhi, boxlo, hi_lambda, lo_lambda, h, h_inv, h_rate, pbc, vdeform, triclinic, dim,
+                    nlocal);
+}
+template <> inline void gpuComputeKEAtom<float>(float *ke, float *mass, float *v, float mvv2e, int *type,
+        int *ilist, int dim, int inum)
+{
+    mdp_gpu_compute_ke_atom_f32(ke, mass, v, mvv2e, type, ilist, dim, inum);
+}
+template <> inline void gpuArraySumEveryColumn<float>(float *b, float *a, int m, int n)
+{
+    mdp_gpu_array_sum_every_column_f32(b, a, m, n);
+}
 #endif /* MDP_B200_GPUCORE_TEMPLATES */
 #endif /* __cplusplus */
 #endif

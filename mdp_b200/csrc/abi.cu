@@ -138,7 +138,14 @@ __global__ void k_scatter_fi(const double4 *__restrict__ dE, const double *__res
 
 // typed pair filter (cpuSnap.cpp:1883-1906; the Julia library's CSR form when
 // csr != 0, src/Julia/Potential/cpuSnap.cpp:258-286)
-__global__ void k_ref_pair_count(int *__restrict__ pairnum, const double *__restrict__ x, const double *__restrict__ rcutsq,
+// correctly rounded sum and product in the precision of the caller's build
+__device__ __forceinline__ double ref_add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float ref_add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double ref_mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float ref_mul_rn(float a, float b) { return __fmul_rn(a, b); }
+
+template <typename T>
+__global__ void k_ref_pair_count(int *__restrict__ pairnum, const T *__restrict__ x, const T *__restrict__ rcutsq,
                                  const int *__restrict__ ilist, const int *__restrict__ nlist, const int *__restrict__ nnum,
                                  const int *__restrict__ atype, const int *__restrict__ alist, int inum, int jnum, int ntypes,
                                  int csr, int *__restrict__ pairlist_rows)
@@ -152,18 +159,19 @@ __global__ void k_ref_pair_count(int *__restrict__ pairnum, const double *__rest
     for (int l = 0; l < m; l++) {
         const int j = nlist[n0 + l];
         const int jt = atype[alist[j]];
-        const double d0 = x[3 * (size_t)j] - x[3 * (size_t)i], d1 = x[3 * (size_t)j + 1] - x[3 * (size_t)i + 1],
+        const T d0 = x[3 * (size_t)j] - x[3 * (size_t)i], d1 = x[3 * (size_t)j + 1] - x[3 * (size_t)i + 1],
                      d2 = x[3 * (size_t)j + 2] - x[3 * (size_t)i + 2];
-        const double dij = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-        if (dij < rcutsq[jt + it * (ntypes + 1)] && dij > 1e-20) {
+        const T dij = ref_add_rn(ref_add_rn(ref_mul_rn(d0, d0), ref_mul_rn(d1, d1)), ref_mul_rn(d2, d2));
+        if (dij < rcutsq[jt + it * (ntypes + 1)] && dij > T(1e-20)) {
             if (pairlist_rows) pairlist_rows[(size_t)jnum * ii + cnt] = j;
             cnt++;
         }
     }
     pairnum[ii] = cnt;
 }
-__global__ void k_ref_pair_emit_csr(int *__restrict__ pairlist, const int *__restrict__ off, const double *__restrict__ x,
-                                    const double *__restrict__ rcutsq, const int *__restrict__ ilist,
+template <typename T>
+__global__ void k_ref_pair_emit_csr(int *__restrict__ pairlist, const int *__restrict__ off, const T *__restrict__ x,
+                                    const T *__restrict__ rcutsq, const int *__restrict__ ilist,
                                     const int *__restrict__ nlist, const int *__restrict__ nnum,
                                     const int *__restrict__ atype, const int *__restrict__ alist, int inum, int ntypes)
 {
@@ -175,15 +183,16 @@ __global__ void k_ref_pair_emit_csr(int *__restrict__ pairlist, const int *__res
     for (int l = 0; l < m; l++) {
         const int j = nlist[n0 + l];
         const int jt = atype[alist[j]];
-        const double d0 = x[3 * (size_t)j] - x[3 * (size_t)i], d1 = x[3 * (size_t)j + 1] - x[3 * (size_t)i + 1],
+        const T d0 = x[3 * (size_t)j] - x[3 * (size_t)i], d1 = x[3 * (size_t)j + 1] - x[3 * (size_t)i + 1],
                      d2 = x[3 * (size_t)j + 2] - x[3 * (size_t)i + 2];
-        const double dij = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
-        if (dij < rcutsq[jt + it * (ntypes + 1)] && dij > 1e-20) pairlist[q++] = j;
+        const T dij = ref_add_rn(ref_add_rn(ref_mul_rn(d0, d0), ref_mul_rn(d1, d1)), ref_mul_rn(d2, d2));
+        if (dij < rcutsq[jt + it * (ntypes + 1)] && dij > T(1e-20)) pairlist[q++] = j;
     }
 }
 // pair geometry and indices (cpuSnap.cpp:1912-1933); rows layout when jnum > 0,
 // CSR (pairlist at pairnumsum[ii]) when jnum == 0
-__global__ void k_ref_pairs(double *__restrict__ xij, const double *__restrict__ x, int *__restrict__ aii,
+template <typename T>
+__global__ void k_ref_pairs(T *__restrict__ xij, const T *__restrict__ x, int *__restrict__ aii,
                             int *__restrict__ ai, int *__restrict__ aj, int *__restrict__ ti, int *__restrict__ tj,
                             const int *__restrict__ pairnum, const int *__restrict__ pairlist,
                             const int *__restrict__ pairnumsum, const int *__restrict__ ilist,
@@ -599,6 +608,26 @@ void mdp_gpu_neigh_pair_list_f64(int *pairnum, int *pairlist, const double *x, c
 }
 
 void mdp_gpu_neigh_pairs_f64(double *xij, const double *x, int *aii, int *ai, int *aj, int *ti, int *tj,
+                             const int *pairnum, const int *pairlist, const int *pairnumsum, const int *ilist,
+                             const int *atomtype, const int *alist, int inum, int jnum, int dim)
+{
+    if (dim != 3) { set_error("dim must be 3"); return; }
+    k_ref_pairs<<<(inum + 255) / 256, 256>>>(xij, x, aii, ai, aj, ti, tj, pairnum, pairlist, pairnumsum, ilist,
+                                              atomtype, alist, inum, jnum);
+}
+
+// PREC_FLOAT builds of MDP: the same pair selection and pair vectors in float,
+// rounded as the reference's float build rounds them
+void mdp_gpu_neigh_pair_list_f32(int *pairnum, int *pairlist, const float *x, const float *rcutsq, const int *ilist,
+                                 const int *neighlist, const int *neighnum, const int *atomtype, const int *alist,
+                                 int inum, int jnum, int dim, int ntypes)
+{
+    if (dim != 3) { set_error("dim must be 3"); return; }
+    k_ref_pair_count<<<(inum + 255) / 256, 256>>>(pairnum, x, rcutsq, ilist, neighlist, neighnum, atomtype, alist,
+                                                   inum, jnum, ntypes, 0, pairlist);
+}
+
+void mdp_gpu_neigh_pairs_f32(float *xij, const float *x, int *aii, int *ai, int *aj, int *ti, int *tj,
                              const int *pairnum, const int *pairlist, const int *pairnumsum, const int *ilist,
                              const int *atomtype, const int *alist, int inum, int jnum, int dim)
 {

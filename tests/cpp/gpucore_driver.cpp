@@ -10,6 +10,9 @@
 //     on `backend` (here 2) and call the gpu* functions;
 //   * src/C++/Core/cpuCore.cpp -- the CPU templates the wrappers' backend-1
 //     branches name (needed to link; not called).
+// Built twice: as MDP builds by default (dstype = double) and with PREC_FLOAT
+// (dstype = float), the reference's single-precision build, whose gpu*
+// templates are the float instantiations.
 // `gpucore_pair_snap3` then runs the stage sequence of ComputePairSnap3
 // (src/C++/Descriptors/snappotential.cpp:634-760) through those wrappers on
 // device arrays, block by block, and returns eatom, fatom and the SoA virial
@@ -77,34 +80,34 @@ int fail(char *msg, const char *what)
 
 extern "C" int gpucore_pair_snap3(
     // outputs (host): eatom[inum], fatom[3 inum], vatom[6 inum]
-    double *eatom_h, double *fatom_h, double *vatom_h,
+    dstype *eatom_h, dstype *fatom_h, dstype *vatom_h,
     // configuration (host, the reference layouts)
-    const double *x_h, const int *atomtype_h, const int *alist_h, const int *neighlist_h, const int *neighnum_h,
-    int inum, int anum, int neighmax, const double *rcutsq_h, int ntypes,
+    const dstype *x_h, const int *atomtype_h, const int *alist_h, const int *neighlist_h, const int *neighnum_h,
+    int inum, int anum, int neighmax, const dstype *rcutsq_h, int ntypes,
     // SNAP tables and parameters (host)
-    const double *rootpq_h, int nrootpq, const double *cglist_h, int idxcg_max, const int *idxz_h, int idxz_max,
+    const dstype *rootpq_h, int nrootpq, const dstype *cglist_h, int idxcg_max, const int *idxz_h, int idxz_max,
     const int *idxz_block_h, const int *idxb_h, int idxb_max, const int *idxb_block_h, const int *idxu_block_h,
-    int idxu_max, const int *idxcg_block_h, int nblock3, const double *bzero_h, const double *coeffelem_h,
-    int ncoeffall, const int *map_h, const double *radelem_h, const double *wjelem_h, double rmin0, double rfac0,
-    double rcutfac, double wself, int twojmax, int switchflag, int bzeroflag, int bnormflag, int wselfallflag,
+    int idxu_max, const int *idxcg_block_h, int nblock3, const dstype *bzero_h, const dstype *coeffelem_h,
+    int ncoeffall, const int *map_h, const dstype *radelem_h, const dstype *wjelem_h, dstype rmin0, dstype rfac0,
+    dstype rcutfac, dstype wself, int twojmax, int switchflag, int bzeroflag, int bnormflag, int wselfallflag,
     int nblocks, char *msg)
 {
     const int dim = 3, backend = 2, chemflag = 0, quadraticflag = 0, nelements = 1, nelem = 1;
     const int jd = twojmax + 1;
     Dev x, atomtype, alist, neighlist, neighnum, rcutsq, rootpq, cglist, idxz, idxz_block, idxb, idxb_block,
         idxu_block, idxcg_block, bzero, coeffelem, map, radelem, wjelem, eatom, fatom, vatom;
-    if (up(x, x_h, sizeof(double) * 3 * anum) || up(atomtype, atomtype_h, sizeof(int) * anum) ||
+    if (up(x, x_h, sizeof(dstype) * 3 * anum) || up(atomtype, atomtype_h, sizeof(int) * anum) ||
         up(alist, alist_h, sizeof(int) * anum) || up(neighlist, neighlist_h, sizeof(int) * (size_t)inum * neighmax) ||
         up(neighnum, neighnum_h, sizeof(int) * inum) ||
-        up(rcutsq, rcutsq_h, sizeof(double) * (ntypes + 1) * (ntypes + 1)) ||
-        up(rootpq, rootpq_h, sizeof(double) * nrootpq) || up(cglist, cglist_h, sizeof(double) * idxcg_max) ||
+        up(rcutsq, rcutsq_h, sizeof(dstype) * (ntypes + 1) * (ntypes + 1)) ||
+        up(rootpq, rootpq_h, sizeof(dstype) * nrootpq) || up(cglist, cglist_h, sizeof(dstype) * idxcg_max) ||
         up(idxz, idxz_h, sizeof(int) * 10 * idxz_max) || up(idxz_block, idxz_block_h, sizeof(int) * nblock3) ||
         up(idxb, idxb_h, sizeof(int) * 3 * idxb_max) || up(idxb_block, idxb_block_h, sizeof(int) * nblock3) ||
         up(idxu_block, idxu_block_h, sizeof(int) * jd) || up(idxcg_block, idxcg_block_h, sizeof(int) * nblock3) ||
-        up(bzero, bzero_h, sizeof(double) * jd) || up(coeffelem, coeffelem_h, sizeof(double) * ncoeffall) ||
-        up(map, map_h, sizeof(int) * (ntypes + 1)) || up(radelem, radelem_h, sizeof(double) * (ntypes + 1)) ||
-        up(wjelem, wjelem_h, sizeof(double) * (ntypes + 1)) || up(eatom, nullptr, sizeof(double) * inum) ||
-        up(fatom, nullptr, sizeof(double) * 3 * inum) || up(vatom, nullptr, sizeof(double) * 6 * inum))
+        up(bzero, bzero_h, sizeof(dstype) * jd) || up(coeffelem, coeffelem_h, sizeof(dstype) * ncoeffall) ||
+        up(map, map_h, sizeof(int) * (ntypes + 1)) || up(radelem, radelem_h, sizeof(dstype) * (ntypes + 1)) ||
+        up(wjelem, wjelem_h, sizeof(dstype) * (ntypes + 1)) || up(eatom, nullptr, sizeof(dstype) * inum) ||
+        up(fatom, nullptr, sizeof(dstype) * 3 * inum) || up(vatom, nullptr, sizeof(dstype) * 6 * inum))
         return fail(msg, "device set-up");
 
     // ComputePairSnap3's block loop (snappotential.cpp:687-758)
@@ -130,9 +133,9 @@ extern "C" int gpucore_pair_snap3(
         const size_t nu = (size_t)idxu_max * nelements * na;
         if (up(ai, nullptr, sizeof(int) * ineighmax) || up(aj, nullptr, sizeof(int) * ineighmax) ||
             up(ti, nullptr, sizeof(int) * ineighmax) || up(tj, nullptr, sizeof(int) * ineighmax) ||
-            up(aii, nullptr, sizeof(int) * ineighmax) || up(rij, nullptr, sizeof(double) * dim * ineighmax) ||
-            up(ur, nullptr, sizeof(double) * nu) || up(ui, nullptr, sizeof(double) * nu) ||
-            up(yr, nullptr, sizeof(double) * nu) || up(yi, nullptr, sizeof(double) * nu))
+            up(aii, nullptr, sizeof(int) * ineighmax) || up(rij, nullptr, sizeof(dstype) * dim * ineighmax) ||
+            up(ur, nullptr, sizeof(dstype) * nu) || up(ui, nullptr, sizeof(dstype) * nu) ||
+            up(yr, nullptr, sizeof(dstype) * nu) || up(yi, nullptr, sizeof(dstype) * nu))
             return fail(msg, "pair arrays");
         NeighborPairs(rij.as<dstype>(), x.as<dstype>(), aii.as<int>(), ai.as<int>(), aj.as<int>(), ti.as<int>(),
                       tj.as<int>(), pairnum.as<int>(), pairlist.as<int>(), pairnumsum.as<int>(), ilist.as<int>(),
@@ -157,9 +160,9 @@ extern "C" int gpucore_pair_snap3(
                       tj.as<int>(), twojmax, idxu_max, na, inum, ineighmax, switchflag, chemflag, backend);
         if (cudaDeviceSynchronize() != cudaSuccess) return fail(msg, "block sequence");
     }
-    if (cudaMemcpy(eatom_h, eatom.p, sizeof(double) * inum, cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(fatom_h, fatom.p, sizeof(double) * 3 * inum, cudaMemcpyDeviceToHost) != cudaSuccess ||
-        cudaMemcpy(vatom_h, vatom.p, sizeof(double) * 6 * inum, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaMemcpy(eatom_h, eatom.p, sizeof(dstype) * inum, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(fatom_h, fatom.p, sizeof(dstype) * 3 * inum, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(vatom_h, vatom.p, sizeof(dstype) * 6 * inum, cudaMemcpyDeviceToHost) != cudaSuccess)
         return fail(msg, "download");
     return 0;
 }
