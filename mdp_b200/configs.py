@@ -51,7 +51,10 @@ class SnapParams:
 
     @property
     def ncoeffall(self) -> int:
-        return self.ncoeff + 1
+        """1 + ncoeff linear coefficients, plus the ncoeff (ncoeff + 1) / 2
+        quadratic ones (upper triangle, row by row) when quadraticflag is set."""
+        n = self.ncoeff
+        return n + 1 + (n * (n + 1) // 2 if self.quadraticflag else 0)
 
 
 def idxb_count(twojmax: int) -> int:
@@ -73,9 +76,17 @@ def seeded_coeff(twojmax: int, seed: int, beta0: float = -11.7, sigma: float = 0
     return c
 
 
-def snap_params(twojmax: int = 8, seed: int = 1234, **kw) -> SnapParams:
+def snap_params(twojmax: int = 8, seed: int = 1234, qsigma: float = 1e-5, **kw) -> SnapParams:
+    """Seeded parameters; with quadraticflag=1 the quadratic coefficients are
+    drawn N(0, qsigma) after the linear ones (1e-5 moves the 2J=8 Ta forces
+    by about a tenth of their size)."""
     p = SnapParams(twojmax=twojmax, **kw)
-    p.coeff = seeded_coeff(twojmax, seed)
+    c = seeded_coeff(twojmax, seed)
+    if p.quadraticflag:
+        n = p.ncoeff
+        q = np.random.default_rng(seed + 7919).normal(0.0, qsigma, n * (n + 1) // 2)
+        c = np.concatenate([c, q])
+    p.coeff = c
     return p
 
 

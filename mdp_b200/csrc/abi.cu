@@ -374,7 +374,8 @@ int ref_snap_yi(double *yr, double *yi, const double *ur, const double *ui, cons
     return 0;
 }
 
-int launch_yi_pa_d(const SnapModel &m, ForcePath &fp, int inum, const double *G, cudaStream_t s);
+int launch_yi_pa_d(const SnapModel &m, const YParams<double> &yp, ForcePath &fp, int inum, const double *G,
+                   cudaStream_t s);
 
 // Y with per-atom coefficients beta [jjb][inum] (cpuSnap4.cpp:601-691): the
 // model's coefficients are all 1, so its per-triple factors carry only the
@@ -389,7 +390,7 @@ int ref_snap_yi_beta(double *yr, double *yi, const double *ur, const double *ui,
     if (load_tiles(c, ur, ui, inum, tj, s)) return -1;
     const long ntiles = (inum + 31) / 32;
     if (c.fp.Y.ensure(sizeof(double2) * ntiles * 32 * yh_count(tj))) return -1;
-    if (launch_yi_pa_d(c.model, c.fp, inum, beta, s)) return -1;
+    if (launch_yi_pa_d(c.model, c.model.yd, c.fp, inum, beta, s)) return -1;
     const long n = (long)inum * idxu_count(tj);
     k_ytiles_to_ref<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(c.fp.Y.as<double2>(), inum, tj, yh_count(tj), yr, yi);
     MDP_CUDA_TRY(cudaGetLastError());

@@ -75,12 +75,25 @@ __device__ __forceinline__ void zbl_pair(const ZblParams &zp, double r, double &
 }
 __global__ void k_zbl(const double4 *, const int *, const int *, int, int, ZblParams, double *, double4 *, double *);
 
+// Quadratic SNAP (quadraticflag): E_i = beta0 + beta . B_i + B_i^T Q B_i / 2 with
+// the coefficient layout of cpuSnap.cpp:1713-1770 (ncoeff linear, then the
+// upper triangle of Q row by row, its diagonal entries taken once)
+constexpr int QUAD_MAXK = 55;   // ncoeff at 2J = 8
+struct QuadParams {
+    double beta0;
+    double beta[QUAD_MAXK];
+    double q[QUAD_MAXK * (QUAD_MAXK + 1) / 2];
+    int ncoeff;
+};
+
 struct SnapModel {
     mdp_snap_params p;
     std::vector<double> coeff;
     SnapGeom geom;
     YParams<double> yd;
     YParams<float> yf;
+    YParams<double> yq;   // quadratic: unit coefficients (multiplicities only), per-atom coefficients from B
+    QuadParams quad;
     int nu, nyh, ncoeff;
     ZblParams zbl;
 };
@@ -97,6 +110,7 @@ struct DevBuf {
 
 struct ForcePath {
     DevBuf pcount, poff, prij, pinfo, pab, smap, dE, Ut, Y, scan_tmp;
+    DevBuf B, G;   // quadratic SNAP: per-atom bispectrum and coefficients [k][atom]
     int natoms_cap = 0, nm_cap = 0;
     // per-stage timing (CUDA events on the launching stream), enabled on demand
     bool timing = false;

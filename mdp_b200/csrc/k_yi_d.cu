@@ -23,7 +23,7 @@ int launch_yi(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, int inum,
 // per-atom coefficients G [k][atom] (k over the bispectrum components), FP64:
 // the beta form of the reference's Yi (cpuSnap4.cpp:601-691); no energy
 template <int TJ>
-static int launch_yi_pa_d_tj(const SnapModel &m, ForcePath &fp, int inum, const double *G, cudaStream_t s)
+static int launch_yi_pa_d_tj(const YParams<double> &yp, ForcePath &fp, int inum, const double *G, cudaStream_t s)
 {
     if (tu_ensure_tables()) return -1;
     const size_t sm = yi_smem_bytes<double, TJ, true>();
@@ -33,17 +33,19 @@ static int launch_yi_pa_d_tj(const SnapModel &m, ForcePath &fp, int inum, const 
         return -1;
     const int ntiles = (inum + 31) / 32;
     const int blocks = std::min(ntiles, num_sms() * per_sm);
-    k_snap_yi<double, TJ, true><<<blocks, YiWarps<double, TJ>::n * 32, sm, s>>>(fp.Ut.as<double2>(), inum, m.yd,
+    k_snap_yi<double, TJ, true><<<blocks, YiWarps<double, TJ>::n * 32, sm, s>>>(fp.Ut.as<double2>(), inum, yp,
                                                                             fp.Y.as<double2>(), nullptr, G);
     return 0;
 }
 
-int launch_yi_pa_d(const SnapModel &m, ForcePath &fp, int inum, const double *G, cudaStream_t s)
+// yp: the per-triple factors of a model whose coefficients are all 1
+int launch_yi_pa_d(const SnapModel &m, const YParams<double> &yp, ForcePath &fp, int inum, const double *G,
+                   cudaStream_t s)
 {
     switch (m.p.twojmax) {
-    case 4: return launch_yi_pa_d_tj<4>(m, fp, inum, G, s);
-    case 6: return launch_yi_pa_d_tj<6>(m, fp, inum, G, s);
-    case 8: return launch_yi_pa_d_tj<8>(m, fp, inum, G, s);
+    case 4: return launch_yi_pa_d_tj<4>(yp, fp, inum, G, s);
+    case 6: return launch_yi_pa_d_tj<6>(yp, fp, inum, G, s);
+    case 8: return launch_yi_pa_d_tj<8>(yp, fp, inum, G, s);
     }
     set_error("twojmax %d not supported", m.p.twojmax);
     return -1;

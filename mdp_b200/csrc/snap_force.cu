@@ -92,7 +92,7 @@ void DevBuf::release()
 
 void ForcePath::release()
 {
-    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &smap, &dE, &Ut, &Y, &scan_tmp};
+    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &smap, &dE, &Ut, &Y, &scan_tmp, &B, &G};
     for (auto x : b) x->release();
     for (auto &e : ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
@@ -121,10 +121,11 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
         set_error("twojmax=%d not supported (4, 6 or 8)", tj);
         return -1;
     }
-    if (p->chemflag != 0 || p->quadraticflag != 0) {
-        set_error("chemflag/quadraticflag SNAP is not supported (single-element linear SNAP only)");
+    if (p->chemflag != 0) {
+        set_error("chemflag SNAP is not supported (single element only)");
         return -1;
     }
+    if (p->quadraticflag != 0 && p->quadraticflag != 1) { set_error("quadraticflag must be 0 or 1"); return -1; }
     if (p->switchflag != 0 && p->switchflag != 1) { set_error("switchflag must be 0 or 1"); return -1; }
     // idxb enumeration (cpuSnap.cpp:44-68)
     int jjb[JD][JD][JD];
@@ -133,8 +134,10 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
         for (int j2 = 0; j2 <= j1; j2++)
             for (int j = j1 - j2; j <= std::min(tj, j1 + j2); j += 2)
                 if (j >= j1) jjb[j1][j2][j] = nb++;
-    if (p->ncoeffall != nb + 1) {
-        set_error("ncoeffall=%d but 2J=%d needs %d coefficients", p->ncoeffall, tj, nb + 1);
+    const int nall = nb + 1 + (p->quadraticflag ? nb * (nb + 1) / 2 : 0);
+    if (p->ncoeffall != nall) {
+        set_error("ncoeffall=%d but 2J=%d%s needs %d coefficients", p->ncoeffall, tj,
+                  p->quadraticflag ? " with quadratic terms" : "", nall);
         return -1;
     }
     if (!p->coeff) { set_error("null coefficient array"); return -1; }
@@ -155,28 +158,47 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
     // beta' per coupling triple (cpuSnap4.cpp:763-787)
     memset(&m.yd, 0, sizeof(m.yd));
     memset(&m.yf, 0, sizeof(m.yf));
+    memset(&m.yq, 0, sizeof(m.yq));
     const double *c = m.coeff.data();
-    for (int j1 = 0; j1 <= tj; j1++)
-        for (int j2 = 0; j2 <= j1; j2++)
-            for (int j = 0; j <= tj; j++) {
-                if (!triple_ok(j1, j2, j, tj)) continue;
-                double b;
-                if (j >= j1) {
-                    b = c[1 + jjb[j1][j2][j]];
-                    if (j1 == j) b *= (j2 == j) ? 3.0 : 2.0;
-                } else if (j >= j2) {
-                    b = c[1 + jjb[j][j2][j1]];
-                    if (j2 == j) b *= 2.0;
-                } else {
-                    b = c[1 + jjb[j2][j][j1]];
+    auto fill_beta = [&](const double *cc, YParams<double> &yd, YParams<float> *yf) {
+        for (int j1 = 0; j1 <= tj; j1++)
+            for (int j2 = 0; j2 <= j1; j2++)
+                for (int j = 0; j <= tj; j++) {
+                    if (!triple_ok(j1, j2, j, tj)) continue;
+                    double b;
+                    if (j >= j1) {
+                        b = cc[1 + jjb[j1][j2][j]];
+                        if (j1 == j) b *= (j2 == j) ? 3.0 : 2.0;
+                    } else if (j >= j2) {
+                        b = cc[1 + jjb[j][j2][j1]];
+                        if (j2 == j) b *= 2.0;
+                    } else {
+                        b = cc[1 + jjb[j2][j][j1]];
+                    }
+                    if (!p->bnormflag && j1 > j) b *= (j1 + 1) / (j + 1.0);
+                    if (p->bnormflag) b /= (j + 1);
+                    const int k = (j >= j1) ? jjb[j1][j2][j] : (j >= j2) ? jjb[j][j2][j1] : jjb[j2][j][j1];
+                    yd.betaY[tri_index(j1, j2, j)] = b;
+                    yd.kmap[tri_index(j1, j2, j)] = (unsigned char)k;
+                    if (yf) {
+                        yf->betaY[tri_index(j1, j2, j)] = (float)b;
+                        yf->kmap[tri_index(j1, j2, j)] = (unsigned char)k;
+                    }
                 }
-                if (!p->bnormflag && j1 > j) b *= (j1 + 1) / (j + 1.0);
-                if (p->bnormflag) b /= (j + 1);
-                m.yd.betaY[tri_index(j1, j2, j)] = b;
-                m.yf.betaY[tri_index(j1, j2, j)] = (float)b;
-                const int k = (j >= j1) ? jjb[j1][j2][j] : (j >= j2) ? jjb[j][j2][j1] : jjb[j2][j][j1];
-                m.yd.kmap[tri_index(j1, j2, j)] = m.yf.kmap[tri_index(j1, j2, j)] = (unsigned char)k;
-            }
+    };
+    fill_beta(c, m.yd, &m.yf);
+    // quadratic SNAP: the Y kernel takes per-atom coefficients G_i = beta + Q B_i,
+    // so its per-triple factors are those of unit coefficients
+    memset(&m.quad, 0, sizeof(m.quad));
+    if (p->quadraticflag) {
+        if (nb > QUAD_MAXK) { set_error("quadratic SNAP supports up to %d components", QUAD_MAXK); return -1; }
+        std::vector<double> ones(nb + 1, 1.0);
+        fill_beta(ones.data(), m.yq, nullptr);
+        m.quad.beta0 = c[0];
+        m.quad.ncoeff = nb;
+        for (int k = 0; k < nb; k++) m.quad.beta[k] = c[1 + k];
+        for (int k = 0; k < nb * (nb + 1) / 2; k++) m.quad.q[k] = c[1 + nb + k];
+    }
     double e0 = c[0];
     if (p->bzeroflag) {
         for (int j1 = 0; j1 <= tj; j1++)
@@ -239,6 +261,9 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
         set_error("Y-kernel warp assignment failed");
         return -1;
     }
+    memcpy(m.yq.lay_mb, m.yd.lay_mb, sizeof(m.yd.lay_mb));
+    memcpy(m.yq.lay_o, m.yd.lay_o, sizeof(m.yd.lay_o));
+    memcpy(m.yq.lay_st, m.yd.lay_st, sizeof(m.yd.lay_st));
 
     return 0;
 }
@@ -253,6 +278,56 @@ static int launch_snap(const SnapModel &m, const YParams<T> &yp, ForcePath &fp, 
     if (launch_ui<T, TJ>(m, fp, inum, s)) return -1;
     if (launch_yi<T, TJ>(m, yp, fp, inum, eatom, s)) return -1;
     return launch_fi<T, TJ>(m, fp, inum, nm, s);
+}
+
+int launch_bi_tiles(const double2 *Ut, int natoms, int tj, int bnorm, int bzero, double *bout, long bstride,
+                    cudaStream_t s);
+int launch_yi_pa_d(const SnapModel &m, const YParams<double> &yp, ForcePath &fp, int inum, const double *G,
+                   cudaStream_t s);
+
+// Quadratic SNAP, one thread per atom: G[k][atom] = beta_k + (Q B)_k (the
+// per-atom coefficients of cpuComputeBeta2, cpuSnap.cpp:1713-1737) and
+// eatom = beta0 + beta . B + B^T Q B / 2 = beta0 + B . (beta + G) / 2
+// (cpuSnapTallyEnergyFull, cpuSnap.cpp:1743-1770).  B [k][atom] is staged in
+// shared memory per block.
+constexpr int QUAD_THREADS = 64;
+__global__ void __launch_bounds__(QUAD_THREADS)
+k_snap_quad(const double *__restrict__ B, int natoms, const __grid_constant__ QuadParams Q, double *__restrict__ G,
+            double *__restrict__ eatom)
+{
+    __shared__ double bs[QUAD_MAXK][QUAD_THREADS];
+    const int t = threadIdx.x, atom = blockIdx.x * QUAD_THREADS + t;
+    const int n = Q.ncoeff;
+    for (int k = 0; k < n; k++) bs[k][t] = atom < natoms ? B[(size_t)k * natoms + atom] : 0.0;
+    if (atom >= natoms) return;
+    double e = 0.0;
+    for (int k = 0; k < n; k++) {
+        double g = Q.beta[k];
+        // row k of the packed upper triangle: q(k, l) for l >= k at off(k) + l - k
+        const int offk = k * n - k * (k - 1) / 2;
+        for (int l = 0; l < k; l++) g += Q.q[l * n - l * (l - 1) / 2 + (k - l)] * bs[l][t];
+        for (int l = k; l < n; l++) g += Q.q[offk + (l - k)] * bs[l][t];
+        G[(size_t)k * natoms + atom] = g;
+        e += bs[k][t] * (Q.beta[k] + g);
+    }
+    eatom[atom] = Q.beta0 + 0.5 * e;
+}
+
+template <int TJ>
+static int launch_snap_quad(const SnapModel &m, ForcePath &fp, int inum, int nm, double *eatom, cudaStream_t s)
+{
+    const int nk = m.ncoeff;
+    if (fp.B.ensure(sizeof(double) * (size_t)nk * inum) || fp.G.ensure(sizeof(double) * (size_t)nk * inum))
+        return -1;
+    if (launch_ui<double, TJ>(m, fp, inum, s)) return -1;
+    if (fp.timing) cudaEventRecord(fp.ev[2], s);
+    if (launch_bi_tiles(fp.Ut.as<double2>(), inum, TJ, m.p.bnormflag, m.p.bzeroflag, fp.B.as<double>(), inum, s))
+        return -1;
+    k_snap_quad<<<(inum + QUAD_THREADS - 1) / QUAD_THREADS, QUAD_THREADS, 0, s>>>(fp.B.as<double>(), inum, m.quad,
+                                                                               fp.G.as<double>(), eatom);
+    count_launches(2);
+    if (launch_yi_pa_d(m, m.yq, fp, inum, fp.G.as<double>(), s)) return -1;
+    return launch_fi<double, TJ>(m, fp, inum, nm, s);
 }
 
 template <typename T>
@@ -293,8 +368,16 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), inum, fp.scan_tmp.as<int>(), s)) return -1;
     k_pair_emit<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, fp.poff.as<int>(), m.geom, fp.prij.as<double4>(),
                                   fp.pinfo.as<int2>(), fp.pab.as<double4>(), fp.smap.as<int>());
-    int rc = (precision == MDP_PREC_FP32) ? launch_snap_tj<float>(m, m.yf, fp, inum, nm, eatom, s)
-                                           : launch_snap_tj<double>(m, m.yd, fp, inum, nm, eatom, s);
+    int rc;
+    if (m.p.quadraticflag) {
+        if (precision != MDP_PREC_FP64) { set_error("quadratic SNAP runs in FP64 only"); return -1; }
+        rc = m.p.twojmax == 8   ? launch_snap_quad<8>(m, fp, inum, nm, eatom, s)
+             : m.p.twojmax == 6 ? launch_snap_quad<6>(m, fp, inum, nm, eatom, s)
+                                : launch_snap_quad<4>(m, fp, inum, nm, eatom, s);
+    } else {
+        rc = (precision == MDP_PREC_FP32) ? launch_snap_tj<float>(m, m.yf, fp, inum, nm, eatom, s)
+                                          : launch_snap_tj<double>(m, m.yd, fp, inum, nm, eatom, s);
+    }
     if (rc) return rc;
     if (fp.timing) cudaEventRecord(fp.ev[4], s);
     k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,

@@ -211,6 +211,90 @@ void ref_snap_force(double *eatom, double *fatom, double *vatom, const double *x
     }
 }
 
+// SNAP forces through the reference's other pair chain, ComputePairSnap
+// (snappotential.cpp:236-410): per-pair U and dU (cpuComputeUij,
+// cpuComputeDuijdrj), U totals, Z and B (cpuComputeZi, cpuComputeBi), energy
+// and per-atom coefficients with the quadratic terms (cpuSnapTallyEnergyFull,
+// cpuComputeBeta2, cpuSnap.cpp:1713-1770), Y from those coefficients, dE/dr
+// and the force / virial tallies.  This is the chain that carries
+// quadraticflag (ComputePairSnap3 leaves it unused).  One atom block,
+// single element; eatom, fatom (AoS) and vatom (SoA 6 x inum) accumulate.
+void ref_snap_force_pairsnap(double *eatom, double *fatom, double *vatom, const double *x,
+                             const int *atomtype, const int *alist, const int *neighlist, const int *neighnum,
+                             int inum, int neighmax, int twojmax, int ncoeffall, const double *coeffelem,
+                             double rcutfac, double rfac0, double rmin0, double radelem1, double wjelem1,
+                             int switchflag, int bzeroflag, int bnormflag, int wselfallflag, int quadraticflag)
+{
+    const int dim = 3, ntypes = 1, nelem = 1, chemflag = 0;
+    int jdim = twojmax + 1;
+    int idx_max[5];
+    int idxcg_count = 0, idxz_count = 0, idxb_count = 0;
+    for (int j1 = 0; j1 <= twojmax; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= MIN(twojmax, j1 + j2); j += 2) {
+                idxcg_count += (j1 + 1) * (j2 + 1);
+                if (j >= j1) idxb_count++;
+                for (int mb = 0; 2 * mb <= j; mb++) idxz_count += j + 1;
+            }
+    std::vector<double> rootpq((jdim + 1) * (jdim + 1)), cglist(idxcg_count), fac(168);
+    std::vector<int> idxz(idxz_count * 10), idxz_block(jdim * jdim * jdim), idxb(idxb_count * 3),
+        idxb_block(jdim * jdim * jdim), idxu_block(jdim), idxcg_block(jdim * jdim * jdim);
+    fac[0] = 1.0;
+    for (int i = 1; i < 168; i++) fac[i] = fac[i - 1] * (double)i;
+    cpuInitSna(rootpq.data(), cglist.data(), fac.data(), idx_max, idxz.data(), idxz_block.data(),
+               idxb.data(), idxb_block.data(), idxu_block.data(), idxcg_block.data(), twojmax);
+    const int idxu_max = idx_max[1], idxb_max = idx_max[2], idxz_max = idx_max[3], ncoeff = idxb_max;
+    double radelem[2] = {0.0, radelem1}, wjelem[2] = {0.0, wjelem1};
+    int map[2] = {0, 0};
+    double cut = (radelem1 + radelem1) * rcutfac;
+    double rcutsq[4] = {0, 0, 0, cut * cut};
+    double bzero[64];
+    for (int j = 0; j <= twojmax; j++) bzero[j] = bnormflag ? 1.0 : (double)(j + 1);
+    const double wself = 1.0;
+    const int na = inum;
+    std::vector<int> pairnum(na), pairlist((size_t)na * neighmax), pairnumsum(na + 1);
+    cpuNeighPairList(pairnum.data(), pairlist.data(), (double *)x, rcutsq, (int *)alist, (int *)neighlist,
+                     (int *)neighnum, (int *)atomtype, (int *)alist, na, neighmax, dim, ntypes);
+    pairnumsum[0] = 0;
+    for (int i = 0; i < na; i++) pairnumsum[i + 1] = pairnumsum[i] + pairnum[i];
+    const int ijnum = pairnumsum[na];
+    std::vector<int> ai(ijnum), aj(ijnum), ti(ijnum), tj(ijnum), aii(ijnum);
+    std::vector<double> rij((size_t)3 * ijnum);
+    cpuNeighPairs(rij.data(), (double *)x, aii.data(), ai.data(), aj.data(), ti.data(), tj.data(), pairnum.data(),
+                  pairlist.data(), pairnumsum.data(), (int *)alist, (int *)atomtype, (int *)alist, na, neighmax, dim);
+    std::vector<double> ur((size_t)idxu_max * ijnum), ui((size_t)idxu_max * ijnum),
+        dur((size_t)idxu_max * dim * ijnum), dui((size_t)idxu_max * dim * ijnum),
+        utr((size_t)idxu_max * na), uti((size_t)idxu_max * na), zr((size_t)idxz_max * na), zi((size_t)idxz_max * na),
+        yr((size_t)idxu_max * na), yi((size_t)idxu_max * na), blist((size_t)idxb_max * na),
+        beta((size_t)ncoeff * na), dedr((size_t)dim * ijnum);
+    cpuComputeUij(ur.data(), ui.data(), rootpq.data(), rij.data(), radelem, rmin0, rfac0, rcutfac,
+                  idxu_block.data(), ai.data(), aj.data(), ti.data(), tj.data(), twojmax, idxu_max, ijnum);
+    cpuZeroUarraytot(utr.data(), uti.data(), wself, idxu_block.data(), (int *)atomtype, map, ai.data(),
+                     wselfallflag, chemflag, idxu_max, nelem, twojmax, inum);
+    cpuAddUarraytot(utr.data(), uti.data(), ur.data(), ui.data(), rij.data(), wjelem, radelem, rmin0, rcutfac,
+                    idxu_block.data(), (int *)alist, (int *)atomtype, pairnum.data(), pairnumsum.data(), map,
+                    tj.data(), twojmax, idxu_max, nelem, inum, switchflag, chemflag);
+    cpuComputeDuijdrj(dur.data(), dui.data(), ur.data(), ui.data(), rootpq.data(), rij.data(), wjelem, radelem,
+                      rmin0, rfac0, rcutfac, idxu_block.data(), ai.data(), aj.data(), ti.data(), tj.data(), twojmax,
+                      idxu_max, ijnum, switchflag);
+    cpuComputeZi(zr.data(), zi.data(), utr.data(), uti.data(), cglist.data(), idxz.data(), idxu_block.data(),
+                 idxcg_block.data(), twojmax, idxu_max, idxz_max, nelem, bnormflag, inum);
+    cpuComputeBi(blist.data(), zr.data(), zi.data(), utr.data(), uti.data(), bzero, (int *)alist, (int *)atomtype,
+                 map, idxb.data(), idxu_block.data(), idxz_block.data(), twojmax, idxb_max, idxu_max, idxz_max,
+                 nelem, bzeroflag, wselfallflag, chemflag, inum);
+    cpuSnapTallyEnergyFull(eatom, blist.data(), (double *)coeffelem, (int *)alist, map, (int *)atomtype, inum,
+                           ncoeff, ncoeffall, quadraticflag);
+    cpuComputeBeta2(beta.data(), blist.data(), (double *)coeffelem, (int *)alist, map, (int *)atomtype, inum,
+                    ncoeff, ncoeffall, quadraticflag);
+    cpuComputeYi(yr.data(), yi.data(), utr.data(), uti.data(), cglist.data(), beta.data(), idxz.data(),
+                 idxb_block.data(), idxu_block.data(), idxcg_block.data(), twojmax, idxb_max, idxu_max, idxz_max,
+                 nelem, bnormflag, ncoeff, inum);
+    cpuComputeDeidrj(dedr.data(), yr.data(), yi.data(), dur.data(), dui.data(), idxu_block.data(), map, ai.data(),
+                     aj.data(), ti.data(), tj.data(), nelem, twojmax, idxu_max, chemflag, ijnum);
+    cpuSnapTallyForceFull(fatom, dedr.data(), ai.data(), aj.data(), (int *)alist, ijnum);
+    cpuSnapTallyVirialFull(vatom, dedr.data(), rij.data(), ai.data(), aj.data(), inum, ijnum);
+}
+
 // Per-configuration SNAP descriptors in the order of ComputeSnap
 // (snappotential.cpp:762-910): bi[ncoeff] = sum_i B_i, bd[3*i + c + 3*inum*k] =
 // d(sum_a B_ak)/dx_ic, bv[6*k + c] (virial), blist[i + inum*k] per-atom B.

@@ -46,6 +46,11 @@ def lib():
                                               C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                               C.c_double, C.c_int, C.c_int, C.c_int, C.c_int]
         _lib.ref_snap_descriptors.restype = None
+        _lib.ref_snap_force_pairsnap.restype = None
+        _lib.ref_snap_force_pairsnap.argtypes = [_dp, _dp, _dp, _dp, _ip, _ip, _ip, _ip, C.c_int, C.c_int,
+                                                 C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_double,
+                                                 C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                 C.c_int]
         _lib.ref_nve_initial.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double, _ip, _ip, C.c_int]
         _lib.ref_nve_final.argtypes = [_dp, _dp, _dp, _dp, C.c_double, _ip, _ip, C.c_int]
         _lib.ref_omp_max_threads.restype = C.c_int
@@ -102,6 +107,25 @@ def snap_force(x_all, alist, neighlist, neighnum, params, nblocks=1, nthreads=1)
                          params.rcutfac, params.rfac0, params.rmin0, params.radelem, params.wjelem,
                          params.switchflag, params.bzeroflag, params.bnormflag, params.wselfallflag,
                          nblocks, nthreads)
+    return e, f.reshape(inum, 3), v.reshape(6, inum)
+
+
+def snap_force_pairsnap(x_all, alist, neighlist, neighnum, params):
+    """Per-atom energy, forces (N,3) and virial (6,N) from the reference's
+    ComputePairSnap chain (snappotential.cpp:236-410), the one that evaluates
+    the quadratic SNAP terms (quadraticflag)."""
+    inum, neighmax = neighlist.shape
+    e = np.zeros(inum); f = np.zeros(3 * inum); v = np.zeros(6 * inum)
+    atype = np.ones(x_all.shape[0], dtype=np.int32)
+    lib().ref_snap_force_pairsnap(e, f, v, np.ascontiguousarray(x_all).ravel(), atype,
+                                  np.ascontiguousarray(alist, dtype=np.int32),
+                                  np.ascontiguousarray(neighlist, dtype=np.int32).ravel(),
+                                  np.ascontiguousarray(neighnum, dtype=np.int32),
+                                  inum, neighmax, params.twojmax, params.ncoeffall,
+                                  np.ascontiguousarray(params.coeff, dtype=np.float64),
+                                  params.rcutfac, params.rfac0, params.rmin0, params.radelem, params.wjelem,
+                                  params.switchflag, params.bzeroflag, params.bnormflag, params.wselfallflag,
+                                  params.quadraticflag)
     return e, f.reshape(inum, 3), v.reshape(6, inum)
 
 

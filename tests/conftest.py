@@ -19,7 +19,7 @@ def pytest_configure(config):
 def golden_names():
     """Force / MD fixtures (the fit_* fixtures hold descriptors and are listed by fit_names)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not os.path.basename(p).startswith(("fit_", "tri_", "c2_", "chem_")))
+                  if not os.path.basename(p).startswith(("fit_", "tri_", "c2_", "chem_", "quad_")))
 
 
 def tri_names():

@@ -269,11 +269,39 @@ def c2_fixture(nthreads):
     print(c["name"], cfg.natoms, "atoms", nreb, "list builds", os.path.getsize(path), "bytes")
 
 
+# quadratic SNAP fixtures (quadraticflag = 1; the reference evaluates the quadratic terms in its
+# ComputePairSnap chain): (name, cells, 2J, temp, jitter, seed, coeff seed, flag overrides)
+QUAD_CASES = [
+    ("quad_bcc128_2j6", (4, 4, 4), 6, 600.0, 0.05, 18, 108, {}),
+    ("quad_bcc250_2j8", (5, 5, 5), 8, 300.0, 0.08, 19, 109, {}),
+    ("quad_bcc54_2j4_flags", (3, 3, 3), 4, 1000.0, 0.10, 20, 110, {"bnormflag": 1, "bzeroflag": 1}),
+]
+
+
+def quad_fixtures():
+    """Quadratic SNAP: positions, the reference's neighbour list and its per-atom energy, forces and
+    virial from the ComputePairSnap chain (cpuComputeBeta2 / cpuSnapTallyEnergyFull)."""
+    for (name, cells, tj, temp, jit, seed, cseed, flags) in QUAD_CASES:
+        p = configs.snap_params(tj, seed=cseed, quadraticflag=1, **flags)
+        cfg = configs.ta_config(cells, temp=temp, jitter=jit, seed=seed)
+        xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+        e, f, va = refpy.snap_force_pairsnap(xa, al, nl, nn, p)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, cells=np.array(cells), twojmax=tj, temp=temp, jitter=jit, seed=seed,
+                            coeff_seed=cseed, flags=np.array([p.bnormflag, p.bzeroflag, p.switchflag]),
+                            quadraticflag=1, skin=SKIN, neighmax=NEIGHMAX, x=cfg.x, box=cfg.box, coeff=p.coeff,
+                            xall=xa, alist=al, neighlist=nl, neighnum=nn, eatom=e, fatom=f, vatom=va)
+        print(name, cfg.natoms, "atoms", os.path.getsize(path), "bytes")
+
+
 def main():
     from oracle.refroot import reference_root
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REFROOT={reference_root() or ''}"])
     if "--c2" in sys.argv:
         c2_fixture(os.cpu_count() or 1)
+        return
+    if "--quad" in sys.argv:
+        quad_fixtures()
         return
     fit_fixtures()
     if "--fit-only" in sys.argv:
