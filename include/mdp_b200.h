@@ -19,7 +19,7 @@ extern "C" {
 
 /* SNAP hyper-parameters and coefficients: the snaparam[12] vector of MDP
  * (src/Julia/Preprocessing/Preprocessing.jl:266, read at
- * src/C++/Descriptors/snappotential.cpp:151-162) for a single element. */
+ * src/C++/Descriptors/snappotential.cpp:151-162) with its per-element arrays. */
 typedef struct {
     int twojmax;          /* 2J: 4, 6 or 8 */
     double rcutfac;
@@ -31,10 +31,18 @@ typedef struct {
     int bzeroflag;
     int bnormflag;
     int wselfallflag;
-    int quadraticflag;    /* must be 0 */
-    int chemflag;         /* must be 0 */
-    int ncoeffall;        /* 1 + number of bispectrum components */
-    const double *coeff;  /* ncoeffall values; coeff[0] = beta_0 */
+    int quadraticflag;    /* 1: quadratic SNAP (one element, FP64) */
+    int chemflag;         /* 1: element-resolved bispectrum (several elements) */
+    int ncoeffall;        /* coefficients per element: 1 + ncoeff (+ ncoeff (ncoeff + 1) / 2 quadratic) */
+    const double *coeff;  /* nelements x ncoeffall values; coeff[e * ncoeffall] = beta_0 of element e */
+    /* Several element types (InitSnap, snappotential.cpp:146-232): atoms carry
+     * types 1..nelements; per-element radii and weights; ncoeff is the number
+     * of bispectrum components times nelements^3 with chemflag.  nelements 0
+     * or 1 with radelems == NULL: the single element of radelem / wjelem.
+     * Several elements run in FP64, linear SNAP, nelements <= 4. */
+    int nelements;
+    const double *radelems;
+    const double *wjelems;
 } mdp_snap_params;
 
 enum { MDP_PREC_FP64 = 0, MDP_PREC_FP32 = 1 };
@@ -57,6 +65,12 @@ int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const doubl
                             const int *neighlist, const int *neighnum, int inum, int anum, int neighmax,
                             double *eatom, double *fatom, double *vatom, void *cuda_stream);
 
+/* Same with the atom types (1..nelements) of the inum owners, on the device;
+ * required by models with several element types. */
+int mdp_snap_compute_device_typed(const mdp_snap_params *p, int precision, const double *x, const int *atomtype,
+                                  const int *alist, const int *neighlist, const int *neighnum, int inum, int anum,
+                                  int neighmax, double *eatom, double *fatom, double *vatom, void *cuda_stream);
+
 /* Same on HOST arrays, including the ghost/neighbour build: natoms positions
  * in an orthogonal or triclinic periodic box with vectors a, b, c (box[0..8]).
  * Optional outputs (NULL to skip): neighlist (natoms x neighmax), neighnum,
@@ -65,6 +79,11 @@ int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, c
                           const double *box, double skin, int neighmax, double *eatom, double *fatom,
                           double *vatom, int *neighlist, int *neighnum, int *anum_out, int *alist_out,
                           double *xall_out, int alist_cap);
+/* Same with the natoms atom types (1..nelements) on the host. */
+int mdp_snap_compute_host_typed(const mdp_snap_params *p, int precision, int natoms, const double *x,
+                                const int *atomtype, const double *box, double skin, int neighmax, double *eatom,
+                                double *fatom, double *vatom, int *neighlist, int *neighnum, int *anum_out,
+                                int *alist_out, double *xall_out, int alist_cap);
 
 /* ---------------------------------------------------------------------------
  * MD engine: NVE velocity Verlet with SNAP forces, neighbour list rebuilt on
@@ -92,6 +111,9 @@ void mdp_md_destroy(mdp_md *h);
 int mdp_md_set_state(mdp_md *h, const double *x, const double *v);
 /* device positions/velocities already resident (natoms x 3 AoS) */
 int mdp_md_set_state_device(mdp_md *h, const double *x_dev, const double *v_dev);
+/* atom types 1..nelements (host, natoms), required before setup by models
+ * with several element types; the mass stays the configuration's one */
+int mdp_md_set_types(mdp_md *h, const int *types);
 /* neighbour list + first force + thermo (IntegrationSetup, Integration.cpp:158) */
 int mdp_md_setup(mdp_md *h);
 /* nsteps velocity-Verlet steps; thermo rows (step, T, PE/atom, TE/atom, P)

@@ -26,7 +26,8 @@ class SnapParamsC(C.Structure):
     _fields_ = [("twojmax", C.c_int), ("rcutfac", C.c_double), ("rfac0", C.c_double), ("rmin0", C.c_double),
                 ("radelem", C.c_double), ("wjelem", C.c_double), ("switchflag", C.c_int), ("bzeroflag", C.c_int),
                 ("bnormflag", C.c_int), ("wselfallflag", C.c_int), ("quadraticflag", C.c_int),
-                ("chemflag", C.c_int), ("ncoeffall", C.c_int), ("coeff", C.POINTER(C.c_double))]
+                ("chemflag", C.c_int), ("ncoeffall", C.c_int), ("coeff", C.POINTER(C.c_double)),
+                ("nelements", C.c_int), ("radelems", C.POINTER(C.c_double)), ("wjelems", C.POINTER(C.c_double))]
 
 
 class MDConfigC(C.Structure):
@@ -53,6 +54,12 @@ def lib():
     L.mdp_snap_compute_device.argtypes = [C.POINTER(SnapParamsC), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_void_p]
+    L.mdp_snap_compute_host_typed.argtypes = [C.POINTER(SnapParamsC), C.c_int, C.c_int, _dp, _ip, _dp, C.c_double,
+                                              C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    L.mdp_snap_compute_device_typed.argtypes = [C.POINTER(SnapParamsC), C.c_int] + [C.c_void_p] * 5 + \
+        [C.c_int] * 3 + [C.c_void_p] * 4
+    L.mdp_md_set_types.argtypes = [C.c_void_p, _ip]
     L.mdp_md_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(SnapParamsC), C.POINTER(MDConfigC)]
     L.mdp_md_destroy.argtypes = [C.c_void_p]
     L.mdp_md_destroy.restype = None
@@ -128,11 +135,17 @@ def check(rc: int, what: str = "mdp call"):
         raise MdpError(f"{what} failed: {msg.decode() if msg else 'unknown error'}")
 
 
-def snap_params_c(p) -> tuple[SnapParamsC, np.ndarray]:
+def snap_params_c(p) -> tuple[SnapParamsC, tuple]:
     """Pack a mdp_b200.configs.SnapParams into the C struct (keeps the
-    coefficient array alive through the returned tuple)."""
+    coefficient and element arrays alive through the returned tuple)."""
     coeff = np.ascontiguousarray(p.coeff, dtype=np.float64)
+    radelems = getattr(p, "radelems", None)
+    ne = len(radelems) if radelems else 0
+    rad = np.ascontiguousarray(radelems if ne else [p.radelem], dtype=np.float64)
+    wj = np.ascontiguousarray(p.wjelems if ne else [p.wjelem], dtype=np.float64)
+    dptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    ncoeffall = p.ncoeffall if hasattr(p, "ncoeffall") else coeff.size
     s = SnapParamsC(p.twojmax, p.rcutfac, p.rfac0, p.rmin0, p.radelem, p.wjelem, p.switchflag, p.bzeroflag,
-                    p.bnormflag, p.wselfallflag, p.quadraticflag, p.chemflag, coeff.size,
-                    coeff.ctypes.data_as(C.POINTER(C.c_double)))
-    return s, coeff
+                    p.bnormflag, p.wselfallflag, p.quadraticflag, p.chemflag, ncoeffall, dptr(coeff), ne,
+                    dptr(rad) if ne else None, dptr(wj) if ne else None)
+    return s, (coeff, rad, wj)

@@ -39,15 +39,27 @@ class SnapParams:
     wselfallflag: int = 0
     quadraticflag: int = 0
     chemflag: int = 0
-    coeff: np.ndarray = None  # ncoeffall values, coeff[0] = beta_0
+    coeff: np.ndarray = None  # nelements x ncoeffall values; coeff[e * ncoeffall] = beta_0 of element e
+    # several elements (types 1..nelements): per-element radius and weight;
+    # None for the single element of radelem / wjelem
+    radelems: tuple = None
+    wjelems: tuple = None
+
+    @property
+    def nelements(self) -> int:
+        return len(self.radelems) if self.radelems else 1
 
     @property
     def rcut(self) -> float:
-        return 2.0 * self.radelem * self.rcutfac
+        """The largest pair cutoff, 2 max(radelem) rcutfac (InitSnap's rcutmax)."""
+        r = max(self.radelems) if self.radelems else self.radelem
+        return 2.0 * r * self.rcutfac
 
     @property
     def ncoeff(self) -> int:
-        return idxb_count(self.twojmax)
+        """Linear coefficients per element: the bispectrum components, once
+        per element triple with chemflag."""
+        return idxb_count(self.twojmax) * (self.nelements ** 3 if self.chemflag else 1)
 
     @property
     def ncoeffall(self) -> int:
@@ -87,6 +99,25 @@ def snap_params(twojmax: int = 8, seed: int = 1234, qsigma: float = 1e-5, **kw) 
         q = np.random.default_rng(seed + 7919).normal(0.0, qsigma, n * (n + 1) // 2)
         c = np.concatenate([c, q])
     p.coeff = c
+    return p
+
+
+def snap_params_elements(twojmax: int, radelems, wjelems, chemflag: int = 1, seed: int = 1234,
+                         sigma: float = 0.01, **kw) -> SnapParams:
+    """Seeded parameters for len(radelems) element types: per element beta_0
+    = -11.7 eV plus a seeded offset and N(0, sigma / sqrt(number of element
+    triples)) linear coefficients, laid out element after element."""
+    p = SnapParams(twojmax=twojmax, chemflag=chemflag, radelems=tuple(float(r) for r in radelems),
+                   wjelems=tuple(float(w) for w in wjelems), **kw)
+    rng = np.random.default_rng(seed)
+    ntri = p.nelements ** 3 if chemflag else 1
+    blocks = []
+    for _ in range(p.nelements):
+        b = np.empty(p.ncoeffall)
+        b[0] = -11.7 + rng.normal(0.0, 0.5)
+        b[1:] = rng.normal(0.0, sigma / np.sqrt(ntri), p.ncoeff)
+        blocks.append(b)
+    p.coeff = np.concatenate(blocks)
     return p
 
 

@@ -111,6 +111,8 @@ struct mdp_md {
     long long fallback_step = -1;
     std::vector<double> judge_log;   // (step, force RMSE) pairs
     DevBuf fjudge;
+    DevBuf types;   // atom types 1..nelements (models with several element types)
+    bool has_types = false;
 };
 
 extern "C" {
@@ -164,7 +166,8 @@ void mdp_md_destroy(mdp_md *m)
     if (!m) return;
     cudaSetDevice(m->device);
     if (m->s) cudaStreamSynchronize(m->s);
-    DevBuf *b[] = {&m->x, &m->v, &m->f, &m->xstart, &m->xhold, &m->e, &m->vatom, &m->scal, &m->stage, &m->fjudge};
+    DevBuf *b[] = {&m->x, &m->v, &m->f, &m->xstart, &m->xhold, &m->e, &m->vatom, &m->scal, &m->stage, &m->fjudge,
+                   &m->types};
     for (auto x : b) x->release();
     m->nb.release();
     m->fp.release();
@@ -222,7 +225,7 @@ static int md_force_plain(mdp_md *m)
     return force_compute(m->fp, m->model, m->cfg.precision, m->x.as<double4>(), n, m->nb.nlist.as<int>(),
                          m->nb.nnum.as<int>(), m->cfg.neighmax, (long)n * m->cfg.neighmax, m->nb.roff.as<int>(),
                          m->nb.rlist.as<long long>(), m->e.as<double>(), m->f.as<double4>(), m->vatom.as<double>(),
-                         m->s);
+                         m->s, m->has_types ? m->types.as<int>() : nullptr, m->nb.alist.as<int>());
 }
 
 // Surrogate forces, judged against the plain model every judge_every steps:
@@ -272,10 +275,32 @@ static int md_thermo(mdp_md *m, double *row)
     return 0;
 }
 
+int mdp_md_set_types(mdp_md *m, const int *types)
+{
+    if (!m || !types) { set_error("null argument"); return -1; }
+    MDP_CUDA_TRY(cudaSetDevice(m->device));
+    const int n = m->cfg.natoms, ne = m->model.ne;
+    for (int i = 0; i < n; i++)
+        if (types[i] < 1 || types[i] > ne) {
+            set_error("atom %d has type %d; the model has types 1..%d", i, types[i], ne);
+            return -1;
+        }
+    if (m->types.ensure(sizeof(int) * n)) return -1;
+    MDP_CUDA_TRY(cudaMemcpyAsync(m->types.p, types, sizeof(int) * n, cudaMemcpyHostToDevice, m->s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(m->s));
+    m->has_types = true;
+    m->ready = false;
+    return 0;
+}
+
 int mdp_md_setup(mdp_md *m)
 {
     if (!m) { set_error("null handle"); return -1; }
     MDP_CUDA_TRY(cudaSetDevice(m->device));
+    if (m->model.ne > 1 && !m->has_types) {
+        set_error("a model with %d element types needs mdp_md_set_types first", m->model.ne);
+        return -1;
+    }
     if (md_rebuild(m) || md_force(m)) return -1;
     double row[5];
     if (md_thermo(m, row)) return -1;
@@ -526,13 +551,25 @@ struct OneShot {
     SnapModel model;
     Neighbors nb;
     ForcePath fp;
-    DevBuf x4, f4, xin, alist_tmp;
+    DevBuf x4, f4, xin, alist_tmp, types;
 };
 static std::mutex g_os_mu;
 
-int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, const double *x, const double *box,
-                          double skin, int neighmax, double *eatom, double *fatom, double *vatom, int *neighlist,
-                          int *neighnum, int *anum_out, int *alist_out, double *xall_out, int alist_cap)
+// types 1..ne on the host; 0 or -1 with the error set
+static int check_types(const int *t, long n, int ne)
+{
+    for (long i = 0; i < n; i++)
+        if (t[i] < 1 || t[i] > ne) {
+            set_error("atom %ld has type %d; the model has types 1..%d", i, t[i], ne);
+            return -1;
+        }
+    return 0;
+}
+
+static int compute_host(const mdp_snap_params *p, int precision, int natoms, const double *x, const int *atomtype,
+                        const double *box, double skin, int neighmax, double *eatom, double *fatom, double *vatom,
+                        int *neighlist, int *neighnum, int *anum_out, int *alist_out, double *xall_out,
+                        int alist_cap)
 {
     std::lock_guard<std::mutex> lk(g_os_mu);
     if (!x || !box || natoms <= 0) { set_error("bad arguments"); return -1; }
@@ -540,6 +577,13 @@ int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, c
     int dev = 0;
     MDP_CUDA_TRY(cudaGetDevice(&dev));
     if (model_init(os.model, p)) return -1;
+    const int *types_dev = nullptr;
+    if (os.model.ne > 1) {
+        if (!atomtype) { set_error("a model with %d element types needs the atom types", os.model.ne); return -1; }
+        if (check_types(atomtype, natoms, os.model.ne) || os.types.ensure(sizeof(int) * natoms)) return -1;
+        MDP_CUDA_TRY(cudaMemcpy(os.types.p, atomtype, sizeof(int) * natoms, cudaMemcpyHostToDevice));
+        types_dev = os.types.as<int>();
+    }
     BoxParams bp;
     const double rc = os.model.geom.rcut + skin;
     box_setup(bp, box, box + 3, box + 6, rc, rc);
@@ -556,7 +600,8 @@ int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, c
     double *ed = xin + 3 * natoms, *vd = xin + 4 * natoms;
     if (force_compute(os.fp, os.model, precision, os.x4.as<double4>(), natoms, os.nb.nlist.as<int>(),
                       os.nb.nnum.as<int>(), neighmax, (long)natoms * neighmax, os.nb.roff.as<int>(),
-                      os.nb.rlist.as<long long>(), ed, os.f4.as<double4>(), vd, s))
+                      os.nb.rlist.as<long long>(), ed, os.f4.as<double4>(), vd, s, types_dev,
+                      os.nb.alist.as<int>()))
         return -1;
     k_d4_to_aos<<<(natoms + 255) / 256, 256, 0, s>>>(os.f4.as<double4>(), xin, natoms);
     MDP_CUDA_TRY(cudaDeviceSynchronize());
@@ -582,15 +627,32 @@ int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, c
     return 0;
 }
 
+int mdp_snap_compute_host(const mdp_snap_params *p, int precision, int natoms, const double *x, const double *box,
+                          double skin, int neighmax, double *eatom, double *fatom, double *vatom, int *neighlist,
+                          int *neighnum, int *anum_out, int *alist_out, double *xall_out, int alist_cap)
+{
+    return compute_host(p, precision, natoms, x, nullptr, box, skin, neighmax, eatom, fatom, vatom, neighlist,
+                        neighnum, anum_out, alist_out, xall_out, alist_cap);
+}
+
+int mdp_snap_compute_host_typed(const mdp_snap_params *p, int precision, int natoms, const double *x,
+                                const int *atomtype, const double *box, double skin, int neighmax, double *eatom,
+                                double *fatom, double *vatom, int *neighlist, int *neighnum, int *anum_out,
+                                int *alist_out, double *xall_out, int alist_cap)
+{
+    return compute_host(p, precision, natoms, x, atomtype, box, skin, neighmax, eatom, fatom, vatom, neighlist,
+                        neighnum, anum_out, alist_out, xall_out, alist_cap);
+}
+
 __global__ void k_copy_int(const int *__restrict__ a, int *__restrict__ b, long n)
 {
     long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = a[i];
 }
 
-int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const double *x, const int *alist,
-                            const int *neighlist, const int *neighnum, int inum, int anum, int neighmax,
-                            double *eatom, double *fatom, double *vatom, void *stream)
+static int compute_device(const mdp_snap_params *p, int precision, const double *x, const int *atomtype,
+                          const int *alist, const int *neighlist, const int *neighnum, int inum, int anum,
+                          int neighmax, double *eatom, double *fatom, double *vatom, void *stream)
 {
     std::lock_guard<std::mutex> lk(g_os_mu);
     static OneShot os;
@@ -598,6 +660,13 @@ int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const doubl
     int dev = 0;
     MDP_CUDA_TRY(cudaGetDevice(&dev));
     if (model_init(os.model, p)) return -1;
+    if (os.model.ne > 1) {
+        if (!atomtype) { set_error("a model with %d element types needs the atom types", os.model.ne); return -1; }
+        std::vector<int> th(inum);
+        MDP_CUDA_TRY(cudaMemcpyAsync(th.data(), atomtype, sizeof(int) * inum, cudaMemcpyDeviceToHost, s));
+        MDP_CUDA_TRY(cudaStreamSynchronize(s));
+        if (check_types(th.data(), inum, os.model.ne)) return -1;
+    }
     if (os.x4.ensure(sizeof(double4) * (size_t)anum) || os.f4.ensure(sizeof(double4) * inum) ||
         os.nb.rcount.ensure(sizeof(int) * inum) || os.nb.roff.ensure(sizeof(int) * ((size_t)inum + 1)) ||
         os.nb.cursor.ensure(sizeof(int) * inum) || os.nb.rlist.ensure(sizeof(long long) * (size_t)inum * neighmax) ||
@@ -614,11 +683,27 @@ int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const doubl
     k_rev_sort<<<std::min((inum + 7) / 8, num_sms() * 8), 256, 0, s>>>(inum, os.nb.roff.as<int>(), os.nb.rlist.as<long long>());
     if (force_compute(os.fp, os.model, precision, os.x4.as<double4>(), inum, neighlist, neighnum, neighmax,
                       (long)inum * neighmax, os.nb.roff.as<int>(), os.nb.rlist.as<long long>(), eatom,
-                      os.f4.as<double4>(), vatom, s))
+                      os.f4.as<double4>(), vatom, s, atomtype, alist))
         return -1;
     k_d4_to_aos<<<(inum + 255) / 256, 256, 0, s>>>(os.f4.as<double4>(), fatom, inum);
     MDP_CUDA_TRY(cudaGetLastError());
     return 0;
+}
+
+int mdp_snap_compute_device(const mdp_snap_params *p, int precision, const double *x, const int *alist,
+                            const int *neighlist, const int *neighnum, int inum, int anum, int neighmax,
+                            double *eatom, double *fatom, double *vatom, void *stream)
+{
+    return compute_device(p, precision, x, nullptr, alist, neighlist, neighnum, inum, anum, neighmax, eatom, fatom,
+                          vatom, stream);
+}
+
+int mdp_snap_compute_device_typed(const mdp_snap_params *p, int precision, const double *x, const int *atomtype,
+                                  const int *alist, const int *neighlist, const int *neighnum, int inum, int anum,
+                                  int neighmax, double *eatom, double *fatom, double *vatom, void *stream)
+{
+    return compute_device(p, precision, x, atomtype, alist, neighlist, neighnum, inum, anum, neighmax, eatom, fatom,
+                          vatom, stream);
 }
 
 int mdp_probe_fma_peak(int device, double *fp64, double *fp32)

@@ -34,7 +34,22 @@ __global__ void k_pair_count(const double4 *, const int *, const int *, int, int
 __global__ void k_pair_emit(const double4 *, const int *, const int *, int, int, const int *, SnapGeom, double4 *,
                             int2 *, double4 *, int *);
 __global__ void k_tally(const double4 *, const double4 *, const int *, const int *, int, const int *,
-                        const long long *, double4 *, double *);
+                        const long long *, double4 *, double *, int nblk, int ipad);
+
+// Several element types: type-pair cutoffs (radelem_i + radelem_j) rcutfac,
+// their squares and the neighbour weights wjelem_j (InitSnap,
+// snappotential.cpp:186-198); nblk U / Y element blocks (nelements with
+// chemflag, else 1) of ipad virtual atoms each
+constexpr int MAXELEM = 4;
+struct ElemGeom {
+    int ne, nblk, chem, ipad;
+    double rcut[MAXELEM][MAXELEM], rcutsq[MAXELEM][MAXELEM], wj[MAXELEM];
+};
+__global__ void k_pair_count_me(const double4 *, const int *, const int *, int, int, const int *, const int *,
+                                const __grid_constant__ ElemGeom, int *);
+__global__ void k_pair_emit_me(const double4 *, const int *, const int *, int, int, const int *, const int *,
+                               const int *, SnapGeom, const __grid_constant__ ElemGeom, double4 *, int2 *,
+                               double4 *, double2 *, int *);
 __global__ void k_nve_initial(double4 *, double4 *, const double4 *, double4 *, int, double, double);
 __global__ void k_nve_final(double4 *, const double4 *, int, double);
 __global__ void k_maxdisp(const double4 *, const double4 *, int, unsigned long long *);
@@ -96,6 +111,11 @@ struct SnapModel {
     QuadParams quad;
     int nu, nyh, ncoeff;
     ZblParams zbl;
+    // several element types (nelements > 1): per-element coefficient table
+    // coeffelem [ne][ncoeffall], type-pair geometry, the Y kernel's multiplicity
+    // factors in yq
+    int ne = 1;
+    ElemGeom eg;
 };
 int model_init(SnapModel &m, const mdp_snap_params *p);
 
@@ -111,6 +131,10 @@ struct DevBuf {
 struct ForcePath {
     DevBuf pcount, poff, prij, pinfo, pab, smap, dE, Ut, Y, scan_tmp;
     DevBuf B, G;   // quadratic SNAP: per-atom bispectrum and coefficients [k][atom]
+    DevBuf pcw, elem, ecoef;   // several elements: per-pair cutoff / weight, atom elements, coeffelem
+    const int *u_welem = nullptr;     // U stage: element of each atom, for wself per element block
+    int u_ipad = 0;
+    const double2 *fr_pcw = nullptr;  // dE/dr stage: per-pair cutoff / weight
     int natoms_cap = 0, nm_cap = 0;
     // per-stage timing (CUDA events on the launching stream), enabled on demand
     bool timing = false;
@@ -129,9 +153,12 @@ template <typename T, int TJ> int launch_fi(const SnapModel &m, ForcePath &fp, i
 // One plain-SNAP force evaluation on device data: x (anum, double4, ghosts
 // appended), neighbour list (inum x nm), reverse list.  Writes eatom[inum],
 // f[inum] (double4) and, when vatom != nullptr, the SoA per-atom virial 6 x inum.
+// Several element types need atype (types 1..nelements of the inum owners)
+// and alist (owner of every atom, ghosts included).
 int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double4 *x, int inum,
                   const int *nlist, const int *nnum, int nm, long pair_cap, const int *roff,
-                  const long long *rlist, double *eatom, double4 *f, double *vatom, cudaStream_t s);
+                  const long long *rlist, double *eatom, double4 *f, double *vatom, cudaStream_t s,
+                  const int *atype = nullptr, const int *alist = nullptr);
 
 // Neighbour structure (ghosts + list + reverse list) owned by a caller
 struct Neighbors {

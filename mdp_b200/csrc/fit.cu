@@ -968,6 +968,7 @@ int mdp_fit_create(mdp_fit **hp, const mdp_snap_params *p, int device)
     mdp_fit *h = new mdp_fit();
     h->device = device;
     if (model_init(h->model, &q)) { delete h; return -1; }
+    if (h->model.ne > 1) { set_error("the batched fit takes one element type"); delete h; return -1; }
     fit_tables(h->tab, p->twojmax, p->bnormflag, p->bzeroflag);
     if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess || h->tabs.ensure(sizeof(FitTables))) {
         mdp_fit_destroy(h);

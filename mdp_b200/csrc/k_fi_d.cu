@@ -17,7 +17,7 @@ int launch_fi(const SnapModel &m, ForcePath &fp, int inum, int /*nm*/, cudaStrea
     const int blocks = num_sms() * per_sm;
     k_snap_fr<T, TJ><<<blocks, FR_THREADS, sm, s>>>(fp.prij.as<double4>(), fp.pinfo.as<int2>(),
                                                     fp.poff.as<int>() + inum, m.geom, fp.Y.as<T2>(),
-                                                    fp.dE.as<double4>());
+                                                    fp.dE.as<double4>(), fp.fr_pcw);
     return 0;
 }
 

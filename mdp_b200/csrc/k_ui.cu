@@ -17,7 +17,8 @@ int launch_ui(const SnapModel &m, ForcePath &fp, int inum, cudaStream_t s)
     const int blocks = std::min(ntiles, num_sms() * per_sm);
     if (fp.timing) cudaEventRecord(fp.ev[1], s);
     k_snap_uc<T, TJ><<<blocks, uc_warps<TJ>() * 32, sm, s>>>(fp.poff.as<int>(), fp.prij.as<double4>(),
-                                                             fp.pab.as<double4>(), inum, fp.Ut.as<T2>());
+                                                             fp.pab.as<double4>(), inum, fp.Ut.as<T2>(),
+                                                             fp.u_welem, fp.u_ipad);
     return 0;
 }
 

@@ -408,23 +408,125 @@ __global__ void k_pair_emit(const double4 *__restrict__ x, const int *__restrict
     }
 }
 
+// Several element types (types 1..nelements, elem = type - 1 per owner atom):
+// a slot is a pair when |r|^2 < ((radelem_i + radelem_j) rcutfac)^2 and
+// > 1e-20 (cpuNeighPairList, cpuSnap.cpp:1883-1905, with InitSnap's type-pair
+// cutoffs).  Pairs are grouped per (element block b, atom): with chemflag the
+// block of the neighbour's element, else one block; counts go to
+// pcount[b * ipad + atom] (callers zero the pad entries).  One warp per atom.
+__global__ void k_pair_count_me(const double4 *__restrict__ x, const int *__restrict__ nlist,
+                                const int *__restrict__ nnum, int inum, int nm, const int *__restrict__ alist,
+                                const int *__restrict__ elem, const __grid_constant__ ElemGeom eg,
+                                int *__restrict__ pcount)
+{
+    const int lane = threadIdx.x & 31;
+    const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= inum) return;   // whole warps leave together
+    const double4 xi = x[i];
+    const int ei = elem[i];
+    const int n = nnum[i];
+    int cnt[MAXELEM] = {0, 0, 0, 0};
+    for (int l0 = 0; l0 < n; l0 += 32) {
+        const int l = l0 + lane;
+        bool pair = false;
+        int b = 0;
+        if (l < n) {
+            const int j = nlist[(size_t)i * nm + l];
+            const int ej = elem[alist[j]];
+            double d0, d1, d2;
+            pair = slot_pair(xi, x[j], eg.rcutsq[ei][ej], d0, d1, d2);
+            b = eg.chem ? ej : 0;
+        }
+#pragma unroll
+        for (int e = 0; e < MAXELEM; e++) cnt[e] += __popc(__ballot_sync(0xffffffffu, pair && b == e));
+    }
+    if (lane < eg.nblk) {
+        int c = cnt[0];
+#pragma unroll
+        for (int e = 1; e < MAXELEM; e++)
+            if (lane == e) c = cnt[e];
+        pcount[(long)lane * eg.ipad + i] = c;
+    }
+}
+
+// compact pairs per (block, atom) in slot order: r and sfac wjelem[tj] in
+// prij, (a, b) in pab, (virtual atom b * ipad + i, pair) in pinfo, the pair's
+// cutoff and neighbour weight in pcw, slot -> pair in smap
+__global__ void k_pair_emit_me(const double4 *__restrict__ x, const int *__restrict__ nlist,
+                               const int *__restrict__ nnum, int inum, int nm, const int *__restrict__ alist,
+                               const int *__restrict__ elem, const int *__restrict__ poff, SnapGeom gp,
+                               const __grid_constant__ ElemGeom eg, double4 *__restrict__ prij,
+                               int2 *__restrict__ pinfo, double4 *__restrict__ pab, double2 *__restrict__ pcw,
+                               int *__restrict__ smap)
+{
+    const int lane = threadIdx.x & 31;
+    const long i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= inum) return;   // whole warps leave together
+    const double4 xi = x[i];
+    const int ei = elem[i];
+    const int n = nnum[i];
+    int base[MAXELEM];
+#pragma unroll
+    for (int e = 0; e < MAXELEM; e++) base[e] = (e < eg.nblk) ? poff[(long)e * eg.ipad + i] : 0;
+    for (int l0 = 0; l0 < n; l0 += 32) {
+        const int l = l0 + lane;
+        const size_t s = (size_t)i * nm + l;
+        bool pair = false;
+        int b = 0, ej = 0;
+        double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+        if (l < n) {
+            const int j = nlist[s];
+            ej = elem[alist[j]];
+            pair = slot_pair(xi, x[j], eg.rcutsq[ei][ej], d0, d1, d2);
+            b = eg.chem ? ej : 0;
+        }
+        int q = 0;
+#pragma unroll
+        for (int e = 0; e < MAXELEM; e++) {
+            const unsigned m = __ballot_sync(0xffffffffu, pair && b == e);
+            if (b == e) q = base[e] + __popc(m & ((1u << lane) - 1u));
+            base[e] += __popc(m);
+        }
+        if (l < n) {
+            if (pair) {
+                SnapGeom ge = gp;
+                ge.rcut = eg.rcut[ei][ej];
+                ge.wj = eg.wj[ej];
+                PairGeo g;
+                pair_geometry<false>(g, d0, d1, d2, ge);
+                prij[q] = make_double4(d0, d1, d2, g.sfac);
+                pab[q] = make_double4(g.ar, g.ai, g.br, g.bi);
+                pinfo[q] = make_int2((int)((long)b * eg.ipad + i), q);
+                pcw[q] = make_double2(ge.rcut, ge.wj);
+                smap[s] = q;
+            } else {
+                smap[s] = -1;
+            }
+        }
+    }
+}
+
 // f_o = sum_{own pairs} dE - sum_{pairs whose neighbour is an image of o} dE;
 // per-atom virial -1/2 r (x) dE on both atoms (cpuSnap4.cpp:1177-1209).  Own
-// pairs in slot order, then the reverse entries in ascending slot order: a
-// fixed summation order without atomics.
+// pairs in slot order (with several element blocks: block by block, the pairs
+// of atom o in block b at poff[b * ipad + o]), then the reverse entries in
+// ascending slot order: a fixed summation order without atomics.
 __global__ void k_tally(const double4 *__restrict__ prij, const double4 *__restrict__ dE,
                         const int *__restrict__ poff, const int *__restrict__ smap, int inum,
                         const int *__restrict__ roff, const long long *__restrict__ rlist, double4 *__restrict__ f,
-                        double *__restrict__ vatom)
+                        double *__restrict__ vatom, int nblk, int ipad)
 {
     int o = blockIdx.x * blockDim.x + threadIdx.x;
     if (o >= inum) return;
     double fx = 0, fy = 0, fz = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-    for (int p = poff[o]; p < poff[o + 1]; p++) {
-        const double4 r = prij[p], d = dE[p];
-        fx += d.x; fy += d.y; fz += d.z;
-        v0 += -0.5 * r.x * d.x; v1 += -0.5 * r.y * d.y; v2 += -0.5 * r.z * d.z;
-        v3 += -0.5 * r.x * d.y; v4 += -0.5 * r.x * d.z; v5 += -0.5 * r.y * d.z;
+    for (int b = 0; b < nblk; b++) {
+        const long v = (long)b * ipad + o;
+        for (int p = poff[v]; p < poff[v + 1]; p++) {
+            const double4 r = prij[p], d = dE[p];
+            fx += d.x; fy += d.y; fz += d.z;
+            v0 += -0.5 * r.x * d.x; v1 += -0.5 * r.y * d.y; v2 += -0.5 * r.z * d.z;
+            v3 += -0.5 * r.x * d.y; v4 += -0.5 * r.x * d.z; v5 += -0.5 * r.y * d.z;
+        }
     }
     const int s0 = roff[o], s1 = roff[o + 1];
     for (int t = s0; t < s1; t++) {

@@ -92,7 +92,7 @@ void DevBuf::release()
 
 void ForcePath::release()
 {
-    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &smap, &dE, &Ut, &Y, &scan_tmp, &B, &G};
+    DevBuf *b[] = {&pcount, &poff, &prij, &pinfo, &pab, &smap, &dE, &Ut, &Y, &scan_tmp, &B, &G, &pcw, &elem, &ecoef};
     for (auto x : b) x->release();
     for (auto &e : ev)
         if (e) { cudaEventDestroy(e); e = nullptr; }
@@ -121,11 +121,20 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
         set_error("twojmax=%d not supported (4, 6 or 8)", tj);
         return -1;
     }
-    if (p->chemflag != 0) {
-        set_error("chemflag SNAP is not supported (single element only)");
+    if (p->chemflag != 0 && p->chemflag != 1) { set_error("chemflag must be 0 or 1"); return -1; }
+    if (p->quadraticflag != 0 && p->quadraticflag != 1) { set_error("quadraticflag must be 0 or 1"); return -1; }
+    const int ne = p->nelements > 1 ? p->nelements : 1;
+    if (ne > MAXELEM) { set_error("nelements=%d: at most %d element types", p->nelements, MAXELEM); return -1; }
+    if (p->nelements > 1 && (!p->radelems || !p->wjelems)) {
+        set_error("nelements=%d needs radelems and wjelems", p->nelements);
         return -1;
     }
-    if (p->quadraticflag != 0 && p->quadraticflag != 1) { set_error("quadraticflag must be 0 or 1"); return -1; }
+    if (ne > 1 && p->quadraticflag) {
+        set_error("quadratic SNAP is supported for one element type only");
+        return -1;
+    }
+    // element triples of the coefficient table (cpuSnapComputeEi, cpuSnap4.cpp:255-280)
+    const int ntri = (ne > 1 && p->chemflag) ? ne * ne * ne : 1;
     if (p->switchflag != 0 && p->switchflag != 1) { set_error("switchflag must be 0 or 1"); return -1; }
     // idxb enumeration (cpuSnap.cpp:44-68)
     int jjb[JD][JD][JD];
@@ -134,25 +143,50 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
         for (int j2 = 0; j2 <= j1; j2++)
             for (int j = j1 - j2; j <= std::min(tj, j1 + j2); j += 2)
                 if (j >= j1) jjb[j1][j2][j] = nb++;
-    const int nall = nb + 1 + (p->quadraticflag ? nb * (nb + 1) / 2 : 0);
+    const int nall = nb * ntri + 1 + (p->quadraticflag ? nb * (nb + 1) / 2 : 0);
     if (p->ncoeffall != nall) {
-        set_error("ncoeffall=%d but 2J=%d%s needs %d coefficients", p->ncoeffall, tj,
-                  p->quadraticflag ? " with quadratic terms" : "", nall);
+        set_error("ncoeffall=%d but 2J=%d%s%s needs %d coefficients", p->ncoeffall, tj,
+                  p->quadraticflag ? " with quadratic terms" : "", ntri > 1 ? " per element (chemflag)" : "", nall);
         return -1;
     }
     if (!p->coeff) { set_error("null coefficient array"); return -1; }
     m.p = *p;
-    m.coeff.assign(p->coeff, p->coeff + p->ncoeffall);
+    m.coeff.assign(p->coeff, p->coeff + (size_t)ne * p->ncoeffall);
     m.p.coeff = m.coeff.data();
+    m.p.radelems = m.p.wjelems = nullptr;
+    m.ne = ne;
     m.ncoeff = nb;
     m.nu = idxu_count(tj);
     m.nyh = yh_count(tj);
-    const double rcut = 2.0 * p->radelem * p->rcutfac;
+    const bool one_listed = p->nelements == 1 && p->radelems && p->wjelems;
+    const double rad1 = one_listed ? p->radelems[0] : p->radelem;
+    const double wj1 = one_listed ? p->wjelems[0] : p->wjelem;
+    m.p.radelem = rad1;
+    m.p.wjelem = wj1;
+    double rcut = 2.0 * rad1 * p->rcutfac;
+    memset(&m.eg, 0, sizeof(m.eg));
+    m.eg.ne = ne;
+    m.eg.chem = (ne > 1 && p->chemflag) ? 1 : 0;
+    m.eg.nblk = m.eg.chem ? ne : 1;
+    if (ne > 1) {
+        // InitSnap: rcutmax = max 2 radelem rcutfac; cut = (radelem_i + radelem_j) rcutfac
+        rcut = 0.0;
+        for (int a = 0; a < ne; a++) {
+            if (!(p->radelems[a] > 0.0)) { set_error("radelems[%d] must be positive", a); return -1; }
+            rcut = std::max(2.0 * p->radelems[a] * p->rcutfac, rcut);
+            m.eg.wj[a] = p->wjelems[a];
+            for (int b = 0; b < ne; b++) {
+                const double cut = (p->radelems[a] + p->radelems[b]) * p->rcutfac;
+                m.eg.rcut[a][b] = cut;
+                m.eg.rcutsq[a][b] = cut * cut;
+            }
+        }
+    }
     m.geom.rcut = rcut;
     m.geom.rcutsq = rcut * rcut;
     m.geom.rfac0 = p->rfac0;
     m.geom.rmin0 = p->rmin0;
-    m.geom.wj = p->wjelem;
+    m.geom.wj = wj1;
     m.geom.switchflag = p->switchflag;
 
     // beta' per coupling triple (cpuSnap4.cpp:763-787)
@@ -187,9 +221,14 @@ int model_init(SnapModel &m, const mdp_snap_params *p)
                 }
     };
     fill_beta(c, m.yd, &m.yf);
-    // quadratic SNAP: the Y kernel takes per-atom coefficients G_i = beta + Q B_i,
-    // so its per-triple factors are those of unit coefficients
+    // quadratic SNAP and several elements: the Y kernel takes per-atom
+    // coefficients (G_i = beta + Q B_i; the atom element's table), so its
+    // per-triple factors are those of unit coefficients
     memset(&m.quad, 0, sizeof(m.quad));
+    if (ne > 1) {
+        std::vector<double> ones(nb + 1, 1.0);
+        fill_beta(ones.data(), m.yq, nullptr);
+    }
     if (p->quadraticflag) {
         if (nb > QUAD_MAXK) { set_error("quadratic SNAP supports up to %d components", QUAD_MAXK); return -1; }
         std::vector<double> ones(nb + 1, 1.0);
@@ -343,11 +382,128 @@ static int launch_snap_tj(const SnapModel &m, const YParams<T> &yp, ForcePath &f
     return -1;
 }
 
+// ---------------------------------------------------------------------------
+// several element types (FP64): pairs grouped per (element block, atom), U
+// over virtual atoms b * ipad + atom, energy from the element-triple
+// bispectrum, Y per element block, dE/dr with per-pair cutoffs and weights
+// ---------------------------------------------------------------------------
+__global__ void k_elem_of_type(const int *__restrict__ atype, int inum, int ipad, int ne, int *__restrict__ elem)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ipad) return;
+    int e = i < inum ? atype[i] - 1 : 0;   // map[t] = t - 1 (InitSnap); types checked by the callers
+    elem[i] = e < 0 ? 0 : (e >= ne ? ne - 1 : e);
+}
+
+template <int TJ>
+static int launch_snap_me(const SnapModel &m, ForcePath &fp, int inum, int nm, double *eatom, const MeArgs &A,
+                          cudaStream_t s)
+{
+    const long nv = (long)A.nblk * A.ntiles * 32;
+    fp.u_welem = (m.eg.chem && !m.p.wselfallflag) ? A.elem : nullptr;
+    fp.u_ipad = A.ntiles * 32;
+    const int rc_u = launch_ui<double, TJ>(m, fp, (int)nv, s);
+    fp.u_welem = nullptr;
+    fp.u_ipad = 0;
+    if (rc_u) return -1;
+    if (fp.timing) cudaEventRecord(fp.ev[2], s);
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_snap_ei_me<TJ>, BI_WARPS * 32, 0, &per_sm, "k_snap_ei_me")) return -1;
+    k_snap_ei_me<TJ><<<std::min(A.ntiles, num_sms() * per_sm), BI_WARPS * 32, 0, s>>>(
+        fp.Ut.as<double2>(), inum, m.p.bnormflag, A, eatom);
+    const size_t sm = yi_me_smem_bytes<TJ>();
+    if (kernel_setup((const void *)k_snap_yi_me<TJ>, YiWarps<double, TJ>::n * 32, sm, &per_sm, "k_snap_yi_me"))
+        return -1;
+    k_snap_yi_me<TJ><<<std::min(A.ntiles, num_sms() * per_sm), YiWarps<double, TJ>::n * 32, sm, s>>>(
+        fp.Ut.as<double2>(), inum, m.yq, A, fp.Y.as<double2>());
+    count_launches(2);
+    fp.fr_pcw = fp.pcw.as<double2>();
+    const int rc_f = launch_fi<double, TJ>(m, fp, (int)nv, nm, s);
+    fp.fr_pcw = nullptr;
+    return rc_f;
+}
+
+static int force_compute_me(ForcePath &fp, const SnapModel &m, int precision, const double4 *x, int inum,
+                            const int *nlist, const int *nnum, int nm, long pair_cap, const int *roff,
+                            const long long *rlist, double *eatom, double4 *f, double *vatom, cudaStream_t s,
+                            const int *atype, const int *alist)
+{
+    if (precision != MDP_PREC_FP64) { set_error("several element types run in FP64 only"); return -1; }
+    if (!atype || !alist) { set_error("several element types need the atom types and the owner list"); return -1; }
+    const int ntiles = (inum + 31) / 32, ipad = ntiles * 32;
+    const int nblk = m.eg.nblk;
+    const long nv = (long)nblk * ipad;
+    if (nv >= (1L << 30)) { set_error("%d atoms x %d element blocks is too many", inum, nblk); return -1; }
+    if (pair_cap < 1) pair_cap = 1;
+    const size_t ncoef = (size_t)m.ne * m.p.ncoeffall;
+    if (fp.pcount.ensure(sizeof(int) * (size_t)nv) || fp.poff.ensure(sizeof(int) * ((size_t)nv + 1)) ||
+        fp.prij.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pinfo.ensure(sizeof(int2) * (size_t)pair_cap) ||
+        fp.pab.ensure(sizeof(double4) * (size_t)pair_cap) || fp.pcw.ensure(sizeof(double2) * (size_t)pair_cap) ||
+        fp.smap.ensure(sizeof(int) * (size_t)inum * nm) || fp.dE.ensure(sizeof(double4) * (size_t)pair_cap) ||
+        fp.Ut.ensure(sizeof(double2) * (size_t)nblk * ntiles * m.nu * 32) ||
+        fp.Y.ensure(sizeof(double2) * (size_t)nblk * ntiles * 32 * m.nyh) ||
+        fp.scan_tmp.ensure(sizeof(int) * scan_tmp_ints(nv)) || fp.elem.ensure(sizeof(int) * (size_t)ipad) ||
+        fp.ecoef.ensure(sizeof(double) * ncoef))
+        return -1;
+    if (fp.timing && !fp.ev[0])
+        for (auto &e : fp.ev) cudaEventCreate(&e);
+    const int tb = 256;
+    if (fp.timing) cudaEventRecord(fp.ev[0], s);
+    MDP_CUDA_TRY(cudaMemcpyAsync(fp.ecoef.p, m.coeff.data(), sizeof(double) * ncoef, cudaMemcpyHostToDevice, s));
+    k_elem_of_type<<<(ipad + tb - 1) / tb, tb, 0, s>>>(atype, inum, ipad, m.ne, fp.elem.as<int>());
+    ElemGeom eg = m.eg;
+    eg.ipad = ipad;
+    MDP_CUDA_TRY(cudaMemsetAsync(fp.pcount.p, 0, sizeof(int) * (size_t)nv, s));
+    const unsigned gw = (unsigned)(((long)inum * 32 + tb - 1) / tb);   // one warp per atom
+    k_pair_count_me<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, alist, fp.elem.as<int>(), eg, fp.pcount.as<int>());
+    if (exclusive_scan(fp.pcount.as<int>(), fp.poff.as<int>(), nv, fp.scan_tmp.as<int>(), s)) return -1;
+    k_pair_emit_me<<<gw, tb, 0, s>>>(x, nlist, nnum, inum, nm, alist, fp.elem.as<int>(), fp.poff.as<int>(), m.geom,
+                                     eg, fp.prij.as<double4>(), fp.pinfo.as<int2>(), fp.pab.as<double4>(),
+                                     fp.pcw.as<double2>(), fp.smap.as<int>());
+    MeArgs A;
+    A.nblk = nblk;
+    A.ntiles = ntiles;
+    A.ncoeffall = m.p.ncoeffall;
+    A.bzero = m.p.bzeroflag;
+    A.wselfall = m.p.wselfallflag;
+    A.elem = fp.elem.as<int>();
+    A.coeff = fp.ecoef.as<double>();
+    const int rc = m.p.twojmax == 8   ? launch_snap_me<8>(m, fp, inum, nm, eatom, A, s)
+                   : m.p.twojmax == 6 ? launch_snap_me<6>(m, fp, inum, nm, eatom, A, s)
+                                      : launch_snap_me<4>(m, fp, inum, nm, eatom, A, s);
+    if (rc) return rc;
+    if (fp.timing) cudaEventRecord(fp.ev[4], s);
+    const int gb = (inum + tb - 1) / tb;
+    k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,
+                              roff, rlist, f, vatom, nblk, ipad);
+    count_launches(6);   // elem, pair_count, pair_emit, ui, fi, tally (+ the scan counts itself)
+    if (m.zbl.on) {
+        k_zbl<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.zbl, eatom, f, vatom);
+        count_launches(1);
+    }
+    if (fp.timing) {
+        cudaEventRecord(fp.ev[5], s);
+        cudaEventSynchronize(fp.ev[5]);
+        float t[5];
+        for (int k = 0; k < 5; k++) cudaEventElapsedTime(&t[k], fp.ev[k], fp.ev[k + 1]);
+        for (int k = 0; k < 5; k++) fp.stage_ms[k] += t[k];
+        float tot;
+        cudaEventElapsedTime(&tot, fp.ev[0], fp.ev[5]);
+        fp.stage_ms[5] += tot;
+        fp.stage_calls++;
+    }
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
 int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double4 *x, int inum, const int *nlist,
                   const int *nnum, int nm, long pair_cap, const int *roff, const long long *rlist, double *eatom,
-                  double4 *f, double *vatom, cudaStream_t s)
+                  double4 *f, double *vatom, cudaStream_t s, const int *atype, const int *alist)
 {
     if (inum <= 0) { set_error("no atoms"); return -1; }
+    if (m.ne > 1)
+        return force_compute_me(fp, m, precision, x, inum, nlist, nnum, nm, pair_cap, roff, rlist, eatom, f, vatom,
+                                s, atype, alist);
     const size_t tsz = (precision == MDP_PREC_FP32) ? sizeof(float2) : sizeof(double2);
     const long ntiles = (inum + 31) / 32;
     if (pair_cap < 1) pair_cap = 1;
@@ -381,7 +537,7 @@ int force_compute(ForcePath &fp, const SnapModel &m, int precision, const double
     if (rc) return rc;
     if (fp.timing) cudaEventRecord(fp.ev[4], s);
     k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,
-                              roff, rlist, f, vatom);
+                              roff, rlist, f, vatom, 1, 0);
     count_launches(6);   // pair_count, pair_emit, ui, yi, fi, tally (+ the scan counts itself)
     if (m.zbl.on) {
         k_zbl<<<gb, tb, 0, s>>>(x, nlist, nnum, inum, nm, m.zbl, eatom, f, vatom);

@@ -462,7 +462,8 @@ __device__ __forceinline__ void uc_dispatch(const int w, UcPairs<T, TJ> &s, type
 template <typename T, int TJ>
 __global__ void __launch_bounds__(uc_warps<TJ>() * 32)
 k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const double4 *__restrict__ pab,
-          int natoms, typename cplx<T>::type *__restrict__ Ut)
+          int natoms, typename cplx<T>::type *__restrict__ Ut, const int *__restrict__ welem = nullptr,
+          int ipad = 0)
 {
     typedef typename cplx<T>::type T2;
     constexpr int NW = uc_warps<TJ>();
@@ -490,22 +491,30 @@ k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const 
             uc_dispatch<T, TJ, 0>(w, s, acc + lane);
         }
         __syncthreads();
-        // full plane out: wself on the diagonal, rows mb > j/2 mirrored
+        // full plane out: wself on the diagonal, rows mb > j/2 mirrored.  With
+        // welem (element blocks of virtual atoms v = b * ipad + atom), wself
+        // goes to the atom's own element block only (cpuAddWself2Ui,
+        // cpuSnap4.cpp:193-244, chemflag without wselfallflag).
         T2 *dst = Ut + (size_t)tile * NU * 32;
         for (int e = threadIdx.x; e < NU * 32; e += NW * 32) {
             const int k = e >> 5, l = e & 31;
+            T ws = T(1);
+            if (welem) {
+                const int v = tile * 32 + l;
+                ws = (welem[v % ipad] == v / ipad) ? T(1) : T(0);
+            }
             int j = 0;
             while (idxu_block(j + 1) <= k) j++;
             const int rem = k - idxu_block(j), mb = rem / (j + 1), ma = rem - mb * (j + 1);
             T2 v;
             if (2 * mb <= j) {
                 v = acc[(yh_block(j) + rem) * 32 + l];
-                if (ma == mb) v.x += T(1);
+                if (ma == mb) v.x += ws;
             } else {
                 const int sb = j - mb, sa = j - ma;
                 const T2 u = acc[(yh_block(j) + (j + 1) * sb + sa) * 32 + l];
                 const T sg = ((sa + sb) & 1) ? T(-1) : T(1);
-                v = T2{sg * (u.x + (sa == sb ? T(1) : T(0))), -sg * u.y};
+                v = T2{sg * (u.x + (sa == sb ? ws : T(0))), -sg * u.y};
             }
             dst[e] = v;
         }
@@ -558,7 +567,8 @@ template <> struct YRow<float> {
 // {im, im}; u1 streams from shared memory one entry at a time.
 template <int J1, int J2, int J>
 __device__ __forceinline__ void z_rows_f32(const int mb, const int o, const int st, const float2 *__restrict__ Us,
-                                           const int lane, const float beta, YRow<float> &acc)
+                                           const float2 *__restrict__ Us2, const int lane, const float beta,
+                                           YRow<float> &acc)
 {
     constexpr int N1 = J1 + 1, N2 = J2 + 1;
     constexpr int CGB = cg_block(J1, J2, J);
@@ -570,7 +580,7 @@ __device__ __forceinline__ void z_rows_f32(const int mb, const int o, const int 
         const int mb1 = mb1min + ib, mb2 = mb2max - ib;
         const float s = beta * cgc<float>(CGB + mb1 * N2 + mb2);
         const float2 *r1 = Us + (idxu_block(J1) + N1 * mb1) * 32 + lane;
-        const float2 *r2 = Us + (idxu_block(J2) + N2 * mb2) * 32 + lane;
+        const float2 *r2 = Us2 + (idxu_block(J2) + N2 * mb2) * 32 + lane;
         float2 br[N2], bi[N2];
 #pragma unroll
         for (int a = 0; a < N2; a++) {
@@ -597,14 +607,17 @@ __device__ __forceinline__ void z_rows_f32(const int mb, const int o, const int 
 }
 
 // Row mb of beta' Z_{J1 J2 J}, restricted to the row pairs ib = o, o+st, ...,
-// accumulated into the warp's row (registers).
+// accumulated into the warp's row (registers).  The J1 factor is read from
+// Us, the J2 factor from Us2 (the same tile for one element; the U blocks of
+// two neighbour elements for the element-pair Z of chemflag SNAP).
 template <typename T, int J1, int J2, int J>
 __device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
-                                       const typename cplx<T>::type *__restrict__ Us, const int lane, const T beta,
+                                       const typename cplx<T>::type *__restrict__ Us,
+                                       const typename cplx<T>::type *__restrict__ Us2, const int lane, const T beta,
                                        YRow<T> &acc)
 {
     if constexpr (std::is_same<T, float>::value) {
-        z_rows_f32<J1, J2, J>(mb, o, st, Us, lane, beta, acc);
+        z_rows_f32<J1, J2, J>(mb, o, st, Us, Us2, lane, beta, acc);
         return;
     } else {
     T(&yr)[JD] = acc.r;
@@ -619,7 +632,7 @@ __device__ __forceinline__ void z_rows(const int mb, const int o, const int st,
         const int mb1 = mb1min + ib, mb2 = mb2max - ib;
         const T s = beta * cgc<T>(CGB + mb1 * N2 + mb2);
         const T2 *r1 = Us + (idxu_block(J1) + N1 * mb1) * 32 + lane;
-        const T2 *r2 = Us + (idxu_block(J2) + N2 * mb2) * 32 + lane;
+        const T2 *r2 = Us2 + (idxu_block(J2) + N2 * mb2) * 32 + lane;
         T u1r[N1], u1i[N1], u2r[N2], u2i[N2];
 #pragma unroll
         for (int a = 0; a < N1; a++) { const T2 v = r1[a * 32]; u1r[a] = s * v.x; u1i[a] = s * v.y; }
@@ -656,7 +669,7 @@ __device__ __forceinline__ void z_layer(const int mb, const int o, const int st,
                 constexpr int TRI = tri_index(J1, J2, J);
                 T beta = P.betaY[TRI];
                 if constexpr (PA) beta *= Gs[P.kmap[TRI] * 32 + lane];
-                z_rows<T, J1, J2, J>(mb, o, st, Us, lane, beta, acc);
+                z_rows<T, J1, J2, J>(mb, o, st, Us, Us, lane, beta, acc);
             }
             z_layer<T, TJ, PA, J, J1, J2 + 1>(mb, o, st, Us, lane, P, Gs, acc);
         } else {
@@ -790,23 +803,36 @@ k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __gri
 // ---------------------------------------------------------------------------
 constexpr int BI_WARPS = 8;
 
+// Arguments of one atom lane's bispectrum sweep.  The Z factors are read
+// from U1 (layer J1) and U2 (layer J2) and contracted with U3 (layer J): one
+// tile three times for one element, the U blocks of the element triple
+// (e1, e2, e3) for chemflag SNAP (cpuSnap4.cpp:255-284: Z^{e1 e2} with
+// U^{e3}).  Without coef, B_k goes to bout[k * bstride + atom]; with coef,
+// sum_k coef[k] B_k accumulates into e.
+template <typename T> struct BiArgs {
+    const typename cplx<T>::type *U1, *U2, *U3;
+    int lane, w, atom, natoms, bnorm, bzero;
+    double *bout;
+    long bstride;
+    const double *coef;
+    double e;
+};
+
 template <typename T, int TJ, int J1, int J2, int J, int C>
-__device__ __forceinline__ void b_triples(const typename cplx<T>::type *__restrict__ Us, const int lane, const int w,
-                                          const int atom, const int natoms, const int bnorm, const int bzero,
-                                          double *__restrict__ bout, const long bstride)
+__device__ __forceinline__ void b_triples(BiArgs<T> &a)
 {
     typedef typename cplx<T>::type T2;
     if constexpr (J1 <= TJ) {
         if constexpr (J2 <= J1) {
             if constexpr (J <= cmin(TJ, J1 + J2)) {
                 if constexpr (J >= J1) {
-                    if (C % BI_WARPS == w) {
+                    if (C % BI_WARPS == a.w) {
                         double sum = 0.0;
                         for (int mb = 0; 2 * mb <= J; mb++) {
                             YRow<T> z;
                             z.zero();
-                            z_rows<T, J1, J2, J>(mb, 0, 1, Us, lane, T(1), z);
-                            const T2 *urow = Us + (idxu_block(J) + (J + 1) * mb) * 32 + lane;
+                            z_rows<T, J1, J2, J>(mb, 0, 1, a.U1, a.U2, a.lane, T(1), z);
+                            const T2 *urow = a.U3 + (idxu_block(J) + (J + 1) * mb) * 32 + a.lane;
 #pragma unroll
                             for (int ma = 0; ma <= J; ma++) {
                                 const double wgt = (2 * mb < J) ? 1.0 : (ma < mb ? 1.0 : (ma == mb ? 0.5 : 0.0));
@@ -815,19 +841,20 @@ __device__ __forceinline__ void b_triples(const typename cplx<T>::type *__restri
                             }
                         }
                         double b = 2.0 * sum;
-                        if (bnorm) b /= (J + 1);
-                        if (bzero) b -= bnorm ? 1.0 : (double)(J + 1);
-                        if (atom < natoms) bout[(long)C * bstride + atom] = b;
+                        if (a.bnorm) b /= (J + 1);
+                        if (a.bzero) b -= a.bnorm ? 1.0 : (double)(J + 1);
+                        if (a.coef) a.e += a.coef[C] * b;
+                        else if (a.atom < a.natoms) a.bout[(long)C * a.bstride + a.atom] = b;
                     }
-                    b_triples<T, TJ, J1, J2, J + 2, C + 1>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+                    b_triples<T, TJ, J1, J2, J + 2, C + 1>(a);
                 } else {
-                    b_triples<T, TJ, J1, J2, J + 2, C>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+                    b_triples<T, TJ, J1, J2, J + 2, C>(a);
                 }
             } else {
-                b_triples<T, TJ, J1, J2 + 1, J1 - J2 - 1, C>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+                b_triples<T, TJ, J1, J2 + 1, J1 - J2 - 1, C>(a);
             }
         } else {
-            b_triples<T, TJ, J1 + 1, 0, J1 + 1, C>(Us, lane, w, atom, natoms, bnorm, bzero, bout, bstride);
+            b_triples<T, TJ, J1 + 1, 0, J1 + 1, C>(a);
         }
     }
 }
@@ -847,8 +874,162 @@ k_snap_bi(const typename cplx<T>::type *__restrict__ Ut, int natoms, int bnorm, 
         const T2 *src = Ut + (size_t)tile * NU * 32;
         for (int k = threadIdx.x; k < NU * 32; k += BI_WARPS * 32) Us[k] = src[k];
         __syncthreads();
-        b_triples<T, TJ, 0, 0, 0, 0>(Us, lane, w, tile * 32 + lane, natoms, bnorm, bzero, bout, bstride);
+        BiArgs<T> a{Us, Us, Us, lane, w, tile * 32 + lane, natoms, bnorm, bzero, bout, bstride, nullptr, 0.0};
+        b_triples<T, TJ, 0, 0, 0, 0>(a);
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Several element types (cpuSnap4.cpp:250-420 and 697-790 with nelements > 1).
+// U is kept per neighbour element block b (chemflag; one block otherwise) as
+// tiles of "virtual atoms" v = b * ipad + atom (ipad = 32 * ntiles), so the
+// U and dE/dr kernels run unchanged over them.  Coefficients come from the
+// reference's table coeffelem [element][ncoeffall]: beta_0 first, then the
+// bispectrum components of element triple t at 1 + t * NK + k.
+// ---------------------------------------------------------------------------
+struct MeArgs {
+    int nblk;              // U / Y element blocks (nelements with chemflag, else 1)
+    int ntiles;            // tiles of 32 atoms per block
+    int ncoeffall;         // coefficients per element
+    int bzero, wselfall;   // bzeroflag, wselfallflag
+    const int *elem;       // element index (type - 1) of each atom [inum]
+    const double *coeff;   // coeffelem [nelements][ncoeffall]
+};
+
+// Per-atom energy: beta_0(e_i) + sum over element triples t = (e1 e2 e3) and
+// components k of beta(e_i, t, k) (B^t_k - bzero_j), with B^t = 2 sum_half
+// Re(U^{e3*} Z^{e1 e2}) and bzero subtracted on t = (e e e) only unless
+// wselfallflag (cpuSnapComputeEi, cpuSnap4.cpp:250-420).  Warps take the
+// components round-robin per triple; the lanes' sums meet in shared memory.
+template <int TJ>
+__global__ void __launch_bounds__(BI_WARPS * 32, 1)
+k_snap_ei_me(const double2 *__restrict__ Ut, int natoms, int bnorm, const __grid_constant__ MeArgs A,
+             double *__restrict__ eatom)
+{
+    constexpr int NU = idxu_count(TJ), NK = nbispec(TJ);
+    __shared__ double ered[BI_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nb = A.nblk;
+    for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x) {
+        const int atom = tile * 32 + lane;
+        const int ie = atom < natoms ? A.elem[atom] : 0;
+        const double *cl = A.coeff + (size_t)ie * A.ncoeffall;
+        BiArgs<double> a{nullptr, nullptr, nullptr, lane, w, atom, natoms, bnorm, 0, nullptr, 0, nullptr, 0.0};
+        for (int e1 = 0; e1 < nb; e1++)
+            for (int e2 = 0; e2 < nb; e2++)
+                for (int e3 = 0; e3 < nb; e3++) {
+                    const int t = (e1 * nb + e2) * nb + e3;
+                    a.U1 = Ut + ((size_t)e1 * A.ntiles + tile) * NU * 32;
+                    a.U2 = Ut + ((size_t)e2 * A.ntiles + tile) * NU * 32;
+                    a.U3 = Ut + ((size_t)e3 * A.ntiles + tile) * NU * 32;
+                    a.bzero = A.bzero && (A.wselfall || (e1 == e2 && e2 == e3));
+                    a.coef = cl + 1 + (size_t)t * NK;
+                    b_triples<double, TJ, 0, 0, 0, 0>(a);
+                }
+        ered[w][lane] = a.e;
+        __syncthreads();
+        if (w == 0 && atom < natoms) {
+            double s = cl[0];
+#pragma unroll
+            for (int k = 0; k < BI_WARPS; k++) s += ered[k][lane];
+            eatom[atom] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// Y of every element block e3: sum over element pairs (e1, e2) and couplings
+// of beta' Z^{e1 e2}, with beta' the coefficient of the element triple and
+// bispectrum component each coupling case names (cpuSnapComputeYi,
+// cpuSnap4.cpp:697-790): (e1 e2 e3) when j >= j1, (e3 e2 e1) when
+// j1 > j >= j2, (e2 e3 e1) otherwise; P.betaY holds the multiplicity factors.
+// U is read from global memory (the tile's blocks stay in L1 / L2), Y is
+// written per block in the single-element tile layout.
+template <int TJ, int J, int J1, int J2>
+__device__ __forceinline__ void z_layer_me(const int mb, const int o, const int st, const double2 *__restrict__ U1,
+                                           const double2 *__restrict__ U2, const int lane,
+                                           const YParams<double> &P, const double *__restrict__ cl, const int tA,
+                                           const int tB, const int tC, YRow<double> &acc)
+{
+    constexpr int NK = nbispec(TJ);
+    if constexpr (J1 <= TJ) {
+        if constexpr (J2 <= J1) {
+            if constexpr (coupling_ok(J1, J2, J)) {
+                constexpr int TRI = tri_index(J1, J2, J);
+                const int t = (J >= J1) ? tA : (J >= J2) ? tB : tC;
+                const double beta = P.betaY[TRI] * cl[t * NK + P.kmap[TRI]];
+                z_rows<double, J1, J2, J>(mb, o, st, U1, U2, lane, beta, acc);
+            }
+            z_layer_me<TJ, J, J1, J2 + 1>(mb, o, st, U1, U2, lane, P, cl, tA, tB, tC, acc);
+        } else {
+            z_layer_me<TJ, J, J1 + 1, 0>(mb, o, st, U1, U2, lane, P, cl, tA, tB, tC, acc);
+        }
+    }
+}
+
+template <int TJ, int NW, int J>
+__device__ __forceinline__ void y_all_me(const double2 *__restrict__ Ut, const int tile, double2 *__restrict__ red,
+                                         double2 *__restrict__ Y, const int lane, const int w,
+                                         const YParams<double> &P, const MeArgs &A, const double *__restrict__ cl)
+{
+    if constexpr (J >= 0) {
+        constexpr int NU = idxu_count(TJ), NYH = yh_count(TJ);
+        const int nb = A.nblk;
+        const int mb = P.lay_mb[J][w];
+        for (int e3 = 0; e3 < nb; e3++) {
+            if (mb != 255) {
+                YRow<double> acc;
+                acc.zero();
+                for (int e1 = 0; e1 < nb; e1++)
+                    for (int e2 = 0; e2 < nb; e2++)
+                        z_layer_me<TJ, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w],
+                                                Ut + ((size_t)e1 * A.ntiles + tile) * NU * 32,
+                                                Ut + ((size_t)e2 * A.ntiles + tile) * NU * 32, lane, P, cl,
+                                                (e1 * nb + e2) * nb + e3, (e3 * nb + e2) * nb + e1,
+                                                (e2 * nb + e3) * nb + e1, acc);
+#pragma unroll
+                for (int ma = 0; ma <= J; ma++) red[(w * JD + ma) * 32 + lane] = acc.get(ma);
+            }
+            __syncthreads();
+            constexpr int NE = (J / 2 + 1) * (J + 1);
+            double2 *dst = Y + ((size_t)e3 * A.ntiles + tile) * NYH * 32;
+            for (int k = w; k < NE; k += NW) {
+                const int rmb = k / (J + 1), ma = k - rmb * (J + 1);
+                double yr = 0.0, yi = 0.0;
+#pragma unroll
+                for (int v = 0; v < NW; v++)
+                    if (P.lay_mb[J][v] == rmb) {
+                        const double2 t = red[(v * JD + ma) * 32 + lane];
+                        yr += t.x; yi += t.y;
+                    }
+                dst[(yh_block(J) + k) * 32 + lane] = double2{yr, yi};
+            }
+            __syncthreads();
+        }
+        y_all_me<TJ, NW, J - 1>(Ut, tile, red, Y, lane, w, P, A, cl);
+    }
+}
+
+template <int TJ>
+constexpr size_t yi_me_smem_bytes()
+{
+    return (size_t)YiWarps<double, TJ>::n * JD * 32 * sizeof(double2);
+}
+
+template <int TJ>
+__global__ void __launch_bounds__(YiWarps<double, TJ>::n * 32, 1)
+k_snap_yi_me(const double2 *__restrict__ Ut, int natoms, const __grid_constant__ YParams<double> P,
+             const __grid_constant__ MeArgs A, double2 *__restrict__ Y)
+{
+    constexpr int NW = YiWarps<double, TJ>::n;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double2 *red = reinterpret_cast<double2 *>(smraw);   // [warp][ma][lane]
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x) {
+        const int atom = tile * 32 + lane;
+        const int ie = atom < natoms ? A.elem[atom] : 0;
+        y_all_me<TJ, NW, TJ>(Ut, tile, red, Y, lane, w, P, A, A.coeff + (size_t)ie * A.ncoeffall + 1);
     }
 }
 
@@ -1146,10 +1327,13 @@ __device__ __forceinline__ void fr_columns(FrState<T, TJ> &st, const typename cp
     }
 }
 
+// pcw (several element types): per pair cutoff and neighbour weight
+// (radelem[ti] + radelem[tj]) rcutfac and wjelem[tj], cpuSnap4.cpp:813-838
 template <typename T, int TJ>
 __device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__ prij, const int2 *__restrict__ pinfo,
                                         const SnapGeom &gp, const typename cplx<T>::type *__restrict__ Y,
-                                        double4 *__restrict__ dEslot, T *__restrict__ qs, double *__restrict__ qg)
+                                        double4 *__restrict__ dEslot, T *__restrict__ qs, double *__restrict__ qg,
+                                        const double2 *__restrict__ pcw)
 {
     typedef typename cplx<T>::type T2;
     typedef typename FAccSel<T>::type Acc;
@@ -1159,7 +1343,15 @@ __device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__
     FrState<T, TJ> st;
     {
         PairGeo g;
-        pair_geometry<true>(g, r.x, r.y, r.z, gp);
+        if (pcw) {
+            SnapGeom ge = gp;
+            const double2 c = pcw[p];
+            ge.rcut = c.x;
+            ge.wj = c.y;
+            pair_geometry<true>(g, r.x, r.y, r.z, ge);
+        } else {
+            pair_geometry<true>(g, r.x, r.y, r.z, gp);
+        }
         st.ar = (T)g.ar; st.ai = (T)g.ai; st.br = (T)g.br; st.bi = (T)g.bi;
         // d(a,b)/dx_k and the radial terms wait in shared memory until the end
 #pragma unroll
@@ -1199,22 +1391,23 @@ template <typename T, int TJ>
 __device__ __forceinline__ void fr_kernel_body(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo,
                                                const int *__restrict__ pnum, const SnapGeom &gp,
                                                const typename cplx<T>::type *__restrict__ Y,
-                                               double4 *__restrict__ dEslot)
+                                               double4 *__restrict__ dEslot, const double2 *__restrict__ pcw)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double *qg = reinterpret_cast<double *>(smraw) + threadIdx.x;
     T *qs = reinterpret_cast<T *>(reinterpret_cast<double *>(smraw) + 16 * FR_THREADS) + threadIdx.x;
     const int npairs = *pnum;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x)
-        fr_pair<T, TJ>(p, prij, pinfo, gp, Y, dEslot, qs, qg);
+        fr_pair<T, TJ>(p, prij, pinfo, gp, Y, dEslot, qs, qg, pcw);
 }
 
 template <typename T, int TJ>
 __global__ void __launch_bounds__(FR_THREADS)
 k_snap_fr(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
-          SnapGeom gp, const typename cplx<T>::type *__restrict__ Y, double4 *__restrict__ dEslot)
+          SnapGeom gp, const typename cplx<T>::type *__restrict__ Y, double4 *__restrict__ dEslot,
+          const double2 *__restrict__ pcw = nullptr)
 {
-    fr_kernel_body<T, TJ>(prij, pinfo, pnum, gp, Y, dEslot);
+    fr_kernel_body<T, TJ>(prij, pinfo, pnum, gp, Y, dEslot, pcw);
 }
 
 // FP32: the state takes half the registers, so the kernel is held to 128 and
@@ -1224,7 +1417,7 @@ __global__ void __launch_bounds__(FR_THREADS, 4)
 k_snap_fr32(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
             SnapGeom gp, const float2 *__restrict__ Y, double4 *__restrict__ dEslot)
 {
-    fr_kernel_body<float, TJ>(prij, pinfo, pnum, gp, Y, dEslot);
+    fr_kernel_body<float, TJ>(prij, pinfo, pnum, gp, Y, dEslot, nullptr);
 }
 
 }  // namespace mdp

@@ -690,7 +690,7 @@ int sur_force(Surrogate &S, ForcePath &fp, const double4 *x, int inum, const int
     const int tb = 256, gb = (inum + tb - 1) / tb;
     if (fp.timing) cudaEventRecord(fp.ev[4], s);
     k_tally<<<gb, tb, 0, s>>>(fp.prij.as<double4>(), fp.dE.as<double4>(), fp.poff.as<int>(), fp.smap.as<int>(), inum,
-                              roff, rlist, f, vatom);
+                              roff, rlist, f, vatom, 1, 0);
     count_launches(4);
     if (fp.timing) {
         cudaEventRecord(fp.ev[5], s);
@@ -728,6 +728,7 @@ int mdp_sur_create(mdp_sur **h, const mdp_snap_params *p4, int device)
     mdp_sur *S = new mdp_sur();
     S->device = device;
     if (model_init(S->model, &q)) { delete S; return -1; }
+    if (S->model.ne > 1) { set_error("the surrogate takes one element type"); delete S; return -1; }
     if (S->model.ncoeff != SUR_NK) { set_error("unexpected feature count"); delete S; return -1; }
     if (S->P.ensure(sizeof(float) * SUR_NPAR) || S->Pb.ensure(sizeof(float) * SUR_NPAR) ||
         S->grad.ensure(sizeof(float) * SUR_NPAR) || S->m1.ensure(sizeof(float) * SUR_NPAR) ||

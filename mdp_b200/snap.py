@@ -35,10 +35,11 @@ def _ptr(a):
 
 
 def snap_compute(params: SnapParams, x: np.ndarray, box, skin: float = 1.0, neighmax: int = 64,
-                 precision: str = "fp64", want_neighbors: bool = False) -> dict:
+                 precision: str = "fp64", want_neighbors: bool = False, types=None) -> dict:
     """Energy per atom, forces (N,3), per-atom virial (6,N) of a periodic
     configuration; optionally the neighbour structure (ghost positions,
-    owner list, neighbour rows)."""
+    owner list, neighbour rows).  types: atom types 1..nelements, required by
+    models with several element types."""
     L = _lib.lib()
     x = np.ascontiguousarray(x, dtype=np.float64)
     n = x.shape[0]
@@ -51,9 +52,17 @@ def snap_compute(params: SnapParams, x: np.ndarray, box, skin: float = 1.0, neig
         nl = np.zeros((n, neighmax), dtype=np.int32); nn = np.zeros(n, dtype=np.int32)
         cap = 30 * n + 4096
         al = np.zeros(cap, dtype=np.int32); xa = np.zeros((cap, 3))
-    rc = L.mdp_snap_compute_host(C.byref(sp), PREC[precision], n, x, _box9(box), float(skin), int(neighmax),
-                                 _ptr(e), _ptr(f), _ptr(v), _ptr(nl), _ptr(nn), C.addressof(anum), _ptr(al),
-                                 _ptr(xa), cap)
+    if types is None:
+        rc = L.mdp_snap_compute_host(C.byref(sp), PREC[precision], n, x, _box9(box), float(skin), int(neighmax),
+                                     _ptr(e), _ptr(f), _ptr(v), _ptr(nl), _ptr(nn), C.addressof(anum), _ptr(al),
+                                     _ptr(xa), cap)
+    else:
+        t = np.ascontiguousarray(types, dtype=np.int32)
+        if t.shape != (n,):
+            raise ValueError(f"types must hold one type per atom ({n}), got shape {t.shape}")
+        rc = L.mdp_snap_compute_host_typed(C.byref(sp), PREC[precision], n, x, t, _box9(box), float(skin),
+                                           int(neighmax), _ptr(e), _ptr(f), _ptr(v), _ptr(nl), _ptr(nn),
+                                           C.addressof(anum), _ptr(al), _ptr(xa), cap)
     _lib.check(rc, "mdp_snap_compute_host")
     out = dict(eatom=e, fatom=f, vatom=v)
     if want_neighbors:
@@ -94,6 +103,11 @@ class SnapMD:
     def set_state(self, x: np.ndarray, v: np.ndarray):
         _lib.check(_lib.lib().mdp_md_set_state(self._h, np.ascontiguousarray(x, dtype=np.float64),
                                                np.ascontiguousarray(v, dtype=np.float64)), "mdp_md_set_state")
+
+    def set_types(self, types: np.ndarray):
+        """Atom types 1..nelements (models with several element types)."""
+        _lib.check(_lib.lib().mdp_md_set_types(self._h, np.ascontiguousarray(types, dtype=np.int32)),
+                   "mdp_md_set_types")
 
     def set_state_device(self, x_ptr: int, v_ptr: int):
         _lib.check(_lib.lib().mdp_md_set_state_device(self._h, C.c_void_p(x_ptr), C.c_void_p(v_ptr)),

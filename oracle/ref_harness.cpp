@@ -211,6 +211,86 @@ void ref_snap_force(double *eatom, double *fatom, double *vatom, const double *x
     }
 }
 
+// Multi-element SNAP through ComputePairSnap3 (snappotential.cpp:634-760)
+// with the parameter set-up of InitSnap (snappotential.cpp:146-232):
+// atom types 1..nelements (atomtype over the owners; ghosts through alist),
+// map[t] = t - 1, per-type radii and weights, cutoffs
+// (radelem[i] + radelem[j]) * rcutfac per type pair, nelements * ncoeffall
+// coefficients (ncoeffall = 1 + idxb_max * nelements^3 with chemflag, else
+// 1 + idxb_max) and element blocks of U and Y when chemflag is set.  One atom
+// block; eatom, fatom (AoS) and vatom (SoA 6 x inum) accumulate.
+void ref_snap_force_me(double *eatom, double *fatom, double *vatom, const double *x, const int *atomtype,
+                       const int *alist, const int *neighlist, const int *neighnum, int inum, int neighmax,
+                       int twojmax, int nelements, int chemflag, int ncoeffall, const double *coeffelem,
+                       double rcutfac, double rfac0, double rmin0, const double *radelems, const double *wjelems,
+                       int switchflag, int bzeroflag, int bnormflag, int wselfallflag)
+{
+    const int dim = 3, ntypes = nelements, quadraticflag = 0;
+    const int nelem = chemflag ? nelements : 1;
+    int jdim = twojmax + 1;
+    int idx_max[5];
+    int idxcg_count = 0, idxz_count = 0, idxb_count = 0;
+    for (int j1 = 0; j1 <= twojmax; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= MIN(twojmax, j1 + j2); j += 2) {
+                idxcg_count += (j1 + 1) * (j2 + 1);
+                if (j >= j1) idxb_count++;
+                for (int mb = 0; 2 * mb <= j; mb++) idxz_count += j + 1;
+            }
+    std::vector<double> rootpq((jdim + 1) * (jdim + 1)), cglist(idxcg_count), fac(168);
+    std::vector<int> idxz(idxz_count * 10), idxz_block(jdim * jdim * jdim), idxb(idxb_count * 3),
+        idxb_block(jdim * jdim * jdim), idxu_block(jdim), idxcg_block(jdim * jdim * jdim);
+    fac[0] = 1.0;
+    for (int i = 1; i < 168; i++) fac[i] = fac[i - 1] * (double)i;
+    cpuInitSna(rootpq.data(), cglist.data(), fac.data(), idx_max, idxz.data(), idxz_block.data(),
+               idxb.data(), idxb_block.data(), idxu_block.data(), idxcg_block.data(), twojmax);
+    int idxu_max = idx_max[1], idxb_max = idx_max[2], idxz_max = idx_max[3];
+    std::vector<double> radelem(nelements + 1, 0.0), wjelem(nelements + 1, 0.0);
+    std::vector<int> map(nelements + 1, 0);
+    for (int t = 0; t < nelements; t++) {
+        radelem[t + 1] = radelems[t];
+        wjelem[t + 1] = wjelems[t];
+        map[t + 1] = t;
+    }
+    std::vector<double> rcutsq((nelements + 1) * (nelements + 1), 0.0);
+    for (int i = 0; i < nelements; i++)
+        for (int j = 0; j < nelements; j++) {
+            double cut = (radelems[i] + radelems[j]) * rcutfac;
+            rcutsq[j + 1 + (i + 1) * (nelements + 1)] = cut * cut;
+        }
+    double bzero[64];
+    for (int j = 0; j <= twojmax; j++) bzero[j] = bnormflag ? 1.0 : (double)(j + 1);
+    double wself = 1.0;
+    const int na = inum;
+    std::vector<int> pairnum(na), pairlist((size_t)na * neighmax), ilist(na), pairnumsum(na + 1);
+    for (int i = 0; i < na; i++) ilist[i] = i;
+    cpuNeighPairList(pairnum.data(), pairlist.data(), (double *)x, rcutsq.data(), ilist.data(), (int *)neighlist,
+                     (int *)neighnum, (int *)atomtype, (int *)alist, na, neighmax, dim, ntypes);
+    pairnumsum[0] = 0;
+    for (int i = 0; i < na; i++) pairnumsum[i + 1] = pairnumsum[i] + pairnum[i];
+    int ijnum = pairnumsum[na];
+    std::vector<int> ai(ijnum), aj(ijnum), ti(ijnum), tj(ijnum), aii(ijnum);
+    std::vector<double> rij((size_t)3 * ijnum);
+    const size_t nub = (size_t)idxu_max * nelem * na;
+    std::vector<double> ur(nub, 0.0), ui(nub, 0.0), yr(nub), yi(nub);
+    cpuNeighPairs(rij.data(), (double *)x, aii.data(), ai.data(), aj.data(), ti.data(), tj.data(), pairnum.data(),
+                  pairlist.data(), pairnumsum.data(), ilist.data(), (int *)atomtype, (int *)alist, na, neighmax, dim);
+    cpuSnapComputeUi(ur.data(), ui.data(), rootpq.data(), rij.data(), wjelem.data(), radelem.data(), rmin0, rfac0,
+                     rcutfac, idxu_block.data(), map.data(), aii.data(), ti.data(), tj.data(), twojmax, idxu_max, na,
+                     ijnum, switchflag, chemflag);
+    cpuAddWself2Ui(ur.data(), ui.data(), wself, idxu_block.data(), (int *)atomtype, map.data(), ai.data(),
+                   wselfallflag, chemflag, idxu_max, nelem, twojmax, na);
+    cpuSnapComputeEi(eatom, ur.data(), ui.data(), cglist.data(), bzero, (double *)coeffelem, ilist.data(),
+                     map.data(), (int *)atomtype, idxb.data(), idxcg_block.data(), idxu_block.data(), twojmax,
+                     idxb_max, idxu_max, nelem, ncoeffall, bnormflag, bzeroflag, wselfallflag, quadraticflag, na);
+    cpuSnapComputeYi(yr.data(), yi.data(), ur.data(), ui.data(), cglist.data(), (double *)coeffelem, map.data(),
+                     (int *)atomtype, idxz.data(), idxb_block.data(), idxu_block.data(), idxcg_block.data(),
+                     twojmax, idxb_max, idxu_max, idxz_max, nelem, ncoeffall, bnormflag, na);
+    cpuSnapComputeFi(fatom, vatom, yr.data(), yi.data(), rootpq.data(), rij.data(), wjelem.data(), radelem.data(),
+                     rmin0, rfac0, rcutfac, idxu_block.data(), map.data(), aii.data(), ai.data(), aj.data(),
+                     ti.data(), tj.data(), twojmax, idxu_max, na, inum, ijnum, switchflag, chemflag);
+}
+
 // SNAP forces through the reference's other pair chain, ComputePairSnap
 // (snappotential.cpp:236-410): per-pair U and dU (cpuComputeUij,
 // cpuComputeDuijdrj), U totals, Z and B (cpuComputeZi, cpuComputeBi), energy

@@ -51,6 +51,10 @@ def lib():
                                                  C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_double,
                                                  C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                                  C.c_int]
+        _lib.ref_snap_force_me.restype = None
+        _lib.ref_snap_force_me.argtypes = [_dp, _dp, _dp, _dp, _ip, _ip, _ip, _ip, C.c_int, C.c_int, C.c_int,
+                                           C.c_int, C.c_int, C.c_int, _dp, C.c_double, C.c_double, C.c_double,
+                                           _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int]
         _lib.ref_nve_initial.argtypes = [_dp, _dp, _dp, _dp, C.c_double, C.c_double, _ip, _ip, C.c_int]
         _lib.ref_nve_final.argtypes = [_dp, _dp, _dp, _dp, C.c_double, _ip, _ip, C.c_int]
         _lib.ref_omp_max_threads.restype = C.c_int
@@ -126,6 +130,26 @@ def snap_force_pairsnap(x_all, alist, neighlist, neighnum, params):
                                   params.rcutfac, params.rfac0, params.rmin0, params.radelem, params.wjelem,
                                   params.switchflag, params.bzeroflag, params.bnormflag, params.wselfallflag,
                                   params.quadraticflag)
+    return e, f.reshape(inum, 3), v.reshape(6, inum)
+
+
+def snap_force_me(x_all, alist, neighlist, neighnum, atomtype, params):
+    """Per-atom energy, forces (N,3) and virial (6,N) of a multi-element model
+    (types 1..nelements in atomtype, one per local atom) from the reference's
+    ComputePairSnap3 chain with InitSnap's per-element set-up."""
+    inum, neighmax = neighlist.shape
+    e = np.zeros(inum); f = np.zeros(3 * inum); v = np.zeros(6 * inum)
+    lib().ref_snap_force_me(e, f, v, np.ascontiguousarray(x_all).ravel(),
+                            np.ascontiguousarray(atomtype, dtype=np.int32),
+                            np.ascontiguousarray(alist, dtype=np.int32),
+                            np.ascontiguousarray(neighlist, dtype=np.int32).ravel(),
+                            np.ascontiguousarray(neighnum, dtype=np.int32), inum, neighmax, params.twojmax,
+                            params.nelements, params.chemflag, params.ncoeffall,
+                            np.ascontiguousarray(params.coeff, dtype=np.float64),
+                            params.rcutfac, params.rfac0, params.rmin0,
+                            np.ascontiguousarray(params.radelems, dtype=np.float64),
+                            np.ascontiguousarray(params.wjelems, dtype=np.float64),
+                            params.switchflag, params.bzeroflag, params.bnormflag, params.wselfallflag)
     return e, f.reshape(inum, 3), v.reshape(6, inum)
 
 

@@ -294,6 +294,38 @@ def quad_fixtures():
         print(name, cfg.natoms, "atoms", os.path.getsize(path), "bytes")
 
 
+# several element types: (name, cells, 2J, T, jitter, seed, coeff seed, radelems, wjelems, chemflag, flags)
+CHEM_CASES = [
+    ("chem_bcc128_2j6", (4, 4, 4), 6, 600.0, 0.05, 21, 111, (0.5, 0.45), (1.0, 0.8), 1, {}),
+    ("chem_bcc250_2j8", (5, 5, 5), 8, 300.0, 0.06, 22, 112, (0.5, 0.47), (1.0, 0.9), 1, {}),
+    ("chem_bcc54_2j4_3el_flags", (3, 3, 3), 4, 1000.0, 0.10, 23, 113, (0.5, 0.44, 0.48), (1.0, 0.7, 1.2), 1,
+     {"bnormflag": 1, "bzeroflag": 1}),
+    ("chem_bcc54_2j6_wselfall", (3, 3, 3), 6, 800.0, 0.08, 24, 114, (0.5, 0.46), (0.9, 1.1), 1,
+     {"bzeroflag": 1, "wselfallflag": 1}),
+    ("chem_bcc128_2j8_chemflag0", (4, 4, 4), 8, 600.0, 0.05, 25, 115, (0.5, 0.45), (1.0, 0.8), 0,
+     {"bzeroflag": 1}),
+]
+
+
+def chem_fixtures():
+    """Several element types (random types 1..nelements): positions, types, the reference's neighbour
+    list and its per-atom energy, forces and virial from ComputePairSnap3 with InitSnap's per-element
+    set-up (element blocks of U and Y with chemflag)."""
+    for (name, cells, tj, temp, jit, seed, cseed, rad, wj, chem, flags) in CHEM_CASES:
+        p = configs.snap_params_elements(tj, rad, wj, chemflag=chem, seed=cseed, **flags)
+        cfg = configs.ta_config(cells, temp=temp, jitter=jit, seed=seed)
+        types = np.random.default_rng(seed + 1000).integers(1, p.nelements + 1, cfg.natoms).astype(np.int32)
+        xa, al, nl, nn = refpy.neighbor_list(cfg.x, cfg.box, p.rcut, SKIN, NEIGHMAX, neighcell=0)
+        e, f, va = refpy.snap_force_me(xa, al, nl, nn, types, p)
+        path = os.path.join(HERE, f"{name}.npz")
+        np.savez_compressed(path, cells=np.array(cells), twojmax=tj, temp=temp, jitter=jit, seed=seed,
+                            coeff_seed=cseed, chemflag=chem, radelems=np.array(rad), wjelems=np.array(wj),
+                            flags=np.array([p.bnormflag, p.bzeroflag, p.switchflag, p.wselfallflag]),
+                            skin=SKIN, neighmax=NEIGHMAX, x=cfg.x, box=cfg.box, types=types, coeff=p.coeff,
+                            xall=xa, alist=al, neighlist=nl, neighnum=nn, eatom=e, fatom=f, vatom=va)
+        print(name, cfg.natoms, "atoms", p.nelements, "elements", os.path.getsize(path), "bytes")
+
+
 def main():
     from oracle.refroot import reference_root
     subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref", f"REFROOT={reference_root() or ''}"])
@@ -302,6 +334,9 @@ def main():
         return
     if "--quad" in sys.argv:
         quad_fixtures()
+        return
+    if "--chem" in sys.argv:
+        chem_fixtures()
         return
     fit_fixtures()
     if "--fit-only" in sys.argv:
