@@ -13,8 +13,11 @@
  * gpuSnap.cu, gpuCumsum.cu, gpuNeighborList3D.cu, gpuVelocityIntegration.cu
  * (modes 0, 1 and 2) and gpuDomain.cu's gpuPBC at link time.  Array layouts are
  * the reference's: U/Y [idxu][inum], rij [ijnum][3], fatom [anum][3],
- * vatom [6][anum], x [natom][dim].  Supported: one element type, 2J = 4, 6, 8,
- * double.  On unsupported input the outputs are untouched and
+ * vatom [6][anum], x [natom][dim]; with chemflag, U and Y hold one such block
+ * per element ([element][idxu][inum], block map[tj] for a pair).  Supported:
+ * 2J = 4, 6, 8, up to four element types (chemflag 0 or 1, per-pair cutoffs
+ * (radelem[ti] + radelem[tj]) rcutfac), double; float through the _f32
+ * entries.  On unsupported input the outputs are untouched and
  * mdp_last_error() says why.
  */
 #ifndef MDP_B200_GPUCORE_H

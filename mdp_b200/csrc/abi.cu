@@ -10,10 +10,10 @@
 //
 // Layouts are the reference's: U and Y are [idxu][inum] (atom fastest) in
 // separate real/imaginary arrays, rij is [ijnum][3], forces [inum][3].
-// Supported: one element type (chemflag = 0, quadraticflag = 0), 2J in
-// {4, 6, 8}, double precision.  The reference's void functions have no error
-// channel: an unsupported argument leaves the outputs untouched and sets
-// mdp_last_error().
+// Supported: 2J in {4, 6, 8}, double precision, up to four element types
+// (chemflag 0 or 1); quadraticflag belongs to the ComputePairSnap chain.  The
+// reference's void functions have no error channel: an unsupported argument
+// leaves the outputs untouched and sets mdp_last_error().
 #include "common.cuh"
 #include "engine.h"
 
@@ -224,7 +224,7 @@ __global__ void k_minmax2(const int *__restrict__ a, const int *__restrict__ b, 
 // ---------------------------------------------------------------------------
 struct RefCtx {
     ForcePath fp;
-    DevBuf cnt, off, cursor, etmp, tmp, mm;
+    DevBuf cnt, off, cursor, etmp, tmp, mm, elem;
     SnapModel model;
 };
 static std::mutex g_ref_mu;
@@ -260,7 +260,8 @@ static int model_from_args(SnapModel &m, int twojmax, const double *coeff_host, 
     return model_init(m, &p);
 }
 
-// single-type check of ti/tj on the device; returns the type or -1
+// single-type check of ti/tj on the device; returns the type, -2 when the
+// pairs have several types, -1 on error
 static int single_type(const int *ti, const int *tj, int n, cudaStream_t s)
 {
     RefCtx &c = ref_ctx();
@@ -272,11 +273,7 @@ static int single_type(const int *ti, const int *tj, int n, cudaStream_t s)
     int h[2];
     MDP_CUDA_TRY(cudaMemcpyAsync(h, c.mm.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     MDP_CUDA_TRY(cudaStreamSynchronize(s));
-    if (h[0] != h[1]) {
-        set_error("only a single element type is supported (pair types range %d..%d)", h[0], h[1]);
-        return -1;
-    }
-    return h[0];
+    return h[0] != h[1] ? -2 : h[0];
 }
 
 // U (reference layout) -> tiles in fp.Ut
@@ -444,11 +441,346 @@ int ref_snap_fi(double *fatom, double *vatom, int vmode, long vstride, const dou
     return 0;
 }
 
-// rcut and weight of the (single) pair type, read from device radelem/wjelem
+// ---------------------------------------------------------------------------
+// several element types in the reference layouts: U / Y [block][k][inum]
+// (block = map[tj] with chemflag, cpuSnap4.cpp:59-61 and 887-888), per-pair
+// cutoffs (radelem[ti] + radelem[tj]) rcutfac and weights wjelem[tj], the
+// coefficient table coeffelem [element][ncoeffall] chosen per atom by
+// map[type[ii]]
+// ---------------------------------------------------------------------------
+__global__ void k_max_block(const int *__restrict__ tj, const int *__restrict__ map, int n, int *__restrict__ out)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < n) atomicMax(out, map[tj[p]]);
+}
+
+// pairs bucketed per virtual atom v = block * inum + aii; pinfo = (block *
+// ipad + aii, pair) for the tiled Y; pcw = per-pair cutoff and weight
+__global__ void k_pair_bucket_count_me(const int *__restrict__ aii, const int *__restrict__ tj,
+                                       const int *__restrict__ map, int chem, int inum, int ijnum, int *__restrict__ cnt)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ijnum) return;
+    const int b = chem ? map[tj[p]] : 0;
+    atomicAdd(&cnt[(long)b * inum + aii[p]], 1);
+}
+__global__ void k_pair_bucket_fill_me(const int *__restrict__ aii, const int *__restrict__ ti,
+                                      const int *__restrict__ tj, const int *__restrict__ map, int chem,
+                                      const double *__restrict__ rij, const double *__restrict__ radelem,
+                                      const double *__restrict__ wjelem, double rcutfac, int ijnum, int inum, int ipad,
+                                      const int *__restrict__ off, int *__restrict__ cursor, double4 *__restrict__ prij,
+                                      int2 *__restrict__ pinfo, double2 *__restrict__ pcw)
+{
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ijnum) return;
+    const int b = chem ? map[tj[p]] : 0, i = aii[p];
+    const long v = (long)b * inum + i;
+    const int q = off[v] + atomicAdd(&cursor[v], 1);
+    prij[q] = make_double4(rij[3 * (size_t)p], rij[3 * (size_t)p + 1], rij[3 * (size_t)p + 2], 0.0);
+    pinfo[q] = make_int2((int)((long)b * ipad + i), p);
+    pcw[q] = make_double2((radelem[ti[p]] + radelem[tj[p]]) * rcutfac, wjelem[tj[p]]);
+}
+
+// wself on the diagonal of block b of atom ii when b is the atom's element
+// (chemflag) or always (wselfallflag, or the one block without chemflag),
+// then the mirror of every block (cpuAddWself2Ui, cpuSnap4.cpp:193-244)
+__global__ void k_wself_ref_me(double *__restrict__ ur, double *__restrict__ ui, double wself, int inum, int tj,
+                               int nblk, const int *__restrict__ type, const int *__restrict__ map, int chem,
+                               int wselfall)
+{
+    long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long per = (long)inum * (tj + 1);
+    if (t >= per * nblk) return;
+    const int b = (int)(t / per);
+    const long r = t - (long)b * per;
+    const int i = (int)(r % inum), j = (int)(r / inum);
+    const int nu = idxu_count(tj);
+    double *br = ur + (size_t)b * nu * inum, *bi = ui + (size_t)b * nu * inum;
+    const int ie = chem ? map[type[i]] : 0;
+    const int b0 = idxu_block(j);
+    if (b == ie || wselfall)
+        for (int m = 0; m <= j; m++) br[(size_t)(b0 + (j + 1) * m + m) * inum + i] += wself;
+    for (int mb = 0; 2 * mb < j; mb++)
+        for (int ma = 0; ma <= j; ma++) {
+            const size_t src = (size_t)(b0 + (j + 1) * mb + ma) * inum + i;
+            const size_t dst = (size_t)(b0 + (j + 1) * (j - mb) + (j - ma)) * inum + i;
+            const double sg = ((ma + mb) & 1) ? -1.0 : 1.0;
+            br[dst] = sg * br[src];
+            bi[dst] = -sg * bi[src];
+        }
+}
+
+// element of each atom's coefficient set: map[type[ii]] when use, else 0;
+// pads (ii >= inum) 0; *emax = the largest
+__global__ void k_elem_map(const int *__restrict__ type, const int *__restrict__ map, int inum, int ipad, int use,
+                           int *__restrict__ elem, int *__restrict__ emax)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ipad) return;
+    int e = (i < inum && use) ? map[type[i]] : 0;
+    e = e < 0 ? 0 : e;
+    elem[i] = e;
+    if (i < inum) atomicMax(emax, e);
+}
+
+// number of element blocks the pairs reach: 1 + max map[tj] (1 without chemflag)
+static int pair_blocks(const int *tj, const int *map, int ijnum, int chem, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    if (!chem || ijnum <= 0) return 1;
+    if (c.mm.ensure(2 * sizeof(int))) return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(c.mm.p, 0, sizeof(int), s));
+    k_max_block<<<(ijnum + 255) / 256, 256, 0, s>>>(tj, map, ijnum, c.mm.as<int>());
+    int h = 0;
+    MDP_CUDA_TRY(cudaMemcpyAsync(&h, c.mm.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h < 0 || h >= MAXELEM) { set_error("element block %d out of range (at most %d elements)", h, MAXELEM); return -1; }
+    return h + 1;
+}
+
+// per-atom elements into c.elem (ipad entries); returns the largest, or -1
+static int atom_elements(const int *type, const int *map, int inum, int use, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    const int ipad = (inum + 31) / 32 * 32;
+    if (c.elem.ensure(sizeof(int) * ipad) || c.mm.ensure(2 * sizeof(int))) return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(c.mm.p, 0, sizeof(int), s));
+    k_elem_map<<<(ipad + 255) / 256, 256, 0, s>>>(type, map, inum, ipad, use, c.elem.as<int>(), c.mm.as<int>());
+    int h = 0;
+    MDP_CUDA_TRY(cudaMemcpyAsync(&h, c.mm.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MDP_CUDA_TRY(cudaStreamSynchronize(s));
+    return h;
+}
+
+// nblk U blocks (reference layout) -> tiles, block after block
+static int load_tiles_blocks(RefCtx &c, const double *ur, const double *ui, int inum, int tj, int nblk,
+                             cudaStream_t s)
+{
+    const int nu = idxu_count(tj);
+    const long ntiles = (inum + 31) / 32;
+    const size_t per = (size_t)ntiles * nu * 32;
+    if (c.fp.Ut.ensure(sizeof(double2) * per * nblk)) return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(c.fp.Ut.p, 0, sizeof(double2) * per * nblk, s));
+    const long n = (long)inum * nu;
+    for (int b = 0; b < nblk; b++)
+        k_uref_to_tiles<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ur + (size_t)b * n, ui + (size_t)b * n, inum, nu,
+                                                                   c.fp.Ut.as<double2>() + per * b);
+    return 0;
+}
+
+static MeArgs me_args(RefCtx &c, int inum, int nblk, int ncoeffall, int bzero, int wselfall, const double *coeff,
+                      int pa)
+{
+    MeArgs A;
+    A.nblk = nblk;
+    A.ntiles = (inum + 31) / 32;
+    A.ncoeffall = ncoeffall;
+    A.bzero = bzero;
+    A.wselfall = wselfall;
+    A.elem = c.elem.as<int>();
+    A.coeff = coeff;
+    A.pa = pa;
+    return A;
+}
+
+// U of the element blocks, accumulated into the reference layout
+int ref_snap_ui_me(double *ur, double *ui, const double *rij, const double *radelem, const double *wjelem,
+                   double rcutfac, double rfac0, double rmin0, const int *aii, const int *ti, const int *tjv,
+                   const int *map, int chem, int tj, int inum, int ijnum, int switchflag, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    if (model_from_args(c.model, tj, nullptr, 0, 0, 0, 0, 1.0, 1.0, rfac0, rmin0, switchflag)) return -1;
+    if (ijnum <= 0) return 0;
+    const int nblk = pair_blocks(tjv, map, ijnum, chem, s);
+    if (nblk < 0) return -1;
+    const long nv = (long)nblk * inum;
+    const int ipad = (inum + 31) / 32 * 32;
+    if (c.cnt.ensure(sizeof(int) * nv) || c.off.ensure(sizeof(int) * (nv + 1)) || c.cursor.ensure(sizeof(int) * nv) ||
+        c.fp.prij.ensure(sizeof(double4) * ijnum) || c.fp.pinfo.ensure(sizeof(int2) * ijnum) ||
+        c.fp.pcw.ensure(sizeof(double2) * ijnum) || c.tmp.ensure(sizeof(int) * scan_tmp_ints(nv)))
+        return -1;
+    MDP_CUDA_TRY(cudaMemsetAsync(c.cnt.p, 0, sizeof(int) * nv, s));
+    MDP_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, sizeof(int) * nv, s));
+    k_pair_bucket_count_me<<<(ijnum + 255) / 256, 256, 0, s>>>(aii, tjv, map, chem, inum, ijnum, c.cnt.as<int>());
+    if (exclusive_scan(c.cnt.as<int>(), c.off.as<int>(), nv, c.tmp.as<int>(), s)) return -1;
+    k_pair_bucket_fill_me<<<(ijnum + 255) / 256, 256, 0, s>>>(aii, ti, tjv, map, chem, rij, radelem, wjelem, rcutfac,
+                                                              ijnum, inum, ipad, c.off.as<int>(), c.cursor.as<int>(),
+                                                              c.fp.prij.as<double4>(), c.fp.pinfo.as<int2>(),
+                                                              c.fp.pcw.as<double2>());
+    if (tu_ensure_tables()) return -1;
+    const int blocks = (int)std::min((nv + UI_WARPS - 1) / UI_WARPS, (long)num_sms() * 16);
+#define MDP_UIREF_ME(TJ)                                                                                           \
+    {                                                                                                              \
+        const size_t sm = (size_t)UI_WARPS * (idxu_count(TJ) + 32 * (TJ + 1)) * sizeof(double2);                  \
+        int per_sm = 0;                                                                                            \
+        if (kernel_setup((const void *)k_snap_ui<double, TJ, true>, UI_WARPS * 32, sm, &per_sm, "k_snap_ui"))      \
+            return -1;                                                                                             \
+        k_snap_ui<double, TJ, true><<<blocks, UI_WARPS * 32, sm, s>>>(c.off.as<int>(), c.fp.prij.as<double4>(),    \
+                                                                      (int)nv, c.model.geom, nullptr, ur, ui,      \
+                                                                      c.fp.pcw.as<double2>(), inum);              \
+    }
+    switch (tj) {
+    case 4: MDP_UIREF_ME(4) break;
+    case 6: MDP_UIREF_ME(6) break;
+    case 8: MDP_UIREF_ME(8) break;
+    default: set_error("twojmax %d not supported", tj); return -1;
+    }
+#undef MDP_UIREF_ME
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int ref_snap_wself_me(double *ur, double *ui, double wself, const int *type, const int *map, int chem, int wselfall,
+                      int nblk, int tj, int inum, cudaStream_t s)
+{
+    const long n = (long)inum * (tj + 1) * nblk;
+    k_wself_ref_me<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(ur, ui, wself, inum, tj, nblk, type, map, chem,
+                                                              wselfall);
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// eatom[ilist[ii]] += beta_0(e) + sum_{t,k} beta(e, t, k) (B^t_k - bzero), e the atom's element
+int ref_snap_ei_me(double *eatom, const double *ur, const double *ui, const double *coeff_dev, const int *ilist,
+                   int tj, int nblk, int ncoeffall, int bnorm, int bzero, int wselfall, int inum, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    if (load_tiles_blocks(c, ur, ui, inum, tj, nblk, s) || c.etmp.ensure(sizeof(double) * inum)) return -1;
+    const MeArgs A = me_args(c, inum, nblk, ncoeffall, bzero, wselfall, coeff_dev, 0);
+    const double2 *Ut = c.fp.Ut.as<double2>();
+    double *et = c.etmp.as<double>();
+    int per_sm = 0;
+#define MDP_EI_ME(TJ)                                                                                              \
+    if (kernel_setup((const void *)k_snap_ei_me<TJ>, BI_WARPS * 32, 0, &per_sm, "k_snap_ei_me")) return -1;        \
+    k_snap_ei_me<TJ><<<std::min(A.ntiles, num_sms() * per_sm), BI_WARPS * 32, 0, s>>>(Ut, inum, bnorm, A, et);
+    switch (tj) {
+    case 4: MDP_EI_ME(4) break;
+    case 6: MDP_EI_ME(6) break;
+    case 8: MDP_EI_ME(8) break;
+    default: set_error("twojmax %d not supported", tj); return -1;
+    }
+#undef MDP_EI_ME
+    k_add_eatom<<<(inum + 255) / 256, 256, 0, s>>>(eatom, et, ilist, inum);
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int ref_snap_bi_me(double *blist, const double *ur, const double *ui, int tj, int nblk, int bnorm, int bzero,
+                   int wselfall, int inum, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    if (load_tiles_blocks(c, ur, ui, inum, tj, nblk, s)) return -1;
+    const MeArgs A = me_args(c, inum, nblk, 0, bzero, wselfall, nullptr, 0);
+    const double2 *Ut = c.fp.Ut.as<double2>();
+    int per_sm = 0;
+#define MDP_BI_ME(TJ)                                                                                              \
+    if (kernel_setup((const void *)k_snap_bi_me<TJ>, BI_WARPS * 32, 0, &per_sm, "k_snap_bi_me")) return -1;        \
+    k_snap_bi_me<TJ><<<std::min(A.ntiles, num_sms() * per_sm), BI_WARPS * 32, 0, s>>>(Ut, inum, bnorm, A, blist);
+    switch (tj) {
+    case 4: MDP_BI_ME(4) break;
+    case 6: MDP_BI_ME(6) break;
+    case 8: MDP_BI_ME(8) break;
+    default: set_error("twojmax %d not supported", tj); return -1;
+    }
+#undef MDP_BI_ME
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// Y of every block from the coefficient table (pa = 0, elements in c.elem)
+// or from per-atom coefficients [triple][k][inum] (pa = 1)
+int ref_snap_yi_me(double *yr, double *yi, const double *ur, const double *ui, const double *coeff_dev, int pa,
+                   int tj, int nblk, int ncoeffall, int bnorm, int inum, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    std::vector<double> ones(mdp_snap_ncoeff(tj) + 1, 1.0);
+    if (model_from_args(c.model, tj, ones.data(), (int)ones.size(), bnorm, 0, 0, 1.0, 1.0, 1.0, 0.0, 1)) return -1;
+    if (load_tiles_blocks(c, ur, ui, inum, tj, nblk, s)) return -1;
+    const long ntiles = (inum + 31) / 32;
+    const int nyh = yh_count(tj);
+    if (c.fp.Y.ensure(sizeof(double2) * ntiles * 32 * nyh * nblk)) return -1;
+    const MeArgs A = me_args(c, inum, nblk, ncoeffall, 0, 0, coeff_dev, pa);
+    const double2 *Ut = c.fp.Ut.as<double2>();
+    double2 *Y = c.fp.Y.as<double2>();
+    int per_sm = 0;
+#define MDP_YI_ME(TJ)                                                                                              \
+    {                                                                                                              \
+        const size_t sm = yi_me_smem_bytes<TJ>();                                                                  \
+        if (kernel_setup((const void *)k_snap_yi_me<TJ>, YiWarps<double, TJ>::n * 32, sm, &per_sm, "k_snap_yi_me")) \
+            return -1;                                                                                             \
+        k_snap_yi_me<TJ><<<std::min(A.ntiles, num_sms() * per_sm), YiWarps<double, TJ>::n * 32, sm, s>>>(          \
+            Ut, inum, c.model.yd, A, Y);                                                                           \
+    }
+    switch (tj) {
+    case 4: MDP_YI_ME(4) break;
+    case 6: MDP_YI_ME(6) break;
+    case 8: MDP_YI_ME(8) break;
+    default: set_error("twojmax %d not supported", tj); return -1;
+    }
+#undef MDP_YI_ME
+    const long n = (long)inum * idxu_count(tj);
+    for (int b = 0; b < nblk; b++)
+        k_ytiles_to_ref<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(Y + (size_t)b * ntiles * nyh * 32, inum, tj, nyh,
+                                                                   yr + (size_t)b * n, yi + (size_t)b * n);
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// dE/dr with each pair's Y block (map[tj] with chemflag), per-pair cutoffs and weights
+int ref_snap_fi_me(double *fatom, double *vatom, int vmode, long vstride, const double *yr, const double *yi,
+                   const double *rij, const double *radelem, const double *wjelem, double rcutfac, double rfac0,
+                   double rmin0, const int *aii, const int *ai, const int *aj, const int *ti, const int *tjv,
+                   const int *map, int chem, int tj, int inum, int ijnum, int switchflag, cudaStream_t s)
+{
+    RefCtx &c = ref_ctx();
+    if (model_from_args(c.model, tj, nullptr, 0, 0, 0, 0, 1.0, 1.0, rfac0, rmin0, switchflag)) return -1;
+    if (ijnum <= 0) return 0;
+    const int nblk = pair_blocks(tjv, map, ijnum, chem, s);
+    if (nblk < 0) return -1;
+    const int nyh = yh_count(tj);
+    const long ntiles = (inum + 31) / 32, nv = (long)nblk * inum;
+    const int ipad = (int)ntiles * 32;
+    if (c.fp.Y.ensure(sizeof(double2) * ntiles * 32 * nyh * nblk) || c.fp.prij.ensure(sizeof(double4) * ijnum) ||
+        c.fp.pinfo.ensure(sizeof(int2) * ijnum) || c.fp.pcw.ensure(sizeof(double2) * ijnum) ||
+        c.fp.dE.ensure(sizeof(double4) * ijnum) || c.fp.poff.ensure(sizeof(int) * (nv + 1)) ||
+        c.cnt.ensure(sizeof(int) * nv) || c.cursor.ensure(sizeof(int) * nv) ||
+        c.tmp.ensure(sizeof(int) * scan_tmp_ints(nv)))
+        return -1;
+    const long n = (long)inum * nyh, nu = (long)inum * idxu_count(tj);
+    for (int b = 0; b < nblk; b++)
+        k_yref_to_tiles<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(yr + (size_t)b * nu, yi + (size_t)b * nu, inum, tj,
+                                                                   nyh, c.fp.Y.as<double2>() + (size_t)b * ntiles * nyh * 32);
+    MDP_CUDA_TRY(cudaMemsetAsync(c.cnt.p, 0, sizeof(int) * nv, s));
+    MDP_CUDA_TRY(cudaMemsetAsync(c.cursor.p, 0, sizeof(int) * nv, s));
+    k_pair_bucket_count_me<<<(ijnum + 255) / 256, 256, 0, s>>>(aii, tjv, map, chem, inum, ijnum, c.cnt.as<int>());
+    if (exclusive_scan(c.cnt.as<int>(), c.fp.poff.as<int>(), nv, c.tmp.as<int>(), s)) return -1;
+    k_pair_bucket_fill_me<<<(ijnum + 255) / 256, 256, 0, s>>>(aii, ti, tjv, map, chem, rij, radelem, wjelem, rcutfac,
+                                                              ijnum, inum, ipad, c.fp.poff.as<int>(), c.cursor.as<int>(),
+                                                              c.fp.prij.as<double4>(), c.fp.pinfo.as<int2>(),
+                                                              c.fp.pcw.as<double2>());
+    c.fp.fr_pcw = c.fp.pcw.as<double2>();
+    int rc;
+    switch (tj) {
+    case 4: rc = launch_fi<double, 4>(c.model, c.fp, (int)nv, 1, s); break;
+    case 6: rc = launch_fi<double, 6>(c.model, c.fp, (int)nv, 1, s); break;
+    case 8: rc = launch_fi<double, 8>(c.model, c.fp, (int)nv, 1, s); break;
+    default: rc = -1; set_error("twojmax %d not supported", tj);
+    }
+    c.fp.fr_pcw = nullptr;
+    if (rc) return rc;
+    k_scatter_fi<<<(ijnum + 255) / 256, 256, 0, s>>>(c.fp.dE.as<double4>(), rij, ai, aj, ijnum, fatom, vatom, vmode,
+                                                     vstride);
+    MDP_CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// rcut and weight of the (single) pair type, read from device radelem/wjelem;
+// returns 0, 1 when the pairs have several types, -1 on error
 static int pair_type_params(const int *ti_d, const int *tj_d, int ijnum, const double *radelem, const double *wjelem,
                             double rcutfac, double &rcut, double &wj, cudaStream_t s)
 {
     int t = single_type(ti_d, tj_d, ijnum, s);
+    if (t == -2) return 1;
     if (t < 0) return -1;
     double r = 0.5, w = 1.0;
     MDP_CUDA_TRY(cudaMemcpy(&r, radelem + t, sizeof(double), cudaMemcpyDeviceToHost));
@@ -504,22 +836,29 @@ void mdp_gpu_snap_compute_ui_f64(double *Utotr, double *Utoti, const double *roo
                                  const int *ti, const int *tj, int twojmax, int idxu_max, int inum, int ijnum,
                                  int switchflag, int chemflag)
 {
-    (void)rootpqarray; (void)idxu_block; (void)map; (void)idxu_max;
+    (void)rootpqarray; (void)idxu_block; (void)idxu_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag) { set_error("chemflag is not supported"); return; }
     double rcut, wj;
-    if (pair_type_params(ti, tj, ijnum, radelem, wjelem, rcutfac, rcut, wj, 0)) return;
-    ref_snap_ui(Utotr, Utoti, rij, rcut, wj, rfac0, rmin0, aii, twojmax, inum, ijnum, switchflag, 0);
+    const int several = chemflag ? 1 : pair_type_params(ti, tj, ijnum, radelem, wjelem, rcutfac, rcut, wj, 0);
+    if (several < 0) return;
+    if (several)
+        ref_snap_ui_me(Utotr, Utoti, rij, radelem, wjelem, rcutfac, rfac0, rmin0, aii, ti, tj, map, chemflag, twojmax,
+                       inum, ijnum, switchflag, 0);
+    else
+        ref_snap_ui(Utotr, Utoti, rij, rcut, wj, rfac0, rmin0, aii, twojmax, inum, ijnum, switchflag, 0);
 }
 
 void mdp_gpu_add_wself2ui_f64(double *Utotr, double *Utoti, double wself, const int *idxu_block, const int *type,
                               const int *map, const int *ai, int wselfall_flag, int chemflag, int idxu_max,
                               int nelements, int twojmax, int inum)
 {
-    (void)idxu_block; (void)type; (void)map; (void)ai; (void)wselfall_flag; (void)idxu_max;
+    (void)idxu_block; (void)ai; (void)idxu_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag || nelements != 1) { set_error("chemflag / multiple elements are not supported"); return; }
-    ref_snap_wself(Utotr, Utoti, wself, twojmax, inum, 0);
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    if (chemflag || nelements != 1)
+        ref_snap_wself_me(Utotr, Utoti, wself, type, map, chemflag, wselfall_flag, nelements, twojmax, inum, 0);
+    else
+        ref_snap_wself(Utotr, Utoti, wself, twojmax, inum, 0);
 }
 
 void mdp_gpu_snap_compute_ei_f64(double *eatom, const double *Utotr, const double *Utoti, const double *cglist,
@@ -528,10 +867,21 @@ void mdp_gpu_snap_compute_ei_f64(double *eatom, const double *Utotr, const doubl
                                  int twojmax, int idxb_max, int idxu_max, int nelements, int ncoeffall,
                                  int bnorm_flag, int bzero_flag, int wselfall_flag, int quadraticflag, int inum)
 {
-    (void)cglist; (void)bzero; (void)map; (void)type; (void)idxb; (void)idxcg_block; (void)idxu_block;
-    (void)idxb_max; (void)idxu_max;
+    (void)cglist; (void)bzero; (void)idxb; (void)idxcg_block; (void)idxu_block; (void)idxu_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (quadraticflag || nelements != 1) { set_error("quadratic / multi-element SNAP is not supported"); return; }
+    if (quadraticflag) { set_error("quadratic SNAP goes through the ComputePairSnap chain, not this stage"); return; }
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    if (ncoeffall != 1 + idxb_max * nelements * nelements * nelements) {
+        set_error("ncoeffall %d does not match idxb_max %d and %d element blocks", ncoeffall, idxb_max, nelements);
+        return;
+    }
+    const int emax = atom_elements(type, map, inum, 1, 0);
+    if (emax < 0) return;
+    if (nelements > 1 || emax > 0) {
+        ref_snap_ei_me(eatom, Utotr, Utoti, coeffelem, ilist, twojmax, nelements, ncoeffall, bnorm_flag, bzero_flag,
+                       wselfall_flag, inum, 0);
+        return;
+    }
     std::vector<double> c(ncoeffall);
     if (cudaMemcpy(c.data(), coeffelem, sizeof(double) * ncoeffall, cudaMemcpyDeviceToHost) != cudaSuccess) {
         set_error("copying coeffelem failed");
@@ -546,10 +896,13 @@ void mdp_gpu_snap_compute_bi_f64(double *blist, const double *Utotr, const doubl
                                  int nelements, int bnorm_flag, int bzero_flag, int wselfall_flag, int inum)
 {
     (void)cglist; (void)bzero; (void)idxb; (void)idxcg_block; (void)idxu_block; (void)idxz_block; (void)idxb_max;
-    (void)idxu_max; (void)idxz_max; (void)wselfall_flag;
+    (void)idxu_max; (void)idxz_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (nelements != 1) { set_error("multi-element SNAP is not supported"); return; }
-    ref_snap_bi(blist, Utotr, Utoti, twojmax, bnorm_flag, bzero_flag, inum, 0);
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    if (nelements > 1)
+        ref_snap_bi_me(blist, Utotr, Utoti, twojmax, nelements, bnorm_flag, bzero_flag, wselfall_flag, inum, 0);
+    else
+        ref_snap_bi(blist, Utotr, Utoti, twojmax, bnorm_flag, bzero_flag, inum, 0);
 }
 
 void mdp_gpu_snap_compute_yi_f64(double *ylist_r, double *ylist_i, const double *Utotr, const double *Utoti,
@@ -558,10 +911,19 @@ void mdp_gpu_snap_compute_yi_f64(double *ylist_r, double *ylist_i, const double 
                                  const int *idxcg_block, int twojmax, int idxb_max, int idxu_max, int idxz_max,
                                  int nelements, int ncoeffall, int bnorm_flag, int inum)
 {
-    (void)cglist; (void)map; (void)type; (void)idxz; (void)idxb_block; (void)idxu_block; (void)idxcg_block;
-    (void)idxb_max; (void)idxu_max; (void)idxz_max;
+    (void)cglist; (void)idxz; (void)idxb_block; (void)idxu_block; (void)idxcg_block; (void)idxu_max; (void)idxz_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (nelements != 1) { set_error("multi-element SNAP is not supported"); return; }
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    if (ncoeffall != 1 + idxb_max * nelements * nelements * nelements) {
+        set_error("ncoeffall %d does not match idxb_max %d and %d element blocks", ncoeffall, idxb_max, nelements);
+        return;
+    }
+    const int emax = atom_elements(type, map, inum, 1, 0);
+    if (emax < 0) return;
+    if (nelements > 1 || emax > 0) {
+        ref_snap_yi_me(ylist_r, ylist_i, Utotr, Utoti, coeffelem, 0, twojmax, nelements, ncoeffall, bnorm_flag, inum, 0);
+        return;
+    }
     std::vector<double> c(ncoeffall);
     if (cudaMemcpy(c.data(), coeffelem, sizeof(double) * ncoeffall, cudaMemcpyDeviceToHost) != cudaSuccess) {
         set_error("copying coeffelem failed");
@@ -578,9 +940,12 @@ void mdp_gpu_snap_compute_yi_beta_f64(double *ylist_r, double *ylist_i, const do
 {
     (void)cglist; (void)idxz; (void)idxb_block; (void)idxu_block; (void)idxcg_block; (void)idxu_max; (void)idxz_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (nelements != 1) { set_error("multi-element SNAP is not supported"); return; }
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
     if (idxb_max != mdp_snap_ncoeff(twojmax)) { set_error("idxb_max %d does not match twojmax %d", idxb_max, twojmax); return; }
-    ref_snap_yi_beta(ylist_r, ylist_i, Utotr, Utoti, beta, twojmax, bnorm_flag, inum, 0);
+    if (nelements > 1)
+        ref_snap_yi_me(ylist_r, ylist_i, Utotr, Utoti, beta, 1, twojmax, nelements, 0, bnorm_flag, inum, 0);
+    else
+        ref_snap_yi_beta(ylist_r, ylist_i, Utotr, Utoti, beta, twojmax, bnorm_flag, inum, 0);
 }
 
 void mdp_gpu_snap_compute_fi_f64(double *fatom, double *vatom, const double *ylist_r, const double *ylist_i,
@@ -590,13 +955,17 @@ void mdp_gpu_snap_compute_fi_f64(double *fatom, double *vatom, const double *yli
                                  const int *ti, const int *tj, int twojmax, int idxu_max, int inum, int anum,
                                  int ijnum, int switchflag, int chemflag)
 {
-    (void)rootpqarray; (void)idxu_block; (void)map; (void)idxu_max;
+    (void)rootpqarray; (void)idxu_block; (void)idxu_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag) { set_error("chemflag is not supported"); return; }
     double rcut, wj;
-    if (pair_type_params(ti, tj, ijnum, radelem, wjelem, rcutfac, rcut, wj, 0)) return;
-    ref_snap_fi(fatom, vatom, 0, anum, ylist_r, ylist_i, rij, rcut, wj, rfac0, rmin0, aii, ai, aj, twojmax, inum,
-                ijnum, switchflag, 0);
+    const int several = chemflag ? 1 : pair_type_params(ti, tj, ijnum, radelem, wjelem, rcutfac, rcut, wj, 0);
+    if (several < 0) return;
+    if (several)
+        ref_snap_fi_me(fatom, vatom, 0, anum, ylist_r, ylist_i, rij, radelem, wjelem, rcutfac, rfac0, rmin0, aii, ai,
+                       aj, ti, tj, map, chemflag, twojmax, inum, ijnum, switchflag, 0);
+    else
+        ref_snap_fi(fatom, vatom, 0, anum, ylist_r, ylist_i, rij, rcut, wj, rfac0, rmin0, aii, ai, aj, twojmax, inum,
+                    ijnum, switchflag, 0);
 }
 
 void mdp_gpu_neigh_pair_list_f64(int *pairnum, int *pairlist, const double *x, const double *rcutsq, const int *ilist,
@@ -766,33 +1135,57 @@ void cpuSnapComputeUi(double *Utotr, double *Utoti, double *rootpqarray, double 
                       double rmin0, double rfac0, double rcutfac, int *map, int *aii, int *ti, int *tj, int twojmax,
                       int idxu_max, int inum, int ijnum, int switchflag, int chemflag)
 {
-    (void)rootpqarray; (void)map;
+    (void)rootpqarray;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag) { set_error("chemflag is not supported"); return; }
-    for (int p = 1; p < ijnum; p++)
-        if (ti[p] != ti[0] || tj[p] != tj[0]) { set_error("only a single element type is supported"); return; }
-    const int t = ijnum > 0 ? tj[0] : 1;
-    const double rcut = (radelem[t] + radelem[t]) * rcutfac, wj = wjelem[t];
-    const size_t nu = (size_t)idxu_max * inum;
+    bool several = chemflag != 0;
+    int tmax = 0;
+    for (int p = 0; p < ijnum; p++) {
+        if (ti[p] != ti[0] || tj[p] != tj[0]) several = true;
+        tmax = std::max(tmax, std::max(ti[p], tj[p]));
+    }
+    int nblk = 1;
+    if (chemflag)
+        for (int p = 0; p < ijnum; p++) nblk = std::max(nblk, map[tj[p]] + 1);
+    if (nblk > MAXELEM) { set_error("element block %d out of range", nblk - 1); return; }
+    const size_t nu = (size_t)idxu_max * inum * nblk;
     Stage st;
     double *ur = st.in(Utotr, nu), *ui = st.in(Utoti, nu), *dr = st.in(rij, 3 * (size_t)ijnum);
     int *da = st.in(aii, ijnum);
     if (!st.ok) { set_error("staging failed"); return; }
-    if (ref_snap_ui(ur, ui, dr, rcut, wj, rfac0, rmin0, da, twojmax, inum, ijnum, switchflag, 0)) return;
+    if (several) {
+        double *drad = st.in(radelem, tmax + 1), *dwj = st.in(wjelem, tmax + 1);
+        int *dti = st.in(ti, ijnum), *dtj = st.in(tj, ijnum), *dmap = st.in(map, tmax + 1);
+        if (!st.ok) { set_error("staging failed"); return; }
+        if (ref_snap_ui_me(ur, ui, dr, drad, dwj, rcutfac, rfac0, rmin0, da, dti, dtj, dmap, chemflag, twojmax, inum,
+                           ijnum, switchflag, 0))
+            return;
+    } else {
+        const int t = ijnum > 0 ? tj[0] : 1;
+        const double rcut = (radelem[t] + radelem[t]) * rcutfac, wj = wjelem[t];
+        if (ref_snap_ui(ur, ui, dr, rcut, wj, rfac0, rmin0, da, twojmax, inum, ijnum, switchflag, 0)) return;
+    }
     if (st.out(Utotr, ur, nu) || st.out(Utoti, ui, nu)) set_error("cpuSnapComputeUi copy-back failed");
 }
 
 void cpuAddWself2Ui(double *Utotr, double *Utoti, double wself, int *idxu_block, int *type, int *map,
                     int wselfall_flag, int chemflag, int idxu_max, int nelements, int twojmax, int inum)
 {
-    (void)idxu_block; (void)type; (void)map; (void)wselfall_flag;
+    (void)idxu_block;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag || nelements != 1) { set_error("chemflag / multiple elements are not supported"); return; }
-    const size_t nu = (size_t)idxu_max * inum;
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    const size_t nu = (size_t)idxu_max * inum * nelements;
     Stage st;
     double *ur = st.in(Utotr, nu), *ui = st.in(Utoti, nu);
     if (!st.ok) { set_error("staging failed"); return; }
-    if (ref_snap_wself(ur, ui, wself, twojmax, inum, 0)) return;
+    if (chemflag || nelements != 1) {
+        int tmax = 0;
+        for (int ii = 0; ii < inum; ii++) tmax = std::max(tmax, type[ii]);
+        int *dt = st.in(type, inum), *dm = st.in(map, tmax + 1);
+        if (!st.ok) { set_error("staging failed"); return; }
+        if (ref_snap_wself_me(ur, ui, wself, dt, dm, chemflag, wselfall_flag, nelements, twojmax, inum, 0)) return;
+    } else if (ref_snap_wself(ur, ui, wself, twojmax, inum, 0)) {
+        return;
+    }
     if (st.out(Utotr, ur, nu) || st.out(Utoti, ui, nu)) set_error("cpuAddWself2Ui copy-back failed");
 }
 
@@ -801,17 +1194,37 @@ void cpuSnapComputeEi(double *eatom, double *Utotr, double *Utoti, double *cglis
                       int idxb_max, int idxu_max, int nelements, int ncoeffall, int bnorm_flag, int bzero_flag,
                       int wselfall_flag, int chemflag, int inum)
 {
-    (void)cglist; (void)bzero; (void)map; (void)type; (void)idxb; (void)idxcg_block; (void)idxu_block; (void)idxb_max;
+    (void)cglist; (void)bzero; (void)idxb; (void)idxcg_block; (void)idxu_block;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag || nelements != 1) { set_error("chemflag / multiple elements are not supported"); return; }
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    if (ncoeffall != 1 + idxb_max * nelements * nelements * nelements) {
+        set_error("ncoeffall %d does not match idxb_max %d and %d element blocks", ncoeffall, idxb_max, nelements);
+        return;
+    }
     int emax = 0;
     for (int ii = 0; ii < inum; ii++) emax = std::max(emax, ilist[ii] + 1);
-    const size_t nu = (size_t)idxu_max * inum;
+    // the Julia library picks the coefficient set map[type] with chemflag, set 0 without
+    int ecount = 1, tmax = 0;
+    for (int ii = 0; ii < inum; ii++) tmax = std::max(tmax, type[ii]);
+    if (chemflag)
+        for (int ii = 0; ii < inum; ii++) ecount = std::max(ecount, map[type[ii]] + 1);
+    const size_t nu = (size_t)idxu_max * inum * nelements;
     Stage st;
     double *ur = st.in(Utotr, nu), *ui = st.in(Utoti, nu), *de = st.in(eatom, emax);
     int *dil = st.in(ilist, inum);
     if (!st.ok) { set_error("staging failed"); return; }
-    if (ref_snap_ei(de, ur, ui, coeffelem, dil, twojmax, ncoeffall, bnorm_flag, bzero_flag, wselfall_flag, inum, 0)) return;
+    if (nelements > 1 || ecount > 1) {
+        double *dc = st.in(coeffelem, (size_t)ecount * ncoeffall);
+        int *dt = st.in(type, inum), *dm = st.in(map, tmax + 1);
+        if (!st.ok) { set_error("staging failed"); return; }
+        if (atom_elements(dt, dm, inum, chemflag, 0) < 0 ||
+            ref_snap_ei_me(de, ur, ui, dc, dil, twojmax, nelements, ncoeffall, bnorm_flag, bzero_flag, wselfall_flag,
+                           inum, 0))
+            return;
+    } else if (ref_snap_ei(de, ur, ui, coeffelem, dil, twojmax, ncoeffall, bnorm_flag, bzero_flag, wselfall_flag,
+                           inum, 0)) {
+        return;
+    }
     if (st.out(eatom, de, emax)) set_error("cpuSnapComputeEi copy-back failed");
 }
 
@@ -820,14 +1233,18 @@ void cpuSnapComputeBi(double *blist, double *Utotr, double *Utoti, double *cglis
                       int idxz_max, int nelements, int bnorm_flag, int bzero_flag, int wselfall_flag, int inum)
 {
     (void)cglist; (void)bzero; (void)idxb; (void)idxcg_block; (void)idxu_block; (void)idxz_block; (void)idxz_max;
-    (void)wselfall_flag;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (nelements != 1) { set_error("multi-element SNAP is not supported"); return; }
-    const size_t nu = (size_t)idxu_max * inum, nb = (size_t)idxb_max * inum;
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    const size_t ntri = (size_t)nelements * nelements * nelements;
+    const size_t nu = (size_t)idxu_max * inum * nelements, nb = (size_t)idxb_max * inum * ntri;
     Stage st;
     double *ur = st.in(Utotr, nu), *ui = st.in(Utoti, nu), *db = st.in(blist, nb);
     if (!st.ok) { set_error("staging failed"); return; }
-    if (ref_snap_bi(db, ur, ui, twojmax, bnorm_flag, bzero_flag, inum, 0)) return;
+    if (nelements > 1) {
+        if (ref_snap_bi_me(db, ur, ui, twojmax, nelements, bnorm_flag, bzero_flag, wselfall_flag, inum, 0)) return;
+    } else if (ref_snap_bi(db, ur, ui, twojmax, bnorm_flag, bzero_flag, inum, 0)) {
+        return;
+    }
     if (st.out(blist, db, nb)) set_error("cpuSnapComputeBi copy-back failed");
 }
 
@@ -836,15 +1253,32 @@ void cpuSnapComputeYi(double *ylist_r, double *ylist_i, double *Utotr, double *U
                       int idxb_max, int idxu_max, int idxz_max, int nelements, int ncoeffall, int bnorm_flag,
                       int chemflag, int inum)
 {
-    (void)cglist; (void)map; (void)type; (void)idxz; (void)idxb_block; (void)idxu_block; (void)idxcg_block;
-    (void)idxb_max; (void)idxz_max;
+    (void)cglist; (void)idxz; (void)idxb_block; (void)idxu_block; (void)idxcg_block; (void)idxz_max;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag || nelements != 1) { set_error("chemflag / multiple elements are not supported"); return; }
-    const size_t nu = (size_t)idxu_max * inum;
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    if (ncoeffall != 1 + idxb_max * nelements * nelements * nelements) {
+        set_error("ncoeffall %d does not match idxb_max %d and %d element blocks", ncoeffall, idxb_max, nelements);
+        return;
+    }
+    // the Julia library picks the coefficient set map[type] with chemflag, set 0 without
+    int ecount = 1, tmax = 0;
+    for (int ii = 0; ii < inum; ii++) tmax = std::max(tmax, type[ii]);
+    if (chemflag)
+        for (int ii = 0; ii < inum; ii++) ecount = std::max(ecount, map[type[ii]] + 1);
+    const size_t nu = (size_t)idxu_max * inum * nelements;
     Stage st;
     double *ur = st.in(Utotr, nu), *ui = st.in(Utoti, nu), *yr = st.alloc<double>(nu), *yi = st.alloc<double>(nu);
     if (!st.ok) { set_error("staging failed"); return; }
-    if (ref_snap_yi(yr, yi, ur, ui, beta, twojmax, ncoeffall, bnorm_flag, inum, 0)) return;
+    if (nelements > 1 || ecount > 1) {
+        double *dc = st.in(beta, (size_t)ecount * ncoeffall);
+        int *dt = st.in(type, inum), *dm = st.in(map, tmax + 1);
+        if (!st.ok) { set_error("staging failed"); return; }
+        if (atom_elements(dt, dm, inum, chemflag, 0) < 0 ||
+            ref_snap_yi_me(yr, yi, ur, ui, dc, 0, twojmax, nelements, ncoeffall, bnorm_flag, inum, 0))
+            return;
+    } else if (ref_snap_yi(yr, yi, ur, ui, beta, twojmax, ncoeffall, bnorm_flag, inum, 0)) {
+        return;
+    }
     if (st.out(ylist_r, yr, nu) || st.out(ylist_i, yi, nu)) set_error("cpuSnapComputeYi copy-back failed");
 }
 
@@ -853,23 +1287,40 @@ void cpuSnapComputeFi(double *fatom, double *vatom, double *ylist_r, double *yli
                       int *ai, int *aj, int *ti, int *tj, int twojmax, int idxu_max, int inum, int anum, int ijnum,
                       int switchflag, int chemflag)
 {
-    (void)rootpqarray; (void)map;
+    (void)rootpqarray;
     std::lock_guard<std::mutex> lk(g_ref_mu);
-    if (chemflag) { set_error("chemflag is not supported"); return; }
-    for (int p = 1; p < ijnum; p++)
-        if (ti[p] != ti[0] || tj[p] != tj[0]) { set_error("only a single element type is supported"); return; }
-    const int t = ijnum > 0 ? tj[0] : 1;
-    const double rcut = (radelem[t] + radelem[t]) * rcutfac, wj = wjelem[t];
+    bool several = chemflag != 0;
+    int tmax = 0;
+    for (int p = 0; p < ijnum; p++) {
+        if (ti[p] != ti[0] || tj[p] != tj[0]) several = true;
+        tmax = std::max(tmax, std::max(ti[p], tj[p]));
+    }
+    int nblk = 1;
+    if (chemflag)
+        for (int p = 0; p < ijnum; p++) nblk = std::max(nblk, map[tj[p]] + 1);
+    if (nblk > MAXELEM) { set_error("element block %d out of range", nblk - 1); return; }
     int fmax = std::max(inum, anum);
     for (int p = 0; p < ijnum; p++) fmax = std::max(fmax, std::max(ai[p], aj[p]) + 1);
-    const size_t nu = (size_t)idxu_max * inum;
+    const size_t nu = (size_t)idxu_max * inum * nblk;
     Stage st;
     double *df = st.in(fatom, 3 * (size_t)fmax), *dv = st.in(vatom, 6 * (size_t)fmax);
     double *yr = st.in(ylist_r, nu), *yi = st.in(ylist_i, nu), *dr = st.in(rij, 3 * (size_t)ijnum);
     int *daii = st.in(aii, ijnum), *dai = st.in(ai, ijnum), *daj = st.in(aj, ijnum);
     if (!st.ok) { set_error("staging failed"); return; }
-    if (ref_snap_fi(df, dv, 1, 0, yr, yi, dr, rcut, wj, rfac0, rmin0, daii, dai, daj, twojmax, inum, ijnum, switchflag, 0))
-        return;
+    if (several) {
+        double *drad = st.in(radelem, tmax + 1), *dwj = st.in(wjelem, tmax + 1);
+        int *dti = st.in(ti, ijnum), *dtj = st.in(tj, ijnum), *dmap = st.in(map, tmax + 1);
+        if (!st.ok) { set_error("staging failed"); return; }
+        if (ref_snap_fi_me(df, dv, 1, 0, yr, yi, dr, drad, dwj, rcutfac, rfac0, rmin0, daii, dai, daj, dti, dtj, dmap,
+                           chemflag, twojmax, inum, ijnum, switchflag, 0))
+            return;
+    } else {
+        const int t = ijnum > 0 ? tj[0] : 1;
+        const double rcut = (radelem[t] + radelem[t]) * rcutfac, wj = wjelem[t];
+        if (ref_snap_fi(df, dv, 1, 0, yr, yi, dr, rcut, wj, rfac0, rmin0, daii, dai, daj, twojmax, inum, ijnum,
+                        switchflag, 0))
+            return;
+    }
     if (st.out(fatom, df, 3 * (size_t)fmax) || st.out(vatom, dv, 6 * (size_t)fmax))
         set_error("cpuSnapComputeFi copy-back failed");
 }

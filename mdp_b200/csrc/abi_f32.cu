@@ -88,6 +88,32 @@ int max_plus_one(const int *ti, const int *tj, long n)
     return h + 1;
 }
 
+// largest map[idx[i]] over i < n, into *out
+__global__ void k_max_mapped(const int *__restrict__ idx, const int *__restrict__ map, long n, int *__restrict__ out)
+{
+    int m = -1;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        m = max(m, map[idx[i]]);
+    atomicMax(out, m);
+}
+
+// 1 + the largest map[idx[i]], i < n (at least 1): the element blocks the pairs
+// reach (idx = tj) or the coefficient sets the atoms use (idx = type); -1 on error
+int mapped_count(const int *idx, const int *map, long n)
+{
+    DevBuf &m = shadows().imax;
+    if (m.ensure(sizeof(int))) return -1;
+    int h = 0;
+    if (cudaMemcpy(m.p, &h, sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+    if (n > 0) {
+        k_max_mapped<<<grid_for(n), 256>>>(idx, map, n, m.as<int>());
+        count_launches(1);
+    }
+    if (cudaMemcpy(&h, m.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (h + 1 > MAXELEM) { set_error("element index %d out of range", h); return -1; }
+    return std::max(h + 1, 1);
+}
+
 }  // namespace
 }  // namespace mdp
 
@@ -102,7 +128,9 @@ void mdp_gpu_snap_compute_ui_f32(float *Utotr, float *Utoti, const float *rootpq
 {
     (void)rootpqarray;
     std::lock_guard<std::mutex> lk(g_f32_mu);
-    const long nu = (long)idxu_max * inum;
+    const int nblk = chemflag ? mapped_count(tj, map, ijnum) : 1;   // U element blocks the pairs reach
+    if (nblk < 1) return;
+    const long nu = (long)idxu_max * inum * nblk;
     const int nt = max_plus_one(ti, tj, ijnum);
     if (nt < 1) { set_error("gpuSnapComputeUi (float): reading the pair types failed"); return; }
     double *ur = widen(0, Utotr, nu), *ui = widen(1, Utoti, nu), *dr = widen(2, rij, 3L * ijnum);
@@ -119,6 +147,7 @@ void mdp_gpu_add_wself2ui_f32(float *Utotr, float *Utoti, float wself, const int
                               int nelements, int twojmax, int inum)
 {
     std::lock_guard<std::mutex> lk(g_f32_mu);
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
     const long nu = (long)idxu_max * nelements * inum;
     double *ur = widen(0, Utotr, nu), *ui = widen(1, Utoti, nu);
     if (!ur || !ui) return;
@@ -138,11 +167,15 @@ void mdp_gpu_snap_compute_ei_f32(float *eatom, const float *Utotr, const float *
 {
     (void)cglist; (void)bzero;
     std::lock_guard<std::mutex> lk(g_f32_mu);
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
     const long nu = (long)idxu_max * nelements * inum;
     const int ne = max_plus_one(ilist, ilist, inum);
     if (ne < 1) { set_error("gpuSnapComputeEi (float): reading ilist failed"); return; }
+    // coefficient sets map[type] (one per element even when nelements is 1 without chemflag)
+    const int nsets = std::max(nelements, mapped_count(type, map, inum));
+    if (nsets < 1) return;
     double *e = widen(0, eatom, ne), *ur = widen(1, Utotr, nu), *ui = widen(2, Utoti, nu);
-    double *c = widen(3, coeffelem, (long)ncoeffall * nelements);
+    double *c = widen(3, coeffelem, (long)ncoeffall * nsets);
     if (!e || !ur || !ui || !c) return;
     mdp_gpu_snap_compute_ei_f64(e, ur, ui, nullptr, nullptr, c, ilist, map, type, idxb, idxcg_block, idxu_block,
                                 twojmax, idxb_max, idxu_max, nelements, ncoeffall, bnorm_flag, bzero_flag,
@@ -157,7 +190,9 @@ void mdp_gpu_snap_compute_bi_f32(float *blist, const float *Utotr, const float *
 {
     (void)cglist; (void)bzero;
     std::lock_guard<std::mutex> lk(g_f32_mu);
-    const long nu = (long)idxu_max * nelements * inum, nb = (long)idxb_max * inum;
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
+    const long nu = (long)idxu_max * nelements * inum;
+    const long nb = (long)idxb_max * inum * nelements * nelements * nelements;   // [triple][k][inum]
     double *b = widen(0, nullptr, nb), *ur = widen(1, Utotr, nu), *ui = widen(2, Utoti, nu);
     if (!b || !ur || !ui) return;
     mdp_gpu_snap_compute_bi_f64(b, ur, ui, nullptr, nullptr, idxb, idxcg_block, idxu_block, idxz_block, twojmax,
@@ -173,9 +208,12 @@ void mdp_gpu_snap_compute_yi_f32(float *ylist_r, float *ylist_i, const float *Ut
 {
     (void)cglist;
     std::lock_guard<std::mutex> lk(g_f32_mu);
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
     const long nu = (long)idxu_max * nelements * inum;
+    const int nsets = std::max(nelements, mapped_count(type, map, inum));
+    if (nsets < 1) return;
     double *yr = widen(0, nullptr, nu), *yi = widen(1, nullptr, nu), *ur = widen(2, Utotr, nu),
-           *ui = widen(3, Utoti, nu), *c = widen(4, coeffelem, (long)ncoeffall * nelements);
+           *ui = widen(3, Utoti, nu), *c = widen(4, coeffelem, (long)ncoeffall * nsets);
     if (!yr || !yi || !ur || !ui || !c) return;
     mdp_gpu_snap_compute_yi_f64(yr, yi, ur, ui, nullptr, c, map, type, idxz, idxb_block, idxu_block, idxcg_block,
                                 twojmax, idxb_max, idxu_max, idxz_max, nelements, ncoeffall, bnorm_flag, inum);
@@ -190,9 +228,11 @@ void mdp_gpu_snap_compute_yi_beta_f32(float *ylist_r, float *ylist_i, const floa
 {
     (void)cglist;
     std::lock_guard<std::mutex> lk(g_f32_mu);
+    if (nelements < 1 || nelements > MAXELEM) { set_error("nelements %d out of range", nelements); return; }
     const long nu = (long)idxu_max * nelements * inum;
     double *yr = widen(0, nullptr, nu), *yi = widen(1, nullptr, nu), *ur = widen(2, Utotr, nu),
-           *ui = widen(3, Utoti, nu), *b = widen(4, beta, (long)idxb_max * inum);
+           *ui = widen(3, Utoti, nu),
+           *b = widen(4, beta, (long)idxb_max * inum * nelements * nelements * nelements);
     if (!yr || !yi || !ur || !ui || !b) return;
     mdp_gpu_snap_compute_yi_beta_f64(yr, yi, ur, ui, nullptr, b, idxz, idxb_block, idxu_block, idxcg_block, twojmax,
                                      idxb_max, idxu_max, idxz_max, nelements, bnorm_flag, inum);
@@ -210,7 +250,9 @@ void mdp_gpu_snap_compute_fi_f32(float *fatom, float *vatom, const float *ylist_
 {
     (void)rootpqarray;
     std::lock_guard<std::mutex> lk(g_f32_mu);
-    const long nu = (long)idxu_max * inum;
+    const int nblk = chemflag ? mapped_count(tj, map, ijnum) : 1;   // Y element blocks the pairs read
+    if (nblk < 1) return;
+    const long nu = (long)idxu_max * inum * nblk;
     const int nt = max_plus_one(ti, tj, ijnum);
     if (nt < 1) { set_error("gpuSnapComputeFi (float): reading the pair types failed"); return; }
     double *f = widen(0, fatom, 3L * anum), *v = widen(1, vatom, 6L * anum), *yr = widen(2, ylist_r, nu),

@@ -468,6 +468,7 @@ static int force_compute_me(ForcePath &fp, const SnapModel &m, int precision, co
     A.wselfall = m.p.wselfallflag;
     A.elem = fp.elem.as<int>();
     A.coeff = fp.ecoef.as<double>();
+    A.pa = 0;
     const int rc = m.p.twojmax == 8   ? launch_snap_me<8>(m, fp, inum, nm, eatom, A, s)
                    : m.p.twojmax == 6 ? launch_snap_me<6>(m, fp, inum, nm, eatom, A, s)
                                       : launch_snap_me<4>(m, fp, inum, nm, eatom, A, s);

@@ -190,11 +190,14 @@ constexpr int UI_WARPS = 4;
 
 // REF = true: no wself/mirror; the computed rows are added into the reference's
 // layout Ur/Ui[k * natoms + atom] (cpuSnapComputeUi semantics, cpuSnap4.cpp:11-187)
+// With pcw, each pair's cutoff and neighbour weight come from pcw[p]; with
+// iblk, atom i is row i % iblk of element block i / iblk of the reference's
+// [block][k][iblk] layout (chemflag U, cpuSnap4.cpp:59-61).
 template <typename T, int TJ, bool REF = false>
 __global__ void __launch_bounds__(UI_WARPS * 32)
 k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int natoms, SnapGeom gp,
           typename cplx<T>::type *__restrict__ Ut, double *__restrict__ Uref_r = nullptr,
-          double *__restrict__ Uref_i = nullptr)
+          double *__restrict__ Uref_i = nullptr, const double2 *__restrict__ pcw = nullptr, int iblk = 0)
 {
     typedef typename cplx<T>::type T2;
     constexpr int NU = idxu_count(TJ);
@@ -215,7 +218,13 @@ k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int na
             const int nact = min(32, p1 - base);
             const double4 r = act ? prij[p] : make_double4(1.0, 0.0, 0.0, 0.0);
             PairGeo g;
-            pair_geometry<false>(g, r.x, r.y, r.z, gp);
+            if (pcw) {
+                SnapGeom ge = gp;
+                if (act) { ge.rcut = pcw[p].x; ge.wj = pcw[p].y; }
+                pair_geometry<false>(g, r.x, r.y, r.z, ge);
+            } else {
+                pair_geometry<false>(g, r.x, r.y, r.z, gp);
+            }
             const T sf = act ? (T)g.sfac : T(0);
             ssum += sf;
             auto emit = [&](int j, int mb, const T *pr, const T *pi) {
@@ -239,13 +248,15 @@ k_snap_ui(const int *__restrict__ poff, const double4 *__restrict__ prij, int na
         if (lane == 0) acc[0].x += ssum;
         __syncwarp();
         if constexpr (REF) {
+            const int nrow = iblk > 0 ? iblk : natoms;
+            const size_t base = (size_t)(i / nrow) * NU * nrow + (i % nrow);
             for (int k = lane; k < NU; k += 32) {
                 int j = 0;
                 while (idxu_block(j + 1) <= k) j++;
                 const int mb = (k - idxu_block(j)) / (j + 1);
                 if (2 * mb <= j) {
-                    Uref_r[(size_t)k * natoms + i] += (double)acc[k].x;
-                    Uref_i[(size_t)k * natoms + i] += (double)acc[k].y;
+                    Uref_r[base + (size_t)k * nrow] += (double)acc[k].x;
+                    Uref_i[base + (size_t)k * nrow] += (double)acc[k].y;
                 }
             }
             __syncwarp();
@@ -893,8 +904,9 @@ struct MeArgs {
     int ntiles;            // tiles of 32 atoms per block
     int ncoeffall;         // coefficients per element
     int bzero, wselfall;   // bzeroflag, wselfallflag
-    const int *elem;       // element index (type - 1) of each atom [inum]
-    const double *coeff;   // coeffelem [nelements][ncoeffall]
+    const int *elem;       // element index (map[type]) of each atom [inum]
+    const double *coeff;   // coeffelem [nelements][ncoeffall], or with pa the
+    int pa;                // per-atom coefficients [triple][k][inum] (cpuSnap4.cpp:601-691)
 };
 
 // Per-atom energy: beta_0(e_i) + sum over element triples t = (e1 e2 e3) and
@@ -949,8 +961,8 @@ k_snap_ei_me(const double2 *__restrict__ Ut, int natoms, int bnorm, const __grid
 template <int TJ, int J, int J1, int J2>
 __device__ __forceinline__ void z_layer_me(const int mb, const int o, const int st, const double2 *__restrict__ U1,
                                            const double2 *__restrict__ U2, const int lane,
-                                           const YParams<double> &P, const double *__restrict__ cl, const int tA,
-                                           const int tB, const int tC, YRow<double> &acc)
+                                           const YParams<double> &P, const double *__restrict__ cl, const int cs,
+                                           const int tA, const int tB, const int tC, YRow<double> &acc)
 {
     constexpr int NK = nbispec(TJ);
     if constexpr (J1 <= TJ) {
@@ -958,12 +970,12 @@ __device__ __forceinline__ void z_layer_me(const int mb, const int o, const int 
             if constexpr (coupling_ok(J1, J2, J)) {
                 constexpr int TRI = tri_index(J1, J2, J);
                 const int t = (J >= J1) ? tA : (J >= J2) ? tB : tC;
-                const double beta = P.betaY[TRI] * cl[t * NK + P.kmap[TRI]];
+                const double beta = P.betaY[TRI] * cl[(size_t)(t * NK + P.kmap[TRI]) * cs];
                 z_rows<double, J1, J2, J>(mb, o, st, U1, U2, lane, beta, acc);
             }
-            z_layer_me<TJ, J, J1, J2 + 1>(mb, o, st, U1, U2, lane, P, cl, tA, tB, tC, acc);
+            z_layer_me<TJ, J, J1, J2 + 1>(mb, o, st, U1, U2, lane, P, cl, cs, tA, tB, tC, acc);
         } else {
-            z_layer_me<TJ, J, J1 + 1, 0>(mb, o, st, U1, U2, lane, P, cl, tA, tB, tC, acc);
+            z_layer_me<TJ, J, J1 + 1, 0>(mb, o, st, U1, U2, lane, P, cl, cs, tA, tB, tC, acc);
         }
     }
 }
@@ -971,7 +983,8 @@ __device__ __forceinline__ void z_layer_me(const int mb, const int o, const int 
 template <int TJ, int NW, int J>
 __device__ __forceinline__ void y_all_me(const double2 *__restrict__ Ut, const int tile, double2 *__restrict__ red,
                                          double2 *__restrict__ Y, const int lane, const int w,
-                                         const YParams<double> &P, const MeArgs &A, const double *__restrict__ cl)
+                                         const YParams<double> &P, const MeArgs &A, const double *__restrict__ cl,
+                                         const int cs)
 {
     if constexpr (J >= 0) {
         constexpr int NU = idxu_count(TJ), NYH = yh_count(TJ);
@@ -985,7 +998,7 @@ __device__ __forceinline__ void y_all_me(const double2 *__restrict__ Ut, const i
                     for (int e2 = 0; e2 < nb; e2++)
                         z_layer_me<TJ, J, 0, 0>(mb, P.lay_o[J][w], P.lay_st[J][w],
                                                 Ut + ((size_t)e1 * A.ntiles + tile) * NU * 32,
-                                                Ut + ((size_t)e2 * A.ntiles + tile) * NU * 32, lane, P, cl,
+                                                Ut + ((size_t)e2 * A.ntiles + tile) * NU * 32, lane, P, cl, cs,
                                                 (e1 * nb + e2) * nb + e3, (e3 * nb + e2) * nb + e1,
                                                 (e2 * nb + e3) * nb + e1, acc);
 #pragma unroll
@@ -1007,7 +1020,7 @@ __device__ __forceinline__ void y_all_me(const double2 *__restrict__ Ut, const i
             }
             __syncthreads();
         }
-        y_all_me<TJ, NW, J - 1>(Ut, tile, red, Y, lane, w, P, A, cl);
+        y_all_me<TJ, NW, J - 1>(Ut, tile, red, Y, lane, w, P, A, cl, cs);
     }
 }
 
@@ -1028,8 +1041,40 @@ k_snap_yi_me(const double2 *__restrict__ Ut, int natoms, const __grid_constant__
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x) {
         const int atom = tile * 32 + lane;
-        const int ie = atom < natoms ? A.elem[atom] : 0;
-        y_all_me<TJ, NW, TJ>(Ut, tile, red, Y, lane, w, P, A, A.coeff + (size_t)ie * A.ncoeffall + 1);
+        if (A.pa) {
+            y_all_me<TJ, NW, TJ>(Ut, tile, red, Y, lane, w, P, A, A.coeff + (atom < natoms ? atom : 0), natoms);
+        } else {
+            const int ie = atom < natoms ? A.elem[atom] : 0;
+            y_all_me<TJ, NW, TJ>(Ut, tile, red, Y, lane, w, P, A, A.coeff + (size_t)ie * A.ncoeffall + 1, 1);
+        }
+    }
+}
+
+// Per-atom bispectrum of every element triple t = (e1 e2 e3):
+// bout[(t * NK + k) * natoms + atom] (cpuSnapComputeBi, cpuSnap4.cpp:427-592),
+// bzero on t = (e e e) only unless wselfallflag
+template <int TJ>
+__global__ void __launch_bounds__(BI_WARPS * 32, 1)
+k_snap_bi_me(const double2 *__restrict__ Ut, int natoms, int bnorm, const __grid_constant__ MeArgs A,
+             double *__restrict__ bout)
+{
+    constexpr int NU = idxu_count(TJ), NK = nbispec(TJ);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int nb = A.nblk;
+    for (int tile = blockIdx.x; tile < A.ntiles; tile += gridDim.x) {
+        BiArgs<double> a{nullptr, nullptr, nullptr, lane, w, tile * 32 + lane, natoms, bnorm, 0, nullptr,
+                         natoms, nullptr, 0.0};
+        for (int e1 = 0; e1 < nb; e1++)
+            for (int e2 = 0; e2 < nb; e2++)
+                for (int e3 = 0; e3 < nb; e3++) {
+                    const int t = (e1 * nb + e2) * nb + e3;
+                    a.U1 = Ut + ((size_t)e1 * A.ntiles + tile) * NU * 32;
+                    a.U2 = Ut + ((size_t)e2 * A.ntiles + tile) * NU * 32;
+                    a.U3 = Ut + ((size_t)e3 * A.ntiles + tile) * NU * 32;
+                    a.bzero = A.bzero && (A.wselfall || (e1 == e2 && e2 == e3));
+                    a.bout = bout + (size_t)t * NK * natoms;
+                    b_triples<double, TJ, 0, 0, 0, 0>(a);
+                }
     }
 }
 

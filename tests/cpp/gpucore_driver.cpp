@@ -78,7 +78,7 @@ int fail(char *msg, const char *what)
 
 }  // namespace
 
-extern "C" int gpucore_pair_snap3(
+static int pair_snap3(
     // outputs (host): eatom[inum], fatom[3 inum], vatom[6 inum]
     dstype *eatom_h, dstype *fatom_h, dstype *vatom_h,
     // configuration (host, the reference layouts)
@@ -90,9 +90,12 @@ extern "C" int gpucore_pair_snap3(
     int idxu_max, const int *idxcg_block_h, int nblock3, const dstype *bzero_h, const dstype *coeffelem_h,
     int ncoeffall, const int *map_h, const dstype *radelem_h, const dstype *wjelem_h, dstype rmin0, dstype rfac0,
     dstype rcutfac, dstype wself, int twojmax, int switchflag, int bzeroflag, int bnormflag, int wselfallflag,
-    int nblocks, char *msg)
+    int nblocks, int chemflag, char *msg)
 {
-    const int dim = 3, backend = 2, chemflag = 0, quadraticflag = 0, nelements = 1, nelem = 1;
+    // InitSnap (snappotential.cpp:186-221): ntypes = nelements; U / Y element
+    // blocks only with chemflag; coeffelem holds nelements x ncoeffall values
+    const int dim = 3, backend = 2, quadraticflag = 0, nelements = ntypes;
+    const int nelem = chemflag ? nelements : 1;
     const int jd = twojmax + 1;
     Dev x, atomtype, alist, neighlist, neighnum, rcutsq, rootpq, cglist, idxz, idxz_block, idxb, idxb_block,
         idxu_block, idxcg_block, bzero, coeffelem, map, radelem, wjelem, eatom, fatom, vatom;
@@ -104,7 +107,7 @@ extern "C" int gpucore_pair_snap3(
         up(idxz, idxz_h, sizeof(int) * 10 * idxz_max) || up(idxz_block, idxz_block_h, sizeof(int) * nblock3) ||
         up(idxb, idxb_h, sizeof(int) * 3 * idxb_max) || up(idxb_block, idxb_block_h, sizeof(int) * nblock3) ||
         up(idxu_block, idxu_block_h, sizeof(int) * jd) || up(idxcg_block, idxcg_block_h, sizeof(int) * nblock3) ||
-        up(bzero, bzero_h, sizeof(dstype) * jd) || up(coeffelem, coeffelem_h, sizeof(dstype) * ncoeffall) ||
+        up(bzero, bzero_h, sizeof(dstype) * jd) || up(coeffelem, coeffelem_h, sizeof(dstype) * ncoeffall * nelements) ||
         up(map, map_h, sizeof(int) * (ntypes + 1)) || up(radelem, radelem_h, sizeof(dstype) * (ntypes + 1)) ||
         up(wjelem, wjelem_h, sizeof(dstype) * (ntypes + 1)) || up(eatom, nullptr, sizeof(dstype) * inum) ||
         up(fatom, nullptr, sizeof(dstype) * 3 * inum) || up(vatom, nullptr, sizeof(dstype) * 6 * inum))
@@ -130,7 +133,7 @@ extern "C" int gpucore_pair_snap3(
         const int ineighmax = IntArrayGetValueAtIndex(pairnumsum.as<int>(), na, backend);
         if (ineighmax < 0 || ineighmax > na * neighmax) return fail(msg, "pair count out of range");
         Dev ai, aj, ti, tj, aii, rij, ur, ui, yr, yi;
-        const size_t nu = (size_t)idxu_max * nelements * na;
+        const size_t nu = (size_t)idxu_max * nelem * na;
         if (up(ai, nullptr, sizeof(int) * ineighmax) || up(aj, nullptr, sizeof(int) * ineighmax) ||
             up(ti, nullptr, sizeof(int) * ineighmax) || up(tj, nullptr, sizeof(int) * ineighmax) ||
             up(aii, nullptr, sizeof(int) * ineighmax) || up(rij, nullptr, sizeof(dstype) * dim * ineighmax) ||
@@ -165,4 +168,47 @@ extern "C" int gpucore_pair_snap3(
         cudaMemcpy(vatom_h, vatom.p, sizeof(dstype) * 6 * inum, cudaMemcpyDeviceToHost) != cudaSuccess)
         return fail(msg, "download");
     return 0;
+}
+
+// one element type (the reference's Ta examples)
+extern "C" int gpucore_pair_snap3(dstype *eatom_h, dstype *fatom_h, dstype *vatom_h, const dstype *x_h,
+                                  const int *atomtype_h, const int *alist_h, const int *neighlist_h,
+                                  const int *neighnum_h, int inum, int anum, int neighmax, const dstype *rcutsq_h,
+                                  int ntypes, const dstype *rootpq_h, int nrootpq, const dstype *cglist_h,
+                                  int idxcg_max, const int *idxz_h, int idxz_max, const int *idxz_block_h,
+                                  const int *idxb_h, int idxb_max, const int *idxb_block_h, const int *idxu_block_h,
+                                  int idxu_max, const int *idxcg_block_h, int nblock3, const dstype *bzero_h,
+                                  const dstype *coeffelem_h, int ncoeffall, const int *map_h, const dstype *radelem_h,
+                                  const dstype *wjelem_h, dstype rmin0, dstype rfac0, dstype rcutfac, dstype wself,
+                                  int twojmax, int switchflag, int bzeroflag, int bnormflag, int wselfallflag,
+                                  int nblocks, char *msg)
+{
+    return pair_snap3(eatom_h, fatom_h, vatom_h, x_h, atomtype_h, alist_h, neighlist_h, neighnum_h, inum, anum,
+                      neighmax, rcutsq_h, ntypes, rootpq_h, nrootpq, cglist_h, idxcg_max, idxz_h, idxz_max,
+                      idxz_block_h, idxb_h, idxb_max, idxb_block_h, idxu_block_h, idxu_max, idxcg_block_h, nblock3,
+                      bzero_h, coeffelem_h, ncoeffall, map_h, radelem_h, wjelem_h, rmin0, rfac0, rcutfac, wself,
+                      twojmax, switchflag, bzeroflag, bnormflag, wselfallflag, nblocks, 0, msg);
+}
+
+// several element types: ntypes = nelements, types 1..nelements in atomtype,
+// map[t] = t - 1, chemflag 0 or 1
+extern "C" int gpucore_pair_snap3_elements(dstype *eatom_h, dstype *fatom_h, dstype *vatom_h, const dstype *x_h,
+                                           const int *atomtype_h, const int *alist_h, const int *neighlist_h,
+                                           const int *neighnum_h, int inum, int anum, int neighmax,
+                                           const dstype *rcutsq_h, int ntypes, const dstype *rootpq_h, int nrootpq,
+                                           const dstype *cglist_h, int idxcg_max, const int *idxz_h, int idxz_max,
+                                           const int *idxz_block_h, const int *idxb_h, int idxb_max,
+                                           const int *idxb_block_h, const int *idxu_block_h, int idxu_max,
+                                           const int *idxcg_block_h, int nblock3, const dstype *bzero_h,
+                                           const dstype *coeffelem_h, int ncoeffall, const int *map_h,
+                                           const dstype *radelem_h, const dstype *wjelem_h, dstype rmin0,
+                                           dstype rfac0, dstype rcutfac, dstype wself, int twojmax, int switchflag,
+                                           int bzeroflag, int bnormflag, int wselfallflag, int nblocks, int chemflag,
+                                           char *msg)
+{
+    return pair_snap3(eatom_h, fatom_h, vatom_h, x_h, atomtype_h, alist_h, neighlist_h, neighnum_h, inum, anum,
+                      neighmax, rcutsq_h, ntypes, rootpq_h, nrootpq, cglist_h, idxcg_max, idxz_h, idxz_max,
+                      idxz_block_h, idxb_h, idxb_max, idxb_block_h, idxu_block_h, idxu_max, idxcg_block_h, nblock3,
+                      bzero_h, coeffelem_h, ncoeffall, map_h, radelem_h, wjelem_h, rmin0, rfac0, rcutfac, wself,
+                      twojmax, switchflag, bzeroflag, bnormflag, wselfallflag, nblocks, chemflag, msg);
 }

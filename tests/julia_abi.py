@@ -150,3 +150,61 @@ def descriptor_sequence(L, g, p, quadratic=0):
     L.cpuSnapTallyBispectrumVirial(bv, bl, dbl, rij, ai, ti, n, ij, nb, nper, 1, quadratic)
     return dict(ulist=(ur, ui), dulist=(dur, dui), sij=tuple(s8), utot=(utr, uti), zlist=(zr, zi), blist=bl,
                 dblist=dbl, bi=bi, bd=bd, bv=bv)
+
+
+def snap_sequence_elements(L, g, p):
+    """The same call sequence for a multi-element fixture (tests/golden/chem_*.npz):
+    types 1..nelements (owners' types through alist for ghosts), map[t] = t - 1,
+    type-pair cutoffs (radelem_i + radelem_j) rcutfac, element blocks of U and
+    Y when chemflag is set.  Returns every stage's output."""
+    tj = p.twojmax
+    t = tables(L, tj)
+    ne = p.nelements
+    chem = int(p.chemflag)
+    nelem = ne if chem else 1
+    x = np.ascontiguousarray(g["xall"]).ravel()
+    n = g["x"].shape[0]
+    nl, nn = g["neighlist"], g["neighnum"]
+    csr = np.zeros(n + 1, dtype=np.int32); csr[1:] = np.cumsum(nn)
+    flat = np.concatenate([nl[i, : nn[i]] for i in range(n)]).astype(np.int32)
+    ilist = np.arange(n, dtype=np.int32)
+    alist = np.ascontiguousarray(g["alist"], dtype=np.int32)
+    atype = np.ascontiguousarray(g["types"][alist], dtype=np.int32)
+    rad = np.concatenate([[0.0], p.radelems]); wj = np.concatenate([[0.0], p.wjelems])
+    mp = np.concatenate([[0], np.arange(ne)]).astype(np.int32)
+    rcutsq = np.zeros((ne + 1) ** 2)
+    for a in range(ne):
+        for b in range(ne):
+            rcutsq[b + 1 + (a + 1) * (ne + 1)] = ((p.radelems[a] + p.radelems[b]) * p.rcutfac) ** 2
+    pairnum = np.zeros(n, dtype=np.int32)
+    pairlist = np.zeros(flat.size + 1, dtype=np.int32)
+    L.cpuNeighPairList(pairnum, pairlist, x, rcutsq, ilist, flat, csr, atype, alist, n, 3, ne)
+    pns = np.zeros(n + 1, dtype=np.int32); pns[1:] = np.cumsum(pairnum)
+    ij = int(pns[-1])
+    rij = np.zeros(3 * ij); aii = np.zeros(ij, dtype=np.int32); ai = np.zeros(ij, dtype=np.int32)
+    aj = np.zeros(ij, dtype=np.int32); ti = np.zeros(ij, dtype=np.int32); tjv = np.zeros(ij, dtype=np.int32)
+    L.cpuNeighPairs(rij, x, aii, ai, aj, ti, tjv, pairlist, pns, ilist, atype, alist, n, 3)
+    nu = t["nu"]
+    ur = np.zeros(n * nu * nelem); ui = np.zeros(n * nu * nelem)
+    L.cpuSnapComputeUi(ur, ui, t["rootpq"], rij, wj, rad, p.rmin0, p.rfac0, p.rcutfac, mp, aii, ti, tjv,
+                       tj, nu, n, ij, p.switchflag, chem)
+    u_pairs = (ur.copy(), ui.copy())
+    ltype = np.ascontiguousarray(atype[:n])
+    L.cpuAddWself2Ui(ur, ui, 1.0, t["idxu_block"], ltype, mp, p.wselfallflag, chem, nu, nelem, tj, n)
+    bzero = np.array([1.0 if p.bnormflag else j + 1.0 for j in range(tj + 1)])
+    coeff = np.ascontiguousarray(p.coeff)
+    e = np.zeros(n)
+    L.cpuSnapComputeEi(e, ur, ui, t["cg"], bzero, coeff, ilist, mp, ltype, t["idxb"], t["idxcg_block"],
+                       t["idxu_block"], tj, t["nb"], nu, nelem, p.ncoeffall, p.bnormflag, p.bzeroflag,
+                       p.wselfallflag, chem, n)
+    b = np.zeros(n * t["nb"] * nelem ** 3)
+    L.cpuSnapComputeBi(b, ur, ui, t["cg"], bzero, t["idxb"], t["idxcg_block"], t["idxu_block"], t["idxz_block"],
+                       tj, t["nb"], nu, t["nz"], nelem, p.bnormflag, p.bzeroflag, p.wselfallflag, n)
+    yr = np.zeros(n * nu * nelem); yi = np.zeros(n * nu * nelem)
+    L.cpuSnapComputeYi(yr, yi, ur, ui, t["cg"], coeff, mp, ltype, t["idxz"], t["idxb_block"], t["idxu_block"],
+                       t["idxcg_block"], tj, t["nb"], nu, t["nz"], nelem, p.ncoeffall, p.bnormflag, chem, n)
+    f = np.zeros(3 * n); v = np.zeros(6 * n)
+    L.cpuSnapComputeFi(f, v, yr, yi, t["rootpq"], rij, wj, rad, p.rmin0, p.rfac0, p.rcutfac, mp, aii, ai, aj,
+                       ti, tjv, tj, nu, n, n, ij, p.switchflag, chem)
+    return dict(pairnum=pairnum, pairlist=pairlist[:ij], rij=rij, u_pairs=u_pairs, u=(ur, ui), eatom=e, blist=b,
+                y=(yr, yi), fatom=f, vatom=v)

@@ -62,3 +62,34 @@ def test_descriptor_chain_matches_reference_library(cuda_lib, name, quadratic):
     dur = a["dulist"][0].reshape(3, -1)
     assert np.count_nonzero(dur) < dur.size
     assert np.array_equal(b["dulist"][0] == 0.0, a["dulist"][0] == 0.0)
+
+
+CHEM = ["chem_bcc128_2j6", "chem_bcc250_2j8", "chem_bcc54_2j4_3el_flags", "chem_bcc54_2j6_wselfall",
+        "chem_bcc128_2j8_chemflag0"]
+
+
+@pytest.mark.parametrize("name", CHEM)
+def test_julia_abi_several_elements_match_reference_library(cuda_lib, name):
+    """Several element types through the cpuSnap.h stages: U per element block,
+    wself per block, element-triple energies and bispectrum, Y per block, dE/dr
+    with per-pair cutoffs, on the reference library and on ours."""
+    from mdp_b200 import _lib, configs
+    ref = os.path.join(refpy.REF_DIR, "libcpuSnap_ref.so")
+    if not os.path.exists(ref):
+        pytest.fail("oracle/_ref/libcpuSnap_ref.so missing (build with make -C oracle ref)")
+    g = load_golden(name)
+    bnorm, bzero, switch, wsa = (int(v) for v in g["flags"])
+    p = configs.snap_params_elements(int(g["twojmax"]), g["radelems"], g["wjelems"], chemflag=int(g["chemflag"]),
+                                     seed=int(g["coeff_seed"]), bnormflag=bnorm, bzeroflag=bzero,
+                                     switchflag=switch, wselfallflag=wsa)
+    a = julia_abi.snap_sequence_elements(julia_abi.bind(ref), g, p)
+    b = julia_abi.snap_sequence_elements(julia_abi.bind(_lib.LIB_PATH), g, p)
+    assert np.array_equal(a["pairnum"], b["pairnum"]) and np.array_equal(a["pairlist"], b["pairlist"])
+    for k in (0, 1):
+        assert rel_inf(b["u_pairs"][k], a["u_pairs"][k]) < 1e-12
+        assert rel_inf(b["u"][k], a["u"][k]) < 1e-12
+        assert rel_inf(b["y"][k], a["y"][k]) < 1e-10
+    assert rel_inf(b["eatom"], a["eatom"]) < 1e-12
+    assert rel_inf(b["blist"], a["blist"]) < 1e-10
+    assert rel_inf(b["fatom"], a["fatom"]) < 1e-10
+    assert rel_inf(b["vatom"], a["vatom"]) < 1e-10
