@@ -24,13 +24,13 @@ unsigned blocks_for(long n) { return (unsigned)std::max<long>(1, (n + TB - 1) / 
 
 // correctly rounded arithmetic without contraction, in the precision of the
 // reference build (double, or float for PREC_FLOAT builds of MDP)
-__device__ __forceinline__ double add_rn(double a, double b) { return add_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ double sub_rn(double a, double b) { return sub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
 __device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ double mul_rn(double a, double b) { return mul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double div_rn(double a, double b) { return div_rn(a, b); }
+__device__ __forceinline__ double div_rn(double a, double b) { return __ddiv_rn(a, b); }
 __device__ __forceinline__ float div_rn(float a, float b) { return __fdiv_rn(a, b); }
 
 // s2rmap * (a, b, c): ((m0 a + m3 b) + m6 c), each product rounded
