@@ -11,7 +11,9 @@
  * this header also defines the reference's gpu* entry points for T = double on
  * top of them, replacing src/C++/Core/gpuSnap4.cu, the pair kernels of
  * gpuSnap.cu, gpuCumsum.cu, gpuNeighborList3D.cu, gpuVelocityIntegration.cu
- * (modes 0, 1 and 2) and gpuDomain.cu's gpuPBC at link time.  Array layouts are
+ * (integrator modes 0, 1 and 2, set-velocity integration and the
+ * velocity-rescaling thermostats), gpuFixes.cu and gpuDomain.cu's gpuPBC at
+ * link time.  Array layouts are
  * the reference's: U/Y [idxu][inum], rij [ijnum][3], fatom [anum][3],
  * vatom [6][anum], x [natom][dim]; with chemflag, U and Y hold one such block
  * per element ([element][idxu][inum], block map[tj] for a pair).  Supported:
@@ -193,6 +195,112 @@ void mdp_gpu_pbc_f32(float *x, float *v, int *image, const float *boxhi, const f
 void mdp_gpu_compute_ke_atom_f32(float *ke, const float *mass, const float *v, float mvv2e, const int *type,
                                  const int *ilist, int dim, int inum);
 void mdp_gpu_array_sum_every_column_f32(float *b, const float *a, int m, int n);
+
+/* ---- force constraints, set-velocity integration, velocity-rescaling
+ * thermostats (mdp_b200/csrc/abi_fix.cu; mdpgpucore.h:303-349).  Device arrays
+ * in the reference's layouts (fix virial vatom [atom][6]); the thermostat's
+ * dtarray, tarray, seed, save and second on the host, ke / tmp device scratch
+ * of inum and 1 values.  Suffix _f64 for double, _f32 for float builds. ---- */
+/* mdpgpucore.h:325-326, gpuFixSetForce */
+void mdp_gpu_fix_set_force_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:327-328, gpuFixLineForce */
+void mdp_gpu_fix_line_force_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:329-330, gpuFixPlaneForce */
+void mdp_gpu_fix_plane_force_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:331-332, gpuFixAveForce */
+void mdp_gpu_fix_ave_force_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:339-340, gpuFixWallReflect */
+void mdp_gpu_fix_wall_reflect_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:341-342, gpuFixWallHarmonic */
+void mdp_gpu_fix_wall_harmonic_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:343-344, gpuFixWallLJ93 */
+void mdp_gpu_fix_wall_lj93_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:345-346, gpuFixWallLJ126 */
+void mdp_gpu_fix_wall_lj126_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:347-348, gpuFixWallLJ1043 */
+void mdp_gpu_fix_wall_lj1043_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:349-350, gpuFixWallMorse */
+void mdp_gpu_fix_wall_morse_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:334-335, gpuFixAddForce (unwrapped positions through image and box) */
+void mdp_gpu_fix_add_force_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const double *box,
+                            const int *iparam, const int *ilist, const int *image, int triclinic, int eflag_atom,
+                            int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:336-337, gpuFixDragForce */
+void mdp_gpu_fix_drag_force_f64(double *x, double *v, double *f, double *eatom, double *vatom, const double *fparam, const double *box,
+                             const int *iparam, const int *ilist, const int *pbc, int triclinic, int eflag_atom,
+                             int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:303-304, gpuSetVelocityInitialIntegrate */
+void mdp_gpu_set_velocity_initial_integrate_f64(double *x, double *v, const double *f, const double *mass, const double *fparam,
+                                             double dtf, double dtv, const int *type, const int *ilist, const int *iparam,
+                                             int dim, int inum);
+/* mdpgpucore.h:306-307, gpuSetVelocityFinalIntegrate */
+void mdp_gpu_set_velocity_final_integrate_f64(double *x, double *v, const double *f, const double *mass, double dtf, const int *type,
+                                           const int *ilist, const int *iparam, int dim, int inum);
+/* mdpgpucore.h:317-319, gpuVelocityRescalingThermostat (mode 0 Berendsen, 1 rescale, 2 CSVR); returns the
+ * updated thermostat energy */
+double mdp_gpu_velocity_rescaling_thermostat_f64(double *v, const double *mass, const double *dtarray, double *tarray, double *ke,
+                                            double *tmp, double *second, double energy, const int *type, const int *ilist,
+                                            int *seed, int *save, int biasflag, int mode, int dim, int inum);
+/* mdpgpucore.h:325-326, gpuFixSetForce */
+void mdp_gpu_fix_set_force_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:327-328, gpuFixLineForce */
+void mdp_gpu_fix_line_force_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:329-330, gpuFixPlaneForce */
+void mdp_gpu_fix_plane_force_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:331-332, gpuFixAveForce */
+void mdp_gpu_fix_ave_force_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:339-340, gpuFixWallReflect */
+void mdp_gpu_fix_wall_reflect_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:341-342, gpuFixWallHarmonic */
+void mdp_gpu_fix_wall_harmonic_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:343-344, gpuFixWallLJ93 */
+void mdp_gpu_fix_wall_lj93_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:345-346, gpuFixWallLJ126 */
+void mdp_gpu_fix_wall_lj126_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:347-348, gpuFixWallLJ1043 */
+void mdp_gpu_fix_wall_lj1043_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:349-350, gpuFixWallMorse */
+void mdp_gpu_fix_wall_morse_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const int *iparam,
+                         const int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:334-335, gpuFixAddForce (unwrapped positions through image and box) */
+void mdp_gpu_fix_add_force_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const float *box,
+                            const int *iparam, const int *ilist, const int *image, int triclinic, int eflag_atom,
+                            int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:336-337, gpuFixDragForce */
+void mdp_gpu_fix_drag_force_f32(float *x, float *v, float *f, float *eatom, float *vatom, const float *fparam, const float *box,
+                             const int *iparam, const int *ilist, const int *pbc, int triclinic, int eflag_atom,
+                             int vflag_atom, int dim, int inum);
+/* mdpgpucore.h:303-304, gpuSetVelocityInitialIntegrate */
+void mdp_gpu_set_velocity_initial_integrate_f32(float *x, float *v, const float *f, const float *mass, const float *fparam,
+                                             float dtf, float dtv, const int *type, const int *ilist, const int *iparam,
+                                             int dim, int inum);
+/* mdpgpucore.h:306-307, gpuSetVelocityFinalIntegrate */
+void mdp_gpu_set_velocity_final_integrate_f32(float *x, float *v, const float *f, const float *mass, float dtf, const int *type,
+                                           const int *ilist, const int *iparam, int dim, int inum);
+/* mdpgpucore.h:317-319, gpuVelocityRescalingThermostat (mode 0 Berendsen, 1 rescale, 2 CSVR); returns the
+ * updated thermostat energy */
+float mdp_gpu_velocity_rescaling_thermostat_f32(float *v, const float *mass, const float *dtarray, float *tarray, float *ke,
+                                            float *tmp, float *second, float energy, const int *type, const int *ilist,
+                                            int *seed, int *save, int biasflag, int mode, int dim, int inum);
 
 /* No counterpart in the reference.  The per-atom bispectrum of
  * mdp_gpu_snap_compute_bi_f64 for callers that must not allocate device memory
@@ -518,6 +626,184 @@ template <> inline void gpuComputeKEAtom<float>(float *ke, float *mass, float *v
 template <> inline void gpuArraySumEveryColumn<float>(float *b, float *a, int m, int n)
 {
     mdp_gpu_array_sum_every_column_f32(b, a, m, n);
+}
+/* force constraints, set-velocity integration, velocity-rescaling thermostats */
+template <typename T> void gpuFixSetForce(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixLineForce(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixPlaneForce(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixAveForce(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixWallReflect(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixWallHarmonic(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixWallLJ93(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixWallLJ126(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixWallLJ1043(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixWallMorse(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixAddForce(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, T *box, int *iparam, int *ilist, int *image, int triclinic, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuFixDragForce(T *x, T *v, T *f, T *eatom, T *vatom, T *fparam, T *box, int *iparam, int *ilist, int *pbc, int triclinic, int eflag_atom, int vflag_atom, int dim, int inum);
+template <typename T> void gpuSetVelocityInitialIntegrate(T *x, T *v, T *f, T *mass, T *fparam, T dtf, T dtv, int *type, int *ilist, int *iparam, int dim, int inum);
+template <typename T> void gpuSetVelocityFinalIntegrate(T *x, T *v, T *f, T *mass, T dtf, int *type, int *ilist, int *iparam, int dim, int inum);
+template <typename T> T gpuVelocityRescalingThermostat(T *v, T *mass, T *dtarray, T *tarray, T *ke, T *tmp, T *second, T energy, int *type, int *ilist, int *seed, int *save, int biasflag, int mode, int dim, int inum);
+template <> inline void gpuFixSetForce<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_set_force_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixLineForce<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_line_force_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixPlaneForce<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_plane_force_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixAveForce<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_ave_force_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallReflect<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_reflect_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallHarmonic<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_harmonic_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallLJ93<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_lj93_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallLJ126<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_lj126_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallLJ1043<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_lj1043_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallMorse<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_morse_f64(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixAddForce<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        double *box, int *iparam, int *ilist, int *image, int triclinic, int eflag_atom, int vflag_atom, int dim,
+        int inum)
+{
+    mdp_gpu_fix_add_force_f64(x, v, f, eatom, vatom, fparam, box, iparam, ilist, image, triclinic, eflag_atom,
+                           vflag_atom, dim, inum);
+}
+template <> inline void gpuFixDragForce<double>(double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+        double *box, int *iparam, int *ilist, int *pbc, int triclinic, int eflag_atom, int vflag_atom, int dim,
+        int inum)
+{
+    mdp_gpu_fix_drag_force_f64(x, v, f, eatom, vatom, fparam, box, iparam, ilist, pbc, triclinic, eflag_atom,
+                            vflag_atom, dim, inum);
+}
+template <> inline void gpuSetVelocityInitialIntegrate<double>(double *x, double *v, double *f, double *mass, double *fparam,
+        double dtf, double dtv, int *type, int *ilist, int *iparam, int dim, int inum)
+{
+    mdp_gpu_set_velocity_initial_integrate_f64(x, v, f, mass, fparam, dtf, dtv, type, ilist, iparam, dim, inum);
+}
+template <> inline void gpuSetVelocityFinalIntegrate<double>(double *x, double *v, double *f, double *mass, double dtf, int *type,
+        int *ilist, int *iparam, int dim, int inum)
+{
+    mdp_gpu_set_velocity_final_integrate_f64(x, v, f, mass, dtf, type, ilist, iparam, dim, inum);
+}
+template <> inline double gpuVelocityRescalingThermostat<double>(double *v, double *mass, double *dtarray, double *tarray, double *ke,
+        double *tmp, double *second, double energy, int *type, int *ilist, int *seed, int *save, int biasflag, int mode,
+        int dim, int inum)
+{
+    return mdp_gpu_velocity_rescaling_thermostat_f64(v, mass, dtarray, tarray, ke, tmp, second, energy, type, ilist,
+                                                    seed, save, biasflag, mode, dim, inum);
+}
+template <> inline void gpuFixSetForce<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_set_force_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixLineForce<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_line_force_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixPlaneForce<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_plane_force_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixAveForce<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_ave_force_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallReflect<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_reflect_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallHarmonic<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_harmonic_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallLJ93<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_lj93_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallLJ126<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_lj126_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallLJ1043<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_lj1043_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixWallMorse<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        int *iparam, int *ilist, int eflag_atom, int vflag_atom, int dim, int inum)
+{
+    mdp_gpu_fix_wall_morse_f32(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum);
+}
+template <> inline void gpuFixAddForce<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        float *box, int *iparam, int *ilist, int *image, int triclinic, int eflag_atom, int vflag_atom, int dim,
+        int inum)
+{
+    mdp_gpu_fix_add_force_f32(x, v, f, eatom, vatom, fparam, box, iparam, ilist, image, triclinic, eflag_atom,
+                           vflag_atom, dim, inum);
+}
+template <> inline void gpuFixDragForce<float>(float *x, float *v, float *f, float *eatom, float *vatom, float *fparam,
+        float *box, int *iparam, int *ilist, int *pbc, int triclinic, int eflag_atom, int vflag_atom, int dim,
+        int inum)
+{
+    mdp_gpu_fix_drag_force_f32(x, v, f, eatom, vatom, fparam, box, iparam, ilist, pbc, triclinic, eflag_atom,
+                            vflag_atom, dim, inum);
+}
+template <> inline void gpuSetVelocityInitialIntegrate<float>(float *x, float *v, float *f, float *mass, float *fparam,
+        float dtf, float dtv, int *type, int *ilist, int *iparam, int dim, int inum)
+{
+    mdp_gpu_set_velocity_initial_integrate_f32(x, v, f, mass, fparam, dtf, dtv, type, ilist, iparam, dim, inum);
+}
+template <> inline void gpuSetVelocityFinalIntegrate<float>(float *x, float *v, float *f, float *mass, float dtf, int *type,
+        int *ilist, int *iparam, int dim, int inum)
+{
+    mdp_gpu_set_velocity_final_integrate_f32(x, v, f, mass, dtf, type, ilist, iparam, dim, inum);
+}
+template <> inline float gpuVelocityRescalingThermostat<float>(float *v, float *mass, float *dtarray, float *tarray, float *ke,
+        float *tmp, float *second, float energy, int *type, int *ilist, int *seed, int *save, int biasflag, int mode,
+        int dim, int inum)
+{
+    return mdp_gpu_velocity_rescaling_thermostat_f32(v, mass, dtarray, tarray, ke, tmp, second, energy, type, ilist,
+                                                    seed, save, biasflag, mode, dim, inum);
 }
 #endif /* MDP_B200_GPUCORE_TEMPLATES */
 #endif /* __cplusplus */

@@ -503,4 +503,53 @@ void ref_nvt_final(double *x, double *v, const double *f, const double *mass, do
                          (int *)type, (int *)ilist, eta_mass_flag, 0, mtchain, nc_tchain, 3, inum);
 }
 
+// Force constraints of cpuFixes.cpp, by kind: 0 set, 1 line, 2 plane, 3 ave,
+// 4 wall reflect, 5 harmonic, 6 LJ93, 7 LJ126, 8 LJ1043, 9 Morse,
+// 10 add (with box / image), 11 drag (with box / pbc).  Host arrays, double.
+void ref_fix(int kind, double *x, double *v, double *f, double *eatom, double *vatom, double *fparam,
+             int *iparam, int *ilist, double *box, int *image, int *pbc, int triclinic, int eflag_atom,
+             int vflag_atom, int dim, int inum)
+{
+    switch (kind) {
+    case 0: cpuFixSetForce(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 1: cpuFixLineForce(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 2: cpuFixPlaneForce(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 3: cpuFixAveForce(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 4: cpuFixWallReflect(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 5: cpuFixWallHarmonic(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 6: cpuFixWallLJ93(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 7: cpuFixWallLJ126(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 8: cpuFixWallLJ1043(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 9: cpuFixWallMorse(x, v, f, eatom, vatom, fparam, iparam, ilist, eflag_atom, vflag_atom, dim, inum); break;
+    case 10:
+        cpuFixAddForce(x, v, f, eatom, vatom, fparam, box, iparam, ilist, image, triclinic, eflag_atom, vflag_atom,
+                       dim, inum);
+        break;
+    case 11:
+        cpuFixDragForce(x, v, f, eatom, vatom, fparam, box, iparam, ilist, pbc, triclinic, eflag_atom, vflag_atom,
+                        dim, inum);
+        break;
+    }
+}
+
+// set-velocity integration (cpuVelocityIntegration.cpp:430-463): stage 0
+// initial, 1 final
+void ref_set_velocity(int stage, double *x, double *v, double *f, double *mass, double *fparam, double dtf,
+                      double dtv, int *type, int *ilist, int *iparam, int dim, int inum)
+{
+    if (stage == 0)
+        cpuSetVelocityInitialIntegrate(x, v, f, mass, fparam, dtf, dtv, type, ilist, iparam, dim, inum);
+    else
+        cpuSetVelocityFinalIntegrate(x, v, f, mass, dtf, type, ilist, iparam, dim, inum);
+}
+
+// velocity-rescaling thermostats (cpuVelocityIntegration.cpp:708-858)
+double ref_velocity_rescaling(double *v, double *mass, double *dtarray, double *tarray, double *second,
+                              double energy, int *type, int *ilist, int *seed, int *save, int biasflag, int mode,
+                              int dim, int inum)
+{
+    return cpuVelocityRescalingThermostat(v, mass, dtarray, tarray, second, energy, type, ilist, seed, save,
+                                          biasflag, mode, dim, inum);
+}
+
 }  // extern "C"
