@@ -644,6 +644,7 @@ int ref_snap_wself_me(double *ur, double *ui, double wself, const int *type, con
 int ref_snap_ei_me(double *eatom, const double *ur, const double *ui, const double *coeff_dev, const int *ilist,
                    int tj, int nblk, int ncoeffall, int bnorm, int bzero, int wselfall, int inum, cudaStream_t s)
 {
+    if (tu_ensure_tables()) return -1;
     RefCtx &c = ref_ctx();
     if (load_tiles_blocks(c, ur, ui, inum, tj, nblk, s) || c.etmp.ensure(sizeof(double) * inum)) return -1;
     const MeArgs A = me_args(c, inum, nblk, ncoeffall, bzero, wselfall, coeff_dev, 0);
@@ -668,6 +669,7 @@ int ref_snap_ei_me(double *eatom, const double *ur, const double *ui, const doub
 int ref_snap_bi_me(double *blist, const double *ur, const double *ui, int tj, int nblk, int bnorm, int bzero,
                    int wselfall, int inum, cudaStream_t s)
 {
+    if (tu_ensure_tables()) return -1;
     RefCtx &c = ref_ctx();
     if (load_tiles_blocks(c, ur, ui, inum, tj, nblk, s)) return -1;
     const MeArgs A = me_args(c, inum, nblk, 0, bzero, wselfall, nullptr, 0);
@@ -692,6 +694,7 @@ int ref_snap_bi_me(double *blist, const double *ur, const double *ui, int tj, in
 int ref_snap_yi_me(double *yr, double *yi, const double *ur, const double *ui, const double *coeff_dev, int pa,
                    int tj, int nblk, int ncoeffall, int bnorm, int inum, cudaStream_t s)
 {
+    if (tu_ensure_tables()) return -1;
     RefCtx &c = ref_ctx();
     std::vector<double> ones(mdp_snap_ncoeff(tj) + 1, 1.0);
     if (model_from_args(c.model, tj, ones.data(), (int)ones.size(), bnorm, 0, 0, 1.0, 1.0, 1.0, 0.0, 1)) return -1;

@@ -73,17 +73,9 @@ static __constant__ float c_unorm_f[JD * JD * JD];
 static __constant__ double c_cg_d[NCG];
 static __constant__ float c_cg_f[NCG];
 
-static inline int tu_ensure_tables()
+// Uploads this translation unit's copy of the tables to the current device.
+static int tu_fill_tables()
 {
-    static std::mutex mu;
-    static bool done[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
-        set_error("no current CUDA device");
-        return -1;
-    }
-    std::lock_guard<std::mutex> lk(mu);
-    if (done[dev]) return 0;
     static double cg[NCG], rp[JD * JD], un[JD * JD * JD];
     static float cgf[NCG], rpf[JD * JD], unf[JD * JD * JD];
     host_cg_table(cg);
@@ -101,9 +93,22 @@ static inline int tu_ensure_tables()
         set_error("uploading SNAP constant tables failed");
         return -1;
     }
-    done[dev] = true;
     return 0;
 }
+
+// A kernel template instantiated in several translation units has one host
+// launch stub, so a launch may run the instantiation compiled into another
+// unit, which reads that unit's tables.  Every unit therefore registers its
+// filler at load time (tables.cu keeps the list), and the first
+// tu_ensure_tables() on a device fills all units' copies there.
+void register_table_filler(int (*fill)());
+int ensure_all_tables();
+struct TableFillerRegistration {
+    explicit TableFillerRegistration(int (*fill)()) { register_table_filler(fill); }
+};
+static TableFillerRegistration tu_table_filler_registration(&tu_fill_tables);
+
+static inline int tu_ensure_tables() { return ensure_all_tables(); }
 
 // SM count of the current device (cached per device).
 int num_sms();

@@ -399,6 +399,7 @@ template <int TJ>
 static int launch_snap_me(const SnapModel &m, ForcePath &fp, int inum, int nm, double *eatom, const MeArgs &A,
                           cudaStream_t s)
 {
+    if (tu_ensure_tables()) return -1;
     const long nv = (long)A.nblk * A.ntiles * 32;
     fp.u_welem = (m.eg.chem && !m.p.wselfallflag) ? A.elem : nullptr;
     fp.u_ipad = A.ntiles * 32;

@@ -62,9 +62,20 @@ struct YParams {
 #ifndef YI_W4_F
 #define YI_W4_F 4
 #endif
+#ifndef YI_W8_F
+#define YI_W8_F 20
+#endif
+#ifndef YI_MINB_F
+#define YI_MINB_F 1
+#endif
 __host__ __device__ constexpr int yi_warps(bool fp32, int tj)
 {
-    return fp32 ? (tj <= 4 ? YI_W4_F : 20) : (tj <= 4 ? YI_W4_D : 10);
+    return fp32 ? (tj <= 4 ? YI_W4_F : YI_W8_F) : (tj <= 4 ? YI_W4_D : 10);
+}
+// CTAs per SM the Y kernel is compiled for (register cap)
+template <typename T> __host__ __device__ constexpr int yi_min_blocks()
+{
+    return std::is_same<T, float>::value ? YI_MINB_F : 1;
 }
 template <typename T, int TJ> struct YiWarps { static constexpr int n = yi_warps(false, TJ); };
 template <int TJ> struct YiWarps<float, TJ> { static constexpr int n = yi_warps(true, TJ); };
@@ -762,7 +773,7 @@ constexpr size_t yi_smem_bytes()
 // PA: per-atom coefficients G[k * natoms + atom] (k over the nbispec(TJ)
 // components) instead of the model's; no energy is written.
 template <typename T, int TJ, bool PA = false>
-__global__ void __launch_bounds__(YiWarps<T, TJ>::n * 32, 1)
+__global__ void __launch_bounds__(YiWarps<T, TJ>::n * 32, yi_min_blocks<T>())
 k_snap_yi(const typename cplx<T>::type *__restrict__ Ut, int natoms, const __grid_constant__ YParams<T> P,
           typename cplx<T>::type *__restrict__ Y, double *__restrict__ eatom, const T *__restrict__ G = nullptr)
 {

@@ -8,6 +8,7 @@
 #include <string.h>
 #include <mutex>
 #include <atomic>
+#include <vector>
 
 namespace mdp {
 
@@ -35,6 +36,41 @@ static int current_device(int *dev)
 }
 
 static PerDeviceMemo g_sms, g_kernels;
+
+// every translation unit's constant-table filler, run once per device
+namespace {
+struct FillerRegistry {
+    std::mutex mu;
+    std::vector<int (*)()> fillers;
+    bool done[64] = {};
+};
+FillerRegistry &filler_registry()
+{
+    static FillerRegistry r;   // constructed on first use, during static initialisation
+    return r;
+}
+}  // namespace
+
+void register_table_filler(int (*fill)())
+{
+    FillerRegistry &r = filler_registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    r.fillers.push_back(fill);
+}
+
+int ensure_all_tables()
+{
+    int dev = 0;
+    if (current_device(&dev)) return -1;
+    if (dev >= 64) { set_error("device index %d out of range", dev); return -1; }
+    FillerRegistry &r = filler_registry();
+    std::lock_guard<std::mutex> lk(r.mu);
+    if (r.done[dev]) return 0;
+    for (auto fill : r.fillers)
+        if (fill()) return -1;
+    r.done[dev] = true;
+    return 0;
+}
 
 int num_sms()
 {
