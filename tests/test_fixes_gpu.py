@@ -223,8 +223,10 @@ def test_velocity_rescaling_thermostats(cuda_lib, mode, tdof):
 
 
 def test_float_entries_follow_the_double_path(cuda_lib):
-    """The _f32 fixes of PREC_FLOAT builds: walls, add force and set force in
-    float against the double reference, within float rounding."""
+    """The _f32 fixes of PREC_FLOAT builds: walls and set force in float
+    against the double reference, within float rounding (the LJ 9-3 wall
+    differences its 1/delta^10 and 1/delta^4 terms, which float resolves to
+    about 1e-3 of the largest force)."""
     R, L32 = ref(), ours("f32")
     _, arrays, ilist = system(21, box=6.0)
     for kind, fp, ip in (("wall_lj93", WALL_PARAMS["wall_lj93"], [1]), ("set_force", [0.3, -1.2, 2.5], [1, 0, 1]),
@@ -238,5 +240,6 @@ def test_float_entries_follow_the_double_path(cuda_lib):
                                                 ptr(d["vatom"]), ptr(dev(fpd, np.float32)), ptr(dev(ipd)),
                                                 ptr(dev(ilist)), 1, 1, 3, len(ilist))
         sync()
+        tol = 2e-3 if kind == "wall_lj93" else 1e-5
         for k in ("f", "eatom", "vatom"):
-            assert rel(d[k].cpu().numpy().astype(np.float64), a[k]) < 1e-5, (kind, k)
+            assert rel(d[k].cpu().numpy().astype(np.float64), a[k]) < tol, (kind, k)
