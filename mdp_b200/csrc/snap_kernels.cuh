@@ -49,9 +49,11 @@ struct YParams {
 };
 // warps per Y CTA: FP64 10 (two per row of the costliest layer; 168
 // registers; measured 65 ms at 2M atoms against 70 / 71 / 68 / 68 / 74 ms for
-// 9 / 8 / 11 / 12 / 14 warps); FP32 20 (packed rows, 92 registers; the FP32
-// form measured 34.9 M atom-steps/s against 33.6 / 34.1 / 34.2 at 12 / 16 /
-// 24 warps).  At 2J <= 4 no layer has more than three rows and the extra
+// 9 / 8 / 11 / 12 / 14 warps; its 146 KB U tile leaves room for one CTA per
+// SM); FP32 8 with two CTAs per SM (92 registers, 93 KB of shared memory
+// each, so one CTA's barrier waits overlap the other's work: the Y stage takes
+// 26.1 ms at 2M atoms against 28.3 / 27.1 / 26.8 / 28.2 ms for 6 / 7 / 10 /
+// 12 warps at two CTAs and 28.4 ms for 20 warps at one).  At 2J <= 4 no layer has more than three rows and the extra
 // warps only wait at the barriers: the FP32 per-atom-coefficient kernel of the
 // surrogate takes 4 (surrogate steps at 2M atoms: 14.8 ms against 14.9 / 15.2
 // / 15.8 / 17.6 / 16.9 ms at 3 / 6 / 8 / 12 / 20 warps; 2 cannot cover the
@@ -63,10 +65,10 @@ struct YParams {
 #define YI_W4_F 4
 #endif
 #ifndef YI_W8_F
-#define YI_W8_F 20
+#define YI_W8_F 8
 #endif
 #ifndef YI_MINB_F
-#define YI_MINB_F 1
+#define YI_MINB_F 2
 #endif
 __host__ __device__ constexpr int yi_warps(bool fp32, int tj)
 {
@@ -373,7 +375,25 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
 // updates; 8.1 against 8.2 ms at 2M atoms); FP64 one (two measured 18.1
 // against 15.7 ms: twice the unrolled code per warp path)
 template <typename T> __host__ __device__ constexpr int uc_pb() { return std::is_same<T, float>::value ? 2 : 1; }
-template <int TJ> __host__ __device__ constexpr int uc_warps() { return TJ / 2; }
+// Work plan.  UC_SPLIT = 0: one warp per column (the top two columns share
+// the last warp).  UC_SPLIT = 1 at 2J = 8: eight jobs (column, first layer
+// added into the tile, last layer); a job steps through its column's rows
+// below its first layer without adding them, so the deep columns are split
+// across two warps and twice the warps share the same tile.
+#ifndef UC_SPLIT
+#define UC_SPLIT 0
+#endif
+struct UcJob {
+    int mb, jlo, jhi;
+};
+template <int TJ> __host__ __device__ constexpr bool uc_split() { return UC_SPLIT && TJ == 8; }
+template <int TJ> __host__ __device__ constexpr int uc_warps() { return uc_split<TJ>() ? 8 : TJ / 2; }
+template <int TJ> __host__ __device__ constexpr UcJob uc_job(int w)
+{
+    constexpr UcJob plan8[8] = {{0, 0, 5}, {0, 6, 8}, {1, 0, 6}, {1, 7, 8},
+                                {2, 0, 6}, {2, 7, 8}, {3, 0, 8}, {4, 0, 8}};
+    return plan8[w];
+}
 template <typename T, int TJ> constexpr size_t uc_smem_bytes()
 {
     return (size_t)yh_count(TJ) * 32 * sizeof(typename cplx<T>::type);
@@ -412,8 +432,9 @@ __device__ __forceinline__ void uc_chain(UcPairs<T, TJ> &s)
     }
 }
 
-// rows J..JEND of column MB (row J's parent in s.pr/pi), each added into the tile
-template <typename T, int TJ, int MB, int J, int JEND>
+// rows J..JEND of column MB (row J's parent in s.pr/pi), each from layer
+// JACC on added into the tile
+template <typename T, int TJ, int MB, int J, int JEND, int JACC = 0>
 __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
 {
     typedef typename cplx<T>::type T2;
@@ -422,6 +443,10 @@ __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::t
 #pragma unroll
             for (int q = 0; q < UcPairs<T, TJ>::PB; q++)
                 cf_fwd<T, TJ, J, MB>(s.ar[q], s.ai[q], s.br[q], s.bi[q], s.pr[q], s.pi[q]);
+        }
+        if constexpr (J < JACC) {
+            uc_column<T, TJ, MB, J + 1, JEND, JACC>(s, acc);
+            return;
         }
         T2 *row = acc + (yh_block(J) + (J + 1) * MB) * 32;
 #pragma unroll
@@ -436,7 +461,7 @@ __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::t
             }
             row[ma * 32] = v;
         }
-        uc_column<T, TJ, MB, J + 1, JEND>(s, acc);
+        uc_column<T, TJ, MB, J + 1, JEND, JACC>(s, acc);
     }
 }
 
@@ -475,7 +500,17 @@ __device__ __forceinline__ void uc_path(UcPairs<T, TJ> &s, typename cplx<T>::typ
 template <typename T, int TJ, int MB>
 __device__ __forceinline__ void uc_dispatch(const int w, UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
 {
-    if constexpr (MB < uc_warps<TJ>()) {
+    if constexpr (uc_split<TJ>()) {
+        if constexpr (MB < uc_warps<TJ>()) {
+            constexpr UcJob jb = uc_job<TJ>(MB);
+            if (w == MB) {
+                uc_chain<T, TJ, jb.mb, 0>(s);
+                uc_column<T, TJ, jb.mb, (jb.mb == 0 ? 0 : 2 * jb.mb), jb.jhi, jb.jlo>(s, acc);
+            } else {
+                uc_dispatch<T, TJ, MB + 1>(w, s, acc);
+            }
+        }
+    } else if constexpr (MB < uc_warps<TJ>()) {
         if (w == MB) uc_path<T, TJ, MB>(s, acc);
         else uc_dispatch<T, TJ, MB + 1>(w, s, acc);
     }

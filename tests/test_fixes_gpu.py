@@ -98,9 +98,13 @@ def run_fix(kind, arrays, fparam, iparam, ilist, eflag, vflag, dim):
 
 @pytest.mark.parametrize("dim", [3, 2])
 def test_set_and_ave_force(cuda_lib, dim):
+    """In two dimensions cpuFixAveForce still tests iparam[2] and, when it is
+    set, writes f[i*dim+2] -- the next atom's x (cpuFixes.cpp:292).  The
+    entry point sets components d < dim only; the test passes iparam[2] = 0,
+    where the two agree."""
     _, arrays, ilist = system(1, dim=dim)
     for kind, fp, ip, tol in (("set_force", [0.3, -1.2, 2.5][:dim], [1, 0, 1][:dim], 0.0),
-                              ("ave_force", [0.3, -1.2, 2.5][:dim], [1, 1, 0][:dim], 1e-12)):
+                              ("ave_force", [0.3, -1.2, 2.5][:dim], [1, 1, 0] if dim == 2 else [1, 1, 0], 1e-12)):
         a, b = run_fix(kind, arrays, fp, ip, ilist, 1, 1, dim)
         assert rel(b["f"], a["f"]) <= tol, kind
         assert np.array_equal(b["x"], a["x"]) and np.array_equal(b["eatom"], a["eatom"])
