@@ -375,19 +375,23 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
 // updates; 8.1 against 8.2 ms at 2M atoms); FP64 one (two measured 18.1
 // against 15.7 ms: twice the unrolled code per warp path)
 template <typename T> __host__ __device__ constexpr int uc_pb() { return std::is_same<T, float>::value ? 2 : 1; }
-// Work plan.  UC_SPLIT = 0: one warp per column (the top two columns share
-// the last warp).  UC_SPLIT = 1 at 2J = 8: eight jobs (column, first layer
-// added into the tile, last layer); a job steps through its column's rows
-// below its first layer without adding them, so the deep columns are split
-// across two warps and twice the warps share the same tile.
+// Work plan.  One warp per column (the top two columns share the last warp),
+// or, for FP64 at 2J = 8, eight jobs (column, first layer added into the
+// tile, last layer): a job steps through its column's rows below its first
+// layer without adding them, so the deep columns are split across two warps
+// and twice the warps share the tile (U 15.3 against 16.1 ms per step at 2M
+// atoms).  FP32, with two pairs per pass, lost by it (12.0 against 8.3 ms).
 #ifndef UC_SPLIT
-#define UC_SPLIT 0
+#define UC_SPLIT 1
 #endif
 struct UcJob {
     int mb, jlo, jhi;
 };
-template <int TJ> __host__ __device__ constexpr bool uc_split() { return UC_SPLIT && TJ == 8; }
-template <int TJ> __host__ __device__ constexpr int uc_warps() { return uc_split<TJ>() ? 8 : TJ / 2; }
+template <typename T, int TJ> __host__ __device__ constexpr bool uc_split()
+{
+    return UC_SPLIT && TJ == 8 && std::is_same<T, double>::value;
+}
+template <typename T, int TJ> __host__ __device__ constexpr int uc_warps() { return uc_split<T, TJ>() ? 8 : TJ / 2; }
 template <int TJ> __host__ __device__ constexpr UcJob uc_job(int w)
 {
     constexpr UcJob plan8[8] = {{0, 0, 5}, {0, 6, 8}, {1, 0, 6}, {1, 7, 8},
@@ -470,7 +474,7 @@ template <typename T, int TJ, int MB>
 __device__ __forceinline__ void uc_path(UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
 {
     uc_chain<T, TJ, MB, 0>(s);
-    if constexpr (MB + 1 < uc_warps<TJ>()) {
+    if constexpr (MB + 1 < uc_warps<T, TJ>()) {
         uc_column<T, TJ, MB, (MB == 0 ? 0 : 2 * MB), TJ>(s, acc);
     } else {
         // last warp: column MB up to its row 2MB+1, mirror to the seed of
@@ -500,8 +504,8 @@ __device__ __forceinline__ void uc_path(UcPairs<T, TJ> &s, typename cplx<T>::typ
 template <typename T, int TJ, int MB>
 __device__ __forceinline__ void uc_dispatch(const int w, UcPairs<T, TJ> &s, typename cplx<T>::type *__restrict__ acc)
 {
-    if constexpr (uc_split<TJ>()) {
-        if constexpr (MB < uc_warps<TJ>()) {
+    if constexpr (uc_split<T, TJ>()) {
+        if constexpr (MB < uc_warps<T, TJ>()) {
             constexpr UcJob jb = uc_job<TJ>(MB);
             if (w == MB) {
                 uc_chain<T, TJ, jb.mb, 0>(s);
@@ -510,20 +514,20 @@ __device__ __forceinline__ void uc_dispatch(const int w, UcPairs<T, TJ> &s, type
                 uc_dispatch<T, TJ, MB + 1>(w, s, acc);
             }
         }
-    } else if constexpr (MB < uc_warps<TJ>()) {
+    } else if constexpr (MB < uc_warps<T, TJ>()) {
         if (w == MB) uc_path<T, TJ, MB>(s, acc);
         else uc_dispatch<T, TJ, MB + 1>(w, s, acc);
     }
 }
 
 template <typename T, int TJ>
-__global__ void __launch_bounds__(uc_warps<TJ>() * 32)
+__global__ void __launch_bounds__(uc_warps<T, TJ>() * 32)
 k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const double4 *__restrict__ pab,
           int natoms, typename cplx<T>::type *__restrict__ Ut, const int *__restrict__ welem = nullptr,
           int ipad = 0)
 {
     typedef typename cplx<T>::type T2;
-    constexpr int NW = uc_warps<TJ>();
+    constexpr int NW = uc_warps<T, TJ>();
     constexpr int NU = idxu_count(TJ), NYH = yh_count(TJ);
     extern __shared__ __align__(16) unsigned char smraw[];
     T2 *acc = reinterpret_cast<T2 *>(smraw);
@@ -1503,8 +1507,11 @@ k_snap_fr(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, cons
 
 // FP32: the state takes half the registers, so the kernel is held to 128 and
 // four CTAs share an SM
+#ifndef FR32_MINB
+#define FR32_MINB 4
+#endif
 template <int TJ>
-__global__ void __launch_bounds__(FR_THREADS, 4)
+__global__ void __launch_bounds__(FR_THREADS, FR32_MINB)
 k_snap_fr32(const double4 *__restrict__ prij, const int2 *__restrict__ pinfo, const int *__restrict__ pnum,
             SnapGeom gp, const float2 *__restrict__ Y, double4 *__restrict__ dEslot)
 {
