@@ -15,7 +15,7 @@
 // Pipeline (all on one stream, captured into one CUDA graph by mdp_fit_run):
 //   pairs (brute force over each configuration's atoms and 27 images)
 //   U      (k_snap_uc, the MD engine's kernel)
-//   Z, B   (k_fit_zb: every coupling's Z rows per atom, B for j >= j1)
+//   Z, B   (k_fit_zbt: every coupling's Z rows per atom, B for j >= j1)
 //   dU/dr  (k_fit_du: forward-mode, coefficient-free recursion, per pair and direction)
 //   dB/dr  (k_fit_dbdr: the three Z . dU terms of cpuComputeDbidrj:826-1013)
 //   rows   (k_fit_rows: atomic-free gather over own and reverse pairs)
@@ -113,62 +113,80 @@ __global__ void k_fit_zbl(const double4 *__restrict__ x, const int *__restrict__
 // Z rows of every coupling and B for j >= j1, per 32-atom tile (lane = atom)
 // Z layout [tile][zoff + (j+1) mb + ma][lane]; B layout [k][atom]
 // ---------------------------------------------------------------------------
-constexpr int FIT_ZB_WARPS = 8;
+// Every coupling is compile-time specialised (the Y kernel's z_rows: CG
+// coefficients as constant operands, U rows in registers), output layer by
+// layer.  Within a layer the (coupling, mb) rows go to the warps round-robin
+// in enumeration order, so the warps run one or two couplings' code at a
+// time; a barrier per layer keeps them together.
+constexpr int FIT_ZBT_WARPS = 10;
 
-__global__ void __launch_bounds__(FIT_ZB_WARPS * 32)
-k_fit_zb(const double2 *__restrict__ Ut, int natoms, const FitTables *__restrict__ T, double2 *__restrict__ Z,
-         double *__restrict__ B, int tile_lo, int tile_hi)
+// offset of coupling (J1, J2, J)'s rows in the Z layout (fit_tables order)
+__host__ __device__ constexpr int fit_zoff(int tj, int J1, int J2, int J)
+{
+    int nz = 0;
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= cmin(tj, j1 + j2); j += 2) {
+                if (j1 == J1 && j2 == J2 && j == J) return nz;
+                nz += (j / 2 + 1) * (j + 1);
+            }
+    return -1;
+}
+
+template <int TJ, int J, int J1, int J2>
+__device__ __forceinline__ void zbt_layer(const double2 *__restrict__ Us, double2 *__restrict__ Zt, const int lane,
+                                          const int w, const double scale, int item)
+{
+    if constexpr (J1 <= TJ) {
+        if constexpr (J2 <= J1) {
+            if constexpr (coupling_ok(J1, J2, J)) {
+                constexpr int ZO = fit_zoff(TJ, J1, J2, J);
+                for (int mb = 0; 2 * mb <= J; mb++, item++) {
+                    if (item % FIT_ZBT_WARPS != w) continue;
+                    YRow<double> acc;
+                    acc.zero();
+                    z_rows<double, J1, J2, J>(mb, 0, 1, Us, Us, lane, scale, acc);
+#pragma unroll
+                    for (int ma = 0; ma <= J; ma++) Zt[(size_t)(ZO + (J + 1) * mb + ma) * 32] = acc.get(ma);
+                }
+            }
+            zbt_layer<TJ, J, J1, J2 + 1>(Us, Zt, lane, w, scale, item);
+        } else {
+            zbt_layer<TJ, J, J1 + 1, 0>(Us, Zt, lane, w, scale, item);
+        }
+    }
+}
+
+template <int TJ, int J>
+__device__ __forceinline__ void zbt_layers(const double2 *__restrict__ Us, double2 *__restrict__ Zt, const int lane,
+                                           const int w, const int bnorm)
+{
+    if constexpr (J <= TJ) {
+        zbt_layer<TJ, J, 0, 0>(Us, Zt, lane, w, bnorm ? 1.0 / (J + 1) : 1.0, 0);
+        __syncthreads();
+        zbt_layers<TJ, J + 1>(Us, Zt, lane, w, bnorm);
+    }
+}
+
+template <int TJ>
+__global__ void __launch_bounds__(FIT_ZBT_WARPS * 32, 1)
+k_fit_zbt(const double2 *__restrict__ Ut, int natoms, const FitTables *__restrict__ T, double2 *__restrict__ Z,
+          double *__restrict__ B, int tile_lo, int tile_hi)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *Us = reinterpret_cast<double2 *>(smraw);
-    const int tj = T->tj, nu = idxu_count(tj), nz = T->nz;
+    constexpr int NU = idxu_count(TJ);
+    const int nz = T->nz;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int tile = tile_lo + blockIdx.x; tile < tile_hi; tile += gridDim.x) {
-        const double2 *src = Ut + (size_t)tile * nu * 32;
-        for (int k = threadIdx.x; k < nu * 32; k += blockDim.x) Us[k] = src[k];
+        const double2 *src = Ut + (size_t)tile * NU * 32;
+        for (int k = threadIdx.x; k < NU * 32; k += blockDim.x) Us[k] = src[k];
         __syncthreads();
         double2 *Zt = Z + (size_t)(tile - tile_lo) * nz * 32 + lane;
-        // work items: (coupling, row mb)
-        int item = 0;
-        for (int c = 0; c < T->ncoup; c++) {
-            const FitCoupling cp = T->cp[c];
-            const int j1 = cp.j1, j2 = cp.j2, j = cp.j;
-            const int cgb = cg_block(j1, j2, j);
-            const double scale = T->bnorm ? 1.0 / (j + 1) : 1.0;
-            for (int mb = 0; 2 * mb <= j; mb++, item++) {
-                if (item % FIT_ZB_WARPS != w) continue;
-                const int mb1min = max(0, (2 * mb - j - j2 + j1) / 2);
-                const int mb2max = (2 * mb - j - (2 * mb1min - j1) + j2) / 2;
-                const int nb = min(j1, (2 * mb - j + j2 + j1) / 2) - mb1min + 1;
-                for (int ma = 0; ma <= j; ma++) {
-                    const int ma1min = max(0, (2 * ma - j - j2 + j1) / 2);
-                    const int ma2max = (2 * ma - j - (2 * ma1min - j1) + j2) / 2;
-                    const int na = min(j1, (2 * ma - j + j2 + j1) / 2) - ma1min + 1;
-                    double zr = 0.0, zi = 0.0;
-                    for (int ib = 0; ib < nb; ib++) {
-                        const int mb1 = mb1min + ib, mb2 = mb2max - ib;
-                        const double cb = cgc<double>(cgb + mb1 * (j2 + 1) + mb2);
-                        const double2 *r1 = Us + (idxu_block(j1) + (j1 + 1) * mb1) * 32 + lane;
-                        const double2 *r2 = Us + (idxu_block(j2) + (j2 + 1) * mb2) * 32 + lane;
-                        double sr = 0.0, si = 0.0;
-                        for (int ia = 0; ia < na; ia++) {
-                            const int ma1 = ma1min + ia, ma2 = ma2max - ia;
-                            const double ca = cgc<double>(cgb + ma1 * (j2 + 1) + ma2);
-                            const double2 u1 = r1[ma1 * 32], u2 = r2[ma2 * 32];
-                            sr += ca * (u1.x * u2.x - u1.y * u2.y);
-                            si += ca * (u1.x * u2.y + u1.y * u2.x);
-                        }
-                        zr += cb * sr;
-                        zi += cb * si;
-                    }
-                    Zt[(size_t)(cp.zoff + (j + 1) * mb + ma) * 32] = make_double2(zr * scale, zi * scale);
-                }
-            }
-        }
-        __syncthreads();
+        zbt_layers<TJ, 0>(Us, Zt, lane, w, T->bnorm);
         // B_k = 2 sum_half w Re(U_j* Z) (- bzero), cpuComputeBi2 (cpuSnap2.cpp:516-541)
         const int atom = tile * 32 + lane;
-        for (int k = w; k < T->ntri; k += FIT_ZB_WARPS) {
+        for (int k = w; k < T->ntri; k += FIT_ZBT_WARPS) {
             const FitTriple tr = T->tr[k];
             const int j = tr.j;
             const FitCoupling cp = T->cp[tr.coup[0]];
@@ -302,9 +320,10 @@ k_fit_du(const double4 *__restrict__ prij, long npairs, SnapGeom gp, double2 *__
 // with the middle row's centre at 1/2.  dbdr[k * stride + t]
 // ---------------------------------------------------------------------------
 // The pair's dU rows of layer L are loaded once (registers) and every dB/dR
-// term on that layer is applied to them: dU is read once per thread, Z rows
-// come through L1 (all of an atom's pair-directions read the same Z).
-template <int L>
+// term on that layer is applied to them: dU is read once per thread.  The Z
+// rows come from shared memory, element e of the atom's row block at
+// Zi[e * ZS].
+template <int L, int ZS>
 __device__ __forceinline__ void fdb_layer(const double2 *__restrict__ d, const long stride,
                                           const double2 *__restrict__ Zi, const FitTables *__restrict__ T,
                                           double *__restrict__ acc)
@@ -315,14 +334,14 @@ __device__ __forceinline__ void fdb_layer(const double2 *__restrict__ d, const l
     for (int e = 0; e < NE; e++) du[e] = d[(long)(YO + e) * stride];
     const int q0 = T->lt_off[L], q1 = q0 + T->lt_n[L];
     for (int q = q0; q < q1; q++) {
-        const double2 *z = Zi + (size_t)T->lt_z[q] * 32;
+        const double2 *z = Zi + (size_t)T->lt_z[q] * ZS;
         double s0 = 0.0, s1 = 0.0;
 #pragma unroll
         for (int e = 0; e < NE; e++) {
             const int mb = e / (L + 1), ma = e % (L + 1);
             if (2 * mb == L && ma > mb) continue;   // right of a middle row's centre
             const double wgt = (2 * mb == L && ma == mb) ? 0.5 : 1.0;
-            const double2 zz = z[(size_t)e * 32];
+            const double2 zz = z[(size_t)e * ZS];
             if (e & 1) s1 += wgt * (du[e].x * zz.x + du[e].y * zz.y);
             else s0 += wgt * (du[e].x * zz.x + du[e].y * zz.y);
         }
@@ -330,34 +349,55 @@ __device__ __forceinline__ void fdb_layer(const double2 *__restrict__ d, const l
     }
 }
 
-template <int TJ, int L>
+template <int TJ, int L, int ZS>
 __device__ __forceinline__ void fdb_layers(const double2 *__restrict__ d, const long stride,
                                            const double2 *__restrict__ Zi, const FitTables *__restrict__ T,
                                            double *__restrict__ acc)
 {
     if constexpr (L <= TJ) {
-        fdb_layer<L>(d, stride, Zi, T, acc);
-        fdb_layers<TJ, L + 1>(d, stride, Zi, T, acc);
+        fdb_layer<L, ZS>(d, stride, Zi, T, acc);
+        fdb_layers<TJ, L + 1, ZS>(d, stride, Zi, T, acc);
     }
 }
 
 // dB_ik/dr_p along one axis: 2 sum over the three terms of cpuComputeDbidrj
 // (Z of the centre atom's couplings against the pair's dU rows), half plane
-// with the middle row's centre at 1/2.  dbdr[k * stride + t]
-template <int TJ>
-__global__ void __launch_bounds__(128)
-k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int2 *__restrict__ pinfo, long npairs,
-           const FitTables *__restrict__ T, const double2 *__restrict__ Z, int tile_lo, double *__restrict__ dbdr)
+// with the middle row's centre at 1/2.  dbdr[k * stride + t], t = (p - p_lo) * 3
+// + dir.  A CTA takes APC adjacent atoms (APC divides 32, so they share a Z
+// tile) and their pairs, 64 threads per atom: the atoms' Z rows (38 KB per
+// atom at 2J = 8) are copied once into shared memory ([entry][atom]), so
+// every pair-direction reads them there.  Read in place from the tile
+// layout, each entry sat in its own 128-byte line, 512 bytes from the next:
+// an atom's rows touched 2,386 lines, more than L1 holds for the atoms in
+// flight, and the dot products waited on L2.
+constexpr int FIT_DB_TPA = 64;   // threads per atom
+template <int TJ, int APC>
+__global__ void __launch_bounds__(FIT_DB_TPA * APC)
+k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int *__restrict__ poff,
+           const int2 *__restrict__ pinfo, int a_lo, int a_hi, long p_lo, const FitTables *__restrict__ T,
+           const double2 *__restrict__ Z, int tile_lo, double *__restrict__ dbdr)
 {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 3 * npairs) return;
-    const int atom = pinfo[t / 3].x;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double2 *Zs = reinterpret_cast<double2 *>(smraw);   // [entry][APC]
     const int nz = T->nz, ntri = T->ntri;
-    const double2 *Zi = Z + (size_t)((atom >> 5) - tile_lo) * nz * 32 + (atom & 31);
-    double acc[FIT_NT];
-    for (int k = 0; k < ntri; k++) acc[k] = 0.0;
-    fdb_layers<TJ, 0>(dul + t, stride, Zi, T, acc);
-    for (int k = 0; k < ntri; k++) dbdr[(long)k * stride + t] = acc[k];
+    const int a0 = (a_lo & ~(APC - 1)) + blockIdx.x * APC;
+    const int alo = max(a0, a_lo), ahi = min(a0 + APC, a_hi);
+    for (int e = threadIdx.x; e < nz * APC; e += blockDim.x) {
+        const int k = e / APC, a = a0 + (e - k * APC);
+        if (a >= alo && a < ahi) Zs[e] = Z[((size_t)((a >> 5) - tile_lo) * nz + k) * 32 + (a & 31)];
+    }
+    __syncthreads();
+    if (alo >= ahi) return;
+    const long q0 = poff[alo], n3 = 3 * (long)(poff[ahi] - q0);
+    for (long i = threadIdx.x; i < n3; i += blockDim.x) {
+        const long p = q0 + i / 3;
+        const long t = (p - p_lo) * 3 + (i - (i / 3) * 3);
+        const int atom = pinfo[p].x;
+        double acc[FIT_NT];
+        for (int k = 0; k < ntri; k++) acc[k] = 0.0;
+        fdb_layers<TJ, 0, APC>(dul + t, stride, Zs + (atom - a0), T, acc);
+        for (int k = 0; k < ntri; k++) dbdr[(long)k * stride + t] = acc[k];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -752,20 +792,68 @@ static int fit_du(mdp_fit *h, const mdp_fit::Chunk &ck)
     return tj == 8 ? fit_launch_du<8>(h, ck) : tj == 6 ? fit_launch_du<6>(h, ck) : fit_launch_du<4>(h, ck);
 }
 
-static void fit_dbdr(mdp_fit *h, const mdp_fit::Chunk &ck, int threads)
+// Z rows and B of one chunk's tiles (the fit takes 2J = 4, 6, 8)
+template <int TJ>
+static int fit_zbt(mdp_fit *h, const mdp_fit::Chunk &ck, unsigned g)
 {
-    const long np = ck.p_hi - ck.p_lo, nt = 3 * np;
-    if (nt == 0) return;
-    const unsigned g = (unsigned)((nt + threads - 1) / threads);
-    const double2 *d = h->dul.as<double2>();
-    const int2 *pi = h->fp.pinfo.as<int2>() + ck.p_lo;
-    const FitTables *T = h->tabs.as<FitTables>();
+    const size_t zsm = (size_t)idxu_count(TJ) * 32 * sizeof(double2);
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_fit_zbt<TJ>, FIT_ZBT_WARPS * 32, zsm, &per_sm, "k_fit_zbt")) return -1;
+    k_fit_zbt<TJ><<<g, FIT_ZBT_WARPS * 32, zsm, h->s>>>(h->fp.Ut.as<double2>(), h->natoms, h->tabs.as<FitTables>(),
+                                                       h->Z.as<double2>(), h->B.as<double>(), ck.t_lo, ck.t_hi);
+    return 0;
+}
+
+static int fit_zb(mdp_fit *h, const mdp_fit::Chunk &ck)
+{
+    const unsigned g = (unsigned)std::max(1, std::min(ck.t_hi - ck.t_lo, num_sms()));
+    int rc = 0;
     switch (h->model.p.twojmax) {
-    case 8: k_fit_dbdr<8><<<g, threads, 0, h->s>>>(d, nt, pi, np, T, h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>()); break;
-    case 6: k_fit_dbdr<6><<<g, threads, 0, h->s>>>(d, nt, pi, np, T, h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>()); break;
-    default: k_fit_dbdr<4><<<g, threads, 0, h->s>>>(d, nt, pi, np, T, h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>()); break;
+    case 8: rc = fit_zbt<8>(h, ck, g); break;
+    case 6: rc = fit_zbt<6>(h, ck, g); break;
+    default: rc = fit_zbt<4>(h, ck, g); break;
     }
     count_launches(1);
+    return rc;
+}
+
+template <int TJ, int APC>
+static int fit_dbdr_apc(mdp_fit *h, const mdp_fit::Chunk &ck)
+{
+    const long nt = 3 * (ck.p_hi - ck.p_lo);
+    const size_t sm = (size_t)h->tab.nz * APC * sizeof(double2);
+    int per_sm = 0;
+    if (kernel_setup((const void *)k_fit_dbdr<TJ, APC>, FIT_DB_TPA * APC, sm, &per_sm, "k_fit_dbdr")) return -1;
+    const int a0 = ck.a_lo & ~(APC - 1);
+    const unsigned g = (unsigned)((ck.a_hi - a0 + APC - 1) / APC);
+    k_fit_dbdr<TJ, APC><<<g, FIT_DB_TPA * APC, sm, h->s>>>(
+        h->dul.as<double2>(), nt, h->poff.as<int>(), h->fp.pinfo.as<int2>(), ck.a_lo, ck.a_hi, ck.p_lo,
+        h->tabs.as<FitTables>(), h->Z.as<double2>(), ck.t_lo, h->dbdr.as<double>());
+    return 0;
+}
+
+template <int TJ>
+static int fit_dbdr_tj(mdp_fit *h, const mdp_fit::Chunk &ck, int threads)
+{
+    switch (threads / FIT_DB_TPA) {
+    case 1: return fit_dbdr_apc<TJ, 1>(h, ck);
+    case 4: return fit_dbdr_apc<TJ, 4>(h, ck);
+    default: return fit_dbdr_apc<TJ, 2>(h, ck);
+    }
+}
+
+// threads = FIT_DB_TPA x atoms per CTA (64, 128 or 256)
+static int fit_dbdr(mdp_fit *h, const mdp_fit::Chunk &ck, int threads)
+{
+    if (ck.p_hi == ck.p_lo) return 0;
+    int rc;
+    switch (h->model.p.twojmax) {
+    case 8: rc = fit_dbdr_tj<8>(h, ck, threads); break;
+    case 6: rc = fit_dbdr_tj<6>(h, ck, threads); break;
+    default: rc = fit_dbdr_tj<4>(h, ck, threads); break;
+    }
+    count_launches(1);
+    return rc;
 }
 
 // Z/B, dU, dB/dR of one chunk, then its rows: into R / tgt (rows) and/or the
@@ -773,12 +861,9 @@ static void fit_dbdr(mdp_fit *h, const mdp_fit::Chunk &ck, int threads)
 static int fit_chunk(mdp_fit *h, const mdp_fit::Chunk &ck, bool rows, double *G, double *bi, double *bv)
 {
     const int n = h->natoms;
-    const size_t zsm = (size_t)idxu_count(h->model.p.twojmax) * 32 * sizeof(double2);
-    k_fit_zb<<<std::max(1, std::min(ck.t_hi - ck.t_lo, num_sms())), FIT_ZB_WARPS * 32, zsm, h->s>>>(
-        h->fp.Ut.as<double2>(), n, h->tabs.as<FitTables>(), h->Z.as<double2>(), h->B.as<double>(), ck.t_lo, ck.t_hi);
-    count_launches(1);
+    if (fit_zb(h, ck)) return -1;
     if (fit_du(h, ck)) return -1;
-    fit_dbdr(h, ck, h->db_threads);
+    if (fit_dbdr(h, ck, h->db_threads)) return -1;
     const long nt = 3 * (ck.p_hi - ck.p_lo);
     const long ta = (long)(ck.a_hi - ck.a_lo) * FIT_KP, tc = (long)(ck.c_hi - ck.c_lo) * FIT_KP;
     k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(
@@ -805,10 +890,6 @@ static int fit_descriptor_stages(mdp_fit *h, bool rows, double *G = nullptr, dou
                             : launch_ui<double, 4>(h->model, h->fp, n, h->s);
     if (urc) return -1;
     count_launches(1);
-    int zb_per_sm = 0;
-    if (kernel_setup((const void *)k_fit_zb, FIT_ZB_WARPS * 32, (size_t)idxu_count(TJMAX) * 32 * sizeof(double2),
-                     &zb_per_sm, "k_fit_zb"))
-        return -1;
     for (const auto &ck : h->chunks)
         if (fit_chunk(h, ck, rows, G, bi, bv)) return -1;
     MDP_CUDA_TRY(cudaGetLastError());
@@ -825,21 +906,14 @@ int fit_pair_derivs(mdp_fit *h, float *dbdr_out, double *blist_out)
                   : tj == 6 ? launch_ui<double, 6>(h->model, h->fp, n, h->s)
                             : launch_ui<double, 4>(h->model, h->fp, n, h->s);
     if (urc) return -1;
-    int zb_per_sm = 0;
-    if (kernel_setup((const void *)k_fit_zb, FIT_ZB_WARPS * 32, (size_t)idxu_count(TJMAX) * 32 * sizeof(double2),
-                     &zb_per_sm, "k_fit_zb"))
-        return -1;
-    const size_t zsm = (size_t)idxu_count(tj) * 32 * sizeof(double2);
     for (const auto &ck : h->chunks) {
-        k_fit_zb<<<std::max(1, std::min(ck.t_hi - ck.t_lo, num_sms())), FIT_ZB_WARPS * 32, zsm, h->s>>>(
-            h->fp.Ut.as<double2>(), n, h->tabs.as<FitTables>(), h->Z.as<double2>(), h->B.as<double>(), ck.t_lo,
-            ck.t_hi);
+        if (fit_zb(h, ck)) return -1;
         if (fit_du(h, ck)) return -1;
-        fit_dbdr(h, ck, h->db_threads);
+        if (fit_dbdr(h, ck, h->db_threads)) return -1;
         const long np = ck.p_hi - ck.p_lo, ne = 3 * np * nk;
         if (ne) k_fit_dbdr_export<<<(unsigned)((ne + 255) / 256), 256, 0, h->s>>>(h->dbdr.as<double>(), np, nk,
                                                                                 ck.p_lo, dbdr_out);
-        count_launches(2);
+        count_launches(1);
     }
     if (blist_out)
         MDP_CUDA_TRY(cudaMemcpyAsync(blist_out, h->B.p, sizeof(double) * nk * (size_t)n, cudaMemcpyDeviceToDevice,
@@ -1253,8 +1327,9 @@ int mdp_fit_tune(mdp_fit *h, int *out3)
     h->du_threads = bsel;
     bt = 1e30f;
     bsel = h->db_threads;
-    for (int c : tcand) {
-        const float t = timeit([&]() { fit_dbdr(h, h->chunks[0], c); return 0; });
+    const int dcand[3] = {FIT_DB_TPA, 2 * FIT_DB_TPA, 4 * FIT_DB_TPA};   // 1, 2, 4 atoms per CTA
+    for (int c : dcand) {
+        const float t = timeit([&]() { return fit_dbdr(h, h->chunks[0], c); });
         if (t >= 0 && t < bt) { bt = t; bsel = c; }
     }
     h->db_threads = bsel;

@@ -18,6 +18,7 @@
 
 #include "common.cuh"
 
+#include <climits>
 #include <type_traits>
 
 namespace mdp {
@@ -1186,9 +1187,24 @@ template <> struct FAccSel<float> { typedef FAccComp type; };
 constexpr int FR_THREADS = 128;
 // per-thread shared memory: seeds/links (2 * sum_mb 2mb values) + 16 geometry values
 template <int TJ> constexpr int fr_seed_vals() { return 2 * (TJ / 2) * (TJ / 2 + 1); }
+// Y staging: a CTA's window of FR_THREADS consecutive pairs spans a few atoms
+// (about seven at 19 pairs per atom); when it spans at most fr_ycap<T>()
+// atoms their Y rows are copied once into shared memory ([k][slot]) and the
+// pairs read them there instead of each through L1 / L2.
+#ifndef FR_YCAP_D
+#define FR_YCAP_D 16
+#endif
+#ifndef FR_YCAP_F
+#define FR_YCAP_F 12
+#endif
+template <typename T> __host__ __device__ constexpr int fr_ycap()
+{
+    return std::is_same<T, float>::value ? FR_YCAP_F : FR_YCAP_D;
+}
 template <typename T, int TJ> constexpr size_t fr_smem_bytes()
 {
-    return (sizeof(T) * fr_seed_vals<TJ>() + sizeof(double) * 16) * FR_THREADS;
+    return (sizeof(T) * fr_seed_vals<TJ>() + sizeof(double) * 16) * FR_THREADS +
+           (size_t)yh_count(TJ) * fr_ycap<T>() * sizeof(typename cplx<T>::type);
 }
 __host__ __device__ constexpr int fr_seed_off(int mb) { return mb * (mb - 1); }   // complex offset of S_mb
 __host__ __device__ constexpr int fr_row_off(int j) { return j * (j + 1) / 2; }   // stored row j
@@ -1303,14 +1319,15 @@ __device__ __forceinline__ void fr_col_fwd(FrState<T, TJ> &st, T (&pr)[TJ + 1], 
 
 // weighted Y row (J, MB) added into the adjoint row (entries 0..J)
 template <typename T, int TJ, int J, int MB>
-__device__ __forceinline__ void fr_add_y(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi)
+__device__ __forceinline__ void fr_add_y(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi,
+                                         const int ys)
 {
     typedef typename cplx<T>::type T2;
-    const T2 *yrow = Yi + (yh_block(J) + (J + 1) * MB) * 32;
+    const T2 *yrow = Yi + (yh_block(J) + (J + 1) * MB) * ys;
     constexpr int MAMAX = (2 * MB == J) ? MB : J;
 #pragma unroll
     for (int ma = 0; ma <= MAMAX; ma++) {
-        const T2 y = yrow[ma * 32];
+        const T2 y = yrow[ma * ys];
         // v-space (FP32): u = unorm v, so the adjoint of the row v is unorm Y
         const T un = fr_cf<T>() ? unorm<T>(J, MB, ma) : T(1);
         const T nu = (2 * MB == J && ma == MB) ? T(0.5) * un : un;
@@ -1321,7 +1338,7 @@ __device__ __forceinline__ void fr_add_y(FrState<T, TJ> &st, const typename cplx
 // phase B backward: adjoint row of layer J (column MB) in st.l*; parent row J-1
 template <typename T, int TJ, int J, int MB, typename Acc>
 __device__ __forceinline__ void fr_col_bwd(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi,
-                                           Acc (&G)[4], T *__restrict__ qs)
+                                           const int ys, Acc (&G)[4], T *__restrict__ qs)
 {
     constexpr int PO = fr_row_off(J - 1);
     const T ar = st.ar, ai = st.ai, br = st.br, bi = st.bi;
@@ -1369,7 +1386,7 @@ __device__ __forceinline__ void fr_col_bwd(FrState<T, TJ> &st, const typename cp
     }
     if constexpr (J - 1 >= 2 * MB) {
         // parent is row (J-1, MB) of this column
-        fr_add_y<T, TJ, J - 1, MB>(st, Yi);
+        fr_add_y<T, TJ, J - 1, MB>(st, Yi, ys);
         if constexpr (J - 1 == 2 * MB + 1 && 2 * (MB + 1) <= TJ) {
             constexpr int O = fr_seed_off(MB + 1);
 #pragma unroll
@@ -1379,7 +1396,7 @@ __device__ __forceinline__ void fr_col_bwd(FrState<T, TJ> &st, const typename cp
             }
         }
         // the column's first computed row is layer max(1, 2MB)
-        if constexpr (J - 1 >= (MB == 0 ? 1 : 2 * MB)) fr_col_bwd<T, TJ, J - 1, MB>(st, Yi, G, qs);
+        if constexpr (J - 1 >= (MB == 0 ? 1 : 2 * MB)) fr_col_bwd<T, TJ, J - 1, MB>(st, Yi, ys, G, qs);
     } else {
         // parent is the seed S_MB = mirror of row (J' = 2MB-1, MB-1): store the
         // adjoint of that row, L[ma] = (-1)^(MB-1+ma) conj(l'[J' - ma])
@@ -1395,7 +1412,7 @@ __device__ __forceinline__ void fr_col_bwd(FrState<T, TJ> &st, const typename cp
 
 template <typename T, int TJ, int MB, typename Acc>
 __device__ __forceinline__ void fr_columns(FrState<T, TJ> &st, const typename cplx<T>::type *__restrict__ Yi,
-                                           Acc (&G)[4], T *__restrict__ qs)
+                                           const int ys, Acc (&G)[4], T *__restrict__ qs)
 {
     if constexpr (MB >= 0) {
         T pr[TJ + 1], pi[TJ + 1];
@@ -1415,26 +1432,24 @@ __device__ __forceinline__ void fr_columns(FrState<T, TJ> &st, const typename cp
         // adjoint row of layer TJ = its weighted Y row
 #pragma unroll
         for (int ma = 0; ma <= TJ; ma++) { st.lr[ma] = T(0); st.li[ma] = T(0); }
-        fr_add_y<T, TJ, TJ, MB>(st, Yi);
-        fr_col_bwd<T, TJ, TJ, MB>(st, Yi, G, qs);
+        fr_add_y<T, TJ, TJ, MB>(st, Yi, ys);
+        fr_col_bwd<T, TJ, TJ, MB>(st, Yi, ys, G, qs);
         asm volatile("" ::: "memory");
-        fr_columns<T, TJ, MB - 1>(st, Yi, G, qs);
+        fr_columns<T, TJ, MB - 1>(st, Yi, ys, G, qs);
     }
 }
 
 // pcw (several element types): per pair cutoff and neighbour weight
 // (radelem[ti] + radelem[tj]) rcutfac and wjelem[tj], cpuSnap4.cpp:813-838
+// Yi: the pair's atom's Y row entries, element k at Yi[k * ys]
 template <typename T, int TJ>
-__device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__ prij, const int2 *__restrict__ pinfo,
-                                        const SnapGeom &gp, const typename cplx<T>::type *__restrict__ Y,
-                                        double4 *__restrict__ dEslot, T *__restrict__ qs, double *__restrict__ qg,
-                                        const double2 *__restrict__ pcw)
+__device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__ prij, const int2 inf,
+                                        const SnapGeom &gp, const typename cplx<T>::type *__restrict__ Yi,
+                                        const int ys, double4 *__restrict__ dEslot, T *__restrict__ qs,
+                                        double *__restrict__ qg, const double2 *__restrict__ pcw)
 {
-    typedef typename cplx<T>::type T2;
     typedef typename FAccSel<T>::type Acc;
-    constexpr int NYH = yh_count(TJ);
     const double4 r = prij[p];
-    const int2 inf = pinfo[p];
     FrState<T, TJ> st;
     {
         PairGeo g;
@@ -1459,7 +1474,6 @@ __device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__
         }
         qg[15 * FR_THREADS] = 2.0 * g.sfac;
     }
-    const T2 *Yi = Y + (size_t)(inf.x >> 5) * NYH * 32 + (inf.x & 31);   // tiled: element k at Yi[k*32]
     {
         T pr[TJ + 1], pi[TJ + 1];
         fr_seeds<T, TJ, 0>(st.ar, st.ai, st.br, st.bi, pr, pi, qs);
@@ -1467,7 +1481,7 @@ __device__ __forceinline__ void fr_pair(const int p, const double4 *__restrict__
     Acc G[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) G[k].init(T(0));
-    fr_columns<T, TJ, TJ / 2>(st, Yi, G, qs);
+    fr_columns<T, TJ, TJ / 2>(st, Yi, ys, G, qs);
     // after column 0, st.l[0] is the adjoint of the root u_0 = 1 (its own
     // half-weighted Y term included), whose real part is F
     const double F = (double)st.lr[0];
@@ -1488,12 +1502,43 @@ __device__ __forceinline__ void fr_kernel_body(const double4 *__restrict__ prij,
                                                const typename cplx<T>::type *__restrict__ Y,
                                                double4 *__restrict__ dEslot, const double2 *__restrict__ pcw)
 {
+    typedef typename cplx<T>::type T2;
+    constexpr int NYH = yh_count(TJ), YC = fr_ycap<T>();
     extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int amm[2 * (FR_THREADS / 32)];
     double *qg = reinterpret_cast<double *>(smraw) + threadIdx.x;
     T *qs = reinterpret_cast<T *>(reinterpret_cast<double *>(smraw) + 16 * FR_THREADS) + threadIdx.x;
+    T2 *Ys = reinterpret_cast<T2 *>(reinterpret_cast<T *>(reinterpret_cast<double *>(smraw) + 16 * FR_THREADS) +
+                                    fr_seed_vals<TJ>() * FR_THREADS);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int npairs = *pnum;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npairs; p += gridDim.x * blockDim.x)
-        fr_pair<T, TJ>(p, prij, pinfo, gp, Y, dEslot, qs, qg, pcw);
+    // windows of FR_THREADS consecutive pairs (the loop bound is uniform over the CTA)
+    for (int base = blockIdx.x * FR_THREADS; base < npairs; base += gridDim.x * FR_THREADS) {
+        const int p = base + threadIdx.x;
+        int2 inf = make_int2(0, 0);
+        int mn = INT_MAX, mx = INT_MIN;
+        if (p < npairs) { inf = pinfo[p]; mn = mx = inf.x; }
+        mn = __reduce_min_sync(0xffffffffu, mn);
+        mx = __reduce_max_sync(0xffffffffu, mx);
+        __syncthreads();   // the previous window is done with Ys and amm
+        if (lane == 0) { amm[w] = mn; amm[FR_THREADS / 32 + w] = mx; }
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < FR_THREADS / 32; v++) { mn = min(mn, amm[v]); mx = max(mx, amm[FR_THREADS / 32 + v]); }
+        const int na = mx - mn + 1;   // atoms the window spans (mx >= mn: the window has a pair)
+        const bool staged = na <= YC;
+        if (staged) {
+            for (int e = threadIdx.x; e < NYH * na; e += FR_THREADS) {
+                const int k = e / na, sl = e - k * na, a = mn + sl;
+                Ys[k * YC + sl] = Y[((size_t)(a >> 5) * NYH + k) * 32 + (a & 31)];
+            }
+            __syncthreads();
+        }
+        if (p < npairs) {
+            const T2 *Yi = staged ? Ys + (inf.x - mn) : Y + (size_t)(inf.x >> 5) * NYH * 32 + (inf.x & 31);
+            fr_pair<T, TJ>(p, prij, inf, gp, Yi, staged ? YC : 32, dEslot, qs, qg, pcw);
+        }
+    }
 }
 
 template <typename T, int TJ>

@@ -131,3 +131,23 @@ def test_fit_recovers_known_coefficients():
     beta = fit.solve(A, b)
     bf.close()
     assert np.max(np.abs(beta - p.coeff)) < 1e-6 * np.max(np.abs(p.coeff))
+
+
+@pytest.mark.parametrize("tj", [4, 6, 8])
+def test_descriptors_contract_to_the_oracle(tj):
+    """At every 2J the fit takes (4, 6, 8): the batch's
+    per-atom bispectrum and dB/dR, contracted with beta, give the oracle's
+    per-atom energies (beta_0 + beta . B_i) and forces (beta . bd_i)."""
+    from oracle import oracle
+    p = configs.snap_params(tj, seed=11)
+    cfg = configs.ta_config((3, 3, 3), temp=300, jitter=0.1, seed=4)
+    xa, al, nl, nn = oracle.neighbor_list(cfg.x, cfg.box, p.rcut, 1.0, 64)
+    e, f, _ = oracle.snap_force(xa, al, nl, nn, p)
+    bf = fit.BatchFit(p)
+    bf.set_batch([fit.FitConfig(x=cfg.x, box=np.asarray(cfg.box, dtype=float), kind="bcc")])
+    bi, bd, _, bl = bf.descriptors()
+    bf.close()
+    beta0, beta = p.coeff[0], np.asarray(p.coeff[1:])
+    assert _rel(beta0 + beta @ bl, e) < 1e-10
+    assert _rel(bd @ beta, f) < 1e-10
+    assert _rel(bi[0], bl.sum(axis=1)) < 1e-12
