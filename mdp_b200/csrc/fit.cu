@@ -113,12 +113,17 @@ __global__ void k_fit_zbl(const double4 *__restrict__ x, const int *__restrict__
 // Z rows of every coupling and B for j >= j1, per 32-atom tile (lane = atom)
 // Z layout [tile][zoff + (j+1) mb + ma][lane]; B layout [k][atom]
 // ---------------------------------------------------------------------------
-// Every coupling is compile-time specialised (the Y kernel's z_rows: CG
-// coefficients as constant operands, U rows in registers), output layer by
-// layer.  Within a layer the (coupling, mb) rows go to the warps round-robin
-// in enumeration order, so the warps run one or two couplings' code at a
-// time; a barrier per layer keeps them together.
+// Every coupling is compile-time specialised (CG coefficients as constant
+// operands, U rows in registers), output layer by layer.  Within a layer all
+// warps walk the couplings in the same order, so the code in flight is one
+// coupling's; each warp owns a row mb and a range [lo, hi) of its entries ma
+// (a plan balanced on the host), which needs no reduction between warps.
+// (Giving each warp whole (coupling, mb) rows round-robin let the warps run
+// different couplings' code at once: 4.9 no_instruction stalls per issue.)
 constexpr int FIT_ZBT_WARPS = 10;
+struct ZbPlan {
+    unsigned char mb[JD][FIT_ZBT_WARPS], lo[JD][FIT_ZBT_WARPS], hi[JD][FIT_ZBT_WARPS];   // mb 255: idle
+};
 
 // offset of coupling (J1, J2, J)'s rows in the Z layout (fit_tables order)
 __host__ __device__ constexpr int fit_zoff(int tj, int J1, int J2, int J)
@@ -133,45 +138,84 @@ __host__ __device__ constexpr int fit_zoff(int tj, int J1, int J2, int J)
     return -1;
 }
 
+// entries lo <= ma < hi of row mb of scale * Z_{J1 J2 J}, summed over every
+// row pair ib, written to the coupling's block Zc ([(J+1) mb + ma][lane])
+template <int J1, int J2, int J>
+__device__ __forceinline__ void zbt_rows(const int mb, const int lo, const int hi, const double2 *__restrict__ Us,
+                                         const int lane, const double scale, double2 *__restrict__ Zc)
+{
+    constexpr int N1 = J1 + 1, N2 = J2 + 1;
+    constexpr int CGB = cg_block(J1, J2, J);
+    double yr[J + 1], yi[J + 1];
+#pragma unroll
+    for (int ma = 0; ma <= J; ma++) { yr[ma] = 0.0; yi[ma] = 0.0; }
+    const int mb1min = max(0, (2 * mb - J - J2 + J1) / 2);
+    const int mb2max = (2 * mb - J - (2 * mb1min - J1) + J2) / 2;
+    const int nb = nb_of(J1, J2, J, mb);
+    for (int ib = 0; ib < nb; ib++) {
+        const int mb1 = mb1min + ib, mb2 = mb2max - ib;
+        const double sc = scale * cgc<double>(CGB + mb1 * N2 + mb2);
+        const double2 *r1 = Us + (idxu_block(J1) + N1 * mb1) * 32 + lane;
+        const double2 *r2 = Us + (idxu_block(J2) + N2 * mb2) * 32 + lane;
+        double u1r[N1], u1i[N1], u2r[N2], u2i[N2];
+#pragma unroll
+        for (int k = 0; k < N1; k++) { const double2 v = r1[k * 32]; u1r[k] = sc * v.x; u1i[k] = sc * v.y; }
+#pragma unroll
+        for (int k = 0; k < N2; k++) { const double2 v = r2[k * 32]; u2r[k] = v.x; u2i[k] = v.y; }
+#pragma unroll
+        for (int ma = 0; ma <= J; ma++) {
+            if (ma < lo || ma >= hi) continue;
+            const int ma1min = cmax(0, (2 * ma - J - J2 + J1) / 2);
+            const int ma2max = (2 * ma - J - (2 * ma1min - J1) + J2) / 2;
+            const int na = cmin(J1, (2 * ma - J + J2 + J1) / 2) - ma1min + 1;
+#pragma unroll
+            for (int ia = 0; ia < na; ia++) {
+                const int ma1 = ma1min + ia, ma2 = ma2max - ia;
+                const double c = cgc<double>(CGB + ma1 * N2 + ma2);
+                const double tr = c * u1r[ma1], ti = c * u1i[ma1];
+                yr[ma] += tr * u2r[ma2] - ti * u2i[ma2];
+                yi[ma] += tr * u2i[ma2] + ti * u2r[ma2];
+            }
+        }
+    }
+#pragma unroll
+    for (int ma = 0; ma <= J; ma++)
+        if (ma >= lo && ma < hi) Zc[(size_t)((J + 1) * mb + ma) * 32] = make_double2(yr[ma], yi[ma]);
+}
+
 template <int TJ, int J, int J1, int J2>
 __device__ __forceinline__ void zbt_layer(const double2 *__restrict__ Us, double2 *__restrict__ Zt, const int lane,
-                                          const int w, const double scale, int item)
+                                          const int mb, const int lo, const int hi, const double scale)
 {
     if constexpr (J1 <= TJ) {
         if constexpr (J2 <= J1) {
             if constexpr (coupling_ok(J1, J2, J)) {
                 constexpr int ZO = fit_zoff(TJ, J1, J2, J);
-                for (int mb = 0; 2 * mb <= J; mb++, item++) {
-                    if (item % FIT_ZBT_WARPS != w) continue;
-                    YRow<double> acc;
-                    acc.zero();
-                    z_rows<double, J1, J2, J>(mb, 0, 1, Us, Us, lane, scale, acc);
-#pragma unroll
-                    for (int ma = 0; ma <= J; ma++) Zt[(size_t)(ZO + (J + 1) * mb + ma) * 32] = acc.get(ma);
-                }
+                zbt_rows<J1, J2, J>(mb, lo, hi, Us, lane, scale, Zt + (size_t)ZO * 32);
             }
-            zbt_layer<TJ, J, J1, J2 + 1>(Us, Zt, lane, w, scale, item);
+            zbt_layer<TJ, J, J1, J2 + 1>(Us, Zt, lane, mb, lo, hi, scale);
         } else {
-            zbt_layer<TJ, J, J1 + 1, 0>(Us, Zt, lane, w, scale, item);
+            zbt_layer<TJ, J, J1 + 1, 0>(Us, Zt, lane, mb, lo, hi, scale);
         }
     }
 }
 
 template <int TJ, int J>
 __device__ __forceinline__ void zbt_layers(const double2 *__restrict__ Us, double2 *__restrict__ Zt, const int lane,
-                                           const int w, const int bnorm)
+                                           const int w, const int bnorm, const ZbPlan &P)
 {
     if constexpr (J <= TJ) {
-        zbt_layer<TJ, J, 0, 0>(Us, Zt, lane, w, bnorm ? 1.0 / (J + 1) : 1.0, 0);
-        __syncthreads();
-        zbt_layers<TJ, J + 1>(Us, Zt, lane, w, bnorm);
+        const int mb = P.mb[J][w];
+        if (mb != 255) zbt_layer<TJ, J, 0, 0>(Us, Zt, lane, mb, P.lo[J][w], P.hi[J][w], bnorm ? 1.0 / (J + 1) : 1.0);
+        __syncthreads();   // keeps the warps on one layer's code
+        zbt_layers<TJ, J + 1>(Us, Zt, lane, w, bnorm, P);
     }
 }
 
 template <int TJ>
 __global__ void __launch_bounds__(FIT_ZBT_WARPS * 32, 1)
-k_fit_zbt(const double2 *__restrict__ Ut, int natoms, const FitTables *__restrict__ T, double2 *__restrict__ Z,
-          double *__restrict__ B, int tile_lo, int tile_hi)
+k_fit_zbt(const double2 *__restrict__ Ut, int natoms, const FitTables *__restrict__ T, const ZbPlan P,
+          double2 *__restrict__ Z, double *__restrict__ B, int tile_lo, int tile_hi)
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *Us = reinterpret_cast<double2 *>(smraw);
@@ -183,7 +227,7 @@ k_fit_zbt(const double2 *__restrict__ Ut, int natoms, const FitTables *__restric
         for (int k = threadIdx.x; k < NU * 32; k += blockDim.x) Us[k] = src[k];
         __syncthreads();
         double2 *Zt = Z + (size_t)(tile - tile_lo) * nz * 32 + lane;
-        zbt_layers<TJ, 0>(Us, Zt, lane, w, T->bnorm);
+        zbt_layers<TJ, 0>(Us, Zt, lane, w, T->bnorm, P);   // ends on a barrier: B reads other warps' Z rows
         // B_k = 2 sum_half w Re(U_j* Z) (- bzero), cpuComputeBi2 (cpuSnap2.cpp:516-541)
         const int atom = tile * 32 + lane;
         for (int k = w; k < T->ntri; k += FIT_ZBT_WARPS) {
@@ -317,7 +361,7 @@ k_fit_du(const double4 *__restrict__ prij, long npairs, SnapGeom gp, double2 *__
 // ---------------------------------------------------------------------------
 // dB_ik/dr_p along one axis: 2 sum over the three terms of cpuComputeDbidrj
 // (Z of the centre atom's couplings against the pair's dU rows), half plane
-// with the middle row's centre at 1/2.  dbdr[k * stride + t]
+// with the middle row's centre at 1/2.
 // ---------------------------------------------------------------------------
 // The pair's dU rows of layer L are loaded once (registers) and every dB/dR
 // term on that layer is applied to them: dU is read once per thread.  The Z
@@ -362,11 +406,12 @@ __device__ __forceinline__ void fdb_layers(const double2 *__restrict__ d, const 
 
 // dB_ik/dr_p along one axis: 2 sum over the three terms of cpuComputeDbidrj
 // (Z of the centre atom's couplings against the pair's dU rows), half plane
-// with the middle row's centre at 1/2.  dbdr[k * stride + t], t = (p - p_lo) * 3
-// + dir.  A CTA takes APC adjacent atoms (APC divides 32, so they share a Z
-// tile) and their pairs, 64 threads per atom: the atoms' Z rows (38 KB per
-// atom at 2J = 8) are copied once into shared memory ([entry][atom]), so
-// every pair-direction reads them there.  Read in place from the tile
+// with the middle row's centre at 1/2.  dbdr[t * ntri + k], t = (p - p_lo) * 3
+// + dir: a pair-direction's components are contiguous, so the row gathers
+// (k fastest over threads) read them coalesced.  A CTA takes APC adjacent
+// atoms (APC divides 32, so they share a Z tile) and their pairs, 64 threads
+// per atom: the atoms' Z rows (38 KB per atom at 2J = 8) are copied once into
+// shared memory ([entry][atom]), so every pair-direction reads them there.  Read in place from the tile
 // layout, each entry sat in its own 128-byte line, 512 bytes from the next:
 // an atom's rows touched 2,386 lines, more than L1 holds for the atoms in
 // flight, and the dot products waited on L2.
@@ -396,7 +441,7 @@ k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int *__restrict__
         double acc[FIT_NT];
         for (int k = 0; k < ntri; k++) acc[k] = 0.0;
         fdb_layers<TJ, 0, APC>(dul + t, stride, Zs + (atom - a0), T, acc);
-        for (int k = 0; k < ntri; k++) dbdr[(long)k * stride + t] = acc[k];
+        for (int k = 0; k < ntri; k++) dbdr[t * ntri + k] = acc[k];
     }
 }
 
@@ -432,7 +477,7 @@ __global__ void k_fit_rev_sort(int natoms, const int *__restrict__ roff, int *__
 // rows of atom a: G[a][c][k] = sum_(p: j = a) dbdr - sum_(p: i = a) dbdr,
 // written as fit rows [wf * (0, G)] with target -wf * f; row = 3 a + c
 __global__ void k_fit_rows(int a_lo, int a_hi, int ntri, const int *__restrict__ poff, const int *__restrict__ roff,
-                           const int *__restrict__ rlist, const double *__restrict__ dbdr, long stride, long p_lo,
+                           const int *__restrict__ rlist, const double *__restrict__ dbdr, long p_lo,
                            const int *__restrict__ cfg, const double *__restrict__ wf, const double *__restrict__ f,
                            double *__restrict__ G, double *__restrict__ R, double *__restrict__ tgt, long row0)
 {
@@ -446,11 +491,11 @@ __global__ void k_fit_rows(int a_lo, int a_hi, int ntri, const int *__restrict__
         for (int q = roff[a]; q < roff[a + 1]; q++) {
             const long p = rlist[q] - p_lo;
 #pragma unroll
-            for (int c = 0; c < 3; c++) g[c] += dbdr[(long)kk * stride + 3 * p + c];
+            for (int c = 0; c < 3; c++) g[c] += dbdr[(3 * p + c) * ntri + kk];
         }
         for (long p = poff[a] - p_lo; p < poff[a + 1] - p_lo; p++) {
 #pragma unroll
-            for (int c = 0; c < 3; c++) g[c] -= dbdr[(long)kk * stride + 3 * p + c];
+            for (int c = 0; c < 3; c++) g[c] -= dbdr[(3 * p + c) * ntri + kk];
         }
         if (G)
             for (int c = 0; c < 3; c++) G[((size_t)a * 3 + c) * ntri + kk] = g[c];
@@ -465,7 +510,7 @@ __global__ void k_fit_rows(int a_lo, int a_hi, int ntri, const int *__restrict__
 // per configuration: bi, the virial, and the energy row [we * (N, bi)] / we * E
 __global__ void k_fit_cfg(int c_lo, int c_hi, int ntri, const int *__restrict__ ca0, const int *__restrict__ cn,
                           const int *__restrict__ poff, const double *__restrict__ B, int natoms,
-                          const double *__restrict__ dbdr, long stride, long p_lo, const double4 *__restrict__ prij,
+                          const double *__restrict__ dbdr, long p_lo, const double4 *__restrict__ prij,
                           const double *__restrict__ we, const double *__restrict__ e, double *__restrict__ bi,
                           double *__restrict__ bv, double *__restrict__ R, double *__restrict__ tgt, long erow0)
 {
@@ -484,8 +529,8 @@ __global__ void k_fit_cfg(int c_lo, int c_hi, int ntri, const int *__restrict__ 
             for (long p = poff[a0]; p < poff[a0 + n]; p++) {
                 const double4 r = prij[p];
                 const long q = p - p_lo;
-                const double bx = dbdr[(long)kk * stride + 3 * q], by = dbdr[(long)kk * stride + 3 * q + 1],
-                             bz = dbdr[(long)kk * stride + 3 * q + 2];
+                const double bx = dbdr[(3 * q) * ntri + kk], by = dbdr[(3 * q + 1) * ntri + kk],
+                             bz = dbdr[(3 * q + 2) * ntri + kk];
                 s[0] -= r.x * bx; s[1] -= r.y * by; s[2] -= r.z * bz;
                 s[3] -= r.x * by; s[4] -= r.x * bz; s[5] -= r.y * bz;
             }
@@ -726,7 +771,7 @@ __global__ void k_fit_dbdr_export(const double *__restrict__ dbdr, long np, int 
     if (t >= 3 * np * ntri) return;
     const int k = (int)(t % ntri);
     const long pd = t / ntri;
-    out[(p_lo * 3 + pd) * ntri + k] = (float)dbdr[(long)k * (3 * np) + pd];
+    out[(p_lo * 3 + pd) * ntri + k] = (float)dbdr[t];
 }
 }  // namespace mdp
 
@@ -792,15 +837,94 @@ static int fit_du(mdp_fit *h, const mdp_fit::Chunk &ck)
     return tj == 8 ? fit_launch_du<8>(h, ck) : tj == 6 ? fit_launch_du<6>(h, ck) : fit_launch_du<4>(h, ck);
 }
 
+// least largest sum of c cut into k contiguous chunks (greedy under a cap)
+static long zb_min_cap(const std::vector<long> &c, int k)
+{
+    long lo = 0, hi = 0;
+    for (long v : c) { lo = std::max(lo, v); hi += v; }
+    while (lo < hi) {
+        const long mid = (lo + hi) / 2;
+        int n = 1;
+        long run = 0;
+        for (long v : c) {
+            if (run + v > mid) { n++; run = v; }
+            else run += v;
+        }
+        if (n <= k) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// The Z-kernel plan of 2J = tj: per layer J, the rows get warps where the
+// costliest chunk is, and each row's entries ma are cut into that many
+// contiguous ranges of least largest cost.  Cost of entry ma: 6 instructions
+// per term over every coupling and row pair; every warp on a row also pays
+// the row pairs' U loads (4 per u1 entry with its scaling, 1 per u2 entry).
+static ZbPlan zb_plan(int tj)
+{
+    ZbPlan P;
+    memset(&P, 0, sizeof(P));
+    memset(P.mb, 255, sizeof(P.mb));
+    for (int J = 0; J <= tj; J++) {
+        const int R = J / 2 + 1;
+        std::vector<std::vector<long>> c(R, std::vector<long>(J + 1, 0));
+        std::vector<long> load(R, 0);
+        for (int mb = 0; mb < R; mb++)
+            for (int j1 = 0; j1 <= tj; j1++)
+                for (int j2 = 0; j2 <= j1; j2++) {
+                    if (!coupling_ok(j1, j2, J)) continue;
+                    const int nb = nb_of(j1, j2, J, mb);
+                    load[mb] += (long)nb * (4 * (j1 + 1) + (j2 + 1));
+                    for (int ma = 0; ma <= J; ma++) {
+                        const int ma1min = std::max(0, (2 * ma - J - j2 + j1) / 2);
+                        const int na = std::min(j1, (2 * ma - J + j2 + j1) / 2) - ma1min + 1;
+                        c[mb][ma] += 6L * nb * na;
+                    }
+                }
+        std::vector<int> nw(R, 1);
+        for (int used = R; used < FIT_ZBT_WARPS; used++) {
+            int best = -1;
+            long bc = -1;
+            for (int r = 0; r < R; r++) {
+                if (nw[r] >= J + 1) continue;
+                const long v = zb_min_cap(c[r], nw[r]) + load[r];
+                if (v > bc) { bc = v; best = r; }
+            }
+            if (best < 0) break;
+            nw[best]++;
+        }
+        int w = 0;
+        for (int r = 0; r < R; r++) {
+            const long cap = zb_min_cap(c[r], nw[r]);
+            int a = 0;
+            for (int k = 0; k < nw[r]; k++, w++) {
+                int b = a;
+                long run = 0;
+                if (k == nw[r] - 1) b = J + 1;
+                else
+                    while (b <= J && run + c[r][b] <= cap) run += c[r][b++];
+                P.mb[J][w] = (unsigned char)r;
+                P.lo[J][w] = (unsigned char)a;
+                P.hi[J][w] = (unsigned char)b;
+                a = b;
+            }
+        }
+    }
+    return P;
+}
+
 // Z rows and B of one chunk's tiles (the fit takes 2J = 4, 6, 8)
 template <int TJ>
 static int fit_zbt(mdp_fit *h, const mdp_fit::Chunk &ck, unsigned g)
 {
+    static const ZbPlan plan = zb_plan(TJ);
     const size_t zsm = (size_t)idxu_count(TJ) * 32 * sizeof(double2);
     int per_sm = 0;
     if (kernel_setup((const void *)k_fit_zbt<TJ>, FIT_ZBT_WARPS * 32, zsm, &per_sm, "k_fit_zbt")) return -1;
     k_fit_zbt<TJ><<<g, FIT_ZBT_WARPS * 32, zsm, h->s>>>(h->fp.Ut.as<double2>(), h->natoms, h->tabs.as<FitTables>(),
-                                                       h->Z.as<double2>(), h->B.as<double>(), ck.t_lo, ck.t_hi);
+                                                       plan, h->Z.as<double2>(), h->B.as<double>(), ck.t_lo,
+                                                       ck.t_hi);
     return 0;
 }
 
@@ -864,15 +988,14 @@ static int fit_chunk(mdp_fit *h, const mdp_fit::Chunk &ck, bool rows, double *G,
     if (fit_zb(h, ck)) return -1;
     if (fit_du(h, ck)) return -1;
     if (fit_dbdr(h, ck, h->db_threads)) return -1;
-    const long nt = 3 * (ck.p_hi - ck.p_lo);
     const long ta = (long)(ck.a_hi - ck.a_lo) * FIT_KP, tc = (long)(ck.c_hi - ck.c_lo) * FIT_KP;
     k_fit_rows<<<(unsigned)((ta + 255) / 256), 256, 0, h->s>>>(
         ck.a_lo, ck.a_hi, h->tab.ntri, h->poff.as<int>(), h->roff.as<int>(), h->rlist.as<int>(), h->dbdr.as<double>(),
-        nt, ck.p_lo, h->cfg.as<int>(), h->wf.as<double>(), h->f.as<double>(), G, rows ? h->R.as<double>() : nullptr,
+        ck.p_lo, h->cfg.as<int>(), h->wf.as<double>(), h->f.as<double>(), G, rows ? h->R.as<double>() : nullptr,
         rows ? h->tgt.as<double>() : nullptr, h->nconf);
     k_fit_cfg<<<(unsigned)((tc + 255) / 256), 256, 0, h->s>>>(
         ck.c_lo, ck.c_hi, h->tab.ntri, h->ca0.as<int>(), h->cn.as<int>(), h->poff.as<int>(), h->B.as<double>(), n,
-        h->dbdr.as<double>(), nt, ck.p_lo, h->fp.prij.as<double4>(), h->we.as<double>(), h->e.as<double>(), bi, bv,
+        h->dbdr.as<double>(), ck.p_lo, h->fp.prij.as<double4>(), h->we.as<double>(), h->e.as<double>(), bi, bv,
         rows ? h->R.as<double>() : nullptr, rows ? h->tgt.as<double>() : nullptr, 0);
     count_launches(2);
     MDP_CUDA_TRY(cudaGetLastError());

@@ -364,12 +364,13 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
 // per pair recomputes the recursion path that reaches its warp's column: the
 // seed chain (rows 1, 2c..2c+1 of the columns c below, each mirrored into the
 // next column's seed) and then the column's own rows, which it adds into a
-// half-plane tile in shared memory ([yh index][lane]).  Every column's path
+// half-plane tile in shared memory ([uh index][lane]).  Every column's path
 // has one row per layer 1..TJ, so the warps' work is equal; the top two
 // columns share the last warp (the top one continues from the row the other
 // ends its chain with).  Warps own disjoint tile entries: no atomics.  The
-// tile is then written out as the full plane with wself on the diagonal and
-// rows mb > j/2 by inversion symmetry (cpuSnap4.cpp:11-244, cpuAddWself2Ui).
+// tile is then written out as the full plane with wself on the diagonal,
+// and rows mb > j/2 and the middle rows' right halves by inversion symmetry
+// (cpuSnap4.cpp:11-244, cpuAddWself2Ui).
 // (a, b, sfac) of each pair come from the pair stage.
 // ---------------------------------------------------------------------------
 // pairs per lane per pass: FP32 takes two (independent chains, half the tile
@@ -393,15 +394,33 @@ template <typename T, int TJ> __host__ __device__ constexpr bool uc_split()
     return UC_SPLIT && TJ == 8 && std::is_same<T, double>::value;
 }
 template <typename T, int TJ> __host__ __device__ constexpr int uc_warps() { return uc_split<T, TJ>() ? 8 : TJ / 2; }
+// CTAs per SM the split FP64 kernel is compiled for: three 74 KB tiles fit an
+// SM's shared memory, which holds 80 registers a thread
+#ifndef UC_MINB_D
+#define UC_MINB_D 3
+#endif
+// (0, the others: no bound, as an explicit 1 makes ptxas spend registers)
+template <typename T, int TJ> __host__ __device__ constexpr int uc_minb() { return uc_split<T, TJ>() ? UC_MINB_D : 0; }
 template <int TJ> __host__ __device__ constexpr UcJob uc_job(int w)
 {
     constexpr UcJob plan8[8] = {{0, 0, 5}, {0, 6, 8}, {1, 0, 6}, {1, 7, 8},
                                 {2, 0, 6}, {2, 7, 8}, {3, 0, 8}, {4, 0, 8}};
     return plan8[w];
 }
+// The tile holds the half plane without the entries right of a middle row's
+// centre (the mirror of its left half): 145 entries at 2J = 8 against 155,
+// which lets three FP64 CTAs share an SM (74 KB each) instead of two.
+__host__ __device__ constexpr int uh_len(int j) { return (j + 1) * ((j + 1) / 2) + (j % 2 == 0 ? j / 2 + 1 : 0); }
+__host__ __device__ constexpr int uh_block(int j)
+{
+    int n = 0;
+    for (int jj = 0; jj < j; jj++) n += uh_len(jj);
+    return n;
+}
+__host__ __device__ constexpr int uh_count(int tj) { return uh_block(tj + 1); }
 template <typename T, int TJ> constexpr size_t uc_smem_bytes()
 {
-    return (size_t)yh_count(TJ) * 32 * sizeof(typename cplx<T>::type);
+    return (size_t)uh_count(TJ) * 32 * sizeof(typename cplx<T>::type);
 }
 
 // per-pair state; the root of the recursion is v_0 = sfac, so every row comes
@@ -453,9 +472,10 @@ __device__ __forceinline__ void uc_column(UcPairs<T, TJ> &s, typename cplx<T>::t
             uc_column<T, TJ, MB, J + 1, JEND, JACC>(s, acc);
             return;
         }
-        T2 *row = acc + (yh_block(J) + (J + 1) * MB) * 32;
+        T2 *row = acc + (uh_block(J) + (J + 1) * MB) * 32;
+        constexpr int MAMAX = (2 * MB == J) ? MB : J;
 #pragma unroll
-        for (int ma = 0; ma <= J; ma++) {
+        for (int ma = 0; ma <= MAMAX; ma++) {
             const T nu = unorm<T>(J, MB, ma);
             T2 v = row[ma * 32];
 #pragma unroll
@@ -522,20 +542,20 @@ __device__ __forceinline__ void uc_dispatch(const int w, UcPairs<T, TJ> &s, type
 }
 
 template <typename T, int TJ>
-__global__ void __launch_bounds__(uc_warps<T, TJ>() * 32)
+__global__ void __launch_bounds__(uc_warps<T, TJ>() * 32, uc_minb<T, TJ>())
 k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const double4 *__restrict__ pab,
           int natoms, typename cplx<T>::type *__restrict__ Ut, const int *__restrict__ welem = nullptr,
           int ipad = 0)
 {
     typedef typename cplx<T>::type T2;
     constexpr int NW = uc_warps<T, TJ>();
-    constexpr int NU = idxu_count(TJ), NYH = yh_count(TJ);
+    constexpr int NU = idxu_count(TJ), NUH = uh_count(TJ);
     extern __shared__ __align__(16) unsigned char smraw[];
     T2 *acc = reinterpret_cast<T2 *>(smraw);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int ntiles = (natoms + 31) >> 5;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        for (int k = threadIdx.x; k < NYH * 32; k += NW * 32) acc[k] = T2{T(0), T(0)};
+        for (int k = threadIdx.x; k < NUH * 32; k += NW * 32) acc[k] = T2{T(0), T(0)};
         __syncthreads();
         const int i = tile * 32 + lane;
         int p = 0, pend = 0;
@@ -569,12 +589,13 @@ k_snap_uc(const int *__restrict__ poff, const double4 *__restrict__ prij, const 
             while (idxu_block(j + 1) <= k) j++;
             const int rem = k - idxu_block(j), mb = rem / (j + 1), ma = rem - mb * (j + 1);
             T2 v;
-            if (2 * mb <= j) {
-                v = acc[(yh_block(j) + rem) * 32 + l];
+            if (2 * mb < j || (2 * mb == j && ma <= mb)) {
+                v = acc[(uh_block(j) + rem) * 32 + l];
                 if (ma == mb) v.x += ws;
             } else {
+                // mirror: rows mb > j/2 and a middle row's right half
                 const int sb = j - mb, sa = j - ma;
-                const T2 u = acc[(yh_block(j) + (j + 1) * sb + sa) * 32 + l];
+                const T2 u = acc[(uh_block(j) + (j + 1) * sb + sa) * 32 + l];
                 const T sg = ((sa + sb) & 1) ? T(-1) : T(1);
                 v = T2{sg * (u.x + (sa == sb ? ws : T(0))), -sg * u.y};
             }
