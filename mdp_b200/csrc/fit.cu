@@ -363,44 +363,86 @@ k_fit_du(const double4 *__restrict__ prij, long npairs, SnapGeom gp, double2 *__
 // (Z of the centre atom's couplings against the pair's dU rows), half plane
 // with the middle row's centre at 1/2.
 // ---------------------------------------------------------------------------
-// The pair's dU rows of layer L are loaded once (registers) and every dB/dR
-// term on that layer is applied to them: dU is read once per thread.  The Z
-// rows come from shared memory, element e of the atom's row block at
-// Zi[e * ZS].
-template <int L, int ZS>
-__device__ __forceinline__ void fdb_layer(const double2 *__restrict__ d, const long stride,
-                                          const double2 *__restrict__ Zi, const FitTables *__restrict__ T,
-                                          double *__restrict__ acc)
+// Every dB/dR term is compile-time: triple k = (j1, j2, j) has the terms
+//   Z(j1, j2, j) . dU_j,  Z(j, j2, j1) . dU_j1,  Z(j, j1, j2) . dU_j2
+// with factors 2, 2 (j+1)/(j1+1), 2 (j+1)/(j2+1) (2, 2, 2 with bnorm), so the
+// 55 sums at 2J = 8 stay in registers and the Z offsets are immediates.  The
+// pair's dU is read one row (layer L, column MB) at a time and every term on
+// layer L is applied to that row.  (With the term list read from a table at
+// run time, acc[k] lived in local memory and each term's read-modify-write
+// waited on the previous one.)
+struct FitTri {
+    int j1, j2, j;
+};
+__host__ __device__ constexpr FitTri fit_tri(int tj, int k)
 {
-    constexpr int YO = yh_block(L), NR = L / 2 + 1, NE = NR * (L + 1);
-    double2 du[NE];
+    int n = 0;
+    for (int j1 = 0; j1 <= tj; j1++)
+        for (int j2 = 0; j2 <= j1; j2++)
+            for (int j = j1 - j2; j <= cmin(tj, j1 + j2); j += 2)
+                if (j >= j1) {
+                    if (n == k) return FitTri{j1, j2, j};
+                    n++;
+                }
+    return FitTri{-1, -1, -1};
+}
+
+// Z(C1, C2, L) row MB against the dU row (dr, di), entries 0..MAMAX
+template <int TJ, int L, int MB, int MAMAX, int ZS, int C1, int C2>
+__device__ __forceinline__ double fdb_dot(const double (&dr)[MAMAX + 1], const double (&di)[MAMAX + 1],
+                                          const double2 *__restrict__ Zi)
+{
+    constexpr int ZO = fit_zoff(TJ, C1, C2, L) + (L + 1) * MB;
+    const double2 *z = Zi + ZO * ZS;
+    double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-    for (int e = 0; e < NE; e++) du[e] = d[(long)(YO + e) * stride];
-    const int q0 = T->lt_off[L], q1 = q0 + T->lt_n[L];
-    for (int q = q0; q < q1; q++) {
-        const double2 *z = Zi + (size_t)T->lt_z[q] * ZS;
-        double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-        for (int e = 0; e < NE; e++) {
-            const int mb = e / (L + 1), ma = e % (L + 1);
-            if (2 * mb == L && ma > mb) continue;   // right of a middle row's centre
-            const double wgt = (2 * mb == L && ma == mb) ? 0.5 : 1.0;
-            const double2 zz = z[(size_t)e * ZS];
-            if (e & 1) s1 += wgt * (du[e].x * zz.x + du[e].y * zz.y);
-            else s0 += wgt * (du[e].x * zz.x + du[e].y * zz.y);
-        }
-        acc[T->lt_k[q]] += T->lt_fac[q] * (s0 + s1);
+    for (int ma = 0; ma <= MAMAX; ma++) {
+        const double2 zz = z[ma * ZS];
+        if (ma & 1) s1 += dr[ma] * zz.x + di[ma] * zz.y;
+        else s0 += dr[ma] * zz.x + di[ma] * zz.y;
+    }
+    return s0 + s1;
+}
+
+template <int TJ, int L, int MB, int MAMAX, int ZS, int K>
+__device__ __forceinline__ void fdb_terms(const double (&dr)[MAMAX + 1], const double (&di)[MAMAX + 1],
+                                          const double2 *__restrict__ Zi, double (&acc)[nbispec(TJ)],
+                                          const int bnorm)
+{
+    if constexpr (K < nbispec(TJ)) {
+        constexpr FitTri t = fit_tri(TJ, K);
+        if constexpr (t.j == L) acc[K] += 2.0 * fdb_dot<TJ, L, MB, MAMAX, ZS, t.j1, t.j2>(dr, di, Zi);
+        if constexpr (t.j1 == L)
+            acc[K] += (bnorm ? 2.0 : 2.0 * (t.j + 1) / (t.j1 + 1.0)) * fdb_dot<TJ, L, MB, MAMAX, ZS, t.j, t.j2>(dr, di, Zi);
+        if constexpr (t.j2 == L)
+            acc[K] += (bnorm ? 2.0 : 2.0 * (t.j + 1) / (t.j2 + 1.0)) * fdb_dot<TJ, L, MB, MAMAX, ZS, t.j, t.j1>(dr, di, Zi);
+        fdb_terms<TJ, L, MB, MAMAX, ZS, K + 1>(dr, di, Zi, acc, bnorm);
     }
 }
 
-template <int TJ, int L, int ZS>
-__device__ __forceinline__ void fdb_layers(const double2 *__restrict__ d, const long stride,
-                                           const double2 *__restrict__ Zi, const FitTables *__restrict__ T,
-                                           double *__restrict__ acc)
+// rows MB.. of layer L (and the layers above): dU row in registers (a middle
+// row's right half has no term; its centre counts 1/2), then its terms
+template <int TJ, int L, int MB, int ZS>
+__device__ __forceinline__ void fdb_rows(const double2 *__restrict__ d, const long stride,
+                                         const double2 *__restrict__ Zi, double (&acc)[nbispec(TJ)],
+                                         const int bnorm)
 {
     if constexpr (L <= TJ) {
-        fdb_layer<L, ZS>(d, stride, Zi, T, acc);
-        fdb_layers<TJ, L + 1, ZS>(d, stride, Zi, T, acc);
+        if constexpr (2 * MB <= L) {
+            constexpr int MAMAX = (2 * MB == L) ? MB : L;
+            double dr[MAMAX + 1], di[MAMAX + 1];
+#pragma unroll
+            for (int ma = 0; ma <= MAMAX; ma++) {
+                const double2 v = d[(long)(yh_block(L) + (L + 1) * MB + ma) * stride];
+                const double w = (2 * MB == L && ma == MB) ? 0.5 : 1.0;
+                dr[ma] = w * v.x;
+                di[ma] = w * v.y;
+            }
+            fdb_terms<TJ, L, MB, MAMAX, ZS, 0>(dr, di, Zi, acc, bnorm);
+            fdb_rows<TJ, L, MB + 1, ZS>(d, stride, Zi, acc, bnorm);
+        } else {
+            fdb_rows<TJ, L + 1, 0, ZS>(d, stride, Zi, acc, bnorm);
+        }
     }
 }
 
@@ -424,7 +466,7 @@ k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int *__restrict__
 {
     extern __shared__ __align__(16) unsigned char smraw[];
     double2 *Zs = reinterpret_cast<double2 *>(smraw);   // [entry][APC]
-    const int nz = T->nz, ntri = T->ntri;
+    const int nz = T->nz, bnorm = T->bnorm;
     const int a0 = (a_lo & ~(APC - 1)) + blockIdx.x * APC;
     const int alo = max(a0, a_lo), ahi = min(a0 + APC, a_hi);
     for (int e = threadIdx.x; e < nz * APC; e += blockDim.x) {
@@ -438,10 +480,13 @@ k_fit_dbdr(const double2 *__restrict__ dul, long stride, const int *__restrict__
         const long p = q0 + i / 3;
         const long t = (p - p_lo) * 3 + (i - (i / 3) * 3);
         const int atom = pinfo[p].x;
-        double acc[FIT_NT];
-        for (int k = 0; k < ntri; k++) acc[k] = 0.0;
-        fdb_layers<TJ, 0, APC>(dul + t, stride, Zs + (atom - a0), T, acc);
-        for (int k = 0; k < ntri; k++) dbdr[t * ntri + k] = acc[k];
+        constexpr int NK = nbispec(TJ);
+        double acc[NK];
+#pragma unroll
+        for (int k = 0; k < NK; k++) acc[k] = 0.0;
+        fdb_rows<TJ, 0, 0, APC>(dul + t, stride, Zs + (atom - a0), acc, bnorm);
+#pragma unroll
+        for (int k = 0; k < NK; k++) dbdr[t * NK + k] = acc[k];
     }
 }
 
@@ -554,38 +599,58 @@ __global__ void k_fit_cfg(int c_lo, int c_hi, int ntri, const int *__restrict__ 
 // ---------------------------------------------------------------------------
 constexpr int FIT_GRAM_THREADS = 256;
 
+// Thread (ti, tj) = (tid / 16, tid % 16) owns A[ti + 16 m][tj + 16 k], m, k in
+// 0..3: per row, 4 + 4 shared loads feed 16 FMAs, and the 16 lanes of a
+// half-warp read 16 consecutive doubles (no bank conflicts).  64 rows are
+// staged per barrier pair.
+constexpr int FIT_GRAM_ROWS = 64;
 __global__ void __launch_bounds__(FIT_GRAM_THREADS)
 k_fit_gram64(const double *__restrict__ R, const double *__restrict__ tgt, long nrows, int rows_per_cta,
              double *__restrict__ part)
 {
-    __shared__ double sr[16][FIT_KP + 1];
-    __shared__ double st[16];
+    __shared__ double sr[FIT_GRAM_ROWS][FIT_KP];
+    __shared__ double st[FIT_GRAM_ROWS];
     const long r0 = (long)blockIdx.x * rows_per_cta, r1 = min(nrows, r0 + rows_per_cta);
-    const int tid = threadIdx.x;
-    double acc[16], accb = 0.0;
+    const int tid = threadIdx.x, ti = tid >> 4, tj = tid & 15;
+    double acc[4][4], accb[4];
 #pragma unroll
-    for (int q = 0; q < 16; q++) acc[q] = 0.0;
-    const int row = tid >> 2, col0 = (tid & 3) * 16;   // thread owns A[row][col0 .. col0+15]
-    for (long rb = r0; rb < r1; rb += 16) {
+    for (int m = 0; m < 4; m++) {
+        accb[m] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) acc[m][k] = 0.0;
+    }
+    for (long rb = r0; rb < r1; rb += FIT_GRAM_ROWS) {
         __syncthreads();
-        for (int e = tid; e < 16 * FIT_KP; e += FIT_GRAM_THREADS) {
+        for (int e = tid; e < FIT_GRAM_ROWS * FIT_KP; e += FIT_GRAM_THREADS) {
             const int rr = e / FIT_KP, cc = e % FIT_KP;
             sr[rr][cc] = (rb + rr < r1) ? R[(size_t)(rb + rr) * FIT_KP + cc] : 0.0;
         }
-        if (tid < 16) st[tid] = (rb + tid < r1) ? tgt[rb + tid] : 0.0;
+        if (tid < FIT_GRAM_ROWS) st[tid] = (rb + tid < r1) ? tgt[rb + tid] : 0.0;
         __syncthreads();
 #pragma unroll 4
-        for (int rr = 0; rr < 16; rr++) {
-            const double a = sr[rr][row];
+        for (int rr = 0; rr < FIT_GRAM_ROWS; rr++) {
+            double a[4], b[4];
 #pragma unroll
-            for (int q = 0; q < 16; q++) acc[q] += a * sr[rr][col0 + q];
-            if ((tid & 3) == 0) accb += a * st[rr];
+            for (int m = 0; m < 4; m++) { a[m] = sr[rr][ti + 16 * m]; b[m] = sr[rr][tj + 16 * m]; }
+#pragma unroll
+            for (int m = 0; m < 4; m++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) acc[m][k] += a[m] * b[k];
+            if (tj == 0) {
+                const double t = st[rr];
+#pragma unroll
+                for (int m = 0; m < 4; m++) accb[m] += a[m] * t;
+            }
         }
     }
     double *o = part + (size_t)blockIdx.x * (FIT_KP * FIT_KP + FIT_KP);
 #pragma unroll
-    for (int q = 0; q < 16; q++) o[row * FIT_KP + col0 + q] = acc[q];
-    if ((tid & 3) == 0) o[FIT_KP * FIT_KP + row] = accb;
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[(ti + 16 * m) * FIT_KP + tj + 16 * k] = acc[m][k];
+    if (tj == 0)
+#pragma unroll
+        for (int m = 0; m < 4; m++) o[FIT_KP * FIT_KP + ti + 16 * m] = accb[m];
 }
 
 // column sums of squares of R (one partial per CTA), for the equilibration
