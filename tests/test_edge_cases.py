@@ -1,6 +1,9 @@
 """Edge cases of the plain force path: an isolated atom (no neighbours at
-all), a dimer, and a sparse gas with ragged neighbour counts, many atoms
-having none.  The oracle is checked against the reference's CPU code on the
+all), a dimer, a sparse gas with ragged neighbour counts, many atoms
+having none, and a crystal slab beside a gas in one box (the dE/dr kernel
+copies a window's Y rows into shared memory when its 128 pairs span at most
+16 atoms and reads them in place otherwise: both kinds of window, and the
+windows between them, occur in one launch).  The oracle is checked against the reference's CPU code on the
 CPU (when the reference build is present); the GPU path is checked against
 the oracle: identical ghosts and neighbour sets, per-atom energy, forces and
 virial within 1e-10 of the largest magnitude (or absolutely, where the
@@ -27,7 +30,17 @@ def _gas():
     return rng.uniform(0.0, 32.0, (40, 3)), np.array([32.0, 32.0, 32.0])
 
 
-CASES = {"isolated": _isolated, "dimer": _dimer, "gas": _gas}
+def _slab_and_gas():
+    rng = np.random.default_rng(11)
+    x, box = configs.lattice((4, 4, 4), "bcc", configs.TA_LATTICE)
+    x = x + rng.normal(0.0, 0.05, x.shape)
+    box = np.array([4.0 * box[0], box[1], box[2]])
+    gas = np.column_stack([rng.uniform(box[0] / 4 + 1.0, box[0] - 1.0, 40),
+                           rng.uniform(0.0, box[1], 40), rng.uniform(0.0, box[2], 40)])
+    return np.mod(np.vstack([x, gas]), box), box
+
+
+CASES = {"isolated": _isolated, "dimer": _dimer, "gas": _gas, "slab_gas": _slab_and_gas}
 
 
 def close(a, b, tol=1e-10):
@@ -47,6 +60,8 @@ def test_case_shapes(name):
         assert nn.tolist() == [0]
     if name == "gas":
         assert (nn == 0).sum() >= 5 and nn.max() >= 2      # isolated atoms and clusters
+    if name == "slab_gas":
+        assert nn[:128].min() >= 20 and np.mean(nn[128:]) < 8   # dense rows, then sparse ones
 
 
 @pytest.mark.skipif(not refpy.available(), reason="reference build absent")
