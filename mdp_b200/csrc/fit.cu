@@ -120,7 +120,12 @@ __global__ void k_fit_zbl(const double4 *__restrict__ x, const int *__restrict__
 // (a plan balanced on the host), which needs no reduction between warps.
 // (Giving each warp whole (coupling, mb) rows round-robin let the warps run
 // different couplings' code at once: 4.9 no_instruction stalls per issue.)
-constexpr int FIT_ZBT_WARPS = 10;
+// warps per CTA (one CTA per SM: the 146 KB U tile): the 4,096-configuration
+// graph took 278-280 ms at 10 warps, 278 ms at 12 and 290 ms at 5
+#ifndef FIT_ZBT_WARPS_N
+#define FIT_ZBT_WARPS_N 10
+#endif
+constexpr int FIT_ZBT_WARPS = FIT_ZBT_WARPS_N;
 struct ZbPlan {
     unsigned char mb[JD][FIT_ZBT_WARPS], lo[JD][FIT_ZBT_WARPS], hi[JD][FIT_ZBT_WARPS];   // mb 255: idle
 };
