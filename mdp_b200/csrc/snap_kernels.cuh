@@ -375,8 +375,12 @@ __device__ __forceinline__ void cf_fwd(const T ar, const T ai, const T br, const
 // ---------------------------------------------------------------------------
 // pairs per lane per pass: FP32 takes two (independent chains, half the tile
 // updates; 8.1 against 8.2 ms at 2M atoms); FP64 one (two measured 18.1
-// against 15.7 ms: twice the unrolled code per warp path)
-template <typename T> __host__ __device__ constexpr int uc_pb() { return std::is_same<T, float>::value ? 2 : 1; }
+// against 15.7 ms: twice the unrolled code per warp path; with the split
+// plan, 19.9 ms at two CTAs per SM and 21.8 ms at three against 15.1 ms)
+#ifndef UC_PB_D
+#define UC_PB_D 1
+#endif
+template <typename T> __host__ __device__ constexpr int uc_pb() { return std::is_same<T, float>::value ? 2 : UC_PB_D; }
 // Work plan.  One warp per column (the top two columns share the last warp),
 // or, for FP64 at 2J = 8, eight jobs (column, first layer added into the
 // tile, last layer): a job steps through its column's rows below its first
